@@ -1,0 +1,153 @@
+/*
+ * ducc_b200.h - C-ABI of the B200 (sm_100a) NUFFT library.
+ *
+ * A drop-in for DUCC's type-1 / type-2 non-uniform FFT: the entry points below
+ * are the ones a binding of DUCC's NUFFT module binds (Python: python/nufft_pymod.cc,
+ * Julia: julia/ducc_julia.cc), with plain pointers, sizes and status codes.
+ * No C++ or torch types cross this boundary.
+ *
+ * Arrays are described by dnufft_array (modelled on DUCC's ArrayDescriptor,
+ * src/ducc0/bindings/array_descriptor.h:35-45).  Data may live in device memory
+ * (used in place, zero-copy) or in host memory (staged through the device inside
+ * the call; host arrays must be C-contiguous).
+ *
+ * Every function returns 0 on success and a DNUFFT_ERR_* code otherwise; the
+ * message of the last failure on the calling thread is dnufft_last_error().
+ * Argument errors are detected before any kernel is launched.
+ */
+#ifndef DUCC_B200_H
+#define DUCC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DNUFFT_OK 0
+#define DNUFFT_ERR_BADARG 1       /* shape / dtype / stride / size mismatch        */
+#define DNUFFT_ERR_EPSILON 2      /* no kernel reaches the requested epsilon       */
+#define DNUFFT_ERR_OOM 3          /* device allocation failed                      */
+#define DNUFFT_ERR_CUDA 4         /* CUDA runtime error                            */
+#define DNUFFT_ERR_TIMEOUT 5      /* a bounded device-side wait gave up            */
+#define DNUFFT_ERR_UNSUPPORTED 6  /* valid request outside what this build handles */
+#define DNUFFT_ERR_INTERNAL 7
+
+/* dtype codes */
+#define DNUFFT_F32 1
+#define DNUFFT_F64 2
+#define DNUFFT_C64 3
+#define DNUFFT_C128 4
+
+/* spreader selection (type 1) */
+#define DNUFFT_SPREAD_AUTO 0   /* tensor-core form where it applies, else plain */
+#define DNUFFT_SPREAD_PLAIN 1  /* per-point FP32/FP64 atomics in shared memory   */
+#define DNUFFT_SPREAD_TC 2     /* split-precision FP16 tcgen05 tile contraction  */
+
+typedef struct dnufft_array {
+  void *data;          /* first element                                       */
+  int32_t dtype;       /* DNUFFT_F32 / F64 / C64 / C128                        */
+  int32_t ndim;        /* 1..4                                                 */
+  int64_t shape[4];
+  int64_t stride[4];   /* in elements (not bytes); may be any non-zero value   */
+} dnufft_array;
+
+typedef struct dnufft_opts {
+  size_t nthreads;        /* as in DUCC; only feeds DUCC's parameter cost model  */
+  double sigma_min;       /* minimum / maximum oversampling factor               */
+  double sigma_max;
+  double periodicity[3];  /* per axis                                            */
+  int32_t fft_order;      /* 0: most negative mode first, 1: zero mode first     */
+  int32_t verbosity;      /* 1: print sizes and a CUDA-event stage profile       */
+  int32_t spreader;       /* DNUFFT_SPREAD_*                                     */
+  int32_t simd_lanes;     /* SIMD width DUCC's cost model assumes (default 8)    */
+  int32_t force_kernel;   /* >=0: use this kernel-table row instead of choosing  */
+  int32_t reserved0;
+  int64_t force_nover[3]; /* with force_kernel: oversampled sizes                */
+} dnufft_opts;
+
+typedef struct dnufft_plan dnufft_plan;
+
+typedef struct dnufft_plan_info {
+  int32_t ndim;
+  int32_t supp;           /* kernel support W                                    */
+  int32_t kernel_index;   /* row of the kernel table                             */
+  int32_t log2tile;
+  int64_t nuni[3];
+  int64_t nover[3];
+  double ofactor;
+  double beta;            /* beta (already multiplied by W) and exponent e0      */
+  double e0;
+  int64_t npoints;
+  int32_t coord_f64;
+  int32_t calc_f64;
+} dnufft_plan_info;
+
+/* Fill *opts with the defaults of DUCC's functions (for_plan=0:
+ * nthreads=1, sigma 1.2..2.51) or of its plan class (for_plan=1:
+ * nthreads=0, sigma 1.1..2.6); periodicity 2*pi, fft_order 0.
+ * Replaces the keyword defaults of python/nufft_pymod.cc:445-471. */
+void dnufft_default_opts(dnufft_opts *opts, int for_plan);
+
+/* Smallest epsilon reachable for ndim / precision / sigma range.
+ * Replaces ducc0.nufft.bestEpsilon (python/nufft_pymod.cc:458-459,
+ * src/ducc0/math/gridding_kernel.cc:1562-1576; Julia nufft_best_epsilon,
+ * julia/ducc_julia.cc:176-186). */
+int dnufft_best_epsilon(size_t ndim, int singleprec, double sigma_min, double sigma_max,
+                        double *out);
+
+/* Type 1: out[k] = sum_j points[j] exp(-+ i 2pi k.coord_j / period).
+ * points: (M,) C64|C128; coord: (M, ndim) F32|F64; out: ndim-D grid of the
+ * points' dtype (its shape defines the grid).  forward!=0 means exponent -1.
+ * Replaces ducc0.nufft.nu2u (python/nufft_pymod.cc:113-137 ->
+ * src/ducc0/nufft/nufft.h:1897-1927; Julia nufft_nu2u, julia/ducc_julia.cc:247-312). */
+int dnufft_nu2u(const dnufft_array *points, const dnufft_array *coord, int forward,
+                double epsilon, dnufft_array *out, const dnufft_opts *opts, void *stream);
+
+/* Type 2: out[j] = sum_k grid[k] exp(-+ i 2pi k.coord_j / period).
+ * Replaces ducc0.nufft.u2nu (python/nufft_pymod.cc:52-94 ->
+ * src/ducc0/nufft/nufft.h:1928-1958; Julia nufft_u2nu, julia/ducc_julia.cc:188-245). */
+int dnufft_u2nu(const dnufft_array *grid, const dnufft_array *coord, int forward,
+                double epsilon, dnufft_array *out, const dnufft_opts *opts, void *stream);
+
+/* Plan for repeated transforms with fixed coordinates: the points are binned,
+ * sorted and their coordinates copied in tile order once.  Coordinate dtype
+ * fixes the precision (F32 coords -> C64 data, F64 coords -> C128 data).
+ * Replaces ducc0.nufft.plan.__init__ (python/nufft_pymod.cc:200-237 ->
+ * src/ducc0/nufft/nufft.h:452-462; Julia nufft_make_plan, julia/ducc_julia.cc:314-370). */
+int dnufft_plan_create(int nu2u, const dnufft_array *coord, const int64_t *grid_shape,
+                       int ndim, double epsilon, const dnufft_opts *opts, void *stream,
+                       dnufft_plan **plan);
+
+/* Replaces plan.nu2u (python/nufft_pymod.cc:240-249, :170-183;
+ * Julia nufft_nu2u_planned, julia/ducc_julia.cc:394-457). */
+int dnufft_plan_nu2u(dnufft_plan *plan, int forward, int verbosity,
+                     const dnufft_array *points, dnufft_array *out, void *stream);
+
+/* Replaces plan.u2nu (python/nufft_pymod.cc:250-259, :184-197;
+ * Julia nufft_u2nu_planned, julia/ducc_julia.cc:459-522). */
+int dnufft_plan_u2nu(dnufft_plan *plan, int forward, int verbosity,
+                     const dnufft_array *grid, dnufft_array *out, void *stream);
+
+/* Replaces plan destruction (Julia nufft_delete_plan, julia/ducc_julia.cc:372-392). */
+int dnufft_plan_destroy(dnufft_plan *plan);
+
+/* Sizes and kernel parameters of a plan (DUCC prints these under verbosity,
+ * src/ducc0/nufft/nufft.h:371-380). */
+int dnufft_plan_get_info(const dnufft_plan *plan, dnufft_plan_info *info);
+
+/* Tile-order permutation of the points (DUCC's coord_idx, nufft.h:266,
+ * produced by build_index + bucket_sort2) copied to a device or host buffer
+ * of npoints uint32. */
+int dnufft_plan_get_permutation(const dnufft_plan *plan, uint32_t *out, void *stream);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *dnufft_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DUCC_B200_H */
