@@ -1,0 +1,776 @@
+// C-ABI of the B200 NUFFT library and the host orchestration behind it.
+//
+// Mirrors DUCC's control flow for one transform (src/ducc0/nufft/nufft.h):
+//   parameter choice + kernel fit + correction factors   (Nufft_ancestor ctor, :392-433)
+//   build_index: fold, tile keys, stable sort            (:1364-1381 and friends)
+//   type 1: zero grid, spread, pruned FFT, correct+crop  (nonuni2uni, :1274-1315)
+//   type 2: correct+pad, pruned FFT, interpolate         (uni2nonuni, :1317-1362)
+// and its argument checks (nufft.h:335-361, :400-424, python/nufft_pymod.cc).
+// Errors become a status code plus dnufft_last_error() (the convention of DUCC's
+// C interface, julia/ducc_julia.cc:58-59); argument errors never launch kernels.
+#include "../../include/ducc_b200.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dnufft_internal.h"
+#include "kernels.h"
+
+static thread_local std::string g_last_error;
+
+#include <map>
+#include <mutex>
+namespace {
+// per-stage CUDA-event times accumulated while profiling is enabled
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::map<std::string, std::pair<double, long>> g_prof;   // name -> (ms, calls)
+std::string g_prof_json;
+}  // namespace
+
+namespace dnufft {
+
+constexpr uint32_t CHUNK = 1024;
+
+// ---------------------------------------------------------------- device buffers
+struct DevBuf {
+  void *p = nullptr;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t bytes, cudaStream_t s) : st(s) {
+    if (bytes) DN_CUDA(cudaMallocAsync(&p, bytes, s));
+  }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), st(o.st) { o.p = nullptr; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    release();
+    p = o.p;
+    st = o.st;
+    o.p = nullptr;
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+  }
+  template <typename X> X *as() const { return static_cast<X *>(p); }
+};
+
+// ---------------------------------------------------------------- stage timers
+// CUDA-event stage profile printed under verbosity>0 (the counterpart of DUCC's
+// TimerHierarchy report, src/ducc0/infra/timers.h:69-266).
+struct StageTimer {
+  bool on;
+  bool print;
+  cudaStream_t st;
+  std::vector<std::pair<std::string, cudaEvent_t>> marks;
+  StageTimer(bool on_, cudaStream_t s) : on(on_ || g_prof_on), print(on_), st(s) {}
+  void mark(const char *name) {
+    if (!on) return;
+    cudaEvent_t e;
+    DN_CUDA(cudaEventCreate(&e));
+    DN_CUDA(cudaEventRecord(e, st));
+    marks.emplace_back(name, e);
+  }
+  void report(const char *title) {
+    if (!on || marks.size() < 2) return;
+    DN_CUDA(cudaEventSynchronize(marks.back().second));
+    float total = 0;
+    DN_CUDA(cudaEventElapsedTime(&total, marks.front().second, marks.back().second));
+    if (print) std::printf("%s (GPU, CUDA events): %.4f ms total\n", title, total);
+    for (size_t i = 0; i + 1 < marks.size(); ++i) {
+      float ms = 0;
+      DN_CUDA(cudaEventElapsedTime(&ms, marks[i].second, marks[i + 1].second));
+      if (print)
+        std::printf("  %-22s %10.4f ms  %5.1f%%\n", marks[i].first.c_str(), ms,
+                    total > 0 ? 100. * ms / total : 0.);
+      if (g_prof_on) {
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        auto &e = g_prof[std::string(title) + "/" + marks[i].first];
+        e.first += ms;
+        e.second += 1;
+      }
+    }
+    if (print) std::fflush(stdout);
+  }
+  ~StageTimer() {
+    for (auto &m : marks) cudaEventDestroy(m.second);
+  }
+};
+
+// ---------------------------------------------------------------- array views
+struct View {
+  void *data;
+  int dtype;
+  int ndim;
+  int64_t shape[4];
+  int64_t stride[4];
+  bool host;
+};
+
+static size_t dtype_size(int dt) {
+  switch (dt) {
+    case DNUFFT_F32: return 4;
+    case DNUFFT_F64: return 8;
+    case DNUFFT_C64: return 8;
+    case DNUFFT_C128: return 16;
+  }
+  return 0;
+}
+
+static bool is_host_pointer(const void *p) {
+  cudaPointerAttributes at;
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return at.type == cudaMemoryTypeUnregistered || at.type == cudaMemoryTypeHost;
+}
+
+static View view_of(const dnufft_array *a, const char *what) {
+  DN_REQUIRE(a != nullptr, ST_BADARG, std::string(what) + ": null array");
+  View v;
+  v.data = a->data;
+  v.dtype = a->dtype;
+  v.ndim = a->ndim;
+  DN_REQUIRE(v.ndim >= 1 && v.ndim <= 4, ST_BADARG, std::string(what) + ": bad ndim");
+  DN_REQUIRE(dtype_size(v.dtype) != 0, ST_BADARG, std::string(what) + ": bad dtype");
+  int64_t size = 1;
+  for (int d = 0; d < v.ndim; ++d) {
+    v.shape[d] = a->shape[d];
+    v.stride[d] = a->stride[d];
+    DN_REQUIRE(v.shape[d] >= 0, ST_BADARG, std::string(what) + ": negative extent");
+    size *= v.shape[d];
+  }
+  DN_REQUIRE(size == 0 || v.data != nullptr, ST_BADARG, std::string(what) + ": null data");
+  for (int d = 0; d < v.ndim; ++d)
+    DN_REQUIRE(v.shape[d] <= 1 || v.stride[d] != 0, ST_BADARG,
+               std::string(what) + ": zero stride");
+  v.host = (size > 0) ? is_host_pointer(v.data) : false;
+  if (v.host) {
+    int64_t s = 1;
+    for (int d = v.ndim - 1; d >= 0; --d) {
+      DN_REQUIRE(v.shape[d] <= 1 || v.stride[d] == s, ST_BADARG,
+                 std::string(what) + ": host arrays must be C-contiguous");
+      s *= v.shape[d];
+    }
+  }
+  return v;
+}
+
+static int64_t nelem(const View &v) {
+  int64_t s = 1;
+  for (int d = 0; d < v.ndim; ++d) s *= v.shape[d];
+  return s;
+}
+
+// Device-side copy of a host array (inputs copied in, outputs copied back).
+struct Staged {
+  View dev;
+  DevBuf buf;
+  const View *orig = nullptr;
+  bool is_output = false;
+  cudaStream_t st;
+  Staged(const View &v, bool input, bool output, cudaStream_t s) : st(s) {
+    dev = v;
+    orig = &v;
+    is_output = output && v.host;
+    if (!v.host) return;
+    size_t bytes = size_t(nelem(v)) * dtype_size(v.dtype);
+    buf = DevBuf(bytes, s);
+    dev.data = buf.p;
+    dev.host = false;
+    if (input && bytes) DN_CUDA(cudaMemcpyAsync(buf.p, v.data, bytes, cudaMemcpyHostToDevice, s));
+  }
+  void finish() {
+    if (!is_output) return;
+    size_t bytes = size_t(nelem(*orig)) * dtype_size(orig->dtype);
+    if (bytes) DN_CUDA(cudaMemcpyAsync(orig->data, buf.p, bytes, cudaMemcpyDeviceToHost, st));
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
+};
+
+// ---------------------------------------------------------------- setup
+struct Setup {
+  Geometry g;
+  bool calc_f64 = false, coord_f64 = false;
+  uint32_t npoints = 0;
+  int kidx = 0;
+  double ofactor = 0, beta = 0, e0 = 0, epsilon = 0;
+  KernelPoly<float> kpf;
+  KernelPoly<double> kpd;
+  std::vector<double> corfac[3];
+  std::vector<int> factors[3];
+  int keybits = 1;
+  int tile_shift = 0;
+  uint64_t max_tiles = 0;
+};
+
+static void fill_poly(Setup &s, const std::vector<double> &coeff) {
+  const int W = s.g.W;
+  const int D = W + 3;
+  const int Dp = W + 3 + (W & 1);
+  const int ofs = Dp - D;
+  const int H = (W + 1) / 2;
+  std::memset(&s.kpf, 0, sizeof(s.kpf));
+  std::memset(&s.kpd, 0, sizeof(s.kpd));
+  for (int j = 0; j <= D; ++j)
+    for (int k = 0; k < H; ++k) {
+      double c = coeff[size_t(j) * W + k];
+      s.kpd.c[j + ofs][k] = c;
+      s.kpf.c[j + ofs][k] = float(c);
+    }
+}
+
+static int bitlen64(uint64_t v) {
+  int b = 0;
+  while (v) {
+    ++b;
+    v >>= 1;
+  }
+  return b;
+}
+
+static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double epsilon,
+                        bool gridding, bool calc_f64, bool coord_f64, const dnufft_opts &o) {
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "transform must be 1D/2D/3D");
+  DN_REQUIRE(npoints <= 0xffffffffull, ST_BADARG, "too many nonuniform points");
+  DN_REQUIRE(epsilon > 0, ST_BADARG, "epsilon must be positive");
+  Setup s;
+  s.calc_f64 = calc_f64;
+  s.coord_f64 = coord_f64;
+  s.npoints = uint32_t(npoints);
+  s.epsilon = epsilon;
+  Geometry &g = s.g;
+  std::memset(&g, 0, sizeof(g));
+  g.ndim = ndim;
+  std::vector<size_t> dims(ndim), nover;
+  for (int d = 0; d < ndim; ++d) {
+    DN_REQUIRE(nuni[d] >= 1, ST_BADARG, "uniform grid dimensions must be positive");
+    dims[d] = size_t(nuni[d]);
+    g.nuni[d] = nuni[d];
+  }
+  if (o.force_kernel >= 0) {
+    DN_REQUIRE(size_t(o.force_kernel) < kernel_db().size(), ST_BADARG, "bad forced kernel");
+    s.kidx = o.force_kernel;
+    for (int d = 0; d < ndim; ++d) nover.push_back(size_t(o.force_nover[d]));
+  } else {
+    size_t vlen = calc_f64 ? size_t(o.simd_lanes > 0 ? o.simd_lanes : 8) : 8;
+    s.kidx = int(find_parameters(epsilon, o.sigma_min, o.sigma_max, dims, npoints, gridding,
+                                 effective_threads(o.nthreads), !calc_f64, vlen, nover));
+  }
+  const KernelShape &ks = kernel_db()[size_t(s.kidx)];
+  DN_REQUIRE(ks.singleprec == !calc_f64 || o.force_kernel >= 0, ST_EPSILON,
+             "no appropriate kernel found");
+  g.W = ks.W;
+  g.nsafe = (g.W + 1) / 2;
+  g.log2tile = (ndim == 1) ? 9 : (ndim == 2 ? (calc_f64 ? 4 : 5) : 4);
+  s.ofactor = ks.ofactor;
+  s.beta = ks.beta * ks.W;
+  s.e0 = ks.e0;
+  const uint64_t max_ntile = ndim == 1 ? 0xffffffffull - 10 : (ndim == 2 ? (1u << 16) - 10 : (1u << 10) - 10);
+  for (int d = 0; d < ndim; ++d) {
+    int64_t n = int64_t(nover[d]);
+    DN_REQUIRE(n >= 2 * g.nsafe, ST_BADARG, "oversampled length too small");
+    DN_REQUIRE((n & 1) == 0, ST_BADARG, "oversampled dimensions must be even");
+    DN_REQUIRE(uint64_t(n >> g.log2tile) <= max_ntile, ST_BADARG, "oversampled grid too large");
+    DN_REQUIRE(n < (int64_t(1) << 30), ST_BADARG, "oversampled grid too large");
+    g.nover[d] = n;
+    g.shift[d] = g.W * (-0.5) + 1 + double(n);
+    g.maxi0[d] = int((n + g.nsafe) - g.W);
+    g.ntiles[d] = (n >> g.log2tile) + 3;
+    double per = o.periodicity[d];
+    DN_REQUIRE(per > 0 && std::isfinite(per), ST_BADARG, "periodicity must be positive");
+    g.coordfct[d] = 1. / per;
+    DN_REQUIRE(g.nuni[d] <= n, ST_BADARG, "oversampled grid smaller than uniform grid");
+    auto f = fft_factors(int(n));
+    for (int r : f)
+      DN_REQUIRE(r <= 11, ST_UNSUPPORTED, "oversampled size must be 11-smooth");
+    DN_REQUIRE(f.size() <= 24, ST_UNSUPPORTED, "too many FFT factors");
+    s.factors[d] = f;
+  }
+  // tile keys (DUCC build_index)
+  uint64_t maxkey;
+  if (ndim == 1) {
+    maxkey = uint64_t(g.ntiles[0]);
+    s.tile_shift = 0;
+    s.max_tiles = maxkey;
+  } else if (ndim == 2) {
+    maxkey = uint64_t(g.ntiles[0]) * uint64_t(g.ntiles[1]);
+    s.tile_shift = 0;
+    s.max_tiles = maxkey;
+  } else {
+    uint64_t prod = uint64_t(g.ntiles[0]) * g.ntiles[1] * g.ntiles[2];
+    int lsq2 = g.log2tile;
+    while (lsq2 >= 1 && (prod << (3 * (g.log2tile - lsq2))) < (uint64_t(1) << 28)) --lsq2;
+    g.lsq2 = lsq2;
+    g.ssmall = g.log2tile - lsq2;
+    maxkey = prod << (3 * g.ssmall);
+    s.tile_shift = 3 * g.ssmall;
+    s.max_tiles = prod;
+  }
+  DN_REQUIRE(maxkey < (uint64_t(1) << 32), ST_UNSUPPORTED, "tile key space too large");
+  s.keybits = std::max(1, bitlen64(maxkey));
+  auto coeff = kernel_coeffs(g.W, s.beta, s.e0);
+  fill_poly(s, coeff);
+  for (int d = 0; d < ndim; ++d)
+    s.corfac[d] = correction_factors(size_t(g.nuni[d] / 2 + 1), 1. / double(g.nover[d]), g.W,
+                                     s.beta, s.e0);
+  return s;
+}
+
+// device-resident per-transform constants: correction factors and twiddles
+struct DevConst {
+  DevBuf corfac[3];
+  DevBuf tw[3];
+  FFTAxisPlan ax[3];
+  const double *cf[3] = {nullptr, nullptr, nullptr};
+};
+
+static void upload_consts(const Setup &s, DevConst &dc, cudaStream_t st) {
+  for (int d = 0; d < s.g.ndim; ++d) {
+    size_t nb = s.corfac[d].size() * sizeof(double);
+    dc.corfac[d] = DevBuf(nb, st);
+    DN_CUDA(cudaMemcpyAsync(dc.corfac[d].p, s.corfac[d].data(), nb, cudaMemcpyHostToDevice, st));
+    dc.cf[d] = dc.corfac[d].as<double>();
+    int n = int(s.g.nover[d]);
+    size_t esz = s.calc_f64 ? 16 : 8;
+    dc.tw[d] = DevBuf(size_t(n) * esz, st);
+    if (s.calc_f64) {
+      std::vector<double> t(2 * size_t(n));
+      for (int k = 0; k < n; ++k) {
+        double a = -2.0 * M_PI * double(k) / double(n);
+        t[2 * k] = std::cos(a);
+        t[2 * k + 1] = std::sin(a);
+      }
+      DN_CUDA(cudaMemcpyAsync(dc.tw[d].p, t.data(), t.size() * 8, cudaMemcpyHostToDevice, st));
+    } else {
+      std::vector<float> t(2 * size_t(n));
+      for (int k = 0; k < n; ++k) {
+        double a = -2.0 * M_PI * double(k) / double(n);
+        t[2 * k] = float(std::cos(a));
+        t[2 * k + 1] = float(std::sin(a));
+      }
+      DN_CUDA(cudaMemcpyAsync(dc.tw[d].p, t.data(), t.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    FFTAxisPlan &p = dc.ax[d];
+    p.n = n;
+    p.nfac = int(s.factors[d].size());
+    for (int i = 0; i < p.nfac; ++i) p.fac[i] = s.factors[d][i];
+    p.tw = dc.tw[d].p;
+  }
+  // host vectors must stay alive until the copies ran
+  DN_CUDA(cudaStreamSynchronize(st));
+}
+
+// index: tile permutation, sorted keys and chunk list
+struct Index {
+  DevBuf perm, keys, chunks, count;
+  uint32_t nchunks = 0;
+};
+
+static void build_index(const Setup &s, const View &coord, Index &ix, cudaStream_t st) {
+  uint32_t M = s.npoints;
+  ix.perm = DevBuf(size_t(M) * 4, st);
+  ix.keys = DevBuf(size_t(M) * 4, st);
+  launch_fold_keys(s.coord_f64, coord.data, coord.stride[0], coord.stride[1], M, s.g,
+                   ix.keys.as<uint32_t>(), ix.perm.as<uint32_t>(), st);
+  {
+    DevBuf ws(radix_workspace_bytes(M, s.keybits), st);
+    radix_sort_pairs(ix.keys.as<uint32_t>(), ix.perm.as<uint32_t>(), M, s.keybits, ws.p, st);
+  }
+  uint64_t maxchunks = std::min<uint64_t>(M, s.max_tiles) + M / CHUNK + 2;
+  ix.chunks = DevBuf(size_t(maxchunks) * sizeof(Chunk), st);
+  ix.count = DevBuf(16, st);
+  DevBuf ws(chunk_workspace_bytes(M), st);
+  ix.nchunks = build_chunks(ix.keys.as<uint32_t>(), M, s.tile_shift, CHUNK, ix.chunks.as<Chunk>(),
+                            ix.count.as<uint32_t>(), ws.p, st);
+}
+
+static size_t grid_cells(const Geometry &g) {
+  size_t c = 1;
+  for (int d = 0; d < g.ndim; ++d) c *= size_t(g.nover[d]);
+  return c;
+}
+
+static void report_sizes(const Setup &s, bool gridding) {
+  const Geometry &g = s.g;
+  std::printf("%s\n  device=B200 (CUDA), grid=(", gridding ? "Nu2u:" : "U2nu:");
+  for (int d = 0; d < g.ndim; ++d) std::printf(d ? "x%lld" : "%lld", (long long)g.nuni[d]);
+  std::printf("), oversampled grid=(");
+  for (int d = 0; d < g.ndim; ++d) std::printf(d ? "x%lld" : "%lld", (long long)g.nover[d]);
+  std::printf("), supp=%d, eps=%g\n  npoints=%u\n  memory overhead: %gGB (index) + %gGB "
+              "(oversampled grid)\n",
+              g.W, s.epsilon, s.npoints, s.npoints * 4.0 / double(1 << 30),
+              double(grid_cells(g)) * (s.calc_f64 ? 16 : 8) / double(1 << 30));
+  std::fflush(stdout);
+}
+
+// ---------------------------------------------------------------- transforms
+template <typename T>
+static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
+                          const ChunkList &cl, const View &points, const View &out, bool forward,
+                          bool fft_order, StageTimer &tm, cudaStream_t st) {
+  size_t cells = grid_cells(s.g);
+  tm.mark("zeroing grid");
+  DevBuf grid(cells * sizeof(T) * 2, st);
+  DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * sizeof(T) * 2, st));
+  tm.mark("spreading");
+  const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
+      sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
+  launch_spread<T>(pts, cl, s.g, kp, points.data, points.stride[0], 0, grid.p, 0, 1, st);
+  tm.mark("FFT + correction");
+  fft_nu2u_tail<T>(grid.p, s.g, dc.ax, forward, dc.cf, fft_order, out.data, out.stride, st);
+  tm.mark("end");
+}
+
+template <typename T>
+static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &pts,
+                          const ChunkList &cl, const View &uni, const View &out, bool forward,
+                          bool fft_order, StageTimer &tm, cudaStream_t st) {
+  size_t cells = grid_cells(s.g);
+  DevBuf grid(cells * sizeof(T) * 2, st);
+  tm.mark("correction + FFT");
+  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st);
+  tm.mark("interpolation");
+  const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
+      sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
+  launch_interp<T>(pts, cl, s.g, kp, grid.p, 0, out.data, out.stride[0], 0, 1, st);
+  tm.mark("end");
+}
+
+static void zero_view(const View &v, cudaStream_t st) {
+  DN_REQUIRE(v.ndim <= 3, ST_BADARG, "bad output rank");
+  zero_strided(v.data, v.ndim, v.shape, v.stride, dtype_size(v.dtype), st);
+}
+
+static void check_coord(const View &coord, int ndim) {
+  DN_REQUIRE(coord.ndim == 2, ST_BADARG, "coord must be a 2D array (npoints, ndim)");
+  DN_REQUIRE(coord.dtype == DNUFFT_F32 || coord.dtype == DNUFFT_F64, ST_BADARG,
+             "coord must be float32 or float64");
+  DN_REQUIRE(coord.shape[1] == ndim, ST_BADARG, "dimensionality mismatch");
+}
+
+static dnufft_opts resolved(const dnufft_opts *o, bool for_plan) {
+  dnufft_opts r;
+  if (o) {
+    r = *o;
+  } else {
+    dnufft_default_opts(&r, for_plan ? 1 : 0);
+  }
+  return r;
+}
+
+static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, int forward,
+                      double eps, dnufft_array *out_, const dnufft_opts *opts_, cudaStream_t st) {
+  dnufft_opts o = resolved(opts_, false);
+  View points = view_of(points_, "points"), coord = view_of(coord_, "coord"),
+       out = view_of(out_, "out");
+  int ndim = out.ndim;
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "transform must be 1D/2D/3D");
+  check_coord(coord, ndim);
+  DN_REQUIRE(points.ndim == 1, ST_BADARG, "points must be 1D");
+  DN_REQUIRE(points.shape[0] == coord.shape[0], ST_BADARG, "number of points mismatch");
+  DN_REQUIRE(points.dtype == DNUFFT_C64 || points.dtype == DNUFFT_C128, ST_BADARG,
+             "points must be complex64 or complex128");
+  DN_REQUIRE(out.dtype == points.dtype, ST_BADARG, "out must have the dtype of points");
+  bool f64 = points.dtype == DNUFFT_C128;
+  Setup s = make_setup(ndim, out.shape, uint64_t(points.shape[0]), eps, true, f64,
+                       coord.dtype == DNUFFT_F64, o);
+  StageTimer tm(o.verbosity > 0, st);
+  if (o.verbosity > 0) report_sizes(s, true);
+  Staged sp(points, true, false, st), sc(coord, true, false, st), so(out, false, true, st);
+  if (s.npoints == 0) {
+    zero_view(so.dev, st);
+    so.finish();
+    return;
+  }
+  tm.mark("upload constants");
+  DevConst dc;
+  upload_consts(s, dc, st);
+  tm.mark("building index");
+  Index ix;
+  build_index(s, sc.dev, ix, st);
+  PointsDesc pts{sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], false, s.coord_f64,
+                 ix.perm.as<uint32_t>(), s.npoints};
+  ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+  if (f64)
+    do_spread_fft<double>(s, dc, pts, cl, sp.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+  else
+    do_spread_fft<float>(s, dc, pts, cl, sp.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+  tm.report("nu2u");
+  so.finish();
+}
+
+static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int forward,
+                      double eps, dnufft_array *out_, const dnufft_opts *opts_, cudaStream_t st) {
+  dnufft_opts o = resolved(opts_, false);
+  View uni = view_of(grid_, "grid"), coord = view_of(coord_, "coord"), out = view_of(out_, "out");
+  int ndim = uni.ndim;
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "transform must be 1D/2D/3D");
+  check_coord(coord, ndim);
+  DN_REQUIRE(out.ndim == 1 && out.shape[0] == coord.shape[0], ST_BADARG,
+             "number of points mismatch");
+  DN_REQUIRE(uni.dtype == DNUFFT_C64 || uni.dtype == DNUFFT_C128, ST_BADARG,
+             "grid must be complex64 or complex128");
+  DN_REQUIRE(out.dtype == uni.dtype, ST_BADARG, "out must have the dtype of grid");
+  bool f64 = uni.dtype == DNUFFT_C128;
+  Setup s = make_setup(ndim, uni.shape, uint64_t(coord.shape[0]), eps, false, f64,
+                       coord.dtype == DNUFFT_F64, o);
+  StageTimer tm(o.verbosity > 0, st);
+  if (o.verbosity > 0) report_sizes(s, false);
+  if (s.npoints == 0) return;
+  Staged su(uni, true, false, st), sc(coord, true, false, st), so(out, false, true, st);
+  tm.mark("upload constants");
+  DevConst dc;
+  upload_consts(s, dc, st);
+  tm.mark("building index");
+  Index ix;
+  build_index(s, sc.dev, ix, st);
+  PointsDesc pts{sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], false, s.coord_f64,
+                 ix.perm.as<uint32_t>(), s.npoints};
+  ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+  if (f64)
+    do_fft_interp<double>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+  else
+    do_fft_interp<float>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+  tm.report("u2nu");
+  so.finish();
+}
+
+}  // namespace dnufft
+
+// ---------------------------------------------------------------- plans
+struct dnufft_plan {
+  dnufft::Setup s;
+  dnufft::DevConst dc;
+  dnufft::Index ix;
+  dnufft::DevBuf sorted_coord;
+  dnufft_opts o;
+  int device = 0;
+};
+
+namespace dnufft {
+
+static void plan_create_impl(int nu2u, const dnufft_array *coord_, const int64_t *shape, int ndim,
+                             double eps, const dnufft_opts *opts_, cudaStream_t st,
+                             dnufft_plan **out) {
+  DN_REQUIRE(out != nullptr, ST_BADARG, "null plan pointer");
+  DN_REQUIRE(shape != nullptr, ST_BADARG, "null grid shape");
+  dnufft_opts o = resolved(opts_, true);
+  View coord = view_of(coord_, "coord");
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "unsupported dimensionality");
+  check_coord(coord, ndim);
+  bool f64 = coord.dtype == DNUFFT_F64;
+  auto p = std::make_unique<dnufft_plan>();
+  p->o = o;
+  DN_CUDA(cudaGetDevice(&p->device));
+  p->s = make_setup(ndim, shape, uint64_t(coord.shape[0]), eps, nu2u != 0, f64, f64, o);
+  upload_consts(p->s, p->dc, st);
+  if (p->s.npoints > 0) {
+    Staged sc(coord, true, false, st);
+    build_index(p->s, sc.dev, p->ix, st);
+    p->sorted_coord = DevBuf(size_t(p->s.npoints) * ndim * (f64 ? 8 : 4), st);
+    launch_gather_coords(f64, sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], ndim,
+                         p->ix.perm.as<uint32_t>(), p->s.npoints, p->sorted_coord.p, st);
+    // the plan keeps only the sorted copy; release the keys
+    p->ix.keys.release();
+  }
+  DN_CUDA(cudaStreamSynchronize(st));
+  *out = p.release();
+}
+
+static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosity,
+                           const dnufft_array *in_, dnufft_array *out_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  bool f64 = s.calc_f64;
+  int cdt = f64 ? DNUFFT_C128 : DNUFFT_C64;
+  View in = view_of(in_, type1 ? "points" : "grid");
+  View out = view_of(out_, "out");
+  DN_REQUIRE(in.dtype == cdt && out.dtype == cdt, ST_BADARG,
+             f64 ? "a float64-coordinate plan needs complex128 data"
+                 : "a float32-coordinate plan needs complex64 data");
+  const View &pv = type1 ? in : out;
+  const View &uv = type1 ? out : in;
+  DN_REQUIRE(pv.ndim == 1 && uint64_t(pv.shape[0]) == s.npoints, ST_BADARG,
+             "number of points mismatch");
+  DN_REQUIRE(uv.ndim == s.g.ndim, ST_BADARG, "uniform grid dimensions mismatch");
+  for (int d = 0; d < s.g.ndim; ++d)
+    DN_REQUIRE(uv.shape[d] == s.g.nuni[d], ST_BADARG, "uniform grid dimensions mismatch");
+  StageTimer tm(verbosity > 0, st);
+  if (verbosity > 0) report_sizes(s, type1);
+  Staged si(in, true, false, st), so(out, false, true, st);
+  if (s.npoints == 0) {
+    if (type1) zero_view(so.dev, st);
+    so.finish();
+    return;
+  }
+  PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
+                 p->ix.perm.as<uint32_t>(), s.npoints};
+  ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
+  bool fo = p->o.fft_order != 0;
+  if (type1) {
+    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
+    else do_spread_fft<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
+    tm.report("nu2u (planned)");
+  } else {
+    if (f64) do_fft_interp<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
+    else do_fft_interp<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
+    tm.report("u2nu (planned)");
+  }
+  so.finish();
+}
+
+}  // namespace dnufft
+
+// ---------------------------------------------------------------- C-ABI
+#define DN_GUARD(body)                                   \
+  try {                                                  \
+    body;                                                \
+    g_last_error.clear();                                \
+    return DNUFFT_OK;                                    \
+  } catch (const dnufft::Error &e) {                     \
+    g_last_error = e.what();                             \
+    return e.code;                                       \
+  } catch (const std::bad_alloc &) {                     \
+    g_last_error = "host allocation failed";             \
+    return DNUFFT_ERR_OOM;                               \
+  } catch (const std::exception &e) {                    \
+    g_last_error = e.what();                             \
+    return DNUFFT_ERR_INTERNAL;                          \
+  }
+
+extern "C" {
+
+void dnufft_default_opts(dnufft_opts *o, int for_plan) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->nthreads = for_plan ? 0 : 1;
+  o->sigma_min = for_plan ? 1.1 : 1.2;
+  o->sigma_max = for_plan ? 2.6 : 2.51;
+  for (int d = 0; d < 3; ++d) o->periodicity[d] = 2 * M_PI;
+  o->fft_order = 0;
+  o->verbosity = 0;
+  o->spreader = DNUFFT_SPREAD_AUTO;
+  o->simd_lanes = 8;
+  o->force_kernel = -1;
+}
+
+int dnufft_best_epsilon(size_t ndim, int singleprec, double sigma_min, double sigma_max,
+                        double *out) {
+  DN_GUARD({
+    DN_REQUIRE(out != nullptr, dnufft::ST_BADARG, "null output");
+    *out = dnufft::best_epsilon(ndim, singleprec != 0, sigma_min, sigma_max);
+  })
+}
+
+int dnufft_nu2u(const dnufft_array *points, const dnufft_array *coord, int forward, double epsilon,
+                dnufft_array *out, const dnufft_opts *opts, void *stream) {
+  DN_GUARD(dnufft::nu2u_impl(points, coord, forward, epsilon, out, opts,
+                             static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_u2nu(const dnufft_array *grid, const dnufft_array *coord, int forward, double epsilon,
+                dnufft_array *out, const dnufft_opts *opts, void *stream) {
+  DN_GUARD(dnufft::u2nu_impl(grid, coord, forward, epsilon, out, opts,
+                             static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_create(int nu2u, const dnufft_array *coord, const int64_t *grid_shape, int ndim,
+                       double epsilon, const dnufft_opts *opts, void *stream, dnufft_plan **plan) {
+  DN_GUARD(dnufft::plan_create_impl(nu2u, coord, grid_shape, ndim, epsilon, opts,
+                                    static_cast<cudaStream_t>(stream), plan))
+}
+
+int dnufft_plan_nu2u(dnufft_plan *plan, int forward, int verbosity, const dnufft_array *points,
+                     dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::plan_exec_impl(plan, true, forward, verbosity, points, out,
+                                  static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_u2nu(dnufft_plan *plan, int forward, int verbosity, const dnufft_array *grid,
+                     dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::plan_exec_impl(plan, false, forward, verbosity, grid, out,
+                                  static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_destroy(dnufft_plan *plan) {
+  DN_GUARD({
+    if (plan) {
+      cudaStream_t st = nullptr;
+      plan->ix.perm.st = plan->ix.chunks.st = plan->ix.count.st = plan->ix.keys.st = st;
+      plan->sorted_coord.st = st;
+      for (int d = 0; d < 3; ++d) plan->dc.corfac[d].st = plan->dc.tw[d].st = st;
+      delete plan;
+      DN_CUDA(cudaDeviceSynchronize());
+    }
+  })
+}
+
+int dnufft_plan_get_info(const dnufft_plan *p, dnufft_plan_info *info) {
+  DN_GUARD({
+    DN_REQUIRE(p && info, dnufft::ST_BADARG, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->ndim = p->s.g.ndim;
+    info->supp = p->s.g.W;
+    info->kernel_index = p->s.kidx;
+    info->log2tile = p->s.g.log2tile;
+    for (int d = 0; d < p->s.g.ndim; ++d) {
+      info->nuni[d] = p->s.g.nuni[d];
+      info->nover[d] = p->s.g.nover[d];
+    }
+    info->ofactor = p->s.ofactor;
+    info->beta = p->s.beta;
+    info->e0 = p->s.e0;
+    info->npoints = p->s.npoints;
+    info->coord_f64 = p->s.coord_f64;
+    info->calc_f64 = p->s.calc_f64;
+  })
+}
+
+int dnufft_plan_get_permutation(const dnufft_plan *p, uint32_t *out, void *stream) {
+  DN_GUARD({
+    DN_REQUIRE(p && out, dnufft::ST_BADARG, "null argument");
+    if (p->s.npoints == 0) return DNUFFT_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DN_CUDA(cudaMemcpyAsync(out, p->ix.perm.p, size_t(p->s.npoints) * 4, cudaMemcpyDefault, st));
+    DN_CUDA(cudaStreamSynchronize(st));
+  })
+}
+
+const char *dnufft_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t dnufft_kernel_launches(void) { return dnufft::launch_count(); }
+
+void dnufft_profile_enable(int enable) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = enable != 0;
+  if (g_prof_on) g_prof.clear();
+}
+
+const char *dnufft_profile_json(void) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  std::string js = "{";
+  bool first = true;
+  for (auto &kv : g_prof) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s\"%s\": [%.6f, %ld]", first ? "" : ", ", kv.first.c_str(),
+                  kv.second.first, kv.second.second);
+    js += buf;
+    first = false;
+  }
+  js += "}";
+  g_prof_json = js;
+  return g_prof_json.c_str();
+}
+
+}  // extern "C"

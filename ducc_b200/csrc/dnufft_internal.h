@@ -36,6 +36,12 @@ struct Error : public std::runtime_error {
 void cuda_check(cudaError_t e, const char *what);
 #define DN_CUDA(call) ::dnufft::cuda_check((call), #call)
 
+// number of kernels this library launched (diagnostics)
+void note_launch(uint64_t n = 1);
+uint64_t launch_count();
+// check a launch and count it
+#define DN_LAUNCHED() do { ::dnufft::cuda_check(cudaGetLastError(), "kernel launch"); ::dnufft::note_launch(); } while (0)
+
 // ---------------------------------------------------------------- planner
 struct KernelShape {
   int W;

@@ -1,0 +1,484 @@
+// Oversampled-grid FFTs and the grid correction (deconvolution + crop / pad).
+//
+// Each CTA transforms 'nl' lines of length n held in shared memory (element k of
+// line l at s[k*nl+l]) with a mixed-radix Stockham FFT (radices 2,3,4,5,7,8,11;
+// DUCC's oversampled sizes are 2*good_size_complex(...), always 11-smooth).
+// Every stage is done in place: each thread first gathers its butterflies into
+// registers, the block synchronises, then it writes the outputs.  Twiddles come
+// from an FP64-accurate table of n entries.
+//
+// The NUFFT needs only the N kept frequencies of every axis, so (as DUCC does,
+// src/ducc0/nufft/nufft.h:1287-1298, :1345-1356, :1743-1773, :1824-1854) the
+// second and third axes are transformed only on kept index ranges.  In addition
+//  - type 1: the last pass multiplies by the correction factors and writes
+//    straight into the caller's uniform array in DUCC's output order
+//    (comp_indices, nufft.h:142-151), so no separate correction pass is run;
+//  - type 2: the first pass gathers the caller's uniform array, multiplies by
+//    the correction factors and zero-pads in shared memory, so the oversampled
+//    grid is never zeroed or written before the first FFT.
+#include "common.cuh"
+#include "kernels.h"
+
+#include <algorithm>
+
+namespace dnufft {
+
+constexpr int FFT_MAXE = 16;   // elements per thread per stage
+
+struct AxisMap {
+  int N, n;   // kept count, full length
+};
+
+// kept index x in [0,N) -> grid index: low half first, then high half
+__device__ __forceinline__ int kept_to_grid(int x, int N, int n) {
+  int lo = (N + 1) / 2;
+  return x < lo ? x : x + n - N;
+}
+// grid index -> uniform index along an axis and the correction-factor index
+// (inverse of comp_indices' i2 = (n - N/2 + i) mod n)
+__device__ __forceinline__ void grid_to_uni(int c, int N, int n, bool fft_order, int &iuni,
+                                            int &icf) {
+  int j = c + N / 2;
+  if (j >= n) j -= n;
+  icf = abs(N / 2 - j);
+  int i1 = fft_order ? N - N / 2 + j : j;
+  if (i1 >= N) i1 -= N;
+  iuni = i1;
+}
+
+enum { IO_FULL = 0, IO_KEPT = 1, IO_UNI = 2 };
+
+struct LineSpec {
+  int n;            // transform length
+  int ax;           // transformed grid axis
+  int64_t es;       // element stride in the grid
+  int nlines;
+  int cntb;         // line index L = a*cntb + b
+  int64_t sa, sb;   // grid strides of a and b
+  int axa, axb;     // grid axes of a and b (-1: unused)
+  int kepta, keptb; // a / b enumerate kept indices of their axis
+  int in_mode, out_mode;
+  int nl;           // lines per CTA
+};
+
+struct UniSpec {
+  void *ptr;
+  int64_t stride[3];
+  const double *corfac[3];
+  int N[3];
+  int n[3];
+  bool fft_order;
+};
+
+template <typename T>
+__device__ __forceinline__ cplx<T> twiddle(const cplx<T> *__restrict__ tw, int t, bool fwd) {
+  cplx<T> w = __ldg(tw + t);
+  if (!fwd) w.y = -w.y;
+  return w;
+}
+
+// y = DFT_R(a) with sign from fwd; generic direct form for odd radices
+template <typename T, int R>
+__device__ __forceinline__ void dft_small(cplx<T> (&a)[R], const cplx<T> *__restrict__ tw, int n,
+                                          bool fwd) {
+  if constexpr (R == 2) {
+    cplx<T> t = a[1];
+    a[1] = csub<T>(a[0], t);
+    a[0] = cadd<T>(a[0], t);
+  } else if constexpr (R == 4) {
+    cplx<T> s02 = cadd<T>(a[0], a[2]), d02 = csub<T>(a[0], a[2]);
+    cplx<T> s13 = cadd<T>(a[1], a[3]), d13 = csub<T>(a[1], a[3]);
+    // multiply d13 by -i (forward) or +i (backward)
+    cplx<T> r = fwd ? mkc<T>(d13.y, -d13.x) : mkc<T>(-d13.y, d13.x);
+    a[0] = cadd<T>(s02, s13);
+    a[2] = csub<T>(s02, s13);
+    a[1] = cadd<T>(d02, r);
+    a[3] = csub<T>(d02, r);
+  } else if constexpr (R == 8) {
+    cplx<T> e[4] = {a[0], a[2], a[4], a[6]};
+    cplx<T> o[4] = {a[1], a[3], a[5], a[7]};
+    dft_small<T, 4>(e, tw, n, fwd);
+    dft_small<T, 4>(o, tw, n, fwd);
+    const T h = T(0.70710678118654752440084436210485);
+    const T s = fwd ? T(-1) : T(1);
+    // W8^1 = h(1 + s i), W8^2 = s i, W8^3 = h(-1 + s i)
+    cplx<T> o1 = mkc<T>(h * (o[1].x - s * o[1].y), h * (o[1].y + s * o[1].x));
+    cplx<T> o2 = mkc<T>(-s * o[2].y, s * o[2].x);
+    cplx<T> o3 = mkc<T>(h * (-o[3].x - s * o[3].y), h * (-o[3].y + s * o[3].x));
+    a[0] = cadd<T>(e[0], o[0]);
+    a[4] = csub<T>(e[0], o[0]);
+    a[1] = cadd<T>(e[1], o1);
+    a[5] = csub<T>(e[1], o1);
+    a[2] = cadd<T>(e[2], o2);
+    a[6] = csub<T>(e[2], o2);
+    a[3] = cadd<T>(e[3], o3);
+    a[7] = csub<T>(e[3], o3);
+  } else {
+    const int step = n / R;
+    cplx<T> w[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) w[m] = twiddle<T>(tw, m * step, fwd);
+    cplx<T> y[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      cplx<T> acc = a[0];
+#pragma unroll
+      for (int m = 1; m < R; ++m) {
+        cplx<T> t = cmul<T>(a[m], w[(m * q) % R]);
+        acc = cadd<T>(acc, t);
+      }
+      y[q] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) a[q] = y[q];
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void stockham_stage(cplx<T> *s, int n, int nl, int Ns,
+                                               const cplx<T> *__restrict__ tw, bool fwd) {
+  constexpr int QM = FFT_MAXE / R + 1;
+  const int B = (n / R) * nl;
+  const int NT = blockDim.x;
+  const int tstep = n / (Ns * R);
+  cplx<T> v[QM][R];
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    int b = threadIdx.x + q * NT;
+    if (b < B) {
+      int l = b % nl, j = b / nl;
+      int k = j % Ns;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        cplx<T> x = s[(j + r * (n / R)) * nl + l];
+        if (r > 0 && k > 0) x = cmul<T>(x, twiddle<T>(tw, k * r * tstep, fwd));
+        v[q][r] = x;
+      }
+      dft_small<T, R>(v[q], tw, n, fwd);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    int b = threadIdx.x + q * NT;
+    if (b < B) {
+      int l = b % nl, j = b / nl;
+      int k = j % Ns;
+      int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[(base + r * Ns) * nl + l] = v[q][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void fft_lines(cplx<T> *s, int n, int nl, const FFTAxisPlan &p, bool fwd) {
+  const cplx<T> *tw = static_cast<const cplx<T> *>(p.tw);
+  int Ns = 1;
+  for (int f = 0; f < p.nfac; ++f) {
+    int R = p.fac[f];
+    switch (R) {
+      case 2: stockham_stage<T, 2>(s, n, nl, Ns, tw, fwd); break;
+      case 3: stockham_stage<T, 3>(s, n, nl, Ns, tw, fwd); break;
+      case 4: stockham_stage<T, 4>(s, n, nl, Ns, tw, fwd); break;
+      case 5: stockham_stage<T, 5>(s, n, nl, Ns, tw, fwd); break;
+      case 7: stockham_stage<T, 7>(s, n, nl, Ns, tw, fwd); break;
+      case 8: stockham_stage<T, 8>(s, n, nl, Ns, tw, fwd); break;
+      case 11: stockham_stage<T, 11>(s, n, nl, Ns, tw, fwd); break;
+      default: break;   // excluded on the host
+    }
+    Ns *= R;
+  }
+}
+
+__device__ __forceinline__ int64_t line_base(const LineSpec &ls, const int *Nk, const int *nk,
+                                             int L, int &ia, int &ib) {
+  int a = L / ls.cntb, b = L - (L / ls.cntb) * ls.cntb;
+  ia = (ls.axa >= 0 && ls.kepta) ? kept_to_grid(a, Nk[ls.axa], nk[ls.axa]) : a;
+  ib = (ls.axb >= 0 && ls.keptb) ? kept_to_grid(b, Nk[ls.axb], nk[ls.axb]) : b;
+  return int64_t(ia) * ls.sa + int64_t(ib) * ls.sb;
+}
+
+// factor and uniform offset for the fixed (non-transformed) coordinates of a line
+__device__ __forceinline__ void line_uni(const LineSpec &ls, const UniSpec &u, int ia, int ib,
+                                         double &fac, int64_t &uoff) {
+  fac = 1.0;
+  uoff = 0;
+  if (ls.axa >= 0) {
+    int iu, icf;
+    grid_to_uni(ia, u.N[ls.axa], u.n[ls.axa], u.fft_order, iu, icf);
+    fac *= u.corfac[ls.axa][icf];
+    uoff += int64_t(iu) * u.stride[ls.axa];
+  }
+  if (ls.axb >= 0) {
+    int iu, icf;
+    grid_to_uni(ib, u.N[ls.axb], u.n[ls.axb], u.fft_order, iu, icf);
+    fac *= u.corfac[ls.axb][icf];
+    uoff += int64_t(iu) * u.stride[ls.axb];
+  }
+}
+
+template <typename T> constexpr int fft_max_threads() { return sizeof(T) == 4 ? 1024 : 512; }
+
+template <typename T>
+__global__ void __launch_bounds__(fft_max_threads<T>())
+    k_fft_lines(cplx<T> *__restrict__ grid, LineSpec ls, FFTAxisPlan plan, UniSpec u, bool fwd) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx<T> *s = reinterpret_cast<cplx<T> *>(smraw);
+  const int n = ls.n, nl = ls.nl;
+  const int L0 = blockIdx.x * nl;
+  const int nloc = min(nl, ls.nlines - L0);
+  const int N = u.N[ls.ax];
+  const int total = n * nl;
+  // ---------------- load
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    int l, k;
+    if (ls.es == 1) {
+      l = idx / n;
+      k = idx - l * n;
+    } else {
+      k = idx / nl;
+      l = idx - k * nl;
+    }
+    cplx<T> v = mkc<T>(T(0), T(0));
+    if (l < nloc) {
+      int ia, ib;
+      int64_t base = line_base(ls, u.N, u.n, L0 + l, ia, ib);
+      if (ls.in_mode == IO_FULL) {
+        v = grid[base + int64_t(k) * ls.es];
+      } else {
+        int lo = (N + 1) / 2;
+        bool kept = (k < lo) || (k >= n - N / 2);
+        if (kept) {
+          if (ls.in_mode == IO_KEPT) {
+            v = grid[base + int64_t(k) * ls.es];
+          } else {   // IO_UNI: gather caller's uniform array with correction
+            double fac;
+            int64_t uoff;
+            line_uni(ls, u, ia, ib, fac, uoff);
+            int iu, icf;
+            grid_to_uni(k, N, n, u.fft_order, iu, icf);
+            fac *= u.corfac[ls.ax][icf];
+            const cplx<T> *up = static_cast<const cplx<T> *>(u.ptr);
+            cplx<T> x = up[uoff + int64_t(iu) * u.stride[ls.ax]];
+            T f = T(fac);
+            v = mkc<T>(x.x * f, x.y * f);
+          }
+        }
+      }
+    }
+    s[k * nl + l] = v;
+  }
+  __syncthreads();
+  fft_lines<T>(s, n, nl, plan, fwd);
+  // ---------------- store
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    int l, k;
+    if (ls.es == 1) {
+      l = idx / n;
+      k = idx - l * n;
+    } else {
+      k = idx / nl;
+      l = idx - k * nl;
+    }
+    if (l >= nloc) continue;
+    int ia, ib;
+    int64_t base = line_base(ls, u.N, u.n, L0 + l, ia, ib);
+    if (ls.out_mode == IO_FULL) {
+      grid[base + int64_t(k) * ls.es] = s[k * nl + l];
+    } else {
+      int lo = (N + 1) / 2;
+      bool kept = (k < lo) || (k >= n - N / 2);
+      if (!kept) continue;
+      if (ls.out_mode == IO_KEPT) {
+        grid[base + int64_t(k) * ls.es] = s[k * nl + l];
+      } else {   // IO_UNI: correction + crop into the caller's array
+        double fac;
+        int64_t uoff;
+        line_uni(ls, u, ia, ib, fac, uoff);
+        int iu, icf;
+        grid_to_uni(k, N, n, u.fft_order, iu, icf);
+        fac *= u.corfac[ls.ax][icf];
+        cplx<T> x = s[k * nl + l];
+        T f = T(fac);
+        cplx<T> *up = static_cast<cplx<T> *>(u.ptr);
+        up[uoff + int64_t(iu) * u.stride[ls.ax]] = mkc<T>(x.x * f, x.y * f);
+      }
+    }
+  }
+}
+
+template <typename T>
+static void run_lines(cplx<T> *grid, LineSpec ls, const FFTAxisPlan &p, const UniSpec &u,
+                      bool fwd, cudaStream_t st) {
+  if (ls.nlines <= 0) return;
+  const int n = ls.n;
+  const size_t maxsm = 200 * 1024;
+  int nl;
+  if (ls.es == 1) {
+    nl = std::max(1, std::min(32, 4096 / n));
+  } else {
+    nl = std::max(1, std::min(16, 16384 / n));
+  }
+  const int maxnt = fft_max_threads<T>();
+  while (nl > 1 && (size_t(n) * nl * sizeof(cplx<T>) > maxsm || n * nl > FFT_MAXE * maxnt)) --nl;
+  nl = std::min(nl, ls.nlines);
+  DN_REQUIRE(size_t(n) * sizeof(cplx<T>) <= maxsm && n <= FFT_MAXE * maxnt, ST_UNSUPPORTED,
+             "oversampled axis too long for the single-CTA FFT of this build");
+  ls.nl = nl;
+  int total = n * nl;
+  int nt = 32 * ((total / 8 + 31) / 32);
+  nt = std::max(64, std::min(maxnt, nt));
+  while (total > FFT_MAXE * nt) nt += 32;
+  size_t sm = size_t(total) * sizeof(cplx<T>);
+  DN_CUDA(cudaFuncSetAttribute(k_fft_lines<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(sm)));
+  unsigned nb = unsigned((ls.nlines + nl - 1) / nl);
+  k_fft_lines<T><<<nb, nt, sm, st>>>(grid, ls, p, u, fwd);
+  DN_LAUNCHED();
+}
+
+static LineSpec mk_spec(int n, int ax, int64_t es, int cnta, int cntb, int64_t sa, int64_t sb,
+                        int axa, int axb, int kepta, int keptb, int in_mode, int out_mode) {
+  LineSpec ls;
+  ls.n = n;
+  ls.ax = ax;
+  ls.es = es;
+  ls.nlines = cnta * cntb;
+  ls.cntb = cntb;
+  ls.sa = sa;
+  ls.sb = sb;
+  ls.axa = axa;
+  ls.axb = axb;
+  ls.kepta = kepta;
+  ls.keptb = keptb;
+  ls.in_mode = in_mode;
+  ls.out_mode = out_mode;
+  ls.nl = 1;
+  return ls;
+}
+
+static UniSpec mk_uni(void *ptr, const int64_t *stride, const Geometry &g,
+                      const double *const corfac[3], bool fft_order) {
+  UniSpec u;
+  u.ptr = ptr;
+  for (int d = 0; d < 3; ++d) {
+    u.stride[d] = d < g.ndim ? stride[d] : 0;
+    u.corfac[d] = d < g.ndim ? corfac[d] : nullptr;
+    u.N[d] = d < g.ndim ? int(g.nuni[d]) : 1;
+    u.n[d] = d < g.ndim ? int(g.nover[d]) : 1;
+  }
+  u.fft_order = fft_order;
+  return u;
+}
+
+template <typename T>
+void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
+                   const double *const corfac[3], bool fft_order, void *out,
+                   const int64_t *ostride, cudaStream_t st) {
+  cplx<T> *grid = static_cast<cplx<T> *>(gridv);
+  UniSpec u = mk_uni(out, ostride, g, corfac, fft_order);
+  const int n0 = int(g.nover[0]);
+  if (g.ndim == 1) {
+    run_lines<T>(grid, mk_spec(n0, 0, 1, 1, 1, 0, 0, -1, -1, 0, 0, IO_FULL, IO_UNI), ax[0], u, fwd, st);
+  } else if (g.ndim == 2) {
+    const int n1 = int(g.nover[1]);
+    const int N1 = int(g.nuni[1]);
+    // rows (axis 1), all n0 rows, keep N1 columns
+    run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_FULL, IO_KEPT), ax[1], u,
+                 fwd, st);
+    // columns (axis 0) of the kept columns, correction + crop
+    run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_FULL, IO_UNI), ax[0], u,
+                 fwd, st);
+  } else {
+    const int n1 = int(g.nover[1]), n2 = int(g.nover[2]);
+    const int N1 = int(g.nuni[1]), N2 = int(g.nuni[2]);
+    // axis 2: all n0*n1 lines, keep N2
+    run_lines<T>(grid, mk_spec(n2, 2, 1, n0 * n1, 1, n2, 0, -1, -1, 0, 0, IO_FULL, IO_KEPT), ax[2],
+                 u, fwd, st);
+    // axis 1: lines (i0, k) for kept k, keep N1
+    run_lines<T>(grid, mk_spec(n1, 1, n2, n0, N2, int64_t(n1) * n2, 1, -1, 2, 0, 1, IO_FULL,
+                               IO_KEPT), ax[1], u, fwd, st);
+    // axis 0: lines (j, k) kept x kept, correction + crop
+    run_lines<T>(grid, mk_spec(n0, 0, int64_t(n1) * n2, N1, N2, n2, 1, 1, 2, 1, 1, IO_FULL, IO_UNI),
+                 ax[0], u, fwd, st);
+  }
+}
+
+template <typename T>
+void fft_u2nu_head(const void *uni, const int64_t *istride, const Geometry &g,
+                   const FFTAxisPlan *ax, bool fwd, const double *const corfac[3],
+                   bool fft_order, void *gridv, cudaStream_t st) {
+  cplx<T> *grid = static_cast<cplx<T> *>(gridv);
+  UniSpec u = mk_uni(const_cast<void *>(uni), istride, g, corfac, fft_order);
+  const int n0 = int(g.nover[0]);
+  if (g.ndim == 1) {
+    run_lines<T>(grid, mk_spec(n0, 0, 1, 1, 1, 0, 0, -1, -1, 0, 0, IO_UNI, IO_FULL), ax[0], u, fwd, st);
+  } else if (g.ndim == 2) {
+    const int n1 = int(g.nover[1]);
+    const int N1 = int(g.nuni[1]);
+    // columns (axis 0) of the kept columns: gather + correction + pad
+    run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_UNI, IO_FULL), ax[0], u,
+                 fwd, st);
+    // rows (axis 1): only kept columns are non-zero
+    run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_KEPT, IO_FULL), ax[1], u,
+                 fwd, st);
+  } else {
+    const int n1 = int(g.nover[1]), n2 = int(g.nover[2]);
+    const int N1 = int(g.nuni[1]), N2 = int(g.nuni[2]);
+    run_lines<T>(grid, mk_spec(n0, 0, int64_t(n1) * n2, N1, N2, n2, 1, 1, 2, 1, 1, IO_UNI, IO_FULL),
+                 ax[0], u, fwd, st);
+    run_lines<T>(grid, mk_spec(n1, 1, n2, n0, N2, int64_t(n1) * n2, 1, -1, 2, 0, 1, IO_KEPT,
+                               IO_FULL), ax[1], u, fwd, st);
+    run_lines<T>(grid, mk_spec(n2, 2, 1, n0 * n1, 1, n2, 0, -1, -1, 0, 0, IO_KEPT, IO_FULL), ax[2],
+                 u, fwd, st);
+  }
+}
+
+// zero a strided array of up to 3 dimensions (element size 8 or 16 bytes)
+template <typename E>
+__global__ void k_zero_strided(E *p, int64_t n0, int64_t n1, int64_t n2, int64_t s0, int64_t s1,
+                               int64_t s2) {
+  int64_t tot = n0 * n1 * n2;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < tot;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    int64_t c = i % n2, r = i / n2, b = r % n1, a = r / n1;
+    E z;
+    memset(&z, 0, sizeof(E));
+    p[a * s0 + b * s1 + c * s2] = z;
+  }
+}
+
+void zero_strided(void *ptr, int ndim, const int64_t *shape, const int64_t *stride, size_t esize,
+                  cudaStream_t st) {
+  int64_t n[3] = {1, 1, 1}, s[3] = {0, 0, 0};
+  for (int d = 0; d < ndim; ++d) {
+    n[3 - ndim + d] = shape[d];
+    s[3 - ndim + d] = stride[d];
+  }
+  int64_t tot = n[0] * n[1] * n[2];
+  if (tot == 0) return;
+  unsigned blocks = unsigned(std::min<int64_t>((tot + 255) / 256, 4096));
+  if (esize == 8)
+    k_zero_strided<float2><<<blocks, 256, 0, st>>>((float2 *)ptr, n[0], n[1], n[2], s[0], s[1], s[2]);
+  else
+    k_zero_strided<double2><<<blocks, 256, 0, st>>>((double2 *)ptr, n[0], n[1], n[2], s[0], s[1],
+                                                    s[2]);
+  DN_LAUNCHED();
+}
+
+template void fft_nu2u_tail<float>(void *, const Geometry &, const FFTAxisPlan *, bool,
+                                   const double *const[3], bool, void *, const int64_t *,
+                                   cudaStream_t);
+template void fft_nu2u_tail<double>(void *, const Geometry &, const FFTAxisPlan *, bool,
+                                    const double *const[3], bool, void *, const int64_t *,
+                                    cudaStream_t);
+template void fft_u2nu_head<float>(const void *, const int64_t *, const Geometry &,
+                                   const FFTAxisPlan *, bool, const double *const[3], bool,
+                                   void *, cudaStream_t);
+template void fft_u2nu_head<double>(const void *, const int64_t *, const Geometry &,
+                                    const FFTAxisPlan *, bool, const double *const[3], bool,
+                                    void *, cudaStream_t);
+
+}  // namespace dnufft

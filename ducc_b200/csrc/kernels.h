@@ -1,0 +1,79 @@
+// Host-callable launchers of the CUDA kernels (defined in the .cu files).
+#pragma once
+
+#include "dnufft_internal.h"
+
+namespace dnufft {
+
+// ---- binning / sorting (binsort.cu)
+void launch_fold_keys(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
+                      uint32_t npts, const Geometry &g, uint32_t *keys, uint32_t *idx,
+                      cudaStream_t st);
+size_t scan_workspace_bytes(uint64_t n);
+void exclusive_scan(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *ws,
+                    cudaStream_t st);
+size_t radix_workspace_bytes(uint32_t n, int keybits);
+void radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t n, int keybits, void *ws,
+                      cudaStream_t st);
+size_t chunk_workspace_bytes(uint32_t n);
+uint32_t build_chunks(const uint32_t *skeys, uint32_t n, int tile_shift, uint32_t chunk,
+                      Chunk *chunks, uint32_t *d_count, void *ws, cudaStream_t st);
+void launch_gather_coords(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
+                          int ndim, const uint32_t *perm, uint32_t n, void *out,
+                          cudaStream_t st);
+
+// ---- spreading / interpolation (spread_*.cu)
+struct PointsDesc {
+  const void *coord;      // sorted==true: contiguous (npts, ndim) in tile order
+  int64_t cs0, cs1;       //   else the caller's array, addressed through perm
+  bool sorted;
+  bool coord_f64;
+  const uint32_t *perm;   // tile order -> caller's point index
+  uint32_t npts;
+};
+
+struct ChunkList {
+  const Chunk *chunks;
+  uint32_t nchunks;
+};
+
+// grid: contiguous oversampled grid (nover[0] x ... ), complex<T>
+// values: caller's point values, complex<T>, element stride vs; ntrans
+// transforms, values of transform t at values + t*vtrans, grids at grid + t*gtrans
+template <typename T>
+void launch_spread(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                   const KernelPoly<T> &kp, const void *values, int64_t vs,
+                   int64_t vtrans, void *grid, int64_t gtrans, int ntrans,
+                   cudaStream_t st);
+
+template <typename T>
+void launch_interp(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                   const KernelPoly<T> &kp, const void *grid, int64_t gtrans,
+                   void *out, int64_t os, int64_t otrans, int ntrans, cudaStream_t st);
+
+// ---- FFT and correction (fft.cu)
+struct FFTAxisPlan {
+  int n;
+  int nfac;
+  int fac[24];
+  const void *tw;   // device table of n twiddles exp(-2 pi i k/n) (float2/double2)
+};
+
+// Type 1 tail: FFTs over the oversampled grid with output pruning, then
+// deconvolution + crop into the caller's uniform array (arbitrary strides).
+template <typename T>
+void fft_nu2u_tail(void *grid, const Geometry &g, const FFTAxisPlan *ax, bool forward,
+                   const double *const corfac[3], bool fft_order, void *out,
+                   const int64_t *ostride, cudaStream_t st);
+
+// Type 2 head: deconvolution + zero-pad of the caller's uniform array into the
+// oversampled grid, then FFTs with input pruning.
+template <typename T>
+void fft_u2nu_head(const void *uni, const int64_t *istride, const Geometry &g,
+                   const FFTAxisPlan *ax, bool forward, const double *const corfac[3],
+                   bool fft_order, void *grid, cudaStream_t st);
+
+void zero_strided(void *ptr, int ndim, const int64_t *shape, const int64_t *stride, size_t esize,
+                  cudaStream_t st);
+
+}  // namespace dnufft

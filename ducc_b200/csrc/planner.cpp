@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <thread>
 #include <sched.h>
+#include <atomic>
 
 namespace dnufft {
 
@@ -251,6 +252,10 @@ std::vector<int> fft_factors(int n) {
   if (f.empty()) f.push_back(1);
   return f;
 }
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void cuda_check(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return;

@@ -1,0 +1,429 @@
+// Plain spreading (type 1) and interpolation (type 2) kernels.
+//
+// One CTA per chunk of tile-sorted points (at most CHUNK points of one tile).
+// Spreading: every warp takes 32 points at a time, each lane folds its point
+// and evaluates the W weights per axis by Horner in registers, stages them in
+// shared memory, then the warp walks the 32 points and its lanes cover the
+// W^d footprint of one point together (no two lanes touch the same cell), adding
+// into a shared-memory copy of the tile plus halo with shared-memory atomics
+// (the per-point FP32/FP64 atomics of the plain form).  The tile buffer is
+// flushed once with vectorised global atomics at wrapped grid positions.
+// Interpolation: the tile plus halo is staged in shared memory and every thread
+// evaluates one point (weights in registers, W^d multiply-adds), writing the
+// result through the tile permutation.
+//
+// Mirrors HelperNu2u / spreading_helper and HelperU2nu / interpolation_helper
+// (src/ducc0/nufft/nufft.h:917-1272 for 2D, :1391-1729 for 3D, :526-834 for 1D).
+#pragma once
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace dnufft {
+
+constexpr int SP_THREADS = 256;
+constexpr int SP_WARPS = SP_THREADS / 32;
+
+template <int NDIM>
+__device__ __forceinline__ void tile_origin(uint32_t tile, const Geometry &g, int (&b0)[NDIM]) {
+  const int L = g.log2tile;
+  if constexpr (NDIM == 1) {
+    b0[0] = (int(tile) << L) - g.nsafe;
+  } else if constexpr (NDIM == 2) {
+    int ntv = int(g.ntiles[1]);
+    b0[0] = ((int(tile) / ntv) << L) - g.nsafe;
+    b0[1] = ((int(tile) % ntv) << L) - g.nsafe;
+  } else {
+    int ntv = int(g.ntiles[1]), ntw = int(g.ntiles[2]);
+    int tu = int(tile) / (ntv * ntw), r = int(tile) % (ntv * ntw);
+    b0[0] = (tu << L) - g.nsafe;
+    b0[1] = ((r / ntw) << L) - g.nsafe;
+    b0[2] = ((r % ntw) << L) - g.nsafe;
+  }
+}
+
+template <typename Tc, int NDIM>
+__device__ __forceinline__ uint32_t load_point(const PointsDesc &pts, uint32_t i, Tc (&x)[NDIM]) {
+  uint32_t j = pts.perm[i];
+  const Tc *c = static_cast<const Tc *>(pts.coord);
+  if (pts.sorted) {
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) x[d] = c[uint64_t(i) * NDIM + d];
+  } else {
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) x[d] = c[int64_t(j) * pts.cs0 + int64_t(d) * pts.cs1];
+  }
+  return j;
+}
+
+template <typename T> struct BufferLayout {
+  // does the tile buffer live in shared memory for this (precision, ndim)?
+  static constexpr bool smem(int ndim) { return !(ndim == 3 && sizeof(T) == 8); }
+};
+
+template <typename T>
+__device__ __forceinline__ void global_add(cplx<T> *p, T re, T im) {
+  if constexpr (sizeof(T) == 4) {
+    atomicAdd(reinterpret_cast<float2 *>(p), make_float2(re, im));
+  } else {
+    atomicAdd(&p->x, re);
+    atomicAdd(&p->y, im);
+  }
+}
+
+template <typename T, typename Tc, int NDIM, int W>
+__global__ void __launch_bounds__(SP_THREADS)
+    k_spread(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
+             const cplx<T> *__restrict__ values, int64_t vs, int64_t vtrans,
+             cplx<T> *__restrict__ grid, int64_t gtrans) {
+  constexpr bool SMEM = BufferLayout<T>::smem(NDIM);
+  constexpr int FP = (NDIM == 1) ? W : (NDIM == 2 ? W * W : W * W * W);
+  constexpr int NIT = (FP + 31) / 32;
+  constexpr int UNR = NIT <= 8 ? NIT : 4;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const Chunk ch = chunks[blockIdx.x];
+  values += int64_t(blockIdx.y) * vtrans;
+  grid += int64_t(blockIdx.y) * gtrans;
+  const int S = (1 << g.log2tile) + W;
+  int ncell = S;
+  if (NDIM >= 2) ncell *= S;
+  if (NDIM >= 3) ncell *= S;
+  int b0[NDIM];
+  tile_origin<NDIM>(ch.tile, g, b0);
+  cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned char *stage = smraw + (SMEM ? size_t(ncell) * sizeof(cplx<T>) : 0);
+  T *stw = reinterpret_cast<T *>(stage) + warp * 32 * NDIM * W;
+  cplx<T> *stv = reinterpret_cast<cplx<T> *>(reinterpret_cast<T *>(stage) + SP_WARPS * 32 * NDIM * W) +
+                 warp * 32;
+  int *sto = reinterpret_cast<int *>(reinterpret_cast<cplx<T> *>(reinterpret_cast<T *>(stage) +
+                                                                 SP_WARPS * 32 * NDIM * W) +
+                                     SP_WARPS * 32) +
+             warp * 32 * NDIM;
+  if constexpr (SMEM) {
+    for (int c = threadIdx.x; c < ncell; c += SP_THREADS) buf[c] = mkc<T>(T(0), T(0));
+    __syncthreads();
+  }
+  const uint32_t end = ch.start + ch.count;
+  for (uint32_t base = ch.start + uint32_t(warp) * 32; base < end; base += SP_WARPS * 32) {
+    uint32_t i = base + lane;
+    if (i < end) {
+      Tc x[NDIM];
+      uint32_t j = load_point<Tc, NDIM>(pts, i, x);
+      cplx<T> v = values[int64_t(j) * vs];
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        int i0;
+        double frac;
+        fold<Tc>(x[d], g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], i0, frac);
+        T w[W];
+        kernel_weights<T, W>(kp, T(double(W - 1) - 2.0 * frac), w);
+#pragma unroll
+        for (int a = 0; a < W; ++a) stw[(lane * NDIM + d) * W + a] = w[a];
+        sto[lane * NDIM + d] = i0 - b0[d];
+      }
+      stv[lane] = v;
+    }
+    __syncwarp();
+    int np = min(32, int(end - base));
+    for (int p = 0; p < np; ++p) {
+      const cplx<T> v = stv[p];
+      const T *wp = stw + p * NDIM * W;
+      int o[NDIM];
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) o[d] = sto[p * NDIM + d];
+#pragma unroll UNR
+      for (int c0 = 0; c0 < FP; c0 += 32) {
+        int c = c0 + lane;
+        if (FP % 32 == 0 || c < FP) {
+          T wt;
+          int cell;
+          if constexpr (NDIM == 1) {
+            wt = wp[c];
+            cell = o[0] + c;
+          } else if constexpr (NDIM == 2) {
+            int a = c / W, b = c - (c / W) * W;
+            wt = wp[a] * wp[W + b];
+            cell = (o[0] + a) * S + (o[1] + b);
+          } else {
+            int a = c / (W * W), r = c - a * (W * W), b = r / W, e = r - b * W;
+            wt = wp[a] * wp[W + b] * wp[2 * W + e];
+            cell = ((o[0] + a) * S + (o[1] + b)) * S + (o[2] + e);
+          }
+          T re = wt * v.x, im = wt * v.y;
+          if constexpr (SMEM) {
+            atomicAdd(&buf[cell].x, re);
+            atomicAdd(&buf[cell].y, im);
+          } else {
+            // direct global accumulation at wrapped positions
+            int gi[NDIM];
+            int rem = cell;
+#pragma unroll
+            for (int d = NDIM - 1; d >= 0; --d) {
+              gi[d] = rem % S;
+              rem /= S;
+            }
+            int64_t gidx = 0;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d)
+              gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
+            global_add<T>(grid + gidx, re, im);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if constexpr (SMEM) {
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncell; c += SP_THREADS) {
+      cplx<T> v = buf[c];
+      if (v.x == T(0) && v.y == T(0)) continue;
+      int gi[NDIM];
+      int rem = c;
+#pragma unroll
+      for (int d = NDIM - 1; d >= 0; --d) {
+        gi[d] = rem % S;
+        rem /= S;
+      }
+      int64_t gidx = 0;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d)
+        gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
+      global_add<T>(grid + gidx, v.x, v.y);
+    }
+  }
+}
+
+template <typename T, typename Tc, int NDIM, int W>
+__global__ void __launch_bounds__(SP_THREADS)
+    k_interp(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
+             const cplx<T> *__restrict__ grid, int64_t gtrans, cplx<T> *__restrict__ out,
+             int64_t os, int64_t otrans) {
+  constexpr bool SMEM = BufferLayout<T>::smem(NDIM);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const Chunk ch = chunks[blockIdx.x];
+  grid += int64_t(blockIdx.y) * gtrans;
+  out += int64_t(blockIdx.y) * otrans;
+  const int S = (1 << g.log2tile) + W;
+  int ncell = S;
+  if (NDIM >= 2) ncell *= S;
+  if (NDIM >= 3) ncell *= S;
+  int b0[NDIM];
+  tile_origin<NDIM>(ch.tile, g, b0);
+  cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
+  if constexpr (SMEM) {
+    for (int c = threadIdx.x; c < ncell; c += SP_THREADS) {
+      int gi[NDIM];
+      int rem = c;
+#pragma unroll
+      for (int d = NDIM - 1; d >= 0; --d) {
+        gi[d] = rem % S;
+        rem /= S;
+      }
+      int64_t gidx = 0;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d)
+        gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
+      buf[c] = grid[gidx];
+    }
+    __syncthreads();
+  }
+  const uint32_t end = ch.start + ch.count;
+  for (uint32_t i = ch.start + threadIdx.x; i < end; i += SP_THREADS) {
+    Tc x[NDIM];
+    uint32_t j = load_point<Tc, NDIM>(pts, i, x);
+    T w[NDIM][W];
+    int o[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      int i0;
+      double frac;
+      fold<Tc>(x[d], g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], i0, frac);
+      kernel_weights<T, W>(kp, T(double(W - 1) - 2.0 * frac), w[d]);
+      o[d] = i0 - b0[d];
+    }
+    T ar = 0, ai = 0;
+    if constexpr (NDIM == 1) {
+#pragma unroll
+      for (int a = 0; a < W; ++a) {
+        cplx<T> gv = buf[o[0] + a];
+        ar += w[0][a] * gv.x;
+        ai += w[0][a] * gv.y;
+      }
+    } else if constexpr (NDIM == 2) {
+#pragma unroll
+      for (int a = 0; a < W; ++a) {
+        const cplx<T> *row = buf + (o[0] + a) * S + o[1];
+        T rr = 0, ri = 0;
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+          cplx<T> gv = row[b];
+          rr += w[1][b] * gv.x;
+          ri += w[1][b] * gv.y;
+        }
+        ar += w[0][a] * rr;
+        ai += w[0][a] * ri;
+      }
+    } else {
+      if constexpr (SMEM) {
+#pragma unroll 1
+        for (int a = 0; a < W; ++a) {
+          T pr = 0, pi = 0;
+#pragma unroll
+          for (int b = 0; b < W; ++b) {
+            const cplx<T> *row = buf + ((o[0] + a) * S + (o[1] + b)) * S + o[2];
+            T rr = 0, ri = 0;
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+              cplx<T> gv = row[e];
+              rr += w[2][e] * gv.x;
+              ri += w[2][e] * gv.y;
+            }
+            pr += w[1][b] * rr;
+            pi += w[1][b] * ri;
+          }
+          ar += w[0][a] * pr;
+          ai += w[0][a] * pi;
+        }
+      } else {
+        const int nu = int(g.nover[0]), nv = int(g.nover[1]), nw = int(g.nover[2]);
+        int iw[W];
+#pragma unroll
+        for (int e = 0; e < W; ++e) iw[e] = wrapi(b0[2] + o[2] + e, nw);
+#pragma unroll 1
+        for (int a = 0; a < W; ++a) {
+          int iu = wrapi(b0[0] + o[0] + a, nu);
+          T pr = 0, pi = 0;
+#pragma unroll
+          for (int b = 0; b < W; ++b) {
+            int iv = wrapi(b0[1] + o[1] + b, nv);
+            const cplx<T> *row = grid + (int64_t(iu) * nv + iv) * nw;
+            T rr = 0, ri = 0;
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+              cplx<T> gv = __ldg(row + iw[e]);
+              rr += w[2][e] * gv.x;
+              ri += w[2][e] * gv.y;
+            }
+            pr += w[1][b] * rr;
+            pi += w[1][b] * ri;
+          }
+          ar += w[0][a] * pr;
+          ai += w[0][a] * pi;
+        }
+      }
+    }
+    out[int64_t(j) * os] = mkc<T>(ar, ai);
+  }
+}
+
+template <typename T, int NDIM, int W>
+size_t spread_smem_bytes(const Geometry &g) {
+  int S = (1 << g.log2tile) + W;
+  size_t ncell = size_t(S);
+  for (int d = 1; d < NDIM; ++d) ncell *= size_t(S);
+  size_t buf = BufferLayout<T>::smem(NDIM) ? ncell * sizeof(cplx<T>) : 0;
+  size_t stage = size_t(SP_WARPS) * 32 * (NDIM * W * sizeof(T) + sizeof(cplx<T>) + NDIM * sizeof(int));
+  return buf + stage;
+}
+
+template <typename T, int NDIM, int W>
+size_t interp_smem_bytes(const Geometry &g) {
+  int S = (1 << g.log2tile) + W;
+  size_t ncell = size_t(S);
+  for (int d = 1; d < NDIM; ++d) ncell *= size_t(S);
+  return BufferLayout<T>::smem(NDIM) ? ncell * sizeof(cplx<T>) : 0;
+}
+
+template <typename T, typename Tc, int NDIM, int W>
+void spread_w(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+              const KernelPoly<T> &kp, const void *values, int64_t vs, int64_t vtrans,
+              void *grid, int64_t gtrans, int ntrans, cudaStream_t st) {
+  size_t sm = spread_smem_bytes<T, NDIM, W>(g);
+  auto kern = k_spread<T, Tc, NDIM, W>;
+  DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  dim3 grd(cl.nchunks, ntrans);
+  kern<<<grd, SP_THREADS, sm, st>>>(pts, cl.chunks, g, kp, static_cast<const cplx<T> *>(values), vs,
+                                    vtrans, static_cast<cplx<T> *>(grid), gtrans);
+  DN_LAUNCHED();
+}
+
+template <typename T, typename Tc, int NDIM, int W>
+void interp_w(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+              const KernelPoly<T> &kp, const void *grid, int64_t gtrans, void *out, int64_t os,
+              int64_t otrans, int ntrans, cudaStream_t st) {
+  size_t sm = interp_smem_bytes<T, NDIM, W>(g);
+  auto kern = k_interp<T, Tc, NDIM, W>;
+  DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  dim3 grd(cl.nchunks, ntrans);
+  kern<<<grd, SP_THREADS, sm, st>>>(pts, cl.chunks, g, kp, static_cast<const cplx<T> *>(grid),
+                                    gtrans, static_cast<cplx<T> *>(out), os, otrans);
+  DN_LAUNCHED();
+}
+
+// W dispatch: float supports W 4..8, double 4..16 (the kernel table's ranges)
+#define DN_FOR_W_FLOAT(M) M(4) M(5) M(6) M(7) M(8)
+#define DN_FOR_W_DOUBLE(M) \
+  M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16)
+
+template <typename T, typename Tc, int NDIM>
+void spread_dispatch(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                     const KernelPoly<T> &kp, const void *values, int64_t vs, int64_t vtrans,
+                     void *grid, int64_t gtrans, int ntrans, cudaStream_t st) {
+#define DN_CASE(WW) \
+  case WW: spread_w<T, Tc, NDIM, WW>(pts, cl, g, kp, values, vs, vtrans, grid, gtrans, ntrans, st); return;
+  if constexpr (sizeof(T) == 4) {
+    switch (g.W) { DN_FOR_W_FLOAT(DN_CASE) }
+  } else {
+    switch (g.W) { DN_FOR_W_DOUBLE(DN_CASE) }
+  }
+#undef DN_CASE
+  throw Error(ST_UNSUPPORTED, "kernel support not supported by this build");
+}
+
+template <typename T, typename Tc, int NDIM>
+void interp_dispatch(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                     const KernelPoly<T> &kp, const void *grid, int64_t gtrans, void *out,
+                     int64_t os, int64_t otrans, int ntrans, cudaStream_t st) {
+#define DN_CASE(WW) \
+  case WW: interp_w<T, Tc, NDIM, WW>(pts, cl, g, kp, grid, gtrans, out, os, otrans, ntrans, st); return;
+  if constexpr (sizeof(T) == 4) {
+    switch (g.W) { DN_FOR_W_FLOAT(DN_CASE) }
+  } else {
+    switch (g.W) { DN_FOR_W_DOUBLE(DN_CASE) }
+  }
+#undef DN_CASE
+  throw Error(ST_UNSUPPORTED, "kernel support not supported by this build");
+}
+
+template <typename T>
+void launch_spread_impl(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                        const KernelPoly<T> &kp, const void *values, int64_t vs,
+                        int64_t vtrans, void *grid, int64_t gtrans, int ntrans,
+                        cudaStream_t st) {
+  if (cl.nchunks == 0 || ntrans == 0) return;
+#define DN_SD(TC, ND) spread_dispatch<T, TC, ND>(pts, cl, g, kp, values, vs, vtrans, grid, gtrans, ntrans, st)
+  if (pts.coord_f64) {
+    if (g.ndim == 1) DN_SD(double, 1); else if (g.ndim == 2) DN_SD(double, 2); else DN_SD(double, 3);
+  } else {
+    if (g.ndim == 1) DN_SD(float, 1); else if (g.ndim == 2) DN_SD(float, 2); else DN_SD(float, 3);
+  }
+#undef DN_SD
+}
+
+template <typename T>
+void launch_interp_impl(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                        const KernelPoly<T> &kp, const void *grid, int64_t gtrans, void *out,
+                        int64_t os, int64_t otrans, int ntrans, cudaStream_t st) {
+  if (cl.nchunks == 0 || ntrans == 0) return;
+#define DN_ID(TC, ND) interp_dispatch<T, TC, ND>(pts, cl, g, kp, grid, gtrans, out, os, otrans, ntrans, st)
+  if (pts.coord_f64) {
+    if (g.ndim == 1) DN_ID(double, 1); else if (g.ndim == 2) DN_ID(double, 2); else DN_ID(double, 3);
+  } else {
+    if (g.ndim == 1) DN_ID(float, 1); else if (g.ndim == 2) DN_ID(float, 2); else DN_ID(float, 3);
+  }
+#undef DN_ID
+}
+
+}  // namespace dnufft

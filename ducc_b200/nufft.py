@@ -1,0 +1,209 @@
+"""Drop-in for ``ducc0.nufft`` running on a B200 GPU.
+
+Same functions, keyword-only arguments, defaults and error behaviour as DUCC's
+Python NUFFT module (python/nufft_pymod.cc:445-471):
+
+* ``nu2u(*, points, coord, forward, epsilon, nthreads=1, out, verbosity=0,
+  sigma_min=1.2, sigma_max=2.51, periodicity=2*pi, fft_order=False)``
+* ``u2nu(*, grid, coord, forward, epsilon, nthreads=1, out=None, ...)``
+* ``bestEpsilon(*, ndim, singleprec, sigma_min=1.1, sigma_max=2.6)``
+* ``plan(*, nu2u, coord, grid_shape, epsilon, nthreads=0, sigma_min=1.1,
+  sigma_max=2.6, periodicity=2*pi, fft_order=False)`` with ``.nu2u`` / ``.u2nu``
+
+Arrays may be numpy arrays (host; copied through the device inside the call)
+or torch CUDA tensors (used in place).  The computation precision is the data
+precision, as in DUCC.  ``nthreads`` only feeds DUCC's parameter cost model, so
+the same (kernel, oversampled size) is chosen as DUCC would choose.
+
+Extensions beyond DUCC's signature (keyword-only, optional): ``spreader``
+('auto' | 'plain' | 'tc') and ``stream`` (a CUDA stream handle).
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _capi as C
+
+__all__ = ["nu2u", "u2nu", "bestEpsilon", "plan"]
+
+
+def _np_complex_for(code):
+    return np.complex128 if code == C.C128 else np.complex64
+
+
+def _prepare_in(x):
+    """numpy inputs become C-contiguous; torch tensors pass through."""
+    if C.is_torch(x):
+        return x
+    x = np.asarray(x)
+    return np.ascontiguousarray(x)
+
+
+class _OutProxy:
+    """Output handling: numpy outputs that are not C-contiguous are computed
+    into a contiguous temporary and copied back."""
+
+    def __init__(self, out):
+        self.user = out
+        if C.is_torch(out) or out.flags.c_contiguous:
+            self.buf = out
+        else:
+            self.buf = np.empty(out.shape, dtype=out.dtype)
+
+    def finish(self):
+        if self.buf is not self.user:
+            self.user[...] = self.buf
+        return self.user
+
+
+def _check_types(data, coord):
+    dc = C.dtype_code(data)
+    cc = C.dtype_code(coord)
+    if dc not in (C.C64, C.C128) or cc not in (C.F32, C.F64):
+        raise RuntimeError("not yet supported")
+    return dc, cc
+
+
+def nu2u(*, points, coord, forward, epsilon, nthreads=1, out=None, verbosity=0,
+         sigma_min=1.2, sigma_max=2.51, periodicity=2 * math.pi, fft_order=False,
+         spreader="auto", stream=None):
+    """Type 1 non-uniform FFT (non-uniform to uniform).  ``out`` is mandatory:
+    its shape defines the uniform grid.  Returns ``out``."""
+    if out is None:
+        raise TypeError("nu2u(): 'out' is mandatory, since its shape defines the grid")
+    points = _prepare_in(points)
+    coord = _prepare_in(coord)
+    _check_types(points, coord)
+    op = _OutProxy(out)
+    ndim = len(out.shape)
+    o = C.make_opts(False, nthreads, sigma_min, sigma_max, periodicity, fft_order, verbosity,
+                    spreader, ndim)
+    a_p, a_c, a_o = C.describe(points), C.describe(coord), C.describe(op.buf)
+    C.check(C.lib().dnufft_nu2u(ctypes.byref(a_p), ctypes.byref(a_c), 1 if forward else 0,
+                                float(epsilon), ctypes.byref(a_o), ctypes.byref(o),
+                                C.stream_of(points, coord, op.buf, stream=stream)))
+    return op.finish()
+
+
+def u2nu(*, grid, coord, forward, epsilon, nthreads=1, out=None, verbosity=0,
+         sigma_min=1.2, sigma_max=2.51, periodicity=2 * math.pi, fft_order=False,
+         stream=None):
+    """Type 2 non-uniform FFT (uniform to non-uniform).  Returns the values at
+    the points (``out`` if given)."""
+    grid = _prepare_in(grid)
+    coord = _prepare_in(coord)
+    dc, _ = _check_types(grid, coord)
+    npts = coord.shape[0]
+    if out is None:
+        if C.is_torch(grid):
+            import torch
+            out = torch.empty(npts, dtype=grid.dtype, device=grid.device)
+        else:
+            out = np.empty(npts, dtype=_np_complex_for(dc))
+    op = _OutProxy(out)
+    ndim = len(grid.shape)
+    o = C.make_opts(False, nthreads, sigma_min, sigma_max, periodicity, fft_order, verbosity,
+                    "auto", ndim)
+    a_g, a_c, a_o = C.describe(grid), C.describe(coord), C.describe(op.buf)
+    C.check(C.lib().dnufft_u2nu(ctypes.byref(a_g), ctypes.byref(a_c), 1 if forward else 0,
+                                float(epsilon), ctypes.byref(a_o), ctypes.byref(o),
+                                C.stream_of(grid, coord, op.buf, stream=stream)))
+    return op.finish()
+
+
+def bestEpsilon(*, ndim, singleprec, sigma_min=1.1, sigma_max=2.6):
+    """Smallest achievable epsilon for the given dimensionality / precision."""
+    r = ctypes.c_double()
+    C.check(C.lib().dnufft_best_epsilon(int(ndim), 1 if singleprec else 0, float(sigma_min),
+                                        float(sigma_max), ctypes.byref(r)))
+    return r.value
+
+
+class plan:
+    """NUFFT plan for fixed coordinates (DUCC's ``ducc0.nufft.plan``).
+
+    Float32 coordinates make a single-precision plan (complex64 data), float64
+    coordinates a double-precision one (complex128 data)."""
+
+    def __init__(self, *, nu2u, coord, grid_shape, epsilon, nthreads=0, sigma_min=1.1,
+                 sigma_max=2.6, periodicity=2 * math.pi, fft_order=False, spreader="auto",
+                 stream=None):
+        self._ptr = None
+        coord = _prepare_in(coord)
+        if C.dtype_code(coord) not in (C.F32, C.F64):
+            raise RuntimeError("unsupported")
+        shape = [int(s) for s in grid_shape]
+        ndim = len(shape)
+        if not 1 <= ndim <= 3:
+            raise RuntimeError("unsupported dimensionality")
+        self.grid_shape = tuple(shape)
+        self.npoints = coord.shape[0]
+        self._f64 = C.dtype_code(coord) == C.F64
+        self._torch_device = coord.device if C.is_torch(coord) else None
+        o = C.make_opts(True, nthreads, sigma_min, sigma_max, periodicity, fft_order, 0,
+                        spreader, ndim)
+        a_c = C.describe(coord)
+        shp = (ctypes.c_int64 * 3)(*(shape + [1] * (3 - ndim)))
+        ptr = ctypes.c_void_p()
+        C.check(C.lib().dnufft_plan_create(1 if nu2u else 0, ctypes.byref(a_c), shp, ndim,
+                                           float(epsilon), ctypes.byref(o),
+                                           C.stream_of(coord, stream=stream),
+                                           ctypes.byref(ptr)))
+        self._ptr = ptr
+
+    def __del__(self):
+        if getattr(self, "_ptr", None):
+            try:
+                C.lib().dnufft_plan_destroy(self._ptr)
+            except Exception:
+                pass
+            self._ptr = None
+
+    def _alloc(self, like, shape):
+        dt = np.complex128 if self._f64 else np.complex64
+        if like is not None and C.is_torch(like):
+            import torch
+            return torch.empty(shape, dtype=torch.complex128 if self._f64 else torch.complex64,
+                               device=like.device)
+        return np.empty(shape, dtype=dt)
+
+    def nu2u(self, *, forward, verbosity=0, points, out=None, stream=None):
+        points = _prepare_in(points)
+        if out is None:
+            out = self._alloc(points, self.grid_shape)
+        op = _OutProxy(out)
+        a_p, a_o = C.describe(points), C.describe(op.buf)
+        C.check(C.lib().dnufft_plan_nu2u(self._ptr, 1 if forward else 0, int(verbosity),
+                                         ctypes.byref(a_p), ctypes.byref(a_o),
+                                         C.stream_of(points, op.buf, stream=stream)))
+        return op.finish()
+
+    def u2nu(self, *, forward, verbosity=0, grid, out=None, stream=None):
+        grid = _prepare_in(grid)
+        if out is None:
+            out = self._alloc(grid, (self.npoints,))
+        op = _OutProxy(out)
+        a_g, a_o = C.describe(grid), C.describe(op.buf)
+        C.check(C.lib().dnufft_plan_u2nu(self._ptr, 1 if forward else 0, int(verbosity),
+                                         ctypes.byref(a_g), ctypes.byref(a_o),
+                                         C.stream_of(grid, op.buf, stream=stream)))
+        return op.finish()
+
+    # -- B200 extras
+    def info(self):
+        """Kernel support, oversampled sizes etc. of this plan."""
+        inf = C.PlanInfo()
+        C.check(C.lib().dnufft_plan_get_info(self._ptr, ctypes.byref(inf)))
+        nd = inf.ndim
+        return {"ndim": nd, "supp": inf.supp, "kernel_index": inf.kernel_index,
+                "log2tile": inf.log2tile, "nuni": list(inf.nuni[:nd]),
+                "nover": list(inf.nover[:nd]), "ofactor": inf.ofactor, "beta": inf.beta,
+                "e0": inf.e0, "npoints": inf.npoints}
+
+    def permutation(self):
+        """The tile-order permutation of the points (DUCC's coord_idx)."""
+        out = np.empty(self.npoints, dtype=np.uint32)
+        C.check(C.lib().dnufft_plan_get_permutation(
+            self._ptr, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), None))
+        return out

@@ -146,6 +146,17 @@ int dnufft_plan_get_permutation(const dnufft_plan *plan, uint32_t *out, void *st
 /* Message of the last failed call on this thread ("" if none). */
 const char *dnufft_last_error(void);
 
+/* Number of CUDA kernels this library has launched in this process (a
+ * diagnostic without a counterpart in DUCC, which has no GPU path). */
+uint64_t dnufft_kernel_launches(void);
+
+/* Stage profiler (no counterpart in DUCC, whose verbosity report prints CPU
+ * stage times): while enabled, every transform records CUDA events between its
+ * stages and accumulates the elapsed time per stage.  Enabling clears the
+ * totals.  dnufft_profile_json() returns {"<transform>/<stage>": [ms, calls]}. */
+void dnufft_profile_enable(int enable);
+const char *dnufft_profile_json(void);
+
 #ifdef __cplusplus
 }
 #endif

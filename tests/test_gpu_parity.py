@@ -1,0 +1,229 @@
+"""Parity of the CUDA path (through the C-ABI) with DUCC and the oracle.
+
+* golden fixtures produced by DUCC itself (tests/golden): outputs within the
+  requested epsilon, tile permutation bit-exact;
+* the oracle (numpy restatement, FP64) and direct FP64 sums on small problems,
+  with DUCC's own tolerances (python/test/test_nufft.py: l2 error <= {4,2,1}*eps
+  for 1D/2D/3D; adjointness within 3e-5 (single) / 2e-13 (double) relative);
+* edge cases DUCC's tests sweep: sizes 1/20/21/257, 1 and few points, both
+  signs, fft_order, per-axis periodicity, float32 and float64 coordinates.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from ducc_b200 import nufft
+from oracle import nufft_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "g*.npz")))
+
+pytestmark = pytest.mark.gpu
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+def torch_dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("device", [False, True])
+def test_golden_nu2u(name, device):
+    g = load(name)
+    eps = float(g["eps"])
+    per = list(g["periodicity"])
+    shape = tuple(int(s) for s in g["shape"])
+    vdt = g["values"].dtype
+    if device:
+        import torch
+        out = torch.zeros(shape, dtype=torch.complex64 if vdt == np.complex64 else torch.complex128,
+                          device="cuda")
+        nufft.nu2u(points=torch_dev(g["values"]), coord=torch_dev(g["coord"]),
+                   forward=bool(g["forward"]), epsilon=eps, out=out, periodicity=per,
+                   fft_order=bool(g["fft_order"]))
+        res = out.cpu().numpy()
+    else:
+        res = np.zeros(shape, dtype=vdt)
+        nufft.nu2u(points=g["values"], coord=g["coord"], forward=bool(g["forward"]), epsilon=eps,
+                   out=res, periodicity=per, fft_order=bool(g["fft_order"]))
+    # both are approximations of the same transform with the same kernel:
+    # they agree far better than eps
+    assert O.l2error(res, g["nu2u"]) < eps
+    ref = O.direct_nu2u(g["coord"], g["values"], shape, bool(g["forward"]), per,
+                        bool(g["fft_order"]))
+    assert O.l2error(res, ref) < 2 * eps * len(shape)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("device", [False, True])
+def test_golden_u2nu(name, device):
+    g = load(name)
+    eps = float(g["eps"])
+    per = list(g["periodicity"])
+    if device:
+        res = nufft.u2nu(grid=torch_dev(g["grid_in"]), coord=torch_dev(g["coord"]),
+                         forward=bool(g["forward"]), epsilon=eps, periodicity=per,
+                         fft_order=bool(g["fft_order"])).cpu().numpy()
+    else:
+        res = nufft.u2nu(grid=g["grid_in"], coord=g["coord"], forward=bool(g["forward"]),
+                         epsilon=eps, periodicity=per, fft_order=bool(g["fft_order"]))
+    assert res.dtype == g["u2nu"].dtype
+    assert O.l2error(res, g["u2nu"]) < eps
+    ref = O.direct_u2nu(g["grid_in"], g["coord"], bool(g["forward"]), per, bool(g["fft_order"]))
+    assert O.l2error(res, ref) < 2 * eps * g["grid_in"].ndim
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_permutation_bit_exact(name):
+    g = load(name)
+    shape = tuple(int(s) for s in g["shape"])
+    coord = g["coord"]
+    sp = bool(g["singleprec"])
+    # a plan's precision follows its coordinates; DUCC's function path for
+    # mixed precision uses the data precision, so compare where they agree
+    if sp != (coord.dtype == np.float32):
+        pytest.skip("mixed-precision fixture (function path only)")
+    p = nufft.plan(nu2u=True, coord=coord, grid_shape=shape, epsilon=float(g["eps"]),
+                   nthreads=1, sigma_min=1.2, sigma_max=2.51, periodicity=list(g["periodicity"]),
+                   fft_order=bool(g["fft_order"]))
+    info = p.info()
+    assert info["supp"] == int(g["W1"])
+    assert info["nover"] == [int(x) for x in g["nover1"]]
+    assert np.array_equal(p.permutation(), g["perm1"])
+
+
+@pytest.mark.parametrize("name", ["g2d_f64", "g3d_f64", "g1d_f64", "g2d_f32", "g3d_f32"])
+def test_golden_planned(name):
+    g = load(name)
+    shape = tuple(int(s) for s in g["shape"])
+    coord = g["coord"]
+    sp = bool(g["singleprec"])
+    if sp != (coord.dtype == np.float32):
+        pytest.skip("mixed precision")
+    eps = float(g["eps"])
+    kw = dict(epsilon=eps, nthreads=1, sigma_min=1.2, sigma_max=2.51,
+              periodicity=list(g["periodicity"]), fft_order=bool(g["fft_order"]))
+    p1 = nufft.plan(nu2u=True, coord=coord, grid_shape=shape, **kw)
+    r1 = p1.nu2u(points=g["values"], forward=bool(g["forward"]))
+    assert O.l2error(r1, g["nu2u"]) < eps
+    p2 = nufft.plan(nu2u=False, coord=coord, grid_shape=shape, **kw)
+    r2 = p2.u2nu(grid=g["grid_in"], forward=bool(g["forward"]))
+    assert O.l2error(r2, g["u2nu"]) < eps
+
+
+def explicit_case(shape, npoints, epsilon, forward, singleprec, periodicity, fft_order, seed=42):
+    rng = np.random.default_rng(seed)
+    ndim = len(shape)
+    per = np.ones(ndim) * np.array(periodicity, dtype=np.float64)
+    uvw = (rng.random((npoints, ndim)) - 0.5) * per
+    ms = rng.random(npoints) - 0.5 + 1j * (rng.random(npoints) - 0.5)
+    dirty = rng.random(shape) - 0.5 + 1j * (rng.random(shape) - 0.5)
+    if singleprec:
+        ms = ms.astype(np.complex64)
+        dirty = dirty.astype(np.complex64)
+    return uvw, ms, dirty
+
+
+SWEEP = []
+for shape in [(1,), (20,), (257,), (1, 21), (20, 32), (21, 257), (250, 1), (257, 257),
+              (1, 1, 1), (20, 21, 22), (21, 1, 35)]:
+    for eps in (1e-1, 3e-5, 2e-13):
+        for sp in (True, False):
+            if sp and eps < 1e-6:
+                continue
+            SWEEP.append((shape, eps, sp))
+
+
+@pytest.mark.parametrize("shape,epsilon,singleprec", SWEEP)
+@pytest.mark.parametrize("npoints", [1, 37])
+@pytest.mark.parametrize("forward,fft_order,per", [(True, False, 2 * np.pi), (False, True, 1.0)])
+def test_explicit_sweep(shape, epsilon, singleprec, npoints, forward, fft_order, per):
+    """The reference's own accuracy and adjointness criteria
+    (python/test/test_nufft.py:46-230), restated."""
+    ndim = len(shape)
+    uvw, ms, dirty = explicit_case(shape, npoints, epsilon, forward, singleprec,
+                                   per if ndim < 3 else [1.0, np.pi, 7.0][:ndim], fft_order)
+    perio = per if ndim < 3 else [1.0, np.pi, 7.0]
+    out = np.empty(shape, dtype=dirty.dtype)
+    d2 = nufft.nu2u(points=ms, coord=uvw, forward=forward, epsilon=epsilon, out=out,
+                    periodicity=perio, fft_order=fft_order).astype(np.complex128)
+    ref = O.direct_nu2u(uvw, ms, shape, forward, perio, fft_order)
+    tol = {1: 4, 2: 2, 3: 1}[ndim] * epsilon
+    assert O.l2error(d2, ref) <= tol
+    m2 = nufft.u2nu(grid=dirty, coord=uvw, forward=not forward, epsilon=epsilon,
+                    periodicity=perio, fft_order=fft_order).astype(np.complex128)
+    r = max(O.vdot(ms, ms).real, O.vdot(m2, m2).real, O.vdot(dirty, dirty).real,
+            O.vdot(d2, d2).real)
+    t = 3e-5 * r if singleprec else 2e-13 * r
+    np.testing.assert_allclose(O.vdot(ms, m2), O.vdot(d2, dirty), rtol=t)
+    if not singleprec:
+        p = nufft.plan(nu2u=True, coord=uvw, grid_shape=shape, epsilon=epsilon,
+                       periodicity=perio, fft_order=fft_order)
+        d3 = p.nu2u(points=ms, forward=forward)
+        assert O.l2error(d3, ref) <= tol
+        p2 = nufft.plan(nu2u=False, coord=uvw, grid_shape=shape, epsilon=epsilon,
+                        periodicity=perio, fft_order=fft_order)
+        m3 = p2.u2nu(grid=dirty, forward=not forward)
+        np.testing.assert_allclose(O.vdot(ms, m3), O.vdot(d3, dirty), rtol=t)
+
+
+def test_zero_points():
+    out = np.ones((16, 16), np.complex64)
+    nufft.nu2u(points=np.zeros(0, np.complex64), coord=np.zeros((0, 2), np.float32),
+               forward=True, epsilon=1e-5, out=out)
+    assert np.all(out == 0)
+    r = nufft.u2nu(grid=np.ones((16, 16), np.complex64), coord=np.zeros((0, 2), np.float32),
+                   forward=True, epsilon=1e-5)
+    assert r.shape == (0,)
+
+
+def test_strided_device_arrays():
+    import torch
+    rng = np.random.default_rng(3)
+    M, N = 500, (40, 44)
+    coord = (rng.random((M, 2)) - 0.5) * 2 * np.pi
+    vals = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    # coords as a transposed view, values with stride 2, output as a transposed view
+    ct = torch.from_numpy(coord.T.copy()).cuda().t()
+    vt = torch.from_numpy(np.repeat(vals, 2)).cuda()[::2]
+    ot = torch.zeros((N[1], N[0]), dtype=torch.complex128, device="cuda").t()
+    nufft.nu2u(points=vt, coord=ct, forward=True, epsilon=1e-9, out=ot)
+    ref = O.direct_nu2u(coord, vals, N, True)
+    assert O.l2error(ot.cpu().numpy(), ref) < 2e-9
+
+
+def test_coordinates_far_outside_period():
+    rng = np.random.default_rng(4)
+    M, N = 300, (30, 31)
+    coord = (rng.random((M, 2)) - 0.5) * 2 * np.pi * 50
+    vals = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    out = np.empty(N, np.complex128)
+    nufft.nu2u(points=vals, coord=coord, forward=False, epsilon=1e-10, out=out)
+    assert O.l2error(out, O.direct_nu2u(coord, vals, N, False)) < 2e-10
+
+
+def test_cfg1_full_size_vs_oracle():
+    """2D type 1, M=2e5 float64 coords, 256^2 complex128, eps=1e-6."""
+    rng = np.random.default_rng(11)
+    M = 200000
+    coord = rng.uniform(-np.pi, np.pi, (M, 2))
+    vals = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    out = np.empty((256, 256), np.complex128)
+    nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=1e-6, out=out)
+    p = O.Params((256, 256), 1e-6, False, M, True, 1)
+    ref = O.nu2u(p, coord, vals, True)
+    # same kernel, FP64 both: agreement to rounding
+    assert O.l2error(out, ref) < 1e-12
+    # and against the exact transform on a few rows of modes
+    ku = np.arange(100, 104) - 128
+    kv = np.arange(256) - 128
+    eu = np.exp(-1j * np.outer(coord[:, 0], ku))
+    ev = np.exp(-1j * np.outer(coord[:, 1], kv))
+    exact = np.einsum("m,mi,mj->ij", vals, eu, ev, optimize=True)
+    assert O.l2error(out[100:104], exact) < 1e-6
