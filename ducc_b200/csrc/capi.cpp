@@ -38,11 +38,27 @@ namespace dnufft {
 constexpr uint32_t CHUNK = 1024;
 
 // ---------------------------------------------------------------- device buffers
+// Keep memory freed with cudaFreeAsync in the device's default pool instead of
+// returning it to the driver at every synchronisation, so repeated transforms
+// do not pay for mapping fresh pages.
+static void keep_pool_memory() {
+  static thread_local int done_for = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev == done_for) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = ~uint64_t(0);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done_for = dev;
+}
+
 struct DevBuf {
   void *p = nullptr;
   cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(size_t bytes, cudaStream_t s) : st(s) {
+    keep_pool_memory();
     if (bytes) DN_CUDA(cudaMallocAsync(&p, bytes, s));
   }
   DevBuf(const DevBuf &) = delete;
@@ -151,9 +167,10 @@ static View view_of(const dnufft_array *a, const char *what) {
     size *= v.shape[d];
   }
   DN_REQUIRE(size == 0 || v.data != nullptr, ST_BADARG, std::string(what) + ": null data");
-  for (int d = 0; d < v.ndim; ++d)
-    DN_REQUIRE(v.shape[d] <= 1 || v.stride[d] != 0, ST_BADARG,
-               std::string(what) + ": zero stride");
+  if (size > 0)
+    for (int d = 0; d < v.ndim; ++d)
+      DN_REQUIRE(v.shape[d] <= 1 || v.stride[d] != 0, ST_BADARG,
+                 std::string(what) + ": zero stride");
   v.host = (size > 0) ? is_host_pointer(v.data) : false;
   if (v.host) {
     int64_t s = 1;
@@ -418,10 +435,12 @@ static void report_sizes(const Setup &s, bool gridding) {
 template <typename T>
 static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
                           const ChunkList &cl, const View &points, const View &out, bool forward,
-                          bool fft_order, StageTimer &tm, cudaStream_t st) {
+                          bool fft_order, StageTimer &tm, cudaStream_t st, DevBuf *ws = nullptr) {
   size_t cells = grid_cells(s.g);
   tm.mark("zeroing grid");
-  DevBuf grid(cells * sizeof(T) * 2, st);
+  DevBuf local;
+  DevBuf &grid = ws ? *ws : local;
+  if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
   DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * sizeof(T) * 2, st));
   tm.mark("spreading");
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
@@ -435,9 +454,11 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
 template <typename T>
 static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &pts,
                           const ChunkList &cl, const View &uni, const View &out, bool forward,
-                          bool fft_order, StageTimer &tm, cudaStream_t st) {
+                          bool fft_order, StageTimer &tm, cudaStream_t st, DevBuf *ws = nullptr) {
   size_t cells = grid_cells(s.g);
-  DevBuf grid(cells * sizeof(T) * 2, st);
+  DevBuf local;
+  DevBuf &grid = ws ? *ws : local;
+  if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
   tm.mark("correction + FFT");
   fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st);
   tm.mark("interpolation");
@@ -554,6 +575,7 @@ struct dnufft_plan {
   dnufft::DevConst dc;
   dnufft::Index ix;
   dnufft::DevBuf sorted_coord;
+  dnufft::DevBuf grid;   // oversampled grid, allocated on first execution
   dnufft_opts o;
   int device = 0;
 };
@@ -614,17 +636,22 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
     so.finish();
     return;
   }
+  if (!p->grid.p) {
+    // allocated once, on first use, and made visible to every stream
+    p->grid = DevBuf(grid_cells(s.g) * (f64 ? 16 : 8), st);
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
   PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
                  p->ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
   bool fo = p->o.fft_order != 0;
   if (type1) {
-    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
-    else do_spread_fft<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
+    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
+    else do_spread_fft<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
     tm.report("nu2u (planned)");
   } else {
-    if (f64) do_fft_interp<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
-    else do_fft_interp<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st);
+    if (f64) do_fft_interp<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
+    else do_fft_interp<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
     tm.report("u2nu (planned)");
   }
   so.finish();
@@ -709,6 +736,7 @@ int dnufft_plan_destroy(dnufft_plan *plan) {
       cudaStream_t st = nullptr;
       plan->ix.perm.st = plan->ix.chunks.st = plan->ix.count.st = plan->ix.keys.st = st;
       plan->sorted_coord.st = st;
+      plan->grid.st = st;
       for (int d = 0; d < 3; ++d) plan->dc.corfac[d].st = plan->dc.tw[d].st = st;
       delete plan;
       DN_CUDA(cudaDeviceSynchronize());

@@ -48,6 +48,12 @@ __device__ __forceinline__ void grid_to_uni(int c, int N, int n, bool fft_order,
 
 enum { IO_FULL = 0, IO_KEPT = 1, IO_UNI = 2 };
 
+// element d of a 3-array held in a by-value kernel parameter, without dynamic
+// indexing (which would force a local-memory copy of the whole parameter)
+template <typename X> __device__ __forceinline__ X sel3(const X (&a)[3], int d) {
+  return d == 0 ? a[0] : (d == 1 ? a[1] : a[2]);
+}
+
 struct LineSpec {
   int n;            // transform length
   int ax;           // transformed grid axis
@@ -192,11 +198,11 @@ __device__ void fft_lines(cplx<T> *s, int n, int nl, const FFTAxisPlan &p, bool 
   }
 }
 
-__device__ __forceinline__ int64_t line_base(const LineSpec &ls, const int *Nk, const int *nk,
-                                             int L, int &ia, int &ib) {
+__device__ __forceinline__ int64_t line_base(const LineSpec &ls, const int (&Nk)[3],
+                                             const int (&nk)[3], int L, int &ia, int &ib) {
   int a = L / ls.cntb, b = L - (L / ls.cntb) * ls.cntb;
-  ia = (ls.axa >= 0 && ls.kepta) ? kept_to_grid(a, Nk[ls.axa], nk[ls.axa]) : a;
-  ib = (ls.axb >= 0 && ls.keptb) ? kept_to_grid(b, Nk[ls.axb], nk[ls.axb]) : b;
+  ia = (ls.axa >= 0 && ls.kepta) ? kept_to_grid(a, sel3(Nk, ls.axa), sel3(nk, ls.axa)) : a;
+  ib = (ls.axb >= 0 && ls.keptb) ? kept_to_grid(b, sel3(Nk, ls.axb), sel3(nk, ls.axb)) : b;
   return int64_t(ia) * ls.sa + int64_t(ib) * ls.sb;
 }
 
@@ -207,15 +213,15 @@ __device__ __forceinline__ void line_uni(const LineSpec &ls, const UniSpec &u, i
   uoff = 0;
   if (ls.axa >= 0) {
     int iu, icf;
-    grid_to_uni(ia, u.N[ls.axa], u.n[ls.axa], u.fft_order, iu, icf);
-    fac *= u.corfac[ls.axa][icf];
-    uoff += int64_t(iu) * u.stride[ls.axa];
+    grid_to_uni(ia, sel3(u.N, ls.axa), sel3(u.n, ls.axa), u.fft_order, iu, icf);
+    fac *= sel3(u.corfac, ls.axa)[icf];
+    uoff += int64_t(iu) * sel3(u.stride, ls.axa);
   }
   if (ls.axb >= 0) {
     int iu, icf;
-    grid_to_uni(ib, u.N[ls.axb], u.n[ls.axb], u.fft_order, iu, icf);
-    fac *= u.corfac[ls.axb][icf];
-    uoff += int64_t(iu) * u.stride[ls.axb];
+    grid_to_uni(ib, sel3(u.N, ls.axb), sel3(u.n, ls.axb), u.fft_order, iu, icf);
+    fac *= sel3(u.corfac, ls.axb)[icf];
+    uoff += int64_t(iu) * sel3(u.stride, ls.axb);
   }
 }
 
@@ -229,7 +235,7 @@ __global__ void __launch_bounds__(fft_max_threads<T>())
   const int n = ls.n, nl = ls.nl;
   const int L0 = blockIdx.x * nl;
   const int nloc = min(nl, ls.nlines - L0);
-  const int N = u.N[ls.ax];
+  const int N = sel3(u.N, ls.ax);
   const int total = n * nl;
   // ---------------- load
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
@@ -259,9 +265,9 @@ __global__ void __launch_bounds__(fft_max_threads<T>())
             line_uni(ls, u, ia, ib, fac, uoff);
             int iu, icf;
             grid_to_uni(k, N, n, u.fft_order, iu, icf);
-            fac *= u.corfac[ls.ax][icf];
+            fac *= sel3(u.corfac, ls.ax)[icf];
             const cplx<T> *up = static_cast<const cplx<T> *>(u.ptr);
-            cplx<T> x = up[uoff + int64_t(iu) * u.stride[ls.ax]];
+            cplx<T> x = up[uoff + int64_t(iu) * sel3(u.stride, ls.ax)];
             T f = T(fac);
             v = mkc<T>(x.x * f, x.y * f);
           }
@@ -299,20 +305,292 @@ __global__ void __launch_bounds__(fft_max_threads<T>())
         line_uni(ls, u, ia, ib, fac, uoff);
         int iu, icf;
         grid_to_uni(k, N, n, u.fft_order, iu, icf);
-        fac *= u.corfac[ls.ax][icf];
+        fac *= sel3(u.corfac, ls.ax)[icf];
         cplx<T> x = s[k * nl + l];
         T f = T(fac);
         cplx<T> *up = static_cast<cplx<T> *>(u.ptr);
-        up[uoff + int64_t(iu) * u.stride[ls.ax]] = mkc<T>(x.x * f, x.y * f);
+        up[uoff + int64_t(iu) * sel3(u.stride, ls.ax)] = mkc<T>(x.x * f, x.y * f);
       }
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// FFT v2: one or more lines per CTA, stages in place with register staging,
+// no runtime integer division in the butterfly indexing (lines per CTA is a
+// power of two, the Stockham group index comes from a precomputed reciprocal),
+// twiddles from a two-level table in shared memory (tw[t] = hi[t>>6]*lo[t&63]),
+// and constant-folded butterflies for radices 2, 3, 4, 5, 7, 8, 11.
+// ---------------------------------------------------------------------------
+struct StageInfo {
+  int nst;
+  int R[24];
+  int Ns[24];
+  int tstep[24];
+  uint32_t mul[24];   // ceil(2^32 / Ns)
+};
+
+// cos / sin of 2*pi*k/R, k < R, for the odd radices 3, 5, 7, 11 (rows 0..3)
+__constant__ double kcos_d[4][11] = {
+  {1.0, -0.5, -0.5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+  {1.0, 0.30901699437494745, -0.8090169943749473, -0.8090169943749476, 0.30901699437494723, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+  {1.0, 0.6234898018587336, -0.22252093395631434, -0.900968867902419, -0.9009688679024191, -0.2225209339563146, 0.6234898018587334, 0.0, 0.0, 0.0, 0.0},
+  {1.0, 0.8412535328311812, 0.41541501300188644, -0.142314838273285, -0.654860733945285, -0.9594929736144974, -0.9594929736144975, -0.6548607339452852, -0.14231483827328523, 0.41541501300188605, 0.8412535328311812}};
+__constant__ double ksin_d[4][11] = {
+  {0.0, 0.8660254037844387, -0.8660254037844384, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+  {0.0, 0.9510565162951535, 0.5877852522924732, -0.587785252292473, -0.9510565162951536, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+  {0.0, 0.7818314824680298, 0.9749279121818236, 0.43388373911755823, -0.433883739117558, -0.9749279121818236, -0.7818314824680299, 0.0, 0.0, 0.0, 0.0},
+  {0.0, 0.5406408174555976, 0.9096319953545183, 0.9898214418809328, 0.7557495743542583, 0.28173255684142967, -0.2817325568414294, -0.7557495743542582, -0.9898214418809327, -0.9096319953545186, -0.5406408174555974}};
+__constant__ float kcos_f[4][11] = {
+  {1.0f, -0.5f, -0.5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+  {1.0f, 0.30901699437494745f, -0.8090169943749473f, -0.8090169943749476f, 0.30901699437494723f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+  {1.0f, 0.6234898018587336f, -0.22252093395631434f, -0.900968867902419f, -0.9009688679024191f, -0.2225209339563146f, 0.6234898018587334f, 0.0f, 0.0f, 0.0f, 0.0f},
+  {1.0f, 0.8412535328311812f, 0.41541501300188644f, -0.142314838273285f, -0.654860733945285f, -0.9594929736144974f, -0.9594929736144975f, -0.6548607339452852f, -0.14231483827328523f, 0.41541501300188605f, 0.8412535328311812f}};
+__constant__ float ksin_f[4][11] = {
+  {0.0f, 0.8660254037844387f, -0.8660254037844384f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+  {0.0f, 0.9510565162951535f, 0.5877852522924732f, -0.587785252292473f, -0.9510565162951536f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+  {0.0f, 0.7818314824680298f, 0.9749279121818236f, 0.43388373911755823f, -0.433883739117558f, -0.9749279121818236f, -0.7818314824680299f, 0.0f, 0.0f, 0.0f, 0.0f},
+  {0.0f, 0.5406408174555976f, 0.9096319953545183f, 0.9898214418809328f, 0.7557495743542583f, 0.28173255684142967f, -0.2817325568414294f, -0.7557495743542582f, -0.9898214418809327f, -0.9096319953545186f, -0.5406408174555974f}};
+
+template <int R> constexpr int radix_row() { return R == 3 ? 0 : R == 5 ? 1 : R == 7 ? 2 : 3; }
+template <typename T, int R> __device__ __forceinline__ T trig_cos(int k) {
+  if constexpr (sizeof(T) == 4) return kcos_f[radix_row<R>()][k]; else return kcos_d[radix_row<R>()][k];
+}
+template <typename T, int R> __device__ __forceinline__ T trig_sin(int k) {
+  if constexpr (sizeof(T) == 4) return ksin_f[radix_row<R>()][k]; else return ksin_d[radix_row<R>()][k];
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void dft_const(cplx<T> (&a)[R], bool fwd) {
+  if constexpr (R == 2 || R == 4 || R == 8) {
+    dft_small<T, R>(a, nullptr, 0, fwd);
+  } else {
+    constexpr int H = (R - 1) / 2;
+    cplx<T> sp[H + 1], sm[H + 1];
+#pragma unroll
+    for (int m = 1; m <= H; ++m) {
+      sp[m] = cadd<T>(a[m], a[R - m]);
+      sm[m] = csub<T>(a[m], a[R - m]);
+    }
+    cplx<T> y0 = a[0];
+#pragma unroll
+    for (int m = 1; m <= H; ++m) y0 = cadd<T>(y0, sp[m]);
+    const T sg = fwd ? T(-1) : T(1);
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      cplx<T> re = a[0];
+      cplx<T> im = mkc<T>(T(0), T(0));
+#pragma unroll
+      for (int m = 1; m <= H; ++m) {
+        const T c = trig_cos<T, R>((m * q) % R), sn = trig_sin<T, R>((m * q) % R);
+        re.x += sp[m].x * c;
+        re.y += sp[m].y * c;
+        im.x += sm[m].x * sn;
+        im.y += sm[m].y * sn;
+      }
+      // y_q = re + sg*i*im, y_{R-q} = re - sg*i*im
+      a[q] = mkc<T>(re.x - sg * im.y, re.y + sg * im.x);
+      a[R - q] = mkc<T>(re.x + sg * im.y, re.y - sg * im.x);
+    }
+    a[0] = y0;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ cplx<T> tw2(const cplx<T> *twh, const cplx<T> *twl, int t, bool fwd) {
+  cplx<T> w = cmul<T>(twh[t >> 6], twl[t & 63]);
+  if (!fwd) w.y = -w.y;
+  return w;
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void stage2(const cplx<T> *__restrict__ src, cplx<T> *__restrict__ dst,
+                                       int n, int lnl, int Ns, uint32_t mul, int tstep,
+                                       const cplx<T> *twh, const cplx<T> *twl, bool fwd) {
+  const int nR = n / R;
+  const int B = nR << lnl;
+  const int lmask = (1 << lnl) - 1;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const int l = b & lmask, j = b >> lnl;
+    const int g = (Ns == 1) ? j : int(__umulhi(uint32_t(j), mul));
+    const int k = j - g * Ns;
+    cplx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      cplx<T> x = src[((j + r * nR) << lnl) + l];
+      if (r > 0 && k > 0) x = cmul<T>(x, tw2<T>(twh, twl, k * r * tstep, fwd));
+      v[r] = x;
+    }
+    dft_const<T, R>(v, fwd);
+    const int ob = ((g * Ns * R + k) << lnl) + l;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[ob + ((r * Ns) << lnl)] = v[r];
+  }
+  __syncthreads();
+}
+
+template <typename T> constexpr int fft2_max_threads() { return sizeof(T) == 4 ? 1024 : 512; }
+constexpr int FFT2_MAXE = 12;   // elements per CTA <= FFT2_MAXE * threads
+
+template <typename T>
+__global__ void __launch_bounds__(fft2_max_threads<T>())
+    k_fft_lines2(cplx<T> *__restrict__ grid, LineSpec ls, StageInfo si, const cplx<T> *__restrict__ tw,
+                 UniSpec u, bool fwd) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int n = ls.n;
+  const int lnl = ls.nl;   // log2 of lines per CTA
+  const int nl = 1 << lnl;
+  const int nh = (n + 63) / 64 + 1;
+  cplx<T> *s = reinterpret_cast<cplx<T> *>(smraw);
+  cplx<T> *s2 = s + (n << lnl);
+  cplx<T> *twl = s2 + (n << lnl);
+  cplx<T> *twh = twl + 64;
+  int64_t *lbase = reinterpret_cast<int64_t *>(twh + nh);
+  int64_t *luoff = lbase + nl;
+  double *lfac = reinterpret_cast<double *>(luoff + nl);
+  __shared__ int stR[24], stNs[24], stT[24];
+  __shared__ uint32_t stM[24];
+  if (threadIdx.x < 24) {
+    stR[threadIdx.x] = si.R[threadIdx.x];
+    stNs[threadIdx.x] = si.Ns[threadIdx.x];
+    stT[threadIdx.x] = si.tstep[threadIdx.x];
+    stM[threadIdx.x] = si.mul[threadIdx.x];
+  }
+  const int L0 = blockIdx.x << lnl;
+  const int nloc = min(nl, ls.nlines - L0);
+  const int N = sel3(u.N, ls.ax);
+  const int lo = (N + 1) / 2, hi0 = n - N / 2;
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) twl[i] = (i < n) ? tw[i] : mkc<T>(T(1), T(0));
+  for (int i = threadIdx.x; i < nh; i += blockDim.x) twh[i] = (64 * i < n) ? tw[64 * i] : mkc<T>(T(1), T(0));
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+    int ia = 0, ib = 0;
+    lbase[l] = (l < nloc) ? line_base(ls, u.N, u.n, L0 + l, ia, ib) : 0;
+    double fac = 1.0;
+    int64_t uoff = 0;
+    if (l < nloc && (ls.in_mode == IO_UNI || ls.out_mode == IO_UNI)) line_uni(ls, u, ia, ib, fac, uoff);
+    lfac[l] = fac;
+    luoff[l] = uoff;
+  }
+  __syncthreads();
+  const cplx<T> *uin = static_cast<const cplx<T> *>(u.ptr);
+  const int64_t ust = sel3(u.stride, ls.ax);
+  const double *cfa = sel3(u.corfac, ls.ax);
+  auto load_elem = [&](int l, int k) -> cplx<T> {
+    cplx<T> v = mkc<T>(T(0), T(0));
+    if (l >= nloc) return v;
+    if (ls.in_mode == IO_FULL) return grid[lbase[l] + int64_t(k) * ls.es];
+    if (k >= lo && k < hi0) return v;
+    if (ls.in_mode == IO_KEPT) return grid[lbase[l] + int64_t(k) * ls.es];
+    int iu, icf;
+    grid_to_uni(k, N, n, u.fft_order, iu, icf);
+    cplx<T> x = uin[luoff[l] + int64_t(iu) * ust];
+    T f = T(lfac[l] * cfa[icf]);
+    return mkc<T>(x.x * f, x.y * f);
+  };
+  auto store_elem = [&](int l, int k, cplx<T> x) {
+    if (l >= nloc) return;
+    if (ls.out_mode == IO_FULL) {
+      grid[lbase[l] + int64_t(k) * ls.es] = x;
+      return;
+    }
+    if (k >= lo && k < hi0) return;
+    if (ls.out_mode == IO_KEPT) {
+      grid[lbase[l] + int64_t(k) * ls.es] = x;
+      return;
+    }
+    int iu, icf;
+    grid_to_uni(k, N, n, u.fft_order, iu, icf);
+    T f = T(lfac[l] * cfa[icf]);
+    static_cast<cplx<T> *>(u.ptr)[luoff[l] + int64_t(iu) * ust] = mkc<T>(x.x * f, x.y * f);
+  };
+  if (ls.es == 1) {
+    for (int l = 0; l < nl; ++l)
+      for (int k = threadIdx.x; k < n; k += blockDim.x) s[(k << lnl) + l] = load_elem(l, k);
+  } else {
+    const int tot = n << lnl;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x)
+      s[idx] = load_elem(idx & (nl - 1), idx >> lnl);
+  }
+  __syncthreads();
+  cplx<T> *src = s, *dst = s2;
+  for (int f = 0; f < si.nst; ++f) {
+    const int R = stR[f], Ns = stNs[f], ts = stT[f];
+    const uint32_t mul = stM[f];
+    switch (R) {
+      case 2: stage2<T, 2>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      case 3: stage2<T, 3>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      case 4: stage2<T, 4>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      case 5: stage2<T, 5>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      case 7: stage2<T, 7>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      case 8: stage2<T, 8>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      case 11: stage2<T, 11>(src, dst, n, lnl, Ns, mul, ts, twh, twl, fwd); break;
+      default: break;
+    }
+    cplx<T> *t = src;
+    src = dst;
+    dst = t;
+  }
+  s = src;
+  if (ls.es == 1) {
+    for (int l = 0; l < nl; ++l)
+      for (int k = threadIdx.x; k < n; k += blockDim.x) store_elem(l, k, s[(k << lnl) + l]);
+  } else {
+    const int tot = n << lnl;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x)
+      store_elem(idx & (nl - 1), idx >> lnl, s[idx]);
+  }
+}
+
+static StageInfo make_stages(const FFTAxisPlan &p) {
+  StageInfo si;
+  si.nst = p.nfac;
+  int Ns = 1;
+  for (int f = 0; f < p.nfac; ++f) {
+    si.R[f] = p.fac[f];
+    si.Ns[f] = Ns;
+    si.tstep[f] = p.n / (Ns * p.fac[f]);
+    si.mul[f] = Ns == 1 ? 0u : uint32_t(((uint64_t(1) << 32) + uint64_t(Ns) - 1) / uint64_t(Ns));
+    Ns *= p.fac[f];
+  }
+  return si;
+}
+
+// v2 launch if the line fits its register / shared-memory budget; false otherwise
+template <typename T>
+static bool run_lines2(cplx<T> *grid, LineSpec ls, const FFTAxisPlan &p, const UniSpec &u,
+                       bool fwd, cudaStream_t st) {
+  const int n = ls.n;
+  const int maxnt = fft2_max_threads<T>();
+  const size_t maxsm = 200 * 1024;
+  if (n > FFT2_MAXE * maxnt || n >= (1 << 16)) return false;
+  int lnl = 0;
+  const int want = (ls.es == 1) ? 2048 : 8192;   // elements per CTA to aim for
+  if (size_t(2 * n) * sizeof(cplx<T>) > maxsm - 8192) return false;
+  while ((n << (lnl + 1)) <= want && (1 << (lnl + 1)) <= 16 && (1 << lnl) < ls.nlines &&
+         size_t(n << (lnl + 2)) * sizeof(cplx<T>) <= maxsm / 2 &&
+         (n << (lnl + 1)) <= FFT2_MAXE * maxnt)
+    ++lnl;
+  const int total = n << lnl;
+  int nt = 32 * ((total + FFT2_MAXE - 1) / FFT2_MAXE / 32 + 1);
+  nt = std::max(64, std::min(maxnt, nt));
+  if (total > FFT2_MAXE * nt) return false;
+  const int nh = (n + 63) / 64 + 1;
+  size_t sm = size_t(2 * total + 64 + nh) * sizeof(cplx<T>) + size_t(1 << lnl) * 24;
+  if (sm > maxsm) return false;
+  ls.nl = lnl;
+  StageInfo si = make_stages(p);
+  DN_CUDA(cudaFuncSetAttribute(k_fft_lines2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  unsigned nb = unsigned((ls.nlines + (1 << lnl) - 1) >> lnl);
+  k_fft_lines2<T><<<nb, nt, sm, st>>>(grid, ls, si, static_cast<const cplx<T> *>(p.tw), u, fwd);
+  DN_LAUNCHED();
+  return true;
 }
 
 template <typename T>
 static void run_lines(cplx<T> *grid, LineSpec ls, const FFTAxisPlan &p, const UniSpec &u,
                       bool fwd, cudaStream_t st) {
   if (ls.nlines <= 0) return;
+  if (run_lines2<T>(grid, ls, p, u, fwd, st)) return;
   const int n = ls.n;
   const size_t maxsm = 200 * 1024;
   int nl;
