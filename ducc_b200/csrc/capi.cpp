@@ -79,6 +79,36 @@ struct DevBuf {
   template <typename X> X *as() const { return static_cast<X *>(p); }
 };
 
+// ---------------------------------------------------------------- device error word
+// Kernels with bounded waits set this word instead of hanging; it is read back
+// after such a kernel (outside stream capture) and turned into ST_TIMEOUT.
+static int *device_error_word() {
+  static thread_local int dev_cached = -1;
+  static int *words[64] = {nullptr};
+  int dev = 0;
+  DN_CUDA(cudaGetDevice(&dev));
+  DN_REQUIRE(dev >= 0 && dev < 64, ST_INTERNAL, "device index out of range");
+  if (!words[dev]) {
+    DN_CUDA(cudaMalloc(&words[dev], sizeof(int)));
+    DN_CUDA(cudaMemset(words[dev], 0, sizeof(int)));
+  }
+  dev_cached = dev;
+  return words[dev];
+}
+
+static void check_device_error(int *word, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  DN_CUDA(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return;
+  int h = 0;
+  DN_CUDA(cudaMemcpyAsync(&h, word, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DN_CUDA(cudaStreamSynchronize(st));
+  if (h != 0) {
+    DN_CUDA(cudaMemsetAsync(word, 0, sizeof(int), st));
+    throw Error(ST_TIMEOUT, "a bounded device-side wait gave up (tensor-core spreader)");
+  }
+}
+
 // ---------------------------------------------------------------- stage timers
 // CUDA-event stage profile printed under verbosity>0 (the counterpart of DUCC's
 // TimerHierarchy report, src/ducc0/infra/timers.h:69-266).
@@ -226,6 +256,7 @@ struct Setup {
   KernelPoly<double> kpd;
   std::vector<double> corfac[3];
   std::vector<int> factors[3];
+  int spreader = DNUFFT_SPREAD_AUTO;
   int keybits = 1;
   int tile_shift = 0;
   uint64_t max_tiles = 0;
@@ -264,6 +295,9 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
   Setup s;
   s.calc_f64 = calc_f64;
   s.coord_f64 = coord_f64;
+  DN_REQUIRE(o.spreader >= DNUFFT_SPREAD_AUTO && o.spreader <= DNUFFT_SPREAD_TC, ST_BADARG,
+             "unknown spreader");
+  s.spreader = o.spreader;
   s.npoints = uint32_t(npoints);
   s.epsilon = epsilon;
   Geometry &g = s.g;
@@ -336,6 +370,9 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
   }
   DN_REQUIRE(maxkey < (uint64_t(1) << 32), ST_UNSUPPORTED, "tile key space too large");
   s.keybits = std::max(1, bitlen64(maxkey));
+  if (s.spreader == DNUFFT_SPREAD_TC)
+    DN_REQUIRE(spread_tc_supported(g, calc_f64), ST_UNSUPPORTED,
+               "tensor-core spreader: 2D single precision (complex64) with support <= 8 only");
   auto coeff = kernel_coeffs(g.W, s.beta, s.e0);
   fill_poly(s, coeff);
   for (int d = 0; d < ndim; ++d)
@@ -445,7 +482,23 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
   tm.mark("spreading");
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
-  launch_spread<T>(pts, cl, s.g, kp, points.data, points.stride[0], 0, grid.p, 0, 1, st);
+  bool use_tc = false;
+  if constexpr (sizeof(T) == 4) {
+    bool ok = spread_tc_supported(s.g, s.calc_f64);
+    DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC || ok, ST_UNSUPPORTED,
+               "tensor-core spreader: 2D single precision with support <= 8 only");
+    use_tc = ok && s.spreader == DNUFFT_SPREAD_TC;
+  } else {
+    DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
+               "tensor-core spreader: single precision (complex64) only");
+  }
+  if (use_tc) {
+    int *err = device_error_word();
+    launch_spread_tc(pts, cl, s.g, s.kpf, points.data, points.stride[0], grid.p, err, st);
+    check_device_error(err, st);
+  } else {
+    launch_spread<T>(pts, cl, s.g, kp, points.data, points.stride[0], 0, grid.p, 0, 1, st);
+  }
   tm.mark("FFT + correction");
   fft_nu2u_tail<T>(grid.p, s.g, dc.ax, forward, dc.cf, fft_order, out.data, out.stride, st);
   tm.mark("end");

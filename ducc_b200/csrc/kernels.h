@@ -51,6 +51,12 @@ void launch_interp(const PointsDesc &pts, const ChunkList &cl, const Geometry &g
                    const KernelPoly<T> &kp, const void *grid, int64_t gtrans,
                    void *out, int64_t os, int64_t otrans, int ntrans, cudaStream_t st);
 
+// ---- split-precision tensor-core spreader (spread_tc.cu): 2D, complex64
+bool spread_tc_supported(const Geometry &g, bool calc_f64);
+void launch_spread_tc(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                      const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
+                      int *err, cudaStream_t st);
+
 // ---- FFT and correction (fft.cu)
 struct FFTAxisPlan {
   int n;

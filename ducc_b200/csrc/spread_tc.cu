@@ -1,0 +1,479 @@
+// Split-precision tensor-core spreader (type 1, 2D, complex64 data).
+//
+// For one tile of the oversampled grid the spread is a dense contraction
+//     subgrid[u][v] = sum_p ku_p[u - ou_p] * c_p * kv_p[v - ov_p]
+//                   = (Ku^T diag(c) Kv)[u][v]
+// over the points p of the tile.  It runs on the 5th-generation tensor cores
+// (tcgen05.mma, kind::f16, FP32 accumulation in tensor memory) with every
+// operand split into FP16 hi + lo parts, x = hi + lo, so that
+//     A.B ~= Ahi.Bhi + Ahi.Blo + Alo.Bhi
+// keeps ~22 significant bits.  One MMA does all three products and both
+// complex parts at once:
+//     A (M=128 x K=16 points) rows = [Re(c)ku hi | Im(c)ku hi | Re(c)ku lo | Im(c)ku lo] x 32
+//     B (K=16 x N=48)         cols = [kv hi | kv lo] x 24
+//     D (128 x 48, FP32, TMEM):  Re = D[0:24, 0:24] + D[0:24, 24:48] + D[64:88, 0:24]
+//                                Im = D[32:56, 0:24] + D[32:56, 24:48] + D[96:120, 0:24]
+// (the Alo.Blo block is computed and ignored).  A 32x32 tile (DUCC's 2D
+// single-precision tile) is split into four 16x16 quadrants, each with its own
+// accumulator, so a point's 8 taps always fit the 24 rows/columns of a quadrant.
+// Operands are built per point in registers (Horner weights, FP16 hi/lo split,
+// funnel-shift placement at the point's row offset) and stored MN-major into
+// shared memory; two operand stages let the CUDA cores build one round of
+// K-blocks while the tensor cores consume the previous one.  Results are
+// combined in shared memory and added to the grid with vector atomics.
+//
+// Values are scaled by a power of two per chunk (largest |Re|,|Im| -> 2^14)
+// so FP16 neither overflows nor loses the small kernel tails to underflow; the
+// scale is removed exactly in the epilogue.
+#include <cuda_fp16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "spread_impl.cuh"
+
+namespace dnufft {
+
+namespace tc {
+
+constexpr int THREADS = 128;       // one warpgroup: TMEM lanes 0..127
+constexpr int KB = 16;             // points per MMA (K)
+constexpr int ROUND = 8;           // K-blocks per round (one operand stage)
+constexpr int A_BYTES = 4096;      // 128 x 16 fp16, MN-major, no swizzle
+constexpr int B_BYTES = 1536;      // 48 x 16 fp16, MN-major, no swizzle
+constexpr int A_LBO = 2048;        // between the two K-groups of 8 points
+constexpr int B_LBO = 768;
+constexpr int SBO = 128;           // between consecutive 8-element MN chunks
+constexpr int M = 128, N = 48;
+constexpr int TMEM_COLS = 256;     // quadrant q accumulates at column 64*q
+constexpr int MAXCHUNK = 1024;
+constexpr int STAGE_BYTES = ROUND * (A_BYTES + B_BYTES);   // 45056
+// shared memory: 2 stages, then padding so that every operand descriptor
+// range stays inside the allocation whatever the hardware's reading order
+constexpr int OPER_BYTES = 2 * STAGE_BYTES + 32768;
+constexpr int LIST_BYTES = 4 * MAXCHUNK * 2;
+constexpr int SMEM_BYTES = OPER_BYTES + LIST_BYTES + 256;
+constexpr uint32_t SPIN_LIMIT = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr & 0x3FFFFu) >> 4);
+  d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+  d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+  d |= uint64_t(1) << 46;   // descriptor version for sm_100
+  return d;                 // base offset 0, relative LBO, no swizzle
+}
+
+// kind::f16 instruction descriptor: F32 accumulate, F16 A/B, both MN-major
+constexpr uint32_t IDESC = (1u << 4) | (0u << 7) | (0u << 10) | (1u << 15) | (1u << 16) |
+                           (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// bounded wait for the phase with the given parity; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t addr = smem_u32(bar);
+  for (uint32_t it = 0; it < SPIN_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_half2(float a, float b) {
+  __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<uint32_t *>(&h);
+}
+
+// x = hi + lo in FP16
+__device__ __forceinline__ void split(float x, float &hi, float &lo) {
+  hi = __half2float(__float2half_rn(x));
+  lo = x - hi;
+}
+
+// 8 halves (4 words) shifted up by r halves (0..7) across two 8-half chunks:
+// z[0..3] = low chunk, z[4..7] = high chunk
+__device__ __forceinline__ void place8(const uint32_t (&h)[4], int r, uint32_t (&z)[8]) {
+  const uint32_t bs = (r & 1) ? 16u : 0u;
+  uint32_t x[5];
+  x[0] = __funnelshift_l(0u, h[0], bs);
+  x[1] = __funnelshift_l(h[0], h[1], bs);
+  x[2] = __funnelshift_l(h[1], h[2], bs);
+  x[3] = __funnelshift_l(h[2], h[3], bs);
+  x[4] = __funnelshift_l(h[3], 0u, bs);
+  const int ws = r >> 1;
+  uint32_t y[8];
+  // shift by two words if ws&2
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    uint32_t a = (j < 5) ? x[j] : 0u;
+    uint32_t b = (j >= 2 && j - 2 < 5) ? x[j - 2] : 0u;
+    y[j] = (ws & 2) ? b : a;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    uint32_t b = (j >= 1) ? y[j - 1] : 0u;
+    z[j] = (ws & 1) ? b : y[j];
+  }
+}
+
+__device__ __forceinline__ void st_v4(uint32_t saddr, uint32_t a, uint32_t b, uint32_t c,
+                                      uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(saddr), "r"(a), "r"(b), "r"(c),
+               "r"(d)
+               : "memory");
+}
+
+}  // namespace tc
+
+template <typename Tc, int W>
+__global__ void __launch_bounds__(tc::THREADS, 1)
+    k_spread_tc(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<float> kp,
+                const float2 *__restrict__ values, int64_t vs, float2 *__restrict__ grid,
+                int *__restrict__ err) {
+  using namespace tc;
+  static_assert(W <= 8, "tensor-core spreader handles supports up to 8");
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ uint64_t bars[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_cnt[4];
+  __shared__ int s_blk[5];
+  __shared__ unsigned s_maxbits;
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const Chunk ch = chunks[blockIdx.x];
+  const int cnt = int(ch.count);
+  int b0[2];
+  {
+    int ntv = int(g.ntiles[1]);
+    b0[0] = ((int(ch.tile) / ntv) << g.log2tile) - g.nsafe;
+    b0[1] = ((int(ch.tile) % ntv) << g.log2tile) - g.nsafe;
+  }
+  unsigned char *oper = tc_smem;
+  uint16_t *lists = reinterpret_cast<uint16_t *>(tc_smem + OPER_BYTES);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(&s_tmem)), "r"(uint32_t(TMEM_COLS)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_maxbits = 0;
+    s_fail = 0;
+  }
+  if (tid < 4) s_cnt[tid] = 0;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  // ---- 1. bucket the chunk's points into quadrants, find max |Re|,|Im|
+  for (int i = tid; i < cnt; i += THREADS) {
+    uint32_t ip = ch.start + uint32_t(i);
+    Tc x[2];
+    uint32_t j = load_point<Tc, 2>(pts, ip, x);
+    int ou, ov;
+    double fr;
+    fold<Tc>(x[0], g.coordfct[0], int(g.nover[0]), g.shift[0], g.maxi0[0], ou, fr);
+    fold<Tc>(x[1], g.coordfct[1], int(g.nover[1]), g.shift[1], g.maxi0[1], ov, fr);
+    ou -= b0[0];
+    ov -= b0[1];
+    int q = ((ou >= 16) ? 2 : 0) + ((ov >= 16) ? 1 : 0);
+    int pos = atomicAdd(&s_cnt[q], 1);
+    lists[q * MAXCHUNK + pos] = uint16_t(i);
+    float2 v = values[int64_t(j) * vs];
+    float m = fmaxf(fabsf(v.x), fabsf(v.y));
+    atomicMax(&s_maxbits, __float_as_uint(m));
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int q = 0; q < 4; ++q) {
+      s_blk[q] = acc;
+      acc += (s_cnt[q] + KB - 1) / KB;
+    }
+    s_blk[4] = acc;
+  }
+  __syncthreads();
+  const float maxc = __uint_as_float(s_maxbits);
+  const int NB = s_blk[4];
+  const int nrounds = (NB + ROUND - 1) / ROUND;
+  bool active = (maxc > 0.f) && isfinite(maxc) && NB > 0;
+  // power-of-two scales: A entries below 2^14, B (kernel values <= ~1) by 2^14
+  int e2 = 0;
+  if (active) frexpf(maxc, &e2);
+  const float sA = ldexpf(1.f, 14 - e2), sB = 16384.f;
+  const float unscale = ldexpf(1.f, e2 - 28);
+
+  // ---- 2. rounds of ROUND K-blocks: build operands, issue MMAs
+  for (int r = 0; active && r < nrounds; ++r) {
+    const int s = r & 1;
+    if (r >= 2) {
+      if (!mbar_wait(&bars[s], uint32_t(((r - 2) >> 1) & 1))) {
+        atomicExch(err, 1);
+        s_fail = 1;
+      }
+      __syncthreads();
+      if (s_fail) {
+        active = false;
+        break;
+      }
+    }
+    unsigned char *stA = oper + s * STAGE_BYTES;
+    unsigned char *stB = stA + ROUND * A_BYTES;
+    const int kbl = tid / KB, e = tid % KB;
+    const int kb = r * ROUND + kbl;
+    if (kb < NB) {
+      int q = 0;
+#pragma unroll
+      for (int qq = 1; qq < 4; ++qq)
+        if (kb >= s_blk[qq]) q = qq;
+      const int slot = (kb - s_blk[q]) * KB + e;
+      uint32_t ah[4][4], bh[2][4];   // [part][word]
+      int ou = 0, ov = 0;
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) ah[p][w] = 0u;
+#pragma unroll
+      for (int p = 0; p < 2; ++p)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) bh[p][w] = 0u;
+      if (slot < s_cnt[q]) {
+        const int i = lists[q * MAXCHUNK + slot];
+        Tc x[2];
+        uint32_t j = load_point<Tc, 2>(pts, ch.start + uint32_t(i), x);
+        float2 v = values[int64_t(j) * vs];
+        double fu, fv;
+        fold<Tc>(x[0], g.coordfct[0], int(g.nover[0]), g.shift[0], g.maxi0[0], ou, fu);
+        fold<Tc>(x[1], g.coordfct[1], int(g.nover[1]), g.shift[1], g.maxi0[1], ov, fv);
+        ou -= b0[0] + ((q & 2) ? 16 : 0);
+        ov -= b0[1] + ((q & 1) ? 16 : 0);
+        float ku[W], kv[W];
+        kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fu), ku);
+        kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fv), kv);
+        const float vr = v.x * sA, vi = v.y * sA;
+        float rh[8], rl[8], ih[8], il[8], kh[8], kl[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+          if (a < W) {
+            split(ku[a] * vr, rh[a], rl[a]);
+            split(ku[a] * vi, ih[a], il[a]);
+            split(kv[a] * sB, kh[a], kl[a]);
+          } else {
+            rh[a] = rl[a] = ih[a] = il[a] = kh[a] = kl[a] = 0.f;
+          }
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          ah[0][w] = pack_half2(rh[2 * w], rh[2 * w + 1]);
+          ah[1][w] = pack_half2(ih[2 * w], ih[2 * w + 1]);
+          ah[2][w] = pack_half2(rl[2 * w], rl[2 * w + 1]);
+          ah[3][w] = pack_half2(il[2 * w], il[2 * w + 1]);
+          bh[0][w] = pack_half2(kh[2 * w], kh[2 * w + 1]);
+          bh[1][w] = pack_half2(kl[2 * w], kl[2 * w + 1]);
+        }
+      }
+      // A column of point e of K-block kbl: part p rows p*32 + ou + a
+      const uint32_t abase = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO;
+      const int ca = ou >> 3;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        uint32_t z[8];
+        place8(ah[p], ou & 7, z);
+        const uint32_t pb = abase + uint32_t(p * 4) * SBO;
+        // chunks ca, ca+1 carry data; the other two of the part are zero
+        tc::st_v4(pb + uint32_t(ca) * SBO, z[0], z[1], z[2], z[3]);
+        tc::st_v4(pb + uint32_t(ca + 1) * SBO, z[4], z[5], z[6], z[7]);
+        tc::st_v4(pb + uint32_t(ca == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
+        tc::st_v4(pb + 3u * SBO, 0u, 0u, 0u, 0u);
+      }
+      // B row of point e: part p columns p*24 + ov + b
+      const uint32_t bbase = smem_u32(stB + kbl * B_BYTES) + (e & 7) * 16 + (e >> 3) * B_LBO;
+      const int cb = ov >> 3;
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        uint32_t z[8];
+        place8(bh[p], ov & 7, z);
+        const uint32_t pb = bbase + uint32_t(p * 3) * SBO;
+        tc::st_v4(pb + uint32_t(cb) * SBO, z[0], z[1], z[2], z[3]);
+        tc::st_v4(pb + uint32_t(cb + 1) * SBO, z[4], z[5], z[6], z[7]);
+        tc::st_v4(pb + uint32_t(cb == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
+      }
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::tc_fence_after();
+      for (int b = 0; b < ROUND; ++b) {
+        const int k = r * ROUND + b;
+        if (k >= NB) break;
+        int q = 0;
+        for (int qq = 1; qq < 4; ++qq)
+          if (k >= s_blk[qq]) q = qq;
+        const uint64_t ad = tc::make_desc(smem_u32(stA + b * A_BYTES), A_LBO, SBO);
+        const uint64_t bd = tc::make_desc(smem_u32(stB + b * B_BYTES), B_LBO, SBO);
+        tc::mma_f16(tmem + uint32_t(64 * q), ad, bd, k == s_blk[q] ? 0u : 1u);
+      }
+      tc::mma_commit(&bars[s]);
+    }
+  }
+
+  // ---- 3. wait for the last round's MMAs (a commit covers all earlier ones)
+  if (active) {
+    const int last = nrounds - 1;
+    if (!tc::mbar_wait(&bars[last & 1], uint32_t((last >> 1) & 1))) {
+      atomicExch(err, 1);
+      s_fail = 1;
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  if (s_fail) active = false;
+
+  // ---- 4. epilogue: combine hi/lo and re/im parts in shared memory, flush
+  const int S = 32 + W;   // tile buffer side (rows 0..32+W-2 used)
+  float2 *tile = reinterpret_cast<float2 *>(oper);   // operands are no longer read
+  if (active) {
+    for (int c = tid; c < S * S; c += THREADS) tile[c] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (int q = 0; q < 4; ++q) {
+      if (s_cnt[q] == 0) continue;
+      uint32_t d0[16], d1[16], d2[16];
+      const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(64 * q);
+      tmem_ld16(ta, d0);
+      tmem_ld16(ta + 16, d1);
+      tmem_ld16(ta + 32, d2);
+      tc::tmem_wait_ld();
+      const int u = lane;   // quadrant row
+      if (u < 24) {
+        const int tu = u + ((q & 2) ? 16 : 0);
+        const int tv0 = (q & 1) ? 16 : 0;
+        float *dst = reinterpret_cast<float *>(tile) + (warp & 1);   // .x for re, .y for im
+#pragma unroll
+        for (int v = 0; v < 24; ++v) {
+          float val;
+          // columns 0..23 = B hi, 24..47 = B lo
+          float c0 = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
+          if (warp < 2) {
+            float c1 = __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
+            val = c0 + c1;
+          } else {
+            val = c0;
+          }
+          if (tu < S && tv0 + v < S) atomicAdd(dst + 2 * (tu * S + tv0 + v), val * unscale);
+        }
+      }
+    }
+    __syncthreads();
+    const int nu = int(g.nover[0]), nv = int(g.nover[1]);
+    for (int c = tid; c < S * S; c += THREADS) {
+      float2 v = tile[c];
+      if (v.x == 0.f && v.y == 0.f) continue;
+      const int a = c / S, b = c - (c / S) * S;
+      const int64_t gi = int64_t(wrapi(b0[0] + a, nu)) * nv + wrapi(b0[1] + b, nv);
+      atomicAdd(grid + gi, v);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(uint32_t(tc::TMEM_COLS)));
+  }
+}
+
+bool spread_tc_supported(const Geometry &g, bool calc_f64) {
+  return !calc_f64 && g.ndim == 2 && g.log2tile == 5 && g.W <= 8;
+}
+
+void launch_spread_tc(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                      const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
+                      int *err, cudaStream_t st) {
+  if (cl.nchunks == 0) return;
+  DN_REQUIRE(spread_tc_supported(g, false), ST_UNSUPPORTED,
+             "tensor-core spreader: 2D single precision with support <= 8 only");
+#define DN_TC(TC, WW)                                                                          \
+  {                                                                                            \
+    auto kern = k_spread_tc<TC, WW>;                                                           \
+    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                                 tc::SMEM_BYTES));                                             \
+    kern<<<cl.nchunks, tc::THREADS, tc::SMEM_BYTES, st>>>(pts, cl.chunks, g, kp,               \
+                                                          static_cast<const float2 *>(values), \
+                                                          vs, static_cast<float2 *>(grid), err); \
+    DN_LAUNCHED();                                                                             \
+    return;                                                                                    \
+  }
+  if (pts.coord_f64) {
+    switch (g.W) {
+      case 4: DN_TC(double, 4) case 5: DN_TC(double, 5) case 6: DN_TC(double, 6)
+      case 7: DN_TC(double, 7) case 8: DN_TC(double, 8)
+    }
+  } else {
+    switch (g.W) {
+      case 4: DN_TC(float, 4) case 5: DN_TC(float, 5) case 6: DN_TC(float, 6)
+      case 7: DN_TC(float, 7) case 8: DN_TC(float, 8)
+    }
+  }
+#undef DN_TC
+  throw Error(ST_UNSUPPORTED, "tensor-core spreader: unsupported kernel support");
+}
+
+}  // namespace dnufft
