@@ -21,7 +21,7 @@ namespace dnufft {
 template <typename Tc, int NDIM>
 __global__ void k_fold_keys(const Tc *__restrict__ coord, int64_t cs0, int64_t cs1,
                             uint32_t npts, Geometry g, uint32_t *__restrict__ keys,
-                            uint32_t *__restrict__ idx) {
+                            uint32_t *__restrict__ idx, bool qbits) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npts) return;
   int t[NDIM];
@@ -38,6 +38,10 @@ __global__ void k_fold_keys(const Tc *__restrict__ coord, int64_t cs0, int64_t c
     key = uint32_t(t[0] >> g.log2tile);
   } else if constexpr (NDIM == 2) {
     key = uint32_t(t[0] >> g.log2tile) * uint32_t(g.ntiles[1]) + uint32_t(t[1] >> g.log2tile);
+    if (qbits) {
+      const int half = 1 << (g.log2tile - 1), m = (1 << g.log2tile) - 1;
+      key = (key << 2) | (((t[0] & m) >= half) ? 2u : 0u) | (((t[1] & m) >= half) ? 1u : 0u);
+    }
   } else {
     uint32_t ss = uint32_t(g.ssmall), ms = (1u << ss) - 1u;
     uint32_t a = uint32_t(t[0] >> g.lsq2), b = uint32_t(t[1] >> g.lsq2),
@@ -53,11 +57,12 @@ __global__ void k_fold_keys(const Tc *__restrict__ coord, int64_t cs0, int64_t c
 
 void launch_fold_keys(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
                       uint32_t npts, const Geometry &g, uint32_t *keys, uint32_t *idx,
-                      cudaStream_t st) {
+                      cudaStream_t st, bool quadrant_bits) {
   if (npts == 0) return;
   dim3 block(256), grid((npts + 255) / 256);
 #define FK(TC, ND) \
-  k_fold_keys<TC, ND><<<grid, block, 0, st>>>((const TC *)coord, cs0, cs1, npts, g, keys, idx)
+  k_fold_keys<TC, ND><<<grid, block, 0, st>>>((const TC *)coord, cs0, cs1, npts, g, keys, idx, \
+                                               quadrant_bits)
   if (coord_f64) {
     if (g.ndim == 1) FK(double, 1); else if (g.ndim == 2) FK(double, 2); else FK(double, 3);
   } else {
@@ -378,6 +383,27 @@ void launch_gather_coords(bool coord_f64, const void *coord, int64_t cs0, int64_
   else
     k_gather_coords<float><<<g, 256, 0, st>>>((const float *)coord, cs0, cs1, ndim, perm, n,
                                               (float *)out);
+  DN_LAUNCHED();
+}
+
+// inverse of the gather: out[perm[i]] = sorted[i]
+template <typename Tc>
+__global__ void k_scatter_coords(const Tc *__restrict__ sorted, int ndim,
+                                 const uint32_t *__restrict__ perm, uint32_t n, Tc *__restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t j = perm[i];
+  for (int d = 0; d < ndim; ++d) out[uint64_t(j) * ndim + d] = sorted[uint64_t(i) * ndim + d];
+}
+
+void launch_scatter_coords(bool coord_f64, const void *sorted, int ndim, const uint32_t *perm,
+                           uint32_t n, void *out, cudaStream_t st) {
+  if (n == 0) return;
+  unsigned g = (n + 255) / 256;
+  if (coord_f64)
+    k_scatter_coords<double><<<g, 256, 0, st>>>((const double *)sorted, ndim, perm, n, (double *)out);
+  else
+    k_scatter_coords<float><<<g, 256, 0, st>>>((const float *)sorted, ndim, perm, n, (float *)out);
   DN_LAUNCHED();
 }
 

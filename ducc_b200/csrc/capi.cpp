@@ -89,8 +89,9 @@ static int *device_error_word() {
   DN_CUDA(cudaGetDevice(&dev));
   DN_REQUIRE(dev >= 0 && dev < 64, ST_INTERNAL, "device index out of range");
   if (!words[dev]) {
-    DN_CUDA(cudaMalloc(&words[dev], sizeof(int)));
-    DN_CUDA(cudaMemset(words[dev], 0, sizeof(int)));
+    // word 0: error flag; word 1: scratch for the operand-scale reduction
+    DN_CUDA(cudaMalloc(&words[dev], 4 * sizeof(int)));
+    DN_CUDA(cudaMemset(words[dev], 0, 4 * sizeof(int)));
   }
   dev_cached = dev;
   return words[dev];
@@ -257,6 +258,7 @@ struct Setup {
   std::vector<double> corfac[3];
   std::vector<int> factors[3];
   int spreader = DNUFFT_SPREAD_AUTO;
+  bool qbits = false;   // sort key carries the 2D tile quadrant (tensor-core order)
   int keybits = 1;
   int tile_shift = 0;
   uint64_t max_tiles = 0;
@@ -368,6 +370,11 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
     s.tile_shift = 3 * g.ssmall;
     s.max_tiles = prod;
   }
+  if (s.spreader == DNUFFT_SPREAD_TC && spread_tc_supported(g, calc_f64)) {
+    s.qbits = true;
+    maxkey <<= 2;
+    s.tile_shift = 2;
+  }
   DN_REQUIRE(maxkey < (uint64_t(1) << 32), ST_UNSUPPORTED, "tile key space too large");
   s.keybits = std::max(1, bitlen64(maxkey));
   if (s.spreader == DNUFFT_SPREAD_TC)
@@ -436,7 +443,7 @@ static void build_index(const Setup &s, const View &coord, Index &ix, cudaStream
   ix.perm = DevBuf(size_t(M) * 4, st);
   ix.keys = DevBuf(size_t(M) * 4, st);
   launch_fold_keys(s.coord_f64, coord.data, coord.stride[0], coord.stride[1], M, s.g,
-                   ix.keys.as<uint32_t>(), ix.perm.as<uint32_t>(), st);
+                   ix.keys.as<uint32_t>(), ix.perm.as<uint32_t>(), st, s.qbits);
   {
     DevBuf ws(radix_workspace_bytes(M, s.keybits), st);
     radix_sort_pairs(ix.keys.as<uint32_t>(), ix.perm.as<uint32_t>(), M, s.keybits, ws.p, st);
@@ -471,8 +478,9 @@ static void report_sizes(const Setup &s, bool gridding) {
 // ---------------------------------------------------------------- transforms
 template <typename T>
 static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
-                          const ChunkList &cl, const View &points, const View &out, bool forward,
-                          bool fft_order, StageTimer &tm, cudaStream_t st, DevBuf *ws = nullptr) {
+                          const ChunkList &cl, const uint32_t *skeys, const View &points,
+                          const View &out, bool forward, bool fft_order, StageTimer &tm,
+                          cudaStream_t st, DevBuf *ws = nullptr) {
   size_t cells = grid_cells(s.g);
   tm.mark("zeroing grid");
   DevBuf local;
@@ -487,14 +495,15 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
     bool ok = spread_tc_supported(s.g, s.calc_f64);
     DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC || ok, ST_UNSUPPORTED,
                "tensor-core spreader: 2D single precision with support <= 8 only");
-    use_tc = ok && s.spreader == DNUFFT_SPREAD_TC;
+    use_tc = ok && s.qbits;
   } else {
     DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
                "tensor-core spreader: single precision (complex64) only");
   }
   if (use_tc) {
     int *err = device_error_word();
-    launch_spread_tc(pts, cl, s.g, s.kpf, points.data, points.stride[0], grid.p, err, st);
+    launch_spread_tc(pts, skeys, cl, s.g, s.kpf, points.data, points.stride[0], grid.p,
+                     reinterpret_cast<unsigned *>(err + 1), err, st);
     check_device_error(err, st);
   } else {
     launch_spread<T>(pts, cl, s.g, kp, points.data, points.stride[0], 0, grid.p, 0, 1, st);
@@ -577,9 +586,11 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
                  ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
   if (f64)
-    do_spread_fft<double>(s, dc, pts, cl, sp.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+    do_spread_fft<double>(s, dc, pts, cl, ix.keys.as<uint32_t>(), sp.dev, so.dev, forward != 0,
+                          o.fft_order != 0, tm, st);
   else
-    do_spread_fft<float>(s, dc, pts, cl, sp.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+    do_spread_fft<float>(s, dc, pts, cl, ix.keys.as<uint32_t>(), sp.dev, so.dev, forward != 0,
+                         o.fft_order != 0, tm, st);
   tm.report("nu2u");
   so.finish();
 }
@@ -656,8 +667,9 @@ static void plan_create_impl(int nu2u, const dnufft_array *coord_, const int64_t
     p->sorted_coord = DevBuf(size_t(p->s.npoints) * ndim * (f64 ? 8 : 4), st);
     launch_gather_coords(f64, sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], ndim,
                          p->ix.perm.as<uint32_t>(), p->s.npoints, p->sorted_coord.p, st);
-    // the plan keeps only the sorted copy; release the keys
-    p->ix.keys.release();
+    // the plan keeps the sorted coordinates; the sorted keys only where the
+    // tensor-core spreader reads the quadrant bits from them
+    if (!p->s.qbits) p->ix.keys.release();
   }
   DN_CUDA(cudaStreamSynchronize(st));
   *out = p.release();
@@ -699,8 +711,9 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
   ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
   bool fo = p->o.fft_order != 0;
   if (type1) {
-    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
-    else do_spread_fft<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
+    const uint32_t *sk = p->ix.keys.as<uint32_t>();
+    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
+    else do_spread_fft<float>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
     tm.report("nu2u (planned)");
   } else {
     if (f64) do_fft_interp<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
@@ -823,7 +836,31 @@ int dnufft_plan_get_permutation(const dnufft_plan *p, uint32_t *out, void *strea
     DN_REQUIRE(p && out, dnufft::ST_BADARG, "null argument");
     if (p->s.npoints == 0) return DNUFFT_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    DN_CUDA(cudaMemcpyAsync(out, p->ix.perm.p, size_t(p->s.npoints) * 4, cudaMemcpyDefault, st));
+    if (!p->s.qbits) {
+      DN_CUDA(cudaMemcpyAsync(out, p->ix.perm.p, size_t(p->s.npoints) * 4, cudaMemcpyDefault, st));
+    } else {
+      // the plan processes points in (tile, quadrant) order; DUCC's permutation
+      // is the stable order by tile alone: re-sort the original coordinates
+      dnufft::Setup s2 = p->s;
+      s2.qbits = false;
+      s2.keybits -= 2;
+      s2.tile_shift = 0;
+      const uint32_t M = s2.npoints;
+      const int nd = s2.g.ndim;
+      // sorted coordinates in original order: scatter back through perm
+      dnufft::Index ix2;
+      ix2.perm = dnufft::DevBuf(size_t(M) * 4, st);
+      ix2.keys = dnufft::DevBuf(size_t(M) * 4, st);
+      dnufft::DevBuf orig(size_t(M) * nd * (s2.coord_f64 ? 8 : 4), st);
+      dnufft::launch_scatter_coords(s2.coord_f64, p->sorted_coord.p, nd, p->ix.perm.as<uint32_t>(),
+                                    M, orig.p, st);
+      dnufft::launch_fold_keys(s2.coord_f64, orig.p, nd, 1, M, s2.g, ix2.keys.as<uint32_t>(),
+                               ix2.perm.as<uint32_t>(), st, false);
+      dnufft::DevBuf ws(dnufft::radix_workspace_bytes(M, s2.keybits), st);
+      dnufft::radix_sort_pairs(ix2.keys.as<uint32_t>(), ix2.perm.as<uint32_t>(), M, s2.keybits,
+                               ws.p, st);
+      DN_CUDA(cudaMemcpyAsync(out, ix2.perm.p, size_t(M) * 4, cudaMemcpyDefault, st));
+    }
     DN_CUDA(cudaStreamSynchronize(st));
   })
 }

@@ -6,9 +6,11 @@
 namespace dnufft {
 
 // ---- binning / sorting (binsort.cu)
+// quadrant_bits: append the point's 16x16 quadrant within its 2D tile as two
+// extra low key bits (the tensor-core spreader's processing order)
 void launch_fold_keys(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
                       uint32_t npts, const Geometry &g, uint32_t *keys, uint32_t *idx,
-                      cudaStream_t st);
+                      cudaStream_t st, bool quadrant_bits = false);
 size_t scan_workspace_bytes(uint64_t n);
 void exclusive_scan(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *ws,
                     cudaStream_t st);
@@ -21,6 +23,9 @@ uint32_t build_chunks(const uint32_t *skeys, uint32_t n, int tile_shift, uint32_
 void launch_gather_coords(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
                           int ndim, const uint32_t *perm, uint32_t n, void *out,
                           cudaStream_t st);
+
+void launch_scatter_coords(bool coord_f64, const void *sorted, int ndim, const uint32_t *perm,
+                           uint32_t n, void *out, cudaStream_t st);
 
 // ---- spreading / interpolation (spread_*.cu)
 struct PointsDesc {
@@ -53,9 +58,10 @@ void launch_interp(const PointsDesc &pts, const ChunkList &cl, const Geometry &g
 
 // ---- split-precision tensor-core spreader (spread_tc.cu): 2D, complex64
 bool spread_tc_supported(const Geometry &g, bool calc_f64);
-void launch_spread_tc(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
-                      const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
-                      int *err, cudaStream_t st);
+// skeys: sorted tile keys carrying the tile quadrant in their two low bits
+void launch_spread_tc(const PointsDesc &pts, const uint32_t *skeys, const ChunkList &cl,
+                      const Geometry &g, const KernelPoly<float> &kp, const void *values,
+                      int64_t vs, void *grid, unsigned *absmax, int *err, cudaStream_t st);
 
 // ---- FFT and correction (fft.cu)
 struct FFTAxisPlan {

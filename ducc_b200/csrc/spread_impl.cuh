@@ -56,6 +56,13 @@ __device__ __forceinline__ uint32_t load_point(const PointsDesc &pts, uint32_t i
   return j;
 }
 
+// per-lane stride of the staged weights: odd, so that the 32 lanes writing
+// their own weights hit 32 different banks; even entry count keeps the
+// following complex values aligned
+template <int NDIM, int W> constexpr int stage_stride() {
+  return ((NDIM * W) % 2 == 0) ? NDIM * W + 1 : NDIM * W;
+}
+
 template <typename T> struct BufferLayout {
   // does the tile buffer live in shared memory for this (precision, ndim)?
   static constexpr bool smem(int ndim) { return !(ndim == 3 && sizeof(T) == 8); }
@@ -93,11 +100,12 @@ __global__ void __launch_bounds__(SP_THREADS)
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned char *stage = smraw + (SMEM ? size_t(ncell) * sizeof(cplx<T>) : 0);
-  T *stw = reinterpret_cast<T *>(stage) + warp * 32 * NDIM * W;
-  cplx<T> *stv = reinterpret_cast<cplx<T> *>(reinterpret_cast<T *>(stage) + SP_WARPS * 32 * NDIM * W) +
+  constexpr int WS = stage_stride<NDIM, W>();   // per-lane weight stride (odd)
+  T *stw = reinterpret_cast<T *>(stage) + warp * 32 * WS;
+  cplx<T> *stv = reinterpret_cast<cplx<T> *>(reinterpret_cast<T *>(stage) + SP_WARPS * 32 * WS) +
                  warp * 32;
   int *sto = reinterpret_cast<int *>(reinterpret_cast<cplx<T> *>(reinterpret_cast<T *>(stage) +
-                                                                 SP_WARPS * 32 * NDIM * W) +
+                                                                 SP_WARPS * 32 * WS) +
                                      SP_WARPS * 32) +
              warp * 32 * NDIM;
   if constexpr (SMEM) {
@@ -119,7 +127,7 @@ __global__ void __launch_bounds__(SP_THREADS)
         T w[W];
         kernel_weights<T, W>(kp, T(double(W - 1) - 2.0 * frac), w);
 #pragma unroll
-        for (int a = 0; a < W; ++a) stw[(lane * NDIM + d) * W + a] = w[a];
+        for (int a = 0; a < W; ++a) stw[lane * WS + d * W + a] = w[a];
         sto[lane * NDIM + d] = i0 - b0[d];
       }
       stv[lane] = v;
@@ -128,7 +136,7 @@ __global__ void __launch_bounds__(SP_THREADS)
     int np = min(32, int(end - base));
     for (int p = 0; p < np; ++p) {
       const cplx<T> v = stv[p];
-      const T *wp = stw + p * NDIM * W;
+      const T *wp = stw + p * WS;
       int o[NDIM];
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) o[d] = sto[p * NDIM + d];
@@ -324,7 +332,9 @@ size_t spread_smem_bytes(const Geometry &g) {
   size_t ncell = size_t(S);
   for (int d = 1; d < NDIM; ++d) ncell *= size_t(S);
   size_t buf = BufferLayout<T>::smem(NDIM) ? ncell * sizeof(cplx<T>) : 0;
-  size_t stage = size_t(SP_WARPS) * 32 * (NDIM * W * sizeof(T) + sizeof(cplx<T>) + NDIM * sizeof(int));
+  constexpr int WS = stage_stride<NDIM, W>();
+  size_t wbytes = (size_t(SP_WARPS) * 32 * WS * sizeof(T) + 15) / 16 * 16;
+  size_t stage = wbytes + size_t(SP_WARPS) * 32 * (sizeof(cplx<T>) + NDIM * sizeof(int));
   return buf + stage;
 }
 

@@ -47,11 +47,10 @@ constexpr int M = 128, N = 48;
 constexpr int TMEM_COLS = 256;     // quadrant q accumulates at column 64*q
 constexpr int MAXCHUNK = 1024;
 constexpr int STAGE_BYTES = ROUND * (A_BYTES + B_BYTES);   // 45056
-// shared memory: 2 stages, then padding so that every operand descriptor
-// range stays inside the allocation whatever the hardware's reading order
-constexpr int OPER_BYTES = 2 * STAGE_BYTES + 32768;
-constexpr int LIST_BYTES = 4 * MAXCHUNK * 2;
-constexpr int SMEM_BYTES = OPER_BYTES + LIST_BYTES + 256;
+// shared memory: 2 operand stages (each descriptor reads only its own 4 KB /
+// 1.5 KB block: 16 resp. 6 chunks of 128 B at SBO, 2 K-groups at LBO)
+constexpr int OPER_BYTES = 2 * STAGE_BYTES;
+constexpr int SMEM_BYTES = OPER_BYTES;
 constexpr uint32_t SPIN_LIMIT = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -177,32 +176,51 @@ __device__ __forceinline__ void st_v4(uint32_t saddr, uint32_t a, uint32_t b, ui
 
 }  // namespace tc
 
+// Largest |Re|, |Im| over the values (for the power-of-two operand scale).
+__global__ void k_absmax(const float2 *__restrict__ values, int64_t vs, uint32_t n,
+                         unsigned *__restrict__ out) {
+  float m = 0.f;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 v = values[int64_t(i) * vs];
+    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
+}
+
+// 256 threads: threads 0..127 build the A column (ku * c, 4 parts) and
+// threads 128..255 the B row (kv, 2 parts) of point slot (tid & 127); the
+// points of a chunk arrive ordered by tile quadrant (the sort key carries the
+// quadrant in its two low bits), so every K-block of 16 consecutive points
+// of one quadrant feeds one MMA into that quadrant's accumulator.
 template <typename Tc, int W>
-__global__ void __launch_bounds__(tc::THREADS, 1)
-    k_spread_tc(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<float> kp,
-                const float2 *__restrict__ values, int64_t vs, float2 *__restrict__ grid,
+__global__ void __launch_bounds__(2 * tc::THREADS, 2)
+    k_spread_tc(PointsDesc pts, const uint32_t *__restrict__ skeys, const Chunk *__restrict__ chunks,
+                Geometry g, KernelPoly<float> kp, const float2 *__restrict__ values, int64_t vs,
+                const unsigned *__restrict__ absmax, float2 *__restrict__ grid,
                 int *__restrict__ err) {
   using namespace tc;
   static_assert(W <= 8, "tensor-core spreader handles supports up to 8");
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   __shared__ uint64_t bars[2];
   __shared__ uint32_t s_tmem;
-  __shared__ int s_cnt[4];
-  __shared__ int s_blk[5];
-  __shared__ unsigned s_maxbits;
+  __shared__ int s_first[5], s_cnt[4], s_blk[5];
   __shared__ int s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool bside = tid >= THREADS;
+  const int slot = tid & (THREADS - 1);
   const Chunk ch = chunks[blockIdx.x];
   const int cnt = int(ch.count);
   int b0[2];
   {
-    int ntv = int(g.ntiles[1]);
-    b0[0] = ((int(ch.tile) / ntv) << g.log2tile) - g.nsafe;
-    b0[1] = ((int(ch.tile) % ntv) << g.log2tile) - g.nsafe;
+    const int ntv = int(g.ntiles[1]);
+    const int tile = int(ch.tile);
+    b0[0] = ((tile / ntv) << g.log2tile) - g.nsafe;
+    b0[1] = ((tile % ntv) << g.log2tile) - g.nsafe;
   }
   unsigned char *oper = tc_smem;
-  uint16_t *lists = reinterpret_cast<uint16_t *>(tc_smem + OPER_BYTES);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -213,54 +231,44 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_maxbits = 0;
     s_fail = 0;
   }
-  if (tid < 4) s_cnt[tid] = 0;
+  if (tid < 5) s_first[tid] = cnt;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
 
-  // ---- 1. bucket the chunk's points into quadrants, find max |Re|,|Im|
-  for (int i = tid; i < cnt; i += THREADS) {
-    uint32_t ip = ch.start + uint32_t(i);
-    Tc x[2];
-    uint32_t j = load_point<Tc, 2>(pts, ip, x);
-    int ou, ov;
-    double fr;
-    fold<Tc>(x[0], g.coordfct[0], int(g.nover[0]), g.shift[0], g.maxi0[0], ou, fr);
-    fold<Tc>(x[1], g.coordfct[1], int(g.nover[1]), g.shift[1], g.maxi0[1], ov, fr);
-    ou -= b0[0];
-    ov -= b0[1];
-    int q = ((ou >= 16) ? 2 : 0) + ((ov >= 16) ? 1 : 0);
-    int pos = atomicAdd(&s_cnt[q], 1);
-    lists[q * MAXCHUNK + pos] = uint16_t(i);
-    float2 v = values[int64_t(j) * vs];
-    float m = fmaxf(fabsf(v.x), fabsf(v.y));
-    atomicMax(&s_maxbits, __float_as_uint(m));
+  // ---- quadrant segments of the (quadrant-sorted) chunk
+  for (int i = tid; i < cnt; i += 2 * THREADS) {
+    const int q = int(skeys[ch.start + uint32_t(i)] & 3u);
+    if (i == 0 || int(skeys[ch.start + uint32_t(i) - 1] & 3u) != q) s_first[q] = i;
   }
   __syncthreads();
   if (tid == 0) {
+    // absent quadrants start where the next present one starts
+    for (int q = 3; q >= 0; --q)
+      if (s_first[q] == cnt) s_first[q] = s_first[q + 1];
     int acc = 0;
     for (int q = 0; q < 4; ++q) {
+      s_cnt[q] = s_first[q + 1] - s_first[q];
       s_blk[q] = acc;
       acc += (s_cnt[q] + KB - 1) / KB;
     }
     s_blk[4] = acc;
   }
   __syncthreads();
-  const float maxc = __uint_as_float(s_maxbits);
+  const float maxc = __uint_as_float(*absmax);
   const int NB = s_blk[4];
   const int nrounds = (NB + ROUND - 1) / ROUND;
   bool active = (maxc > 0.f) && isfinite(maxc) && NB > 0;
-  // power-of-two scales: A entries below 2^14, B (kernel values <= ~1) by 2^14
   int e2 = 0;
   if (active) frexpf(maxc, &e2);
   const float sA = ldexpf(1.f, 14 - e2), sB = 16384.f;
   const float unscale = ldexpf(1.f, e2 - 28);
+  const Tc *crd = static_cast<const Tc *>(pts.coord);
 
-  // ---- 2. rounds of ROUND K-blocks: build operands, issue MMAs
+  // ---- rounds of ROUND K-blocks
   for (int r = 0; active && r < nrounds; ++r) {
     const int s = r & 1;
     if (r >= 2) {
@@ -276,167 +284,171 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
     }
     unsigned char *stA = oper + s * STAGE_BYTES;
     unsigned char *stB = stA + ROUND * A_BYTES;
-    const int kbl = tid / KB, e = tid % KB;
+    const int kbl = slot / KB, e = slot % KB;
     const int kb = r * ROUND + kbl;
     if (kb < NB) {
       int q = 0;
 #pragma unroll
       for (int qq = 1; qq < 4; ++qq)
         if (kb >= s_blk[qq]) q = qq;
-      const int slot = (kb - s_blk[q]) * KB + e;
-      uint32_t ah[4][4], bh[2][4];   // [part][word]
-      int ou = 0, ov = 0;
+      const int j = (kb - s_blk[q]) * KB + e;
+      const bool valid = j < s_cnt[q];
+      uint32_t hw[4][4];
 #pragma unroll
       for (int p = 0; p < 4; ++p)
 #pragma unroll
-        for (int w = 0; w < 4; ++w) ah[p][w] = 0u;
+        for (int w = 0; w < 4; ++w) hw[p][w] = 0u;
+      int off = 0;
+      const int d = bside ? 1 : 0;
+      if (valid) {
+        const uint32_t i = ch.start + uint32_t(s_first[q] + j);
+        Tc x = pts.sorted ? crd[uint64_t(i) * 2 + d]
+                          : crd[int64_t(pts.perm[i]) * pts.cs0 + int64_t(d) * pts.cs1];
+        double fr;
+        fold<Tc>(x, g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], off, fr);
+        off -= b0[d] + ((bside ? (q & 1) : (q & 2)) ? 16 : 0);
+        float k[W];
+        kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fr), k);
+        float hv[8], lv[8];
+        if (!bside) {
+          const float2 v = values[int64_t(pts.perm[i]) * vs];
+          const float vr = v.x * sA, vi = v.y * sA;
+          float a[2][8];
 #pragma unroll
-      for (int p = 0; p < 2; ++p)
+          for (int t = 0; t < 8; ++t) {
+            a[0][t] = (t < W) ? k[t] * vr : 0.f;
+            a[1][t] = (t < W) ? k[t] * vi : 0.f;
+          }
 #pragma unroll
-        for (int w = 0; w < 4; ++w) bh[p][w] = 0u;
-      if (slot < s_cnt[q]) {
-        const int i = lists[q * MAXCHUNK + slot];
-        Tc x[2];
-        uint32_t j = load_point<Tc, 2>(pts, ch.start + uint32_t(i), x);
-        float2 v = values[int64_t(j) * vs];
-        double fu, fv;
-        fold<Tc>(x[0], g.coordfct[0], int(g.nover[0]), g.shift[0], g.maxi0[0], ou, fu);
-        fold<Tc>(x[1], g.coordfct[1], int(g.nover[1]), g.shift[1], g.maxi0[1], ov, fv);
-        ou -= b0[0] + ((q & 2) ? 16 : 0);
-        ov -= b0[1] + ((q & 1) ? 16 : 0);
-        float ku[W], kv[W];
-        kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fu), ku);
-        kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fv), kv);
-        const float vr = v.x * sA, vi = v.y * sA;
-        float rh[8], rl[8], ih[8], il[8], kh[8], kl[8];
+          for (int c = 0; c < 2; ++c) {
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          if (a < W) {
-            split(ku[a] * vr, rh[a], rl[a]);
-            split(ku[a] * vi, ih[a], il[a]);
-            split(kv[a] * sB, kh[a], kl[a]);
-          } else {
-            rh[a] = rl[a] = ih[a] = il[a] = kh[a] = kl[a] = 0.f;
+            for (int t = 0; t < 8; ++t) split(a[c][t], hv[t], lv[t]);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+              hw[c][w] = pack_half2(hv[2 * w], hv[2 * w + 1]);
+              hw[c + 2][w] = pack_half2(lv[2 * w], lv[2 * w + 1]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int t = 0; t < 8; ++t) split((t < W) ? k[t] * sB : 0.f, hv[t], lv[t]);
+#pragma unroll
+          for (int w = 0; w < 4; ++w) {
+            hw[0][w] = pack_half2(hv[2 * w], hv[2 * w + 1]);
+            hw[1][w] = pack_half2(lv[2 * w], lv[2 * w + 1]);
           }
         }
+      }
+      const int c0 = off >> 3;
+      if (!bside) {
+        // A column of point e: part p rows p*32 + off + a
+        const uint32_t base = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-          ah[0][w] = pack_half2(rh[2 * w], rh[2 * w + 1]);
-          ah[1][w] = pack_half2(ih[2 * w], ih[2 * w + 1]);
-          ah[2][w] = pack_half2(rl[2 * w], rl[2 * w + 1]);
-          ah[3][w] = pack_half2(il[2 * w], il[2 * w + 1]);
-          bh[0][w] = pack_half2(kh[2 * w], kh[2 * w + 1]);
-          bh[1][w] = pack_half2(kl[2 * w], kl[2 * w + 1]);
+        for (int p = 0; p < 4; ++p) {
+          uint32_t z[8];
+          place8(hw[p], off & 7, z);
+          const uint32_t pb = base + uint32_t(p * 4) * SBO;
+          st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
+          st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
+          st_v4(pb + uint32_t(c0 == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
+          st_v4(pb + 3u * SBO, 0u, 0u, 0u, 0u);
+        }
+      } else {
+        // B row of point e: part p columns p*24 + off + b
+        const uint32_t base = smem_u32(stB + kbl * B_BYTES) + (e & 7) * 16 + (e >> 3) * B_LBO;
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          uint32_t z[8];
+          place8(hw[p], off & 7, z);
+          const uint32_t pb = base + uint32_t(p * 3) * SBO;
+          st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
+          st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
+          st_v4(pb + uint32_t(c0 == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
         }
       }
-      // A column of point e of K-block kbl: part p rows p*32 + ou + a
-      const uint32_t abase = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO;
-      const int ca = ou >> 3;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        uint32_t z[8];
-        place8(ah[p], ou & 7, z);
-        const uint32_t pb = abase + uint32_t(p * 4) * SBO;
-        // chunks ca, ca+1 carry data; the other two of the part are zero
-        tc::st_v4(pb + uint32_t(ca) * SBO, z[0], z[1], z[2], z[3]);
-        tc::st_v4(pb + uint32_t(ca + 1) * SBO, z[4], z[5], z[6], z[7]);
-        tc::st_v4(pb + uint32_t(ca == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
-        tc::st_v4(pb + 3u * SBO, 0u, 0u, 0u, 0u);
-      }
-      // B row of point e: part p columns p*24 + ov + b
-      const uint32_t bbase = smem_u32(stB + kbl * B_BYTES) + (e & 7) * 16 + (e >> 3) * B_LBO;
-      const int cb = ov >> 3;
-#pragma unroll
-      for (int p = 0; p < 2; ++p) {
-        uint32_t z[8];
-        place8(bh[p], ov & 7, z);
-        const uint32_t pb = bbase + uint32_t(p * 3) * SBO;
-        tc::st_v4(pb + uint32_t(cb) * SBO, z[0], z[1], z[2], z[3]);
-        tc::st_v4(pb + uint32_t(cb + 1) * SBO, z[4], z[5], z[6], z[7]);
-        tc::st_v4(pb + uint32_t(cb == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
-      }
     }
-    tc::fence_proxy_async();
+    fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      tc::tc_fence_after();
-      for (int b = 0; b < ROUND; ++b) {
-        const int k = r * ROUND + b;
+      tc_fence_after();
+      for (int bb = 0; bb < ROUND; ++bb) {
+        const int k = r * ROUND + bb;
         if (k >= NB) break;
         int q = 0;
         for (int qq = 1; qq < 4; ++qq)
           if (k >= s_blk[qq]) q = qq;
-        const uint64_t ad = tc::make_desc(smem_u32(stA + b * A_BYTES), A_LBO, SBO);
-        const uint64_t bd = tc::make_desc(smem_u32(stB + b * B_BYTES), B_LBO, SBO);
-        tc::mma_f16(tmem + uint32_t(64 * q), ad, bd, k == s_blk[q] ? 0u : 1u);
+        const uint64_t ad = make_desc(smem_u32(stA + bb * A_BYTES), A_LBO, SBO);
+        const uint64_t bd = make_desc(smem_u32(stB + bb * B_BYTES), B_LBO, SBO);
+        mma_f16(tmem + uint32_t(64 * q), ad, bd, k == s_blk[q] ? 0u : 1u);
       }
-      tc::mma_commit(&bars[s]);
+      mma_commit(&bars[s]);
     }
   }
 
-  // ---- 3. wait for the last round's MMAs (a commit covers all earlier ones)
+  // ---- wait for the last round's MMAs (a commit covers all earlier ones)
   if (active) {
     const int last = nrounds - 1;
-    if (!tc::mbar_wait(&bars[last & 1], uint32_t((last >> 1) & 1))) {
+    if (!mbar_wait(&bars[last & 1], uint32_t((last >> 1) & 1))) {
       atomicExch(err, 1);
       s_fail = 1;
     }
   }
-  tc::tc_fence_before();
+  tc_fence_before();
   __syncthreads();
-  tc::tc_fence_after();
+  tc_fence_after();
   if (s_fail) active = false;
 
-  // ---- 4. epilogue: combine hi/lo and re/im parts in shared memory, flush
-  const int S = 32 + W;   // tile buffer side (rows 0..32+W-2 used)
-  float2 *tile = reinterpret_cast<float2 *>(oper);   // operands are no longer read
+  // ---- epilogue: combine hi/lo and re/im parts in shared memory, flush
+  //      (separate real / imaginary planes with an odd row pitch, so the
+  //      32 lanes of a warp, one row each, hit 32 different banks)
+  const int S = 32 + W;
+  const int P = S | 1;
+  float *tre = reinterpret_cast<float *>(oper);
+  float *tim = tre + S * P;
   if (active) {
-    for (int c = tid; c < S * S; c += THREADS) tile[c] = make_float2(0.f, 0.f);
+    for (int c = tid; c < 2 * S * P; c += 2 * THREADS) tre[c] = 0.f;
     __syncthreads();
-    for (int q = 0; q < 4; ++q) {
-      if (s_cnt[q] == 0) continue;
-      uint32_t d0[16], d1[16], d2[16];
-      const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(64 * q);
-      tmem_ld16(ta, d0);
-      tmem_ld16(ta + 16, d1);
-      tmem_ld16(ta + 32, d2);
-      tc::tmem_wait_ld();
-      const int u = lane;   // quadrant row
-      if (u < 24) {
-        const int tu = u + ((q & 2) ? 16 : 0);
-        const int tv0 = (q & 1) ? 16 : 0;
-        float *dst = reinterpret_cast<float *>(tile) + (warp & 1);   // .x for re, .y for im
+    if (warp < 4) {
+      for (int q = 0; q < 4; ++q) {
+        if (s_cnt[q] == 0) continue;
+        uint32_t d0[16], d1[16], d2[16];
+        const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(64 * q);
+        tmem_ld16(ta, d0);
+        tmem_ld16(ta + 16, d1);
+        tmem_ld16(ta + 32, d2);
+        tmem_wait_ld();
+        const int u = lane;
+        if (u < 24) {
+          const int tu = u + ((q & 2) ? 16 : 0);
+          const int tv0 = (q & 1) ? 16 : 0;
+          float *dst = ((warp & 1) ? tim : tre) + tu * P + tv0;
+          if (tu < S) {
 #pragma unroll
-        for (int v = 0; v < 24; ++v) {
-          float val;
-          // columns 0..23 = B hi, 24..47 = B lo
-          float c0 = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
-          if (warp < 2) {
-            float c1 = __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
-            val = c0 + c1;
-          } else {
-            val = c0;
+            for (int v = 0; v < 24; ++v) {
+              float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
+              if (warp < 2) val += __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
+              if (tv0 + v < S) atomicAdd(dst + v, val * unscale);
+            }
           }
-          if (tu < S && tv0 + v < S) atomicAdd(dst + 2 * (tu * S + tv0 + v), val * unscale);
         }
       }
     }
     __syncthreads();
     const int nu = int(g.nover[0]), nv = int(g.nover[1]);
-    for (int c = tid; c < S * S; c += THREADS) {
-      float2 v = tile[c];
+    for (int c = tid; c < S * S; c += 2 * THREADS) {
+      const int a = c / S, bcol = c - (c / S) * S;
+      const float2 v = make_float2(tre[a * P + bcol], tim[a * P + bcol]);
       if (v.x == 0.f && v.y == 0.f) continue;
-      const int a = c / S, b = c - (c / S) * S;
-      const int64_t gi = int64_t(wrapi(b0[0] + a, nu)) * nv + wrapi(b0[1] + b, nv);
+      const int64_t gi = int64_t(wrapi(b0[0] + a, nu)) * nv + wrapi(b0[1] + bcol, nv);
       atomicAdd(grid + gi, v);
     }
   }
-  tc::tc_fence_before();
+  tc_fence_before();
   __syncthreads();
   if (warp == 0) {
-    tc::tc_fence_after();
+    tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(uint32_t(tc::TMEM_COLS)));
+                 "r"(uint32_t(TMEM_COLS)));
   }
 }
 
@@ -444,22 +456,28 @@ bool spread_tc_supported(const Geometry &g, bool calc_f64) {
   return !calc_f64 && g.ndim == 2 && g.log2tile == 5 && g.W <= 8;
 }
 
-void launch_spread_tc(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
-                      const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
-                      int *err, cudaStream_t st) {
+void launch_spread_tc(const PointsDesc &pts, const uint32_t *skeys, const ChunkList &cl,
+                      const Geometry &g, const KernelPoly<float> &kp, const void *values,
+                      int64_t vs, void *grid, unsigned *absmax, int *err, cudaStream_t st) {
   if (cl.nchunks == 0) return;
   DN_REQUIRE(spread_tc_supported(g, false), ST_UNSUPPORTED,
              "tensor-core spreader: 2D single precision with support <= 8 only");
-#define DN_TC(TC, WW)                                                                          \
-  {                                                                                            \
-    auto kern = k_spread_tc<TC, WW>;                                                           \
-    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
-                                 tc::SMEM_BYTES));                                             \
-    kern<<<cl.nchunks, tc::THREADS, tc::SMEM_BYTES, st>>>(pts, cl.chunks, g, kp,               \
-                                                          static_cast<const float2 *>(values), \
-                                                          vs, static_cast<float2 *>(grid), err); \
-    DN_LAUNCHED();                                                                             \
-    return;                                                                                    \
+  DN_CUDA(cudaMemsetAsync(absmax, 0, sizeof(unsigned), st));
+  {
+    unsigned nb = unsigned(std::min<uint64_t>((uint64_t(pts.npts) + 255) / 256, 148 * 8));
+    k_absmax<<<nb, 256, 0, st>>>(static_cast<const float2 *>(values), vs, pts.npts, absmax);
+    DN_LAUNCHED();
+  }
+#define DN_TC(TC, WW)                                                                           \
+  {                                                                                             \
+    auto kern = k_spread_tc<TC, WW>;                                                            \
+    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
+                                 tc::SMEM_BYTES));                                              \
+    kern<<<cl.nchunks, 2 * tc::THREADS, tc::SMEM_BYTES, st>>>(                                  \
+        pts, skeys, cl.chunks, g, kp, static_cast<const float2 *>(values), vs, absmax,          \
+        static_cast<float2 *>(grid), err);                                                      \
+    DN_LAUNCHED();                                                                              \
+    return;                                                                                     \
   }
   if (pts.coord_f64) {
     switch (g.W) {

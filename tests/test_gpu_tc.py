@@ -75,3 +75,20 @@ def test_tc_rejects_double():
     with pytest.raises(RuntimeError, match="tensor-core"):
         nufft.nu2u(points=np.zeros(10, np.complex128), coord=coord, forward=True, epsilon=1e-5,
                    out=np.zeros((8, 8), np.complex128), spreader="tc")
+
+
+def test_tc_plan_permutation_is_duccs():
+    """A tensor-core plan processes points in (tile, quadrant) order but still
+    reports DUCC's stable tile permutation."""
+    import os
+    g = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "g2d_f32.npz")))
+    shape = tuple(int(s) for s in g["shape"])
+    for spreader in ("tc", "plain"):
+        p = nufft.plan(nu2u=True, coord=g["coord"], grid_shape=shape, epsilon=float(g["eps"]),
+                       nthreads=1, sigma_min=1.2, sigma_max=2.51,
+                       periodicity=list(g["periodicity"]), spreader=spreader)
+        assert np.array_equal(p.permutation(), g["perm1"])
+        r = p.nu2u(points=g["values"], forward=bool(g["forward"]))
+        assert O.l2error(r, g["nu2u"]) < float(g["eps"])
+        r2 = p.u2nu(grid=g["grid_in"], forward=bool(g["forward"]))
+        assert O.l2error(r2, g["u2nu"]) < float(g["eps"])
