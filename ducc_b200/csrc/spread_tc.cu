@@ -50,7 +50,8 @@ constexpr int STAGE_BYTES = ROUND * (A_BYTES + B_BYTES);   // 45056
 // shared memory: 2 operand stages (each descriptor reads only its own 4 KB /
 // 1.5 KB block: 16 resp. 6 chunks of 128 B at SBO, 2 K-groups at LBO)
 constexpr int OPER_BYTES = 2 * STAGE_BYTES;
-constexpr int SMEM_BYTES = OPER_BYTES;
+// + the FP32 combine planes (re, im), 2 x 40 x 41 floats
+constexpr int SMEM_BYTES = OPER_BYTES + 2 * 40 * 41 * 4;
 constexpr uint32_t SPIN_LIMIT = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -189,28 +190,67 @@ __global__ void k_absmax(const float2 *__restrict__ values, int64_t vs, uint32_t
   if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
 }
 
-// 256 threads: threads 0..127 build the A column (ku * c, 4 parts) and
-// threads 128..255 the B row (kv, 2 parts) of point slot (tid & 127); the
-// points of a chunk arrive ordered by tile quadrant (the sort key carries the
-// quadrant in its two low bits), so every K-block of 16 consecutive points
-// of one quadrant feeds one MMA into that quadrant's accumulator.
+// 384 threads in three builder groups of 128, one point slot each:
+//   group 0: A rows of Re(c)*ku (hi and lo parts), group 1: A rows of
+//   Im(c)*ku, group 2: the B row kv (hi and lo) - balanced work per thread.
+// The points of a chunk arrive ordered by tile quadrant (the sort key carries
+// the quadrant in its two low bits), so every K-block of 16 consecutive points
+// of one quadrant feeds one MMA into that quadrant's accumulator.  The
+// tensor-memory accumulators are added into FP32 shared-memory planes and
+// restarted once one of them has taken DRAIN_AT
+// MMAs, which bounds the length of each tensor-core accumulation chain (and
+// with it the accumulation error); typical chunks never need a drain.
+constexpr int TC_GROUPS = 3;
+constexpr int DRAIN_AT = 24;   // drain when an accumulator has taken this many MMAs
+
+template <int W>
+__device__ __forceinline__ void tc_drain(uint32_t tmem, int warp, int lane, const int *s_dirty,
+                                         float *tre, float *tim, int P, float unscale) {
+  constexpr int S = 32 + W;
+  for (int q = 0; q < 4; ++q) {
+    if (!s_dirty[q]) continue;
+    uint32_t d0[16], d1[16], d2[16];
+    const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(64 * q);
+    tc::tmem_ld16(ta, d0);
+    tc::tmem_ld16(ta + 16, d1);
+    tc::tmem_ld16(ta + 32, d2);
+    tc::tmem_wait_ld();
+    const int u = lane;
+    const int tu = u + ((q & 2) ? 16 : 0);
+    const int tv0 = (q & 1) ? 16 : 0;
+    if (u < 24 && tu < S) {
+      float *dst = ((warp & 1) ? tim : tre) + tu * P + tv0;
+#pragma unroll
+      for (int v = 0; v < 24; ++v) {
+        float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
+        if (warp < 2) val += __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
+        if (tv0 + v < S) atomicAdd(dst + v, val * unscale);
+      }
+    }
+  }
+}
+
 template <typename Tc, int W>
-__global__ void __launch_bounds__(2 * tc::THREADS, 2)
+__global__ void __launch_bounds__(TC_GROUPS * tc::THREADS, 2)
     k_spread_tc(PointsDesc pts, const uint32_t *__restrict__ skeys, const Chunk *__restrict__ chunks,
                 Geometry g, KernelPoly<float> kp, const float2 *__restrict__ values, int64_t vs,
                 const unsigned *__restrict__ absmax, float2 *__restrict__ grid,
                 int *__restrict__ err) {
   using namespace tc;
   static_assert(W <= 8, "tensor-core spreader handles supports up to 8");
+  constexpr int NT = TC_GROUPS * THREADS;
+  constexpr int S = 32 + W;   // tile buffer side (rows 0..32+W-2 used)
+  constexpr int P = S | 1;    // odd pitch of the FP32 planes (conflict-free rows)
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   __shared__ uint64_t bars[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_first[5], s_cnt[4], s_blk[5];
+  __shared__ int s_dirty[4];
   __shared__ int s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const bool bside = tid >= THREADS;
-  const int slot = tid & (THREADS - 1);
+  const int grp = tid / THREADS;            // 0: Re A, 1: Im A, 2: B
+  const int slot = tid - grp * THREADS;
   const Chunk ch = chunks[blockIdx.x];
   const int cnt = int(ch.count);
   int b0[2];
@@ -221,6 +261,8 @@ __global__ void __launch_bounds__(2 * tc::THREADS, 2)
     b0[1] = ((tile % ntv) << g.log2tile) - g.nsafe;
   }
   unsigned char *oper = tc_smem;
+  float *tre = reinterpret_cast<float *>(tc_smem + OPER_BYTES);
+  float *tim = tre + S * P;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -234,19 +276,20 @@ __global__ void __launch_bounds__(2 * tc::THREADS, 2)
     s_fail = 0;
   }
   if (tid < 5) s_first[tid] = cnt;
+  if (tid < 4) s_dirty[tid] = 0;
+  for (int c = tid; c < 2 * S * P; c += NT) tre[c] = 0.f;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
 
   // ---- quadrant segments of the (quadrant-sorted) chunk
-  for (int i = tid; i < cnt; i += 2 * THREADS) {
+  for (int i = tid; i < cnt; i += NT) {
     const int q = int(skeys[ch.start + uint32_t(i)] & 3u);
     if (i == 0 || int(skeys[ch.start + uint32_t(i) - 1] & 3u) != q) s_first[q] = i;
   }
   __syncthreads();
   if (tid == 0) {
-    // absent quadrants start where the next present one starts
     for (int q = 3; q >= 0; --q)
       if (s_first[q] == cnt) s_first[q] = s_first[q + 1];
     int acc = 0;
@@ -267,100 +310,99 @@ __global__ void __launch_bounds__(2 * tc::THREADS, 2)
   const float sA = ldexpf(1.f, 14 - e2), sB = 16384.f;
   const float unscale = ldexpf(1.f, e2 - 28);
   const Tc *crd = static_cast<const Tc *>(pts.coord);
+  unsigned fresh = 0xFu;   // quadrants whose next MMA overwrites (issuing thread only)
+  const int d = (grp == 2) ? 1 : 0;
+  const int kbl = slot / KB, e = slot % KB;
 
-  // ---- rounds of ROUND K-blocks
+  // point data of this thread's slot in round rr (loads only; used one round later)
+  auto fetch = [&](int rr, Tc &x, float &sc, int &q, bool &valid) {
+    const int kb = rr * ROUND + kbl;
+    q = 0;
+    valid = false;
+    x = Tc(0);
+    sc = 0.f;
+    if (kb >= NB) return;
+#pragma unroll
+    for (int qq = 1; qq < 4; ++qq)
+      if (kb >= s_blk[qq]) q = qq;
+    const int j = (kb - s_blk[q]) * KB + e;
+    if (j >= s_cnt[q]) return;
+    valid = true;
+    const uint32_t i = ch.start + uint32_t(s_first[q] + j);
+    const uint32_t pi = pts.perm[i];
+    x = pts.sorted ? crd[uint64_t(i) * 2 + d] : crd[int64_t(pi) * pts.cs0 + int64_t(d) * pts.cs1];
+    if (grp < 2) {
+      const float2 v = values[int64_t(pi) * vs];
+      sc = (grp == 0 ? v.x : v.y) * sA;
+    } else {
+      sc = sB;
+    }
+  };
+  Tc xc = Tc(0);
+  float scc = 0.f;
+  int qc = 0;
+  bool vc = false;
+  if (active) fetch(0, xc, scc, qc, vc);
+  uint32_t chains = 0;   // MMAs per accumulator since its last drain, 8 bits each (uniform)
+
   for (int r = 0; active && r < nrounds; ++r) {
     const int s = r & 1;
-    if (r >= 2) {
-      if (!mbar_wait(&bars[s], uint32_t(((r - 2) >> 1) & 1))) {
-        atomicExch(err, 1);
-        s_fail = 1;
-      }
-      __syncthreads();
-      if (s_fail) {
-        active = false;
-        break;
-      }
-    }
+    bool timed_out = false;
+    if (r >= 2) timed_out = !mbar_wait(&bars[s], uint32_t(((r - 2) >> 1) & 1));
+    // prefetch the next round's point data
+    Tc xn;
+    float scn;
+    int qn;
+    bool vn;
+    fetch(r + 1, xn, scn, qn, vn);
     unsigned char *stA = oper + s * STAGE_BYTES;
     unsigned char *stB = stA + ROUND * A_BYTES;
-    const int kbl = slot / KB, e = slot % KB;
     const int kb = r * ROUND + kbl;
     if (kb < NB) {
-      int q = 0;
+      uint32_t hw[2][4];
 #pragma unroll
-      for (int qq = 1; qq < 4; ++qq)
-        if (kb >= s_blk[qq]) q = qq;
-      const int j = (kb - s_blk[q]) * KB + e;
-      const bool valid = j < s_cnt[q];
-      uint32_t hw[4][4];
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
+      for (int p = 0; p < 2; ++p)
 #pragma unroll
         for (int w = 0; w < 4; ++w) hw[p][w] = 0u;
       int off = 0;
-      const int d = bside ? 1 : 0;
-      if (valid) {
-        const uint32_t i = ch.start + uint32_t(s_first[q] + j);
-        Tc x = pts.sorted ? crd[uint64_t(i) * 2 + d]
-                          : crd[int64_t(pts.perm[i]) * pts.cs0 + int64_t(d) * pts.cs1];
+      if (vc) {
         double fr;
-        fold<Tc>(x, g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], off, fr);
-        off -= b0[d] + ((bside ? (q & 1) : (q & 2)) ? 16 : 0);
+        fold<Tc>(xc, g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], off, fr);
+        off -= b0[d] + (((grp == 2) ? (qc & 1) : (qc & 2)) ? 16 : 0);
         float k[W];
         kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fr), k);
         float hv[8], lv[8];
-        if (!bside) {
-          const float2 v = values[int64_t(pts.perm[i]) * vs];
-          const float vr = v.x * sA, vi = v.y * sA;
-          float a[2][8];
 #pragma unroll
-          for (int t = 0; t < 8; ++t) {
-            a[0][t] = (t < W) ? k[t] * vr : 0.f;
-            a[1][t] = (t < W) ? k[t] * vi : 0.f;
-          }
+        for (int t = 0; t < 8; ++t) split((t < W) ? k[t] * scc : 0.f, hv[t], lv[t]);
 #pragma unroll
-          for (int c = 0; c < 2; ++c) {
-#pragma unroll
-            for (int t = 0; t < 8; ++t) split(a[c][t], hv[t], lv[t]);
-#pragma unroll
-            for (int w = 0; w < 4; ++w) {
-              hw[c][w] = pack_half2(hv[2 * w], hv[2 * w + 1]);
-              hw[c + 2][w] = pack_half2(lv[2 * w], lv[2 * w + 1]);
-            }
-          }
-        } else {
-#pragma unroll
-          for (int t = 0; t < 8; ++t) split((t < W) ? k[t] * sB : 0.f, hv[t], lv[t]);
-#pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            hw[0][w] = pack_half2(hv[2 * w], hv[2 * w + 1]);
-            hw[1][w] = pack_half2(lv[2 * w], lv[2 * w + 1]);
-          }
+        for (int w = 0; w < 4; ++w) {
+          hw[0][w] = pack_half2(hv[2 * w], hv[2 * w + 1]);
+          hw[1][w] = pack_half2(lv[2 * w], lv[2 * w + 1]);
         }
       }
       const int c0 = off >> 3;
-      if (!bside) {
-        // A column of point e: part p rows p*32 + off + a
+      if (grp < 2) {
+        // A column of point e: part p rows p*32 + off + a; group g owns
+        // parts g (hi) and g+2 (lo)
         const uint32_t base = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO;
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
+        for (int h = 0; h < 2; ++h) {
           uint32_t z[8];
-          place8(hw[p], off & 7, z);
-          const uint32_t pb = base + uint32_t(p * 4) * SBO;
+          place8(hw[h], off & 7, z);
+          const uint32_t pb = base + uint32_t((grp + 2 * h) * 4) * SBO;
           st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
           st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
           st_v4(pb + uint32_t(c0 == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
           st_v4(pb + 3u * SBO, 0u, 0u, 0u, 0u);
         }
       } else {
-        // B row of point e: part p columns p*24 + off + b
+        // B row of point e: part h columns h*24 + off + b
         const uint32_t base = smem_u32(stB + kbl * B_BYTES) + (e & 7) * 16 + (e >> 3) * B_LBO;
 #pragma unroll
-        for (int p = 0; p < 2; ++p) {
+        for (int h = 0; h < 2; ++h) {
           uint32_t z[8];
-          place8(hw[p], off & 7, z);
-          const uint32_t pb = base + uint32_t(p * 3) * SBO;
+          place8(hw[h], off & 7, z);
+          const uint32_t pb = base + uint32_t(h * 3) * SBO;
           st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
           st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
           st_v4(pb + uint32_t(c0 == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
@@ -368,21 +410,57 @@ __global__ void __launch_bounds__(2 * tc::THREADS, 2)
       }
     }
     fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      for (int bb = 0; bb < ROUND; ++bb) {
-        const int k = r * ROUND + bb;
-        if (k >= NB) break;
-        int q = 0;
-        for (int qq = 1; qq < 4; ++qq)
-          if (k >= s_blk[qq]) q = qq;
+    tc_fence_before();
+    if (__syncthreads_or(timed_out ? 1 : 0)) {
+      if (tid == 0) atomicExch(err, 1);
+      s_fail = 1;
+      active = false;
+      break;
+    }
+    // this round's K-blocks per accumulator (computed identically by all threads)
+    int maxchain = 0;
+    for (int bb = 0; bb < ROUND; ++bb) {
+      const int k = r * ROUND + bb;
+      if (k >= NB) break;
+      int q = 0;
+      for (int qq = 1; qq < 4; ++qq)
+        if (k >= s_blk[qq]) q = qq;
+      if (tid == 0) {
+        if (bb == 0) tc_fence_after();
         const uint64_t ad = make_desc(smem_u32(stA + bb * A_BYTES), A_LBO, SBO);
         const uint64_t bd = make_desc(smem_u32(stB + bb * B_BYTES), B_LBO, SBO);
-        mma_f16(tmem + uint32_t(64 * q), ad, bd, k == s_blk[q] ? 0u : 1u);
+        mma_f16(tmem + uint32_t(64 * q), ad, bd, ((fresh >> q) & 1u) ? 0u : 1u);
+        fresh &= ~(1u << q);
+        s_dirty[q] = 1;
       }
-      mma_commit(&bars[s]);
+      chains += 1u << (8 * q);
+      maxchain = max(maxchain, int((chains >> (8 * q)) & 0xFFu));
     }
+    if (tid == 0) mma_commit(&bars[s]);
+    // bound the tensor-core accumulation chains: drain into the FP32 planes
+    if (maxchain >= DRAIN_AT && r != nrounds - 1) {
+      const bool to2 = !mbar_wait(&bars[s], uint32_t((r >> 1) & 1));
+      tc_fence_before();
+      if (__syncthreads_or(to2 ? 1 : 0)) {
+        if (tid == 0) atomicExch(err, 1);
+        s_fail = 1;
+        active = false;
+        break;
+      }
+      tc_fence_after();
+      if (warp < 4) tc_drain<W>(tmem, warp, lane, s_dirty, tre, tim, P, unscale);
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        fresh = 0xFu;
+        for (int q = 0; q < 4; ++q) s_dirty[q] = 0;
+      }
+      chains = 0;
+    }
+    xc = xn;
+    scc = scn;
+    qc = qn;
+    vc = vn;
   }
 
   // ---- wait for the last round's MMAs (a commit covers all earlier ones)
@@ -398,49 +476,19 @@ __global__ void __launch_bounds__(2 * tc::THREADS, 2)
   tc_fence_after();
   if (s_fail) active = false;
 
-  // ---- epilogue: combine hi/lo and re/im parts in shared memory, flush
-  //      (separate real / imaginary planes with an odd row pitch, so the
-  //      32 lanes of a warp, one row each, hit 32 different banks)
-  const int S = 32 + W;
-  const int P = S | 1;
-  float *tre = reinterpret_cast<float *>(oper);
-  float *tim = tre + S * P;
+  // ---- epilogue: remaining accumulators into the planes, then the grid
   if (active) {
-    for (int c = tid; c < 2 * S * P; c += 2 * THREADS) tre[c] = 0.f;
-    __syncthreads();
-    if (warp < 4) {
-      for (int q = 0; q < 4; ++q) {
-        if (s_cnt[q] == 0) continue;
-        uint32_t d0[16], d1[16], d2[16];
-        const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(64 * q);
-        tmem_ld16(ta, d0);
-        tmem_ld16(ta + 16, d1);
-        tmem_ld16(ta + 32, d2);
-        tmem_wait_ld();
-        const int u = lane;
-        if (u < 24) {
-          const int tu = u + ((q & 2) ? 16 : 0);
-          const int tv0 = (q & 1) ? 16 : 0;
-          float *dst = ((warp & 1) ? tim : tre) + tu * P + tv0;
-          if (tu < S) {
-#pragma unroll
-            for (int v = 0; v < 24; ++v) {
-              float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
-              if (warp < 2) val += __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
-              if (tv0 + v < S) atomicAdd(dst + v, val * unscale);
-            }
-          }
-        }
-      }
-    }
+    if (warp < 4) tc_drain<W>(tmem, warp, lane, s_dirty, tre, tim, P, unscale);
     __syncthreads();
     const int nu = int(g.nover[0]), nv = int(g.nover[1]);
-    for (int c = tid; c < S * S; c += 2 * THREADS) {
+    for (int c = tid; c < S * S; c += NT) {
       const int a = c / S, bcol = c - (c / S) * S;
       const float2 v = make_float2(tre[a * P + bcol], tim[a * P + bcol]);
       if (v.x == 0.f && v.y == 0.f) continue;
-      const int64_t gi = int64_t(wrapi(b0[0] + a, nu)) * nv + wrapi(b0[1] + bcol, nv);
-      atomicAdd(grid + gi, v);
+      int gu = b0[0] + a, gv = b0[1] + bcol;
+      gu += (gu < 0) ? nu : ((gu >= nu) ? -nu : 0);
+      gv += (gv < 0) ? nv : ((gv >= nv) ? -nv : 0);
+      atomicAdd(grid + int64_t(gu) * nv + gv, v);
     }
   }
   tc_fence_before();
@@ -473,7 +521,7 @@ void launch_spread_tc(const PointsDesc &pts, const uint32_t *skeys, const ChunkL
     auto kern = k_spread_tc<TC, WW>;                                                            \
     DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
                                  tc::SMEM_BYTES));                                              \
-    kern<<<cl.nchunks, 2 * tc::THREADS, tc::SMEM_BYTES, st>>>(                                  \
+    kern<<<cl.nchunks, TC_GROUPS * tc::THREADS, tc::SMEM_BYTES, st>>>(                                  \
         pts, skeys, cl.chunks, g, kp, static_cast<const float2 *>(values), vs, absmax,          \
         static_cast<float2 *>(grid), err);                                                      \
     DN_LAUNCHED();                                                                              \
