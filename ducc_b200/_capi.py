@@ -47,6 +47,7 @@ EXPORTS = [
     "dnufft_plan_create", "dnufft_plan_nu2u", "dnufft_plan_u2nu", "dnufft_plan_destroy",
     "dnufft_plan_get_info", "dnufft_plan_get_permutation", "dnufft_last_error",
     "dnufft_kernel_launches", "dnufft_profile_enable", "dnufft_profile_json",
+    "dnufft_nu2u_noalloc", "dnufft_noalloc_scratch_bytes",
 ]
 
 
@@ -65,8 +66,9 @@ def lib():
     L.dnufft_default_opts.restype = None
     L.dnufft_best_epsilon.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, P(ctypes.c_double)]
-    for f in (L.dnufft_nu2u, L.dnufft_u2nu):
+    for f in (L.dnufft_nu2u, L.dnufft_u2nu, L.dnufft_nu2u_noalloc):
         f.argtypes = [P(Array), P(Array), ctypes.c_int, ctypes.c_double, P(Array), P(Opts), vp]
+    L.dnufft_noalloc_scratch_bytes.restype = ctypes.c_size_t
     L.dnufft_plan_create.argtypes = [ctypes.c_int, P(Array), P(ctypes.c_int64), ctypes.c_int,
                                      ctypes.c_double, P(Opts), vp, P(vp)]
     for f in (L.dnufft_plan_nu2u, L.dnufft_plan_u2nu):

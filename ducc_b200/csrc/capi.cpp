@@ -723,6 +723,164 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
   so.finish();
 }
 
+// ---------------------------------------------------------------- scratch-only type 1
+// A type-1 transform whose every temporary (correction factors, twiddles,
+// tile keys and permutation, sort / chunk workspaces, chunk list, oversampled
+// grid) is carved from a device region the caller owns, so nothing is
+// allocated.  Device arrays only; the plain spreader.
+struct Carver {
+  char *base;
+  size_t cap, used = 0;
+  Carver(void *b, size_t c) : base(static_cast<char *>(b)), cap(c) {}
+  void *take(size_t bytes) {
+    size_t off = (used + 255) & ~size_t(255);
+    if (off + bytes > cap) return nullptr;
+    used = off + bytes;
+    return base + off;
+  }
+};
+
+template <typename T>
+static void nu2u_scratch_typed(const Setup &s, const View &points, const View &coord,
+                               const View &out, bool forward, bool fft_order, void *scratch,
+                               size_t cap, cudaStream_t st) {
+  const Geometry &g = s.g;
+  const uint32_t M = s.npoints;
+  const size_t csz = sizeof(T) * 2;
+  uint64_t maxchunks = std::min<uint64_t>(M, s.max_tiles) + M / CHUNK + 2;
+  Carver cv(scratch, cap);
+  double *cf[3] = {nullptr, nullptr, nullptr};
+  void *tw[3] = {nullptr, nullptr, nullptr};
+  for (int d = 0; d < g.ndim; ++d) {
+    cf[d] = static_cast<double *>(cv.take(s.corfac[d].size() * sizeof(double)));
+    tw[d] = cv.take(size_t(g.nover[d]) * csz);
+  }
+  uint32_t *keys = static_cast<uint32_t *>(cv.take(size_t(M) * 4));
+  uint32_t *perm = static_cast<uint32_t *>(cv.take(size_t(M) * 4));
+  void *rws = cv.take(radix_workspace_bytes(M, s.keybits));
+  void *cws = cv.take(chunk_workspace_bytes(M));
+  Chunk *chunks = static_cast<Chunk *>(cv.take(size_t(maxchunks) * sizeof(Chunk)));
+  uint32_t *count = static_cast<uint32_t *>(cv.take(16));
+  void *grid = cv.take(grid_cells(g) * csz);
+  bool fits = grid != nullptr;
+  for (int d = 0; d < g.ndim; ++d) fits = fits && cf[d] && tw[d];
+  fits = fits && keys && perm && rws && cws && chunks && count;
+  if (!fits) {
+    // measure what would have been needed for the message
+    Carver probe(nullptr, ~size_t(0));
+    for (int d = 0; d < g.ndim; ++d) {
+      probe.take(s.corfac[d].size() * sizeof(double));
+      probe.take(size_t(g.nover[d]) * csz);
+    }
+    probe.take(size_t(M) * 4);
+    probe.take(size_t(M) * 4);
+    probe.take(radix_workspace_bytes(M, s.keybits));
+    probe.take(chunk_workspace_bytes(M));
+    probe.take(size_t(maxchunks) * sizeof(Chunk));
+    probe.take(16);
+    probe.take(grid_cells(g) * csz);
+    throw Error(ST_BADARG, "problem needs " + std::to_string(probe.used) +
+                               " bytes of scratch, more than the " + std::to_string(cap) +
+                               " bytes of the no-allocation scratch area");
+  }
+  // constants: correction factors and FP64-accurate twiddles
+  FFTAxisPlan ax[3];
+  std::vector<std::vector<double>> hd(g.ndim);
+  std::vector<std::vector<float>> hf(g.ndim);
+  for (int d = 0; d < g.ndim; ++d) {
+    DN_CUDA(cudaMemcpyAsync(cf[d], s.corfac[d].data(), s.corfac[d].size() * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    const int n = int(g.nover[d]);
+    if (sizeof(T) == 8) {
+      hd[d].resize(2 * size_t(n));
+      for (int k = 0; k < n; ++k) {
+        double a = -2.0 * M_PI * double(k) / double(n);
+        hd[d][2 * k] = std::cos(a);
+        hd[d][2 * k + 1] = std::sin(a);
+      }
+      DN_CUDA(cudaMemcpyAsync(tw[d], hd[d].data(), hd[d].size() * 8, cudaMemcpyHostToDevice, st));
+    } else {
+      hf[d].resize(2 * size_t(n));
+      for (int k = 0; k < n; ++k) {
+        double a = -2.0 * M_PI * double(k) / double(n);
+        hf[d][2 * k] = float(std::cos(a));
+        hf[d][2 * k + 1] = float(std::sin(a));
+      }
+      DN_CUDA(cudaMemcpyAsync(tw[d], hf[d].data(), hf[d].size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    ax[d].n = n;
+    ax[d].nfac = int(s.factors[d].size());
+    for (int i = 0; i < ax[d].nfac; ++i) ax[d].fac[i] = s.factors[d][i];
+    ax[d].tw = tw[d];
+  }
+  // index: fold + stable sort + chunks (the chunk count read-back synchronises
+  // the stream, after which the host constant buffers may be released)
+  launch_fold_keys(s.coord_f64, coord.data, coord.stride[0], coord.stride[1], M, g, keys, perm, st);
+  radix_sort_pairs(keys, perm, M, s.keybits, rws, st);
+  uint32_t nch = build_chunks(keys, M, s.tile_shift, CHUNK, chunks, count, cws, st);
+  PointsDesc pts{coord.data, coord.stride[0], coord.stride[1], false, s.coord_f64, perm, M};
+  ChunkList cl{chunks, nch};
+  // the scratch keeps the previous call's contents: the grid must start at zero
+  DN_CUDA(cudaMemsetAsync(grid, 0, grid_cells(g) * csz, st));
+  const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
+      sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
+  launch_spread<T>(pts, cl, g, kp, points.data, points.stride[0], 0, grid, 0, 1, st);
+  const double *cfc[3] = {cf[0], cf[1], cf[2]};
+  fft_nu2u_tail<T>(grid, g, ax, forward, cfc, fft_order, out.data, out.stride, st);
+}
+
+static void nu2u_scratch_impl(const dnufft_array *points_, const dnufft_array *coord_, int forward,
+                              double eps, dnufft_array *out_, const dnufft_opts *opts_,
+                              cudaStream_t st, void *scratch, size_t cap) {
+  dnufft_opts o = resolved(opts_, false);
+  DN_REQUIRE(o.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
+             "the no-allocation entry point uses the plain spreader only");
+  View points = view_of(points_, "points"), coord = view_of(coord_, "coord"),
+       out = view_of(out_, "out");
+  DN_REQUIRE(!points.host && !coord.host && !out.host, ST_BADARG,
+             "the no-allocation entry point needs device arrays");
+  int ndim = out.ndim;
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "transform must be 1D/2D/3D");
+  check_coord(coord, ndim);
+  DN_REQUIRE(points.ndim == 1, ST_BADARG, "points must be 1D");
+  DN_REQUIRE(points.shape[0] == coord.shape[0], ST_BADARG, "number of points mismatch");
+  DN_REQUIRE(points.dtype == DNUFFT_C64 || points.dtype == DNUFFT_C128, ST_BADARG,
+             "points must be complex64 or complex128");
+  DN_REQUIRE(out.dtype == points.dtype, ST_BADARG, "out must have the dtype of points");
+  bool f64 = points.dtype == DNUFFT_C128;
+  Setup s = make_setup(ndim, out.shape, uint64_t(points.shape[0]), eps, true, f64,
+                       coord.dtype == DNUFFT_F64, o);
+  if (s.npoints == 0) {
+    zero_view(out, st);
+    return;
+  }
+  if (f64)
+    nu2u_scratch_typed<double>(s, points, coord, out, forward != 0, o.fft_order != 0, scratch, cap,
+                               st);
+  else
+    nu2u_scratch_typed<float>(s, points, coord, out, forward != 0, o.fft_order != 0, scratch, cap,
+                              st);
+}
+
+int nu2u_in_scratch(const dnufft_array *points, const dnufft_array *coord, int forward,
+                    double epsilon, dnufft_array *out, const dnufft_opts *opts, void *stream,
+                    void *scratch, size_t scratch_bytes) {
+  try {
+    nu2u_scratch_impl(points, coord, forward, epsilon, out, opts, static_cast<cudaStream_t>(stream),
+                      scratch, scratch_bytes);
+    g_last_error.clear();
+    return DNUFFT_OK;
+  } catch (const Error &e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return DNUFFT_ERR_INTERNAL;
+  }
+}
+
+void set_last_error(const char *msg) { g_last_error = msg; }
+
 }  // namespace dnufft
 
 // ---------------------------------------------------------------- C-ABI

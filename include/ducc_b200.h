@@ -143,6 +143,23 @@ int dnufft_plan_get_info(const dnufft_plan *plan, dnufft_plan_info *info);
  * of npoints uint32. */
 int dnufft_plan_get_permutation(const dnufft_plan *plan, uint32_t *out, void *stream);
 
+/* Type 1 like dnufft_nu2u, for callers that cannot allocate device memory
+ * while they run it: code recording into a CUDA stream capture, plugins inside
+ * a framework that owns the whole device memory pool, and services with a fixed
+ * memory budget.  It has no counterpart in the reference (DUCC allocates its
+ * temporaries on the host heap).  Every temporary comes from one area of
+ * dnufft_noalloc_scratch_bytes() bytes (32 MiB) compiled into the library and
+ * held by every GPU that loads it until the process exits; problems that need
+ * more are rejected with DNUFFT_ERR_BADARG before any launch.  All arrays must
+ * be device arrays.  The first call on a device looks up the area's address,
+ * so make it before any stream capture.  All calls share the one area and it
+ * keeps the previous call's contents: calls that can overlap on the GPU (other
+ * streams, other host threads) race, so serialise them.  Plain spreader only. */
+int dnufft_nu2u_noalloc(const dnufft_array *points, const dnufft_array *coord, int forward,
+                        double epsilon, dnufft_array *out, const dnufft_opts *opts,
+                        void *stream);
+size_t dnufft_noalloc_scratch_bytes(void);
+
 /* Message of the last failed call on this thread ("" if none). */
 const char *dnufft_last_error(void);
 

@@ -18,7 +18,7 @@ def declared_functions():
     for fn in os.listdir(os.path.join(ROOT, "include")):
         if fn.endswith(".h"):
             src = open(os.path.join(ROOT, "include", fn)).read()
-            names += re.findall(r"^(?:int|void|uint64_t|const char \*)\s*(dnufft_\w+)\s*\(", src, re.M)
+            names += re.findall(r"^(?:int|void|uint64_t|size_t|const char \*)\s*(dnufft_\w+)\s*\(", src, re.M)
     return names
 
 
