@@ -35,7 +35,8 @@ std::string g_prof_json;
 
 namespace dnufft {
 
-constexpr uint32_t CHUNK = 1024;
+constexpr uint32_t CHUNK = 1024;       // points per chunk (one CTA)
+constexpr uint32_t CHUNK_TC = 4096;    // tensor-core plans: fewer, longer chunks
 
 // ---------------------------------------------------------------- device buffers
 // Keep memory freed with cudaFreeAsync in the device's default pool instead of
@@ -262,6 +263,7 @@ struct Setup {
   int keybits = 1;
   int tile_shift = 0;
   uint64_t max_tiles = 0;
+  uint32_t chunk = CHUNK;   // largest chunk (consecutive sorted points of one tile)
 };
 
 static void fill_poly(Setup &s, const std::vector<double> &coeff) {
@@ -374,6 +376,9 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
     s.qbits = true;
     maxkey <<= 2;
     s.tile_shift = 2;
+    // per-chunk set-up and flush of the tensor-core spreader cost more than
+    // the plain one's: amortise them over longer chunks
+    s.chunk = CHUNK_TC;
   }
   DN_REQUIRE(maxkey < (uint64_t(1) << 32), ST_UNSUPPORTED, "tile key space too large");
   s.keybits = std::max(1, bitlen64(maxkey));
@@ -436,7 +441,18 @@ static void upload_consts(const Setup &s, DevConst &dc, cudaStream_t st) {
 struct Index {
   DevBuf perm, keys, chunks, count;
   uint32_t nchunks = 0;
+  // tensor-core order only: K-block list and per-CTA ranges
+  DevBuf kblk, kbrange;
+  uint32_t nkblk = 0, groups = 0;
+  TcBlocks tc() const { return TcBlocks{kblk.as<uint2>(), kbrange.as<uint32_t>(), groups, nkblk}; }
 };
+
+static uint32_t sm_count() {
+  int dev = 0, n = 0;
+  DN_CUDA(cudaGetDevice(&dev));
+  DN_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  return uint32_t(n > 0 ? n : 1);
+}
 
 static void build_index(const Setup &s, const View &coord, Index &ix, cudaStream_t st) {
   uint32_t M = s.npoints;
@@ -448,12 +464,21 @@ static void build_index(const Setup &s, const View &coord, Index &ix, cudaStream
     DevBuf ws(radix_workspace_bytes(M, s.keybits), st);
     radix_sort_pairs(ix.keys.as<uint32_t>(), ix.perm.as<uint32_t>(), M, s.keybits, ws.p, st);
   }
-  uint64_t maxchunks = std::min<uint64_t>(M, s.max_tiles) + M / CHUNK + 2;
+  uint64_t maxchunks = std::min<uint64_t>(M, s.max_tiles) + M / s.chunk + 2;
   ix.chunks = DevBuf(size_t(maxchunks) * sizeof(Chunk), st);
   ix.count = DevBuf(16, st);
   DevBuf ws(chunk_workspace_bytes(M), st);
-  ix.nchunks = build_chunks(ix.keys.as<uint32_t>(), M, s.tile_shift, CHUNK, ix.chunks.as<Chunk>(),
+  ix.nchunks = build_chunks(ix.keys.as<uint32_t>(), M, s.tile_shift, s.chunk, ix.chunks.as<Chunk>(),
                             ix.count.as<uint32_t>(), ws.p, st);
+  if (s.qbits && ix.nchunks > 0) {
+    ix.groups = sm_count();
+    ix.kblk = DevBuf(size_t(tc_kblock_upper_bound(M, ix.nchunks)) * sizeof(uint2), st);
+    ix.kbrange = DevBuf(size_t(ix.groups + 1) * sizeof(uint32_t), st);
+    DevBuf kws(tc_kblock_workspace_bytes(ix.nchunks), st);
+    ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+    ix.nkblk = build_tc_kblocks(ix.keys.as<uint32_t>(), cl, ix.groups, kws.p, ix.kblk.as<uint2>(),
+                                ix.kbrange.as<uint32_t>(), ix.count.as<uint32_t>(), st);
+  }
 }
 
 static size_t grid_cells(const Geometry &g) {
@@ -478,7 +503,7 @@ static void report_sizes(const Setup &s, bool gridding) {
 // ---------------------------------------------------------------- transforms
 template <typename T>
 static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
-                          const ChunkList &cl, const uint32_t *skeys, const View &points,
+                          const ChunkList &cl, const TcBlocks *tb, const View &points,
                           const View &out, bool forward, bool fft_order, StageTimer &tm,
                           cudaStream_t st, DevBuf *ws = nullptr) {
   size_t cells = grid_cells(s.g);
@@ -495,14 +520,14 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
     bool ok = spread_tc_supported(s.g, s.calc_f64);
     DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC || ok, ST_UNSUPPORTED,
                "tensor-core spreader: 2D single precision with support <= 8 only");
-    use_tc = ok && s.qbits;
+    use_tc = ok && s.qbits && tb != nullptr;
   } else {
     DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
                "tensor-core spreader: single precision (complex64) only");
   }
   if (use_tc) {
     int *err = device_error_word();
-    launch_spread_tc(pts, skeys, cl, s.g, s.kpf, points.data, points.stride[0], grid.p,
+    launch_spread_tc(pts, *tb, s.g, s.kpf, points.data, points.stride[0], grid.p,
                      reinterpret_cast<unsigned *>(err + 1), err, st);
     check_device_error(err, st);
   } else {
@@ -528,6 +553,35 @@ static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
   launch_interp<T>(pts, cl, s.g, kp, grid.p, 0, out.data, out.stride[0], 0, 1, st);
   tm.mark("end");
+}
+
+template <typename T>
+static void do_fft_dcoord(const Setup &s, const DevConst &dc, const PointsDesc &pts,
+                          const ChunkList &cl, const View &uni, const View &wts,
+                          const View &grad, bool forward, bool fft_order, StageTimer &tm,
+                          cudaStream_t st, DevBuf *ws = nullptr) {
+  size_t cells = grid_cells(s.g);
+  DevBuf local;
+  DevBuf &grid = ws ? *ws : local;
+  if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
+  tm.mark("correction + FFT");
+  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st);
+  tm.mark("derivative interpolation");
+  const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
+      sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
+  launch_interp_dcoord<T>(pts, cl, s.g, kp, grid.p, wts.data, wts.stride[0], grad.data,
+                          grad.stride[0], grad.stride[1], st);
+  tm.mark("end");
+}
+
+static void check_dcoord_args(const View &wts, const View &grad, int cdt, int coord_dt,
+                              uint64_t npoints, int ndim) {
+  DN_REQUIRE(wts.ndim == 1 && uint64_t(wts.shape[0]) == npoints, ST_BADARG,
+             "weights: number of points mismatch");
+  DN_REQUIRE(wts.dtype == cdt, ST_BADARG, "weights must have the grid's dtype");
+  DN_REQUIRE(grad.ndim == 2 && uint64_t(grad.shape[0]) == npoints && grad.shape[1] == ndim,
+             ST_BADARG, "grad must be (npoints, ndim)");
+  DN_REQUIRE(grad.dtype == coord_dt, ST_BADARG, "grad must have the coordinates' dtype");
 }
 
 static void zero_view(const View &v, cudaStream_t st) {
@@ -585,11 +639,12 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
   PointsDesc pts{sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], false, s.coord_f64,
                  ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+  const TcBlocks tb = ix.tc();
   if (f64)
-    do_spread_fft<double>(s, dc, pts, cl, ix.keys.as<uint32_t>(), sp.dev, so.dev, forward != 0,
+    do_spread_fft<double>(s, dc, pts, cl, &tb, sp.dev, so.dev, forward != 0,
                           o.fft_order != 0, tm, st);
   else
-    do_spread_fft<float>(s, dc, pts, cl, ix.keys.as<uint32_t>(), sp.dev, so.dev, forward != 0,
+    do_spread_fft<float>(s, dc, pts, cl, &tb, sp.dev, so.dev, forward != 0,
                          o.fft_order != 0, tm, st);
   tm.report("nu2u");
   so.finish();
@@ -631,6 +686,44 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
   so.finish();
 }
 
+static void u2nu_dcoord_impl(const dnufft_array *grid_, const dnufft_array *coord_, int forward,
+                             double eps, const dnufft_array *wts_, dnufft_array *grad_,
+                             const dnufft_opts *opts_, cudaStream_t st) {
+  dnufft_opts o = resolved(opts_, false);
+  View uni = view_of(grid_, "grid"), coord = view_of(coord_, "coord");
+  View wts = view_of(wts_, "weights"), grad = view_of(grad_, "grad");
+  int ndim = uni.ndim;
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "transform must be 1D/2D/3D");
+  check_coord(coord, ndim);
+  DN_REQUIRE(uni.dtype == DNUFFT_C64 || uni.dtype == DNUFFT_C128, ST_BADARG,
+             "grid must be complex64 or complex128");
+  check_dcoord_args(wts, grad, uni.dtype, coord.dtype, uint64_t(coord.shape[0]), ndim);
+  bool f64 = uni.dtype == DNUFFT_C128;
+  Setup s = make_setup(ndim, uni.shape, uint64_t(coord.shape[0]), eps, false, f64,
+                       coord.dtype == DNUFFT_F64, o);
+  StageTimer tm(o.verbosity > 0, st);
+  if (s.npoints == 0) return;
+  Staged su(uni, true, false, st), sc(coord, true, false, st), sw(wts, true, false, st),
+      sg(grad, false, true, st);
+  tm.mark("upload constants");
+  DevConst dc;
+  upload_consts(s, dc, st);
+  tm.mark("building index");
+  Index ix;
+  build_index(s, sc.dev, ix, st);
+  PointsDesc pts{sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], false, s.coord_f64,
+                 ix.perm.as<uint32_t>(), s.npoints};
+  ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+  if (f64)
+    do_fft_dcoord<double>(s, dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, o.fft_order != 0,
+                          tm, st);
+  else
+    do_fft_dcoord<float>(s, dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, o.fft_order != 0,
+                         tm, st);
+  tm.report("u2nu_dcoord");
+  sg.finish();
+}
+
 }  // namespace dnufft
 
 // ---------------------------------------------------------------- plans
@@ -667,9 +760,9 @@ static void plan_create_impl(int nu2u, const dnufft_array *coord_, const int64_t
     p->sorted_coord = DevBuf(size_t(p->s.npoints) * ndim * (f64 ? 8 : 4), st);
     launch_gather_coords(f64, sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], ndim,
                          p->ix.perm.as<uint32_t>(), p->s.npoints, p->sorted_coord.p, st);
-    // the plan keeps the sorted coordinates; the sorted keys only where the
-    // tensor-core spreader reads the quadrant bits from them
-    if (!p->s.qbits) p->ix.keys.release();
+    // the plan keeps the sorted coordinates (and, for the tensor-core
+    // spreader, the K-block list); the sorted keys are no longer needed
+    p->ix.keys.release();
   }
   DN_CUDA(cudaStreamSynchronize(st));
   *out = p.release();
@@ -711,7 +804,8 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
   ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
   bool fo = p->o.fft_order != 0;
   if (type1) {
-    const uint32_t *sk = p->ix.keys.as<uint32_t>();
+    const TcBlocks tb = p->ix.tc();
+    const TcBlocks *sk = s.qbits ? &tb : nullptr;
     if (f64) do_spread_fft<double>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
     else do_spread_fft<float>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
     tm.report("nu2u (planned)");
@@ -721,6 +815,37 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
     tm.report("u2nu (planned)");
   }
   so.finish();
+}
+
+static void plan_dcoord_impl(dnufft_plan *p, int forward, const dnufft_array *grid_,
+                             const dnufft_array *wts_, dnufft_array *grad_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  bool f64 = s.calc_f64;
+  int cdt = f64 ? DNUFFT_C128 : DNUFFT_C64;
+  View uni = view_of(grid_, "grid"), wts = view_of(wts_, "weights"), grad = view_of(grad_, "grad");
+  DN_REQUIRE(uni.dtype == cdt, ST_BADARG,
+             f64 ? "a float64-coordinate plan needs complex128 data"
+                 : "a float32-coordinate plan needs complex64 data");
+  DN_REQUIRE(uni.ndim == s.g.ndim, ST_BADARG, "uniform grid dimensions mismatch");
+  for (int d = 0; d < s.g.ndim; ++d)
+    DN_REQUIRE(uni.shape[d] == s.g.nuni[d], ST_BADARG, "uniform grid dimensions mismatch");
+  check_dcoord_args(wts, grad, cdt, s.coord_f64 ? DNUFFT_F64 : DNUFFT_F32, s.npoints, s.g.ndim);
+  if (s.npoints == 0) return;
+  StageTimer tm(false, st);
+  Staged su(uni, true, false, st), sw(wts, true, false, st), sg(grad, false, true, st);
+  if (!p->grid.p) {
+    p->grid = DevBuf(grid_cells(s.g) * (f64 ? 16 : 8), st);
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
+  PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
+                 p->ix.perm.as<uint32_t>(), s.npoints};
+  ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
+  bool fo = p->o.fft_order != 0;
+  if (f64) do_fft_dcoord<double>(s, p->dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, fo, tm, st, &p->grid);
+  else do_fft_dcoord<float>(s, p->dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, fo, tm, st, &p->grid);
+  tm.report("u2nu_dcoord (planned)");
+  sg.finish();
 }
 
 // ---------------------------------------------------------------- scratch-only type 1
@@ -747,7 +872,7 @@ static void nu2u_scratch_typed(const Setup &s, const View &points, const View &c
   const Geometry &g = s.g;
   const uint32_t M = s.npoints;
   const size_t csz = sizeof(T) * 2;
-  uint64_t maxchunks = std::min<uint64_t>(M, s.max_tiles) + M / CHUNK + 2;
+  uint64_t maxchunks = std::min<uint64_t>(M, s.max_tiles) + M / s.chunk + 2;
   Carver cv(scratch, cap);
   double *cf[3] = {nullptr, nullptr, nullptr};
   void *tw[3] = {nullptr, nullptr, nullptr};
@@ -817,7 +942,7 @@ static void nu2u_scratch_typed(const Setup &s, const View &points, const View &c
   // the stream, after which the host constant buffers may be released)
   launch_fold_keys(s.coord_f64, coord.data, coord.stride[0], coord.stride[1], M, g, keys, perm, st);
   radix_sort_pairs(keys, perm, M, s.keybits, rws, st);
-  uint32_t nch = build_chunks(keys, M, s.tile_shift, CHUNK, chunks, count, cws, st);
+  uint32_t nch = build_chunks(keys, M, s.tile_shift, s.chunk, chunks, count, cws, st);
   PointsDesc pts{coord.data, coord.stride[0], coord.stride[1], false, s.coord_f64, perm, M};
   ChunkList cl{chunks, nch};
   // the scratch keeps the previous call's contents: the grid must start at zero
@@ -954,11 +1079,25 @@ int dnufft_plan_u2nu(dnufft_plan *plan, int forward, int verbosity, const dnufft
                                   static_cast<cudaStream_t>(stream)))
 }
 
+int dnufft_u2nu_dcoord(const dnufft_array *grid, const dnufft_array *coord, int forward,
+                       double epsilon, const dnufft_array *weights, dnufft_array *grad,
+                       const dnufft_opts *opts, void *stream) {
+  DN_GUARD(dnufft::u2nu_dcoord_impl(grid, coord, forward, epsilon, weights, grad, opts,
+                                    static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_u2nu_dcoord(dnufft_plan *plan, int forward, const dnufft_array *grid,
+                            const dnufft_array *weights, dnufft_array *grad, void *stream) {
+  DN_GUARD(dnufft::plan_dcoord_impl(plan, forward, grid, weights, grad,
+                                    static_cast<cudaStream_t>(stream)))
+}
+
 int dnufft_plan_destroy(dnufft_plan *plan) {
   DN_GUARD({
     if (plan) {
       cudaStream_t st = nullptr;
       plan->ix.perm.st = plan->ix.chunks.st = plan->ix.count.st = plan->ix.keys.st = st;
+      plan->ix.kblk.st = plan->ix.kbrange.st = st;
       plan->sorted_coord.st = st;
       plan->grid.st = st;
       for (int d = 0; d < 3; ++d) plan->dc.corfac[d].st = plan->dc.tw[d].st = st;
@@ -1003,6 +1142,7 @@ int dnufft_plan_get_permutation(const dnufft_plan *p, uint32_t *out, void *strea
       s2.qbits = false;
       s2.keybits -= 2;
       s2.tile_shift = 0;
+      s2.chunk = dnufft::CHUNK;
       const uint32_t M = s2.npoints;
       const int nd = s2.g.ndim;
       // sorted coordinates in original order: scatter back through perm

@@ -56,12 +56,32 @@ void launch_interp(const PointsDesc &pts, const ChunkList &cl, const Geometry &g
                    const KernelPoly<T> &kp, const void *grid, int64_t gtrans,
                    void *out, int64_t os, int64_t otrans, int ntrans, cudaStream_t st);
 
+// grad[j*gs0 + d*gs1] = Re(conj(wts[j*ws]) * d/dx_{j,d} interp(grid)(x_j)), in
+// the coordinates' dtype (interp_grad.cu)
+template <typename T>
+void launch_interp_dcoord(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
+                          const KernelPoly<T> &kp, const void *grid, const void *wts,
+                          int64_t ws, void *grad, int64_t gs0, int64_t gs1, cudaStream_t st);
+
 // ---- split-precision tensor-core spreader (spread_tc.cu): 2D, complex64
 bool spread_tc_supported(const Geometry &g, bool calc_f64);
-// skeys: sorted tile keys carrying the tile quadrant in their two low bits
-void launch_spread_tc(const PointsDesc &pts, const uint32_t *skeys, const ChunkList &cl,
-                      const Geometry &g, const KernelPoly<float> &kp, const void *values,
-                      int64_t vs, void *grid, unsigned *absmax, int *err, cudaStream_t st);
+// K-block list of a (tile, quadrant)-sorted point set: records {first sorted
+// point, meta} of <= 16 points of one quadrant of one chunk, and the K-block
+// range [range[b], range[b+1]) of each of 'groups' persistent CTAs
+struct TcBlocks {
+  const uint2 *kblk;
+  const uint32_t *range;
+  uint32_t groups;
+  uint32_t total;
+};
+size_t tc_kblock_workspace_bytes(uint32_t nchunks);
+uint32_t tc_kblock_upper_bound(uint32_t npts, uint32_t nchunks);
+// returns the number of K-blocks (reads it back: synchronises the stream)
+uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t groups, void *ws,
+                          uint2 *kblk, uint32_t *range, uint32_t *d_total, cudaStream_t st);
+void launch_spread_tc(const PointsDesc &pts, const TcBlocks &tb, const Geometry &g,
+                      const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
+                      unsigned *absmax, int *err, cudaStream_t st);
 
 // ---- FFT and correction (fft.cu)
 struct FFTAxisPlan {

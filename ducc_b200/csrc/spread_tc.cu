@@ -9,22 +9,45 @@
 //     A.B ~= Ahi.Bhi + Ahi.Blo + Alo.Bhi
 // keeps ~22 significant bits.  One MMA does all three products and both
 // complex parts at once:
-//     A (M=128 x K=16 points) rows = [Re(c)ku hi | Im(c)ku hi | Re(c)ku lo | Im(c)ku lo] x 32
-//     B (K=16 x N=48)         cols = [kv hi | kv lo] x 24
-//     D (128 x 48, FP32, TMEM):  Re = D[0:24, 0:24] + D[0:24, 24:48] + D[64:88, 0:24]
-//                                Im = D[32:56, 0:24] + D[32:56, 24:48] + D[96:120, 0:24]
+//     A (M=128 x K=16 points) rows = [Re(c)ku hi | Im(c)ku hi | Re(c)ku lo | Im(c)ku lo]
+//                                    24 rows each (rows 96..127 stay zero)
+//     B (K=16 x N=48)         cols = [kv hi | kv lo], 24 columns each
+//     D (128 x 48, FP32, TMEM):  Re = D[0:24, 0:24] + D[0:24, 24:48] + D[48:72, 0:24]
+//                                Im = D[24:48, 0:24] + D[24:48, 24:48] + D[72:96, 0:24]
 // (the Alo.Blo block is computed and ignored).  A 32x32 tile (DUCC's 2D
-// single-precision tile) is split into four 16x16 quadrants, each with its own
-// accumulator, so a point's 8 taps always fit the 24 rows/columns of a quadrant.
-// Operands are built per point in registers (Horner weights, FP16 hi/lo split,
-// funnel-shift placement at the point's row offset) and stored MN-major into
-// shared memory; two operand stages let the CUDA cores build one round of
-// K-blocks while the tensor cores consume the previous one.  Results are
-// combined in shared memory and added to the grid with vector atomics.
+// single-precision tile) is split into four 16x16 quadrants with their own
+// accumulators, so a point's <= 8 taps always fit the 24 rows/columns of its
+// quadrant window.  Points arrive sorted by (tile, quadrant); the plan cuts
+// them into K-blocks of <= 16 points of one quadrant of one chunk.
 //
-// Values are scaled by a power of two per chunk (largest |Re|,|Im| -> 2^14)
-// so FP16 neither overflows nor loses the small kernel tails to underflow; the
+// The kernel is persistent (one CTA per SM, a contiguous range of K-blocks
+// per CTA, balanced at chunk boundaries) and warp-specialised, every hand-off
+// an mbarrier:
+//   loader warps (4)   : K-block records, permutation, then cp.async of the
+//                        coordinates and values of one round (8 K-blocks) into
+//                        a 16-slot ring;
+//   builder warps (12) : 3 threads per point (A rows of Re(c)ku, of Im(c)ku,
+//                        B row of kv): fold, Horner weights, FP16 hi/lo split,
+//                        placement; MN-major operand tiles in 2 stages;
+//   MMA warp (1)       : one thread issues the MMAs of a round into the
+//                        accumulator of each K-block's quadrant and commits;
+//   epilogue warps (4) : read finished accumulators from tensor memory, add
+//                        them into FP32 shared-memory planes (no atomics), and
+//                        at the end of a chunk add the planes to the grid with
+//                        float2 atomics.
+// Tensor memory holds two accumulator sets (2 x 4 quadrants x 64 columns), so
+// the MMA thread continues with the next chunk while the epilogue drains the
+// previous one.  An accumulator is also handed to the epilogue once any of its
+// quadrants has taken DRAIN_AT MMAs, which bounds each tensor-core
+// accumulation chain and with it the accumulation error.
+//
+// Values are scaled by a global power of two (largest |Re|,|Im| -> 2^14) so
+// FP16 neither overflows nor loses the small kernel tails to underflow; the
 // scale is removed exactly in the epilogue.
+//
+// Every wait is bounded (wall clock) and on expiry sets the device error word
+// and a shared abort flag that ends every role's loop; the host turns the
+// word into DNUFFT_ERR_TIMEOUT.
 #include <cuda_fp16.h>
 
 #include "common.cuh"
@@ -35,24 +58,50 @@ namespace dnufft {
 
 namespace tc {
 
-constexpr int THREADS = 128;       // one warpgroup: TMEM lanes 0..127
 constexpr int KB = 16;             // points per MMA (K)
 constexpr int ROUND = 8;           // K-blocks per round (one operand stage)
+constexpr int NST = 3;             // operand stages
+constexpr int NPRE = 16;           // point-data ring slots (rounds)
 constexpr int A_BYTES = 4096;      // 128 x 16 fp16, MN-major, no swizzle
 constexpr int B_BYTES = 1536;      // 48 x 16 fp16, MN-major, no swizzle
 constexpr int A_LBO = 2048;        // between the two K-groups of 8 points
 constexpr int B_LBO = 768;
 constexpr int SBO = 128;           // between consecutive 8-element MN chunks
+constexpr int PART = 3;            // 8-element chunks per operand part (24 rows / columns)
 constexpr int M = 128, N = 48;
-constexpr int TMEM_COLS = 256;     // quadrant q accumulates at column 64*q
-constexpr int MAXCHUNK = 1024;
 constexpr int STAGE_BYTES = ROUND * (A_BYTES + B_BYTES);   // 45056
-// shared memory: 2 operand stages (each descriptor reads only its own 4 KB /
-// 1.5 KB block: 16 resp. 6 chunks of 128 B at SBO, 2 K-groups at LBO)
-constexpr int OPER_BYTES = 2 * STAGE_BYTES;
-// + the FP32 combine planes (re, im), 2 x 40 x 41 floats
-constexpr int SMEM_BYTES = OPER_BYTES + 2 * 40 * 41 * 4;
-constexpr uint32_t SPIN_LIMIT = 1u << 26;
+constexpr int TMEM_COLS = 512;     // quadrant q, buffer b at column 128*q + 64*b
+constexpr int PL = 40, PP = 41;    // FP32 plane rows, odd pitch
+constexpr int PLANE_FLOATS = PL * PP;
+constexpr int DRAIN_AT = 24;       // K-blocks per quadrant per sub-chunk (chain bound)
+constexpr uint32_t FLUSH_COST = 4; // CTA balancing: one sub-chunk flush ~ this many records
+
+// warp roles
+constexpr int EPI_W0 = 0, N_EPI = 4;     // warps 0..3: tensor-memory lane quarters 0..3
+constexpr int MMA_W0 = 4, N_MMA = 4;     // warp 4+q issues the MMAs of quadrant q
+constexpr int LOAD_W0 = 8, N_LOAD = 4;
+constexpr int BUILD_W0 = 12, N_BUILD = 12;
+constexpr int WARPS = BUILD_W0 + N_BUILD;   // 24
+constexpr int THREADS = 32 * WARPS;         // 768
+constexpr int BUILDERS = 32 * N_BUILD;      // 384 = 3 groups x 128 point slots
+
+// K-block record in global memory: {first sorted point index, meta}
+//   meta bits 0-4 points (0..16), 5-6 quadrant, 7 last record of its quadrant
+//   in its sub-chunk, 8-31 tile id.  Every sub-chunk has at least one record per
+//   quadrant (an empty one, 0 points, if the quadrant has no points there);
+//   padding records at the end of a CTA's range are all zero.
+constexpr uint32_t META_LAST = 1u << 7;
+constexpr int TILE_SHIFT_META = 8;
+constexpr uint32_t MAX_TILES = 1u << 24;
+
+// decoded record in the point-data ring
+struct KRec {
+  uint32_t start;   // first sorted point index
+  uint32_t meta;    // as above
+  int b0u, b0v;     // grid origin of the quadrant window
+};
+
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -75,21 +124,50 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// bounded wait for the phase with the given parity; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t addr = smem_u32(bar);
-  for (uint32_t it = 0; it < SPIN_LIMIT; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (ok) return true;
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// one potentially blocking test: the thread may be suspended (without taking
+// issue slots) for up to the hint while the phase is incomplete
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(addr), "r"(parity), "r"(1000u)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase with the given parity.  Gives up (returning
+// false) when another role has raised the abort flag, or after WAIT_NS, in
+// which case it raises the flag and the device error word itself.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                          int *err) {
+  const uint32_t addr = smem_u32(bar);
+  if (mbar_try(addr, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try(addr, parity)) return true;
+    if ((it & 3u) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > WAIT_NS) {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+        return false;
+      }
+    }
   }
-  return false;
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
@@ -131,15 +209,46 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ uint32_t pack_half2(float a, float b) {
-  __half2 h = __floats2half2_rn(a, b);
-  return *reinterpret_cast<uint32_t *>(&h);
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// x = hi + lo in FP16
-__device__ __forceinline__ void split(float x, float &hi, float &lo) {
-  hi = __half2float(__float2half_rn(x));
-  lo = x - hi;
+// named barrier that also returns whether any participating thread passed true
+__device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "barrier.cta.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(v ? 1u : 0u), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void cp_async(void *dst, const void *src, int bytes) {
+  const uint32_t d = smem_u32(dst);
+  if (bytes == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// hi = RN_fp16(x), lo = RN_fp16(x - hi) for a pair, packed as half2 words
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo) {
+  const __half2 h = __floats2half2_rn(a, b);
+  const float2 hf = __half22float2(h);
+  const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
 // 8 halves (4 words) shifted up by r halves (0..7) across two 8-half chunks:
@@ -154,7 +263,6 @@ __device__ __forceinline__ void place8(const uint32_t (&h)[4], int r, uint32_t (
   x[4] = __funnelshift_l(h[3], 0u, bs);
   const int ws = r >> 1;
   uint32_t y[8];
-  // shift by two words if ws&2
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     uint32_t a = (j < 5) ? x[j] : 0u;
@@ -175,6 +283,19 @@ __device__ __forceinline__ void st_v4(uint32_t saddr, uint32_t a, uint32_t b, ui
                : "memory");
 }
 
+// per-slot layout of the point-data ring
+template <typename Tc> struct PreLayout {
+  static constexpr int REC = 0;                                     // 8 KRec
+  static constexpr int PLAN = ROUND * int(sizeof(KRec));            // 4 x u32 issue plans
+  static constexpr int COORD = PLAN + 16;                           // 128 x 2 Tc
+  static constexpr int VAL = COORD + ROUND * KB * 2 * int(sizeof(Tc));   // 128 float2
+  static constexpr int BYTES = VAL + ROUND * KB * 8;
+};
+
+template <typename Tc> constexpr int smem_bytes() {
+  return NST * STAGE_BYTES + 4 * PLANE_FLOATS * 4 + NPRE * PreLayout<Tc>::BYTES;
+}
+
 }  // namespace tc
 
 // Largest |Re|, |Im| over the values (for the power-of-two operand scale).
@@ -190,324 +311,555 @@ __global__ void k_absmax(const float2 *__restrict__ values, int64_t vs, uint32_t
   if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
 }
 
-// 384 threads in three builder groups of 128, one point slot each:
-//   group 0: A rows of Re(c)*ku (hi and lo parts), group 1: A rows of
-//   Im(c)*ku, group 2: the B row kv (hi and lo) - balanced work per thread.
-// The points of a chunk arrive ordered by tile quadrant (the sort key carries
-// the quadrant in its two low bits), so every K-block of 16 consecutive points
-// of one quadrant feeds one MMA into that quadrant's accumulator.  The
-// tensor-memory accumulators are added into FP32 shared-memory planes and
-// restarted once one of them has taken DRAIN_AT
-// MMAs, which bounds the length of each tensor-core accumulation chain (and
-// with it the accumulation error); typical chunks never need a drain.
-constexpr int TC_GROUPS = 3;
-constexpr int DRAIN_AT = 24;   // drain when an accumulator has taken this many MMAs
-
-template <int W>
-__device__ __forceinline__ void tc_drain(uint32_t tmem, int warp, int lane, const int *s_dirty,
-                                         float *tre, float *tim, int P, float unscale) {
-  constexpr int S = 32 + W;
-  for (int q = 0; q < 4; ++q) {
-    if (!s_dirty[q]) continue;
-    uint32_t d0[16], d1[16], d2[16];
-    const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(64 * q);
-    tc::tmem_ld16(ta, d0);
-    tc::tmem_ld16(ta + 16, d1);
-    tc::tmem_ld16(ta + 32, d2);
-    tc::tmem_wait_ld();
-    const int u = lane;
-    const int tu = u + ((q & 2) ? 16 : 0);
-    const int tv0 = (q & 1) ? 16 : 0;
-    if (u < 24 && tu < S) {
-      float *dst = ((warp & 1) ? tim : tre) + tu * P + tv0;
-#pragma unroll
-      for (int v = 0; v < 24; ++v) {
-        float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
-        if (warp < 2) val += __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
-        if (tv0 + v < S) atomicAdd(dst + v, val * unscale);
-      }
-    }
-  }
-}
-
 template <typename Tc, int W>
-__global__ void __launch_bounds__(TC_GROUPS * tc::THREADS, 2)
-    k_spread_tc(PointsDesc pts, const uint32_t *__restrict__ skeys, const Chunk *__restrict__ chunks,
-                Geometry g, KernelPoly<float> kp, const float2 *__restrict__ values, int64_t vs,
+__global__ void __launch_bounds__(tc::THREADS, 1)
+    k_spread_tc(PointsDesc pts, const uint2 *__restrict__ kblk,
+                const uint32_t *__restrict__ kb_range, Geometry g, KernelPoly<float> kp,
+                const float2 *__restrict__ values, int64_t vs,
                 const unsigned *__restrict__ absmax, float2 *__restrict__ grid,
                 int *__restrict__ err) {
   using namespace tc;
   static_assert(W <= 8, "tensor-core spreader handles supports up to 8");
-  constexpr int NT = TC_GROUPS * THREADS;
-  constexpr int S = 32 + W;   // tile buffer side (rows 0..32+W-2 used)
-  constexpr int P = S | 1;    // odd pitch of the FP32 planes (conflict-free rows)
+  using PL_ = PreLayout<Tc>;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  __shared__ uint64_t bars[2];
+  __shared__ uint64_t full_bar[NST], empty_bar[NST];
+  __shared__ uint64_t pre_full[NPRE], pre_empty[NPRE];
+  __shared__ uint64_t acc_full[4][2], acc_empty[4][2], done_bar;
+  __shared__ uint2 acc_info[4][2];   // {flags (1 dirty, 2 exit), tile}
   __shared__ uint32_t s_tmem;
-  __shared__ int s_first[5], s_cnt[4], s_blk[5];
-  __shared__ int s_dirty[4];
-  __shared__ int s_fail;
+  __shared__ int s_abort;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int grp = tid / THREADS;            // 0: Re A, 1: Im A, 2: B
-  const int slot = tid - grp * THREADS;
-  const Chunk ch = chunks[blockIdx.x];
-  const int cnt = int(ch.count);
-  int b0[2];
-  {
-    const int ntv = int(g.ntiles[1]);
-    const int tile = int(ch.tile);
-    b0[0] = ((tile / ntv) << g.log2tile) - g.nsafe;
-    b0[1] = ((tile % ntv) << g.log2tile) - g.nsafe;
-  }
-  unsigned char *oper = tc_smem;
-  float *tre = reinterpret_cast<float *>(tc_smem + OPER_BYTES);
-  float *tim = tre + S * P;
+  const uint32_t kb0 = kb_range[blockIdx.x], kb1 = kb_range[blockIdx.x + 1];
+  const int nrounds = int((kb1 - kb0 + ROUND - 1) / ROUND);
+  const float maxc = __uint_as_float(*absmax);
+  // nothing to add (no K-blocks, or all values zero): uniform early exit
+  if (nrounds == 0 || maxc == 0.f) return;
+  int e2 = 0;
+  if (isfinite(maxc)) frexpf(maxc, &e2);
+  const float sA = ldexpf(1.f, 14 - e2), sB = 16384.f;
+  const float unscale = ldexpf(1.f, e2 - 28);
 
-  if (warp == 0) {
+  unsigned char *stages = tc_smem;
+  float *planes = reinterpret_cast<float *>(tc_smem + NST * STAGE_BYTES);
+  unsigned char *pre = tc_smem + NST * STAGE_BYTES + 4 * PLANE_FLOATS * 4;
+
+  if (warp == MMA_W0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  ::"r"(smem_u32(&s_tmem)), "r"(uint32_t(TMEM_COLS)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(&full_bar[s], BUILDERS);
+      mbar_init(&empty_bar[s], N_MMA);
+    }
+    for (int s = 0; s < NPRE; ++s) {
+      mbar_init(&pre_full[s], 33);                  // 32 cp.async arrivals + 1 record arrival
+      mbar_init(&pre_empty[s], BUILDERS + N_MMA);   // builders + MMA threads
+    }
+    for (int q = 0; q < 4; ++q)
+      for (int b = 0; b < 2; ++b) {
+        mbar_init(&acc_full[q][b], 2);              // MMA commit + MMA thread (info)
+        mbar_init(&acc_empty[q][b], 32 * N_EPI);
+      }
+    mbar_init(&done_bar, N_MMA);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_fail = 0;
+    s_abort = 0;
   }
-  if (tid < 5) s_first[tid] = cnt;
-  if (tid < 4) s_dirty[tid] = 0;
-  for (int c = tid; c < 2 * S * P; c += NT) tre[c] = 0.f;
+  // zero the operand stages (A rows 96..127 are never written again) and planes
+  {
+    const uint32_t zb = smem_u32(tc_smem);
+    const int nvec = (NST * STAGE_BYTES + 4 * PLANE_FLOATS * 4) / 16;
+    for (int i = tid; i < nvec; i += THREADS) st_v4(zb + uint32_t(i) * 16u, 0u, 0u, 0u, 0u);
+  }
+  fence_proxy_async();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
+  volatile int *abortp = &s_abort;
+  const int ntv = int(g.ntiles[1]);
 
-  // ---- quadrant segments of the (quadrant-sorted) chunk
-  for (int i = tid; i < cnt; i += NT) {
-    const int q = int(skeys[ch.start + uint32_t(i)] & 3u);
-    if (i == 0 || int(skeys[ch.start + uint32_t(i) - 1] & 3u) != q) s_first[q] = i;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    for (int q = 3; q >= 0; --q)
-      if (s_first[q] == cnt) s_first[q] = s_first[q + 1];
-    int acc = 0;
-    for (int q = 0; q < 4; ++q) {
-      s_cnt[q] = s_first[q + 1] - s_first[q];
-      s_blk[q] = acc;
-      acc += (s_cnt[q] + KB - 1) / KB;
-    }
-    s_blk[4] = acc;
-  }
-  __syncthreads();
-  const float maxc = __uint_as_float(*absmax);
-  const int NB = s_blk[4];
-  const int nrounds = (NB + ROUND - 1) / ROUND;
-  bool active = (maxc > 0.f) && isfinite(maxc) && NB > 0;
-  int e2 = 0;
-  if (active) frexpf(maxc, &e2);
-  const float sA = ldexpf(1.f, 14 - e2), sB = 16384.f;
-  const float unscale = ldexpf(1.f, e2 - 28);
-  const Tc *crd = static_cast<const Tc *>(pts.coord);
-  unsigned fresh = 0xFu;   // quadrants whose next MMA overwrites (issuing thread only)
-  const int d = (grp == 2) ? 1 : 0;
-  const int kbl = slot / KB, e = slot % KB;
-
-  // point data of this thread's slot in round rr (loads only; used one round later)
-  auto fetch = [&](int rr, Tc &x, float &sc, int &q, bool &valid) {
-    const int kb = rr * ROUND + kbl;
-    q = 0;
-    valid = false;
-    x = Tc(0);
-    sc = 0.f;
-    if (kb >= NB) return;
+  if (warp >= LOAD_W0 && warp < LOAD_W0 + N_LOAD) {
+    // ------------------------------------------------------------ loaders
+    const int lw = warp - LOAD_W0;
+    const Tc *crd = static_cast<const Tc *>(pts.coord);
+    auto load_rec = [&](int r) -> uint2 {
+      uint2 v = make_uint2(0u, 0u);
+      if (r < nrounds && lane < ROUND) {
+        const uint32_t k = kb0 + uint32_t(r) * ROUND + uint32_t(lane);
+        if (k < kb1) v = kblk[k];
+      }
+      return v;
+    };
+    uint2 rec_next = load_rec(lw);
+    for (int r = lw; r < nrounds; r += N_LOAD) {
+      const uint2 rec = rec_next;
+      rec_next = load_rec(r + N_LOAD);   // in flight during this round
+      uint32_t idx[4], pj[4];
+      bool ok[4];
 #pragma unroll
-    for (int qq = 1; qq < 4; ++qq)
-      if (kb >= s_blk[qq]) q = qq;
-    const int j = (kb - s_blk[q]) * KB + e;
-    if (j >= s_cnt[q]) return;
-    valid = true;
-    const uint32_t i = ch.start + uint32_t(s_first[q] + j);
-    const uint32_t pi = pts.perm[i];
-    x = pts.sorted ? crd[uint64_t(i) * 2 + d] : crd[int64_t(pi) * pts.cs0 + int64_t(d) * pts.cs1];
-    if (grp < 2) {
-      const float2 v = values[int64_t(pi) * vs];
-      sc = (grp == 0 ? v.x : v.y) * sA;
-    } else {
-      sc = sB;
+      for (int j = 0; j < 4; ++j) {
+        const int p = lane + 32 * j, kbl = p >> 4, e = p & 15;
+        const uint32_t st = __shfl_sync(0xffffffffu, rec.x, kbl);
+        const uint32_t np = __shfl_sync(0xffffffffu, rec.y, kbl) & 31u;
+        ok[j] = uint32_t(e) < np;
+        idx[j] = st + uint32_t(e);
+        pj[j] = ok[j] ? pts.perm[idx[j]] : 0u;
+      }
+      const int slot = r % NPRE;
+      if (r >= NPRE && !mbar_wait(&pre_empty[slot], uint32_t((r / NPRE - 1) & 1), abortp, err))
+        break;
+      unsigned char *sl = pre + slot * PL_::BYTES;
+      if (lane < ROUND) {
+        KRec kr;
+        kr.start = rec.x;
+        kr.meta = rec.y;
+        const int tile = int(rec.y >> TILE_SHIFT_META), q = int((rec.y >> 5) & 3u);
+        const int tu = tile / ntv, tv = tile - tu * ntv;
+        kr.b0u = (tu << 5) - g.nsafe + ((q & 2) ? 16 : 0);
+        kr.b0v = (tv << 5) - g.nsafe + ((q & 1) ? 16 : 0);
+        reinterpret_cast<KRec *>(sl + PL_::REC)[lane] = kr;
+      }
+      {
+        // per quadrant: slots with points (bits 0-7) and slots closing the
+        // quadrant's sub-chunk event (bits 8-15)
+        const uint32_t meta = rec.y;
+        const int rq = int((meta >> 5) & 3u);
+        const bool has = lane < ROUND && (meta & 31u) != 0u;
+        const bool cls = lane < ROUND && (meta & META_LAST) != 0u;
+        uint32_t plan[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          plan[q] = (__ballot_sync(0xffffffffu, has && rq == q) & 0xFFu) |
+                    ((__ballot_sync(0xffffffffu, cls && rq == q) & 0xFFu) << 8);
+        if (lane == 0)
+          *reinterpret_cast<uint4 *>(sl + PL_::PLAN) = make_uint4(plan[0], plan[1], plan[2], plan[3]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!ok[j]) continue;
+        const int p = lane + 32 * j;
+        Tc *cdst = reinterpret_cast<Tc *>(sl + PL_::COORD) + 2 * p;
+        if (pts.sorted) {
+          cp_async(cdst, crd + uint64_t(idx[j]) * 2, 2 * int(sizeof(Tc)));
+        } else {
+          cp_async(cdst, crd + int64_t(pj[j]) * pts.cs0, int(sizeof(Tc)));
+          cp_async(cdst + 1, crd + int64_t(pj[j]) * pts.cs0 + pts.cs1, int(sizeof(Tc)));
+        }
+        cp_async(sl + PL_::VAL + 8 * p, values + int64_t(pj[j]) * vs, 8);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&pre_full[slot]);
+      cp_async_arrive(&pre_full[slot]);
     }
-  };
-  Tc xc = Tc(0);
-  float scc = 0.f;
-  int qc = 0;
-  bool vc = false;
-  if (active) fetch(0, xc, scc, qc, vc);
-  uint32_t chains = 0;   // MMAs per accumulator since its last drain, 8 bits each (uniform)
-
-  for (int r = 0; active && r < nrounds; ++r) {
-    const int s = r & 1;
-    bool timed_out = false;
-    if (r >= 2) timed_out = !mbar_wait(&bars[s], uint32_t(((r - 2) >> 1) & 1));
-    // prefetch the next round's point data
-    Tc xn;
-    float scn;
-    int qn;
-    bool vn;
-    fetch(r + 1, xn, scn, qn, vn);
-    unsigned char *stA = oper + s * STAGE_BYTES;
-    unsigned char *stB = stA + ROUND * A_BYTES;
-    const int kb = r * ROUND + kbl;
-    if (kb < NB) {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp >= BUILD_W0) {
+    // ------------------------------------------------------------ builders
+    const int bt = tid - BUILD_W0 * 32;
+    const int grp = bt >> 7;   // 0: Re A rows, 1: Im A rows, 2: B row
+    const int slot = bt & 127, kbl = slot >> 4, e = slot & 15;
+    const int d = (grp == 2) ? 1 : 0;
+    for (int r = 0; r < nrounds; ++r) {
+      const int ps = r % NPRE;
+      if (!mbar_wait(&pre_full[ps], uint32_t((r / NPRE) & 1), abortp, err)) break;
+      const unsigned char *sl = pre + ps * PL_::BYTES;
+      const KRec kr = reinterpret_cast<const KRec *>(sl + PL_::REC)[kbl];
+      const int np = int(kr.meta & 31u);
+      const bool valid = e < np;
+      Tc x = Tc(0);
+      float sc = 0.f;
+      if (valid) {
+        x = reinterpret_cast<const Tc *>(sl + PL_::COORD)[2 * slot + d];
+        const float2 v = reinterpret_cast<const float2 *>(sl + PL_::VAL)[slot];
+        sc = (grp == 0) ? v.x * sA : ((grp == 1) ? v.y * sA : sB);
+      }
+      mbar_arrive(&pre_empty[ps]);
       uint32_t hw[2][4];
 #pragma unroll
-      for (int p = 0; p < 2; ++p)
-#pragma unroll
-        for (int w = 0; w < 4; ++w) hw[p][w] = 0u;
+      for (int w = 0; w < 4; ++w) hw[0][w] = hw[1][w] = 0u;
       int off = 0;
-      if (vc) {
+      if (valid) {
+        int i0;
         double fr;
-        fold<Tc>(xc, g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], off, fr);
-        off -= b0[d] + (((grp == 2) ? (qc & 1) : (qc & 2)) ? 16 : 0);
+        fold<Tc>(x, g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], i0, fr);
+        off = i0 - (d ? kr.b0v : kr.b0u);
         float k[W];
         kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fr), k);
-        float hv[8], lv[8];
 #pragma unroll
-        for (int t = 0; t < 8; ++t) split((t < W) ? k[t] * scc : 0.f, hv[t], lv[t]);
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {
-          hw[0][w] = pack_half2(hv[2 * w], hv[2 * w + 1]);
-          hw[1][w] = pack_half2(lv[2 * w], lv[2 * w + 1]);
-        }
+        for (int w = 0; w < 4; ++w)
+          split2((2 * w < W) ? k[2 * w] * sc : 0.f, (2 * w + 1 < W) ? k[2 * w + 1] * sc : 0.f,
+                 hw[0][w], hw[1][w]);
       }
-      const int c0 = off >> 3;
-      if (grp < 2) {
-        // A column of point e: part p rows p*32 + off + a; group g owns
-        // parts g (hi) and g+2 (lo)
-        const uint32_t base = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          uint32_t z[8];
-          place8(hw[h], off & 7, z);
-          const uint32_t pb = base + uint32_t((grp + 2 * h) * 4) * SBO;
-          st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
-          st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
-          st_v4(pb + uint32_t(c0 == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
-          st_v4(pb + 3u * SBO, 0u, 0u, 0u, 0u);
-        }
-      } else {
-        // B row of point e: part h columns h*24 + off + b
-        const uint32_t base = smem_u32(stB + kbl * B_BYTES) + (e & 7) * 16 + (e >> 3) * B_LBO;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          uint32_t z[8];
-          place8(hw[h], off & 7, z);
-          const uint32_t pb = base + uint32_t(h * 3) * SBO;
-          st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
-          st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
-          st_v4(pb + uint32_t(c0 == 0 ? 2 : 0) * SBO, 0u, 0u, 0u, 0u);
-        }
-      }
-    }
-    fence_proxy_async();
-    tc_fence_before();
-    if (__syncthreads_or(timed_out ? 1 : 0)) {
-      if (tid == 0) atomicExch(err, 1);
-      s_fail = 1;
-      active = false;
-      break;
-    }
-    // this round's K-blocks per accumulator (computed identically by all threads)
-    int maxchain = 0;
-    for (int bb = 0; bb < ROUND; ++bb) {
-      const int k = r * ROUND + bb;
-      if (k >= NB) break;
-      int q = 0;
-      for (int qq = 1; qq < 4; ++qq)
-        if (k >= s_blk[qq]) q = qq;
-      if (tid == 0) {
-        if (bb == 0) tc_fence_after();
-        const uint64_t ad = make_desc(smem_u32(stA + bb * A_BYTES), A_LBO, SBO);
-        const uint64_t bd = make_desc(smem_u32(stB + bb * B_BYTES), B_LBO, SBO);
-        mma_f16(tmem + uint32_t(64 * q), ad, bd, ((fresh >> q) & 1u) ? 0u : 1u);
-        fresh &= ~(1u << q);
-        s_dirty[q] = 1;
-      }
-      chains += 1u << (8 * q);
-      maxchain = max(maxchain, int((chains >> (8 * q)) & 0xFFu));
-    }
-    if (tid == 0) mma_commit(&bars[s]);
-    // bound the tensor-core accumulation chains: drain into the FP32 planes
-    if (maxchain >= DRAIN_AT && r != nrounds - 1) {
-      const bool to2 = !mbar_wait(&bars[s], uint32_t((r >> 1) & 1));
-      tc_fence_before();
-      if (__syncthreads_or(to2 ? 1 : 0)) {
-        if (tid == 0) atomicExch(err, 1);
-        s_fail = 1;
-        active = false;
+      const int s = r % NST;
+      if (r >= NST &&
+          !mbar_wait(&empty_bar[s], uint32_t((r / NST - 1) & 1), abortp, err))
         break;
+      if (np > 0) {
+        unsigned char *stA = stages + s * STAGE_BYTES;
+        const int c0 = off >> 3;   // 0 or 1: taps in chunks c0, c0+1 of the part
+        const int cz = (c0 == 0) ? 2 : 0;
+        uint32_t base, pstep;
+        if (grp < 2) {
+          // A column of point e: part p (rows 24p..24p+23); group g owns
+          // parts g (hi) and g+2 (lo)
+          base = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO +
+                 uint32_t(grp * PART) * SBO;
+          pstep = uint32_t(2 * PART) * SBO;
+        } else {
+          // B row of point e: part h columns 24h..24h+23
+          base = smem_u32(stA + ROUND * A_BYTES + kbl * B_BYTES) + (e & 7) * 16 +
+                 (e >> 3) * B_LBO;
+          pstep = uint32_t(PART) * SBO;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t pb = base + uint32_t(h) * pstep;
+          if (valid) {
+            uint32_t z[8];
+            place8(hw[h], off & 7, z);
+            st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
+            st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
+            st_v4(pb + uint32_t(cz) * SBO, 0u, 0u, 0u, 0u);
+          } else {
+            st_v4(pb, 0u, 0u, 0u, 0u);
+            st_v4(pb + SBO, 0u, 0u, 0u, 0u);
+            st_v4(pb + 2 * SBO, 0u, 0u, 0u, 0u);
+          }
+        }
       }
-      tc_fence_after();
-      if (warp < 4) tc_drain<W>(tmem, warp, lane, s_dirty, tre, tim, P, unscale);
-      tc_fence_before();
-      __syncthreads();
-      if (tid == 0) {
-        fresh = 0xFu;
-        for (int q = 0; q < 4; ++q) s_dirty[q] = 0;
+      fence_proxy_async();
+      mbar_arrive(&full_bar[s]);
+    }
+  } else if (warp >= MMA_W0) {
+    // ------------------------------------------------------------ MMA issue
+    // Warp 4+q issues every MMA into quadrant q's accumulators (so MMAs into
+    // one accumulator keep their order), four issuers in parallel.  Event k of
+    // quadrant q (one per sub-chunk) uses tensor-memory buffer k & 1.
+    const int q = warp - MMA_W0;
+    if (lane == 0) {
+      uint32_t k = 0;          // events sent
+      bool waited = true;      // buffer k & 1 released by the epilogue
+      bool fresh = true, dirty = false;
+      bool failed = false;
+      auto acquire = [&]() -> bool {
+        if (waited) return true;
+        if (!mbar_wait(&acc_empty[q][k & 1], ((k >> 1) - 1) & 1u, abortp, err)) return false;
+        tc_fence_after();
+        waited = true;
+        return true;
+      };
+      for (int r = 0; r < nrounds && !failed; ++r) {
+        // the builders waited for the point-data slot before completing
+        // full_bar, so its records are visible once full_bar is
+        const int ps = r % NPRE;
+        const KRec *src = reinterpret_cast<const KRec *>(pre + ps * PL_::BYTES + PL_::REC);
+        const int s = r % NST;
+        if (!mbar_wait(&full_bar[s], uint32_t((r / NST) & 1), abortp, err)) break;
+        tc_fence_after();
+        const uint32_t sA_ = smem_u32(stages + s * STAGE_BYTES);
+        const uint32_t plan =
+            reinterpret_cast<const uint32_t *>(pre + ps * PL_::BYTES + PL_::PLAN)[q];
+        uint32_t todo = (plan | (plan >> 8)) & 0xFFu;
+        while (todo) {
+          const int b = __ffs(todo) - 1;
+          todo &= todo - 1;
+          if (!acquire()) {
+            failed = true;
+            break;
+          }
+          const uint32_t buf = k & 1;
+          if ((plan >> b) & 1u) {
+            const uint64_t ad = make_desc(sA_ + uint32_t(b * A_BYTES), A_LBO, SBO);
+            const uint64_t bd =
+                make_desc(sA_ + uint32_t(ROUND * A_BYTES + b * B_BYTES), B_LBO, SBO);
+            mma_f16(tmem + uint32_t(128 * q + 64 * buf), ad, bd, fresh ? 0u : 1u);
+            fresh = false;
+            dirty = true;
+          }
+          if ((plan >> (8 + b)) & 1u) {
+            acc_info[q][buf] = make_uint2(dirty ? 1u : 0u, src[b].meta >> TILE_SHIFT_META);
+            mma_commit(&acc_full[q][buf]);
+            mbar_arrive(&acc_full[q][buf]);
+            ++k;
+            waited = (k < 2);
+            fresh = true;
+            dirty = false;
+          }
+        }
+        mma_commit(&empty_bar[s]);
+        mbar_arrive(&pre_empty[ps]);   // records read: release the point-data slot
       }
-      chains = 0;
+      // exit record (after the epilogue released the buffer)
+      if (*abortp || acquire()) {
+        acc_info[q][k & 1] = make_uint2(2u, 0u);
+        mma_commit(&acc_full[q][k & 1]);
+        mbar_arrive(&acc_full[q][k & 1]);
+      }
+      // every MMA of this CTA has completed before tensor memory is released
+      mma_commit(&done_bar);
+      mbar_wait(&done_bar, 0u, abortp, err);
     }
-    xc = xn;
-    scc = scn;
-    qc = qn;
-    vc = vn;
-  }
-
-  // ---- wait for the last round's MMAs (a commit covers all earlier ones)
-  if (active) {
-    const int last = nrounds - 1;
-    if (!mbar_wait(&bars[last & 1], uint32_t((last >> 1) & 1))) {
-      atomicExch(err, 1);
-      s_fail = 1;
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (s_fail) active = false;
-
-  // ---- epilogue: remaining accumulators into the planes, then the grid
-  if (active) {
-    if (warp < 4) tc_drain<W>(tmem, warp, lane, s_dirty, tre, tim, P, unscale);
-    __syncthreads();
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    // One event per quadrant per sub-chunk, taken in quadrant order: the
+    // accumulators are added into the FP32 planes (part p of tensor-memory
+    // lane L = 24p + u is row u of plane p), then the sub-chunk's planes are
+    // added to the grid and zeroed.
+    const int L = tid;                   // tensor-memory lane 0..127
+    const int p = L / 24, u = L - 24 * (L / 24);
+    float *plane = planes + (p < 4 ? p : 0) * PLANE_FLOATS;
+    const int S = 32 + W;
     const int nu = int(g.nover[0]), nv = int(g.nover[1]);
-    for (int c = tid; c < S * S; c += NT) {
-      const int a = c / S, bcol = c - (c / S) * S;
-      const float2 v = make_float2(tre[a * P + bcol], tim[a * P + bcol]);
-      if (v.x == 0.f && v.y == 0.f) continue;
-      int gu = b0[0] + a, gv = b0[1] + bcol;
-      gu += (gu < 0) ? nu : ((gu >= nu) ? -nu : 0);
-      gv += (gv < 0) ? nv : ((gv >= nv) ? -nv : 0);
-      atomicAdd(grid + int64_t(gu) * nv + gv, v);
+    for (uint32_t k = 0;; ++k) {
+      const uint32_t buf = k & 1, par = (k >> 1) & 1;
+      // 'stop' (a failed wait or the exit record) is uniform in a warp, and
+      // made uniform across the four warps at each named barrier
+      bool stop = false;
+      uint32_t tile = 0, dq = 0;   // dq: dirty quadrants
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {
+        // rows 16..23 are shared by both halves of the quadrants
+        if (q == 2 && named_bar_or(1, 32 * N_EPI, stop)) stop = true;
+        if (stop) continue;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[q][buf], par, abortp, err));
+        if (!ok) {
+          stop = true;
+          continue;
+        }
+        tc_fence_after();
+        const uint2 info = acc_info[q][buf];
+        if (info.x & 2u) {
+          stop = true;
+          continue;
+        }
+        tile = info.y;
+        dq |= (info.x & 1u) << q;
+        if (info.x & 1u) {
+          uint32_t d0[16], d1[16], d2[16];
+          const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(128 * q + 64 * buf);
+          tmem_ld16(ta, d0);
+          tmem_ld16(ta + 16, d1);
+          tmem_ld16(ta + 32, d2);
+          tmem_wait_ld();
+          if (p < 4) {
+            float *dst = plane + (u + ((q & 2) ? 16 : 0)) * PP + ((q & 1) ? 16 : 0);
+#pragma unroll
+            for (int v = 0; v < 24; ++v) {
+              float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
+              if (p < 2) val += __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
+              dst[v] += val;
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acc_empty[q][buf]);
+      }
+      if (named_bar_or(1, 32 * N_EPI, stop)) break;
+      // sub-chunk complete: planes -> grid, and zero them for the next one
+      const int tu = int(tile) / ntv, tv = int(tile) - tu * ntv;
+      const int b0u = (tu << 5) - g.nsafe, b0v = (tv << 5) - g.nsafe;
+      // only the windows of the dirty quadrants hold data: their bounding box
+      const int r0 = (dq & 3u) ? 0 : 16, r1 = min((dq & 12u) ? 40 : 24, S);
+      const int c0 = (dq & 5u) ? 0 : 16, c1 = min((dq & 10u) ? 40 : 24, S);
+      // thread -> one column of the box and every nph-th row: the column's
+      // wrapped index once, rows wrapped incrementally, no divisions per cell
+      const int bw = c1 - c0, nph = (32 * N_EPI) / bw;
+      if (L < nph * bw) {
+        const int col = c0 + L % bw;
+        const int gv = wrapi(b0v + col, nv);
+        int a = r0 + L / bw;
+        int gu = wrapi(b0u + a, nu);
+#pragma unroll 4
+        for (; a < r1; a += nph) {
+          const int o = a * PP + col;
+          const float re = planes[o] + planes[2 * PLANE_FLOATS + o];
+          const float im = planes[PLANE_FLOATS + o] + planes[3 * PLANE_FLOATS + o];
+          planes[o] = 0.f;
+          planes[PLANE_FLOATS + o] = 0.f;
+          planes[2 * PLANE_FLOATS + o] = 0.f;
+          planes[3 * PLANE_FLOATS + o] = 0.f;
+          if (re != 0.f || im != 0.f)
+            atomicAdd(grid + int64_t(gu) * nv + gv, make_float2(re * unscale, im * unscale));
+          gu += nph;
+          gu -= (gu >= nu) ? nu : 0;
+        }
+      }
+      named_bar(1, 32 * N_EPI);
     }
   }
+
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == MMA_W0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(uint32_t(TMEM_COLS)));
   }
 }
 
-bool spread_tc_supported(const Geometry &g, bool calc_f64) {
-  return !calc_f64 && g.ndim == 2 && g.log2tile == 5 && g.W <= 8;
+// ---------------------------------------------------------------- K-block lists
+// A chunk (consecutive sorted points of one tile, ordered by quadrant) is cut
+// into sub-chunks with at most DRAIN_AT K-blocks per quadrant, which bounds
+// every tensor-core accumulation chain; a sub-chunk is one accumulator event
+// per quadrant and one flush of the tile planes.  Inside a sub-chunk the
+// records take the quadrants in turn, so the four MMA issuers share each round.
+__device__ __forceinline__ void tc_chunk_bounds(const uint32_t *__restrict__ skeys, const Chunk &ch,
+                                                uint32_t (&b)[5]) {
+  b[0] = ch.start;
+  b[4] = ch.start + ch.count;
+  for (uint32_t q = 1; q < 4; ++q) {
+    uint32_t lo = b[q - 1], hi = b[4];
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if ((skeys[mid] & 3u) < q) lo = mid + 1;
+      else hi = mid;
+    }
+    b[q] = lo;
+  }
 }
 
-void launch_spread_tc(const PointsDesc &pts, const uint32_t *skeys, const ChunkList &cl,
-                      const Geometry &g, const KernelPoly<float> &kp, const void *values,
-                      int64_t vs, void *grid, unsigned *absmax, int *err, cudaStream_t st) {
-  if (cl.nchunks == 0) return;
+__device__ __forceinline__ uint32_t tc_subchunks(const uint32_t (&kq)[4]) {
+  uint32_t m = 0;
+  for (int q = 0; q < 4; ++q) m = max(m, (kq[q] + tc::DRAIN_AT - 1) / tc::DRAIN_AT);
+  return max(m, 1u);
+}
+
+// Per chunk: the first sorted index of quadrants 1..3 (binary search on the
+// quadrant bits of the sorted keys) and the number of records.
+__global__ void k_tc_count(const uint32_t *__restrict__ skeys, const Chunk *__restrict__ chunks,
+                           uint32_t nch, uint4 *__restrict__ qb, uint32_t *__restrict__ nrec,
+                           uint32_t *__restrict__ cost) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  const Chunk ch = chunks[c];
+  uint32_t b[5];
+  tc_chunk_bounds(skeys, ch, b);
+  uint32_t kq[4];
+  for (int q = 0; q < 4; ++q) kq[q] = (b[q + 1] - b[q] + tc::KB - 1) / tc::KB;
+  const uint32_t S = tc_subchunks(kq);
+  uint32_t n = 0;
+  for (uint32_t j = 0; j < S; ++j)
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t done = j * tc::DRAIN_AT;
+      const uint32_t m = kq[q] > done ? min(kq[q] - done, uint32_t(tc::DRAIN_AT)) : 0u;
+      n += max(m, 1u);
+    }
+  qb[c] = make_uint4(b[1], b[2], b[3], b[4]);
+  nrec[c] = n;
+  cost[c] = n + tc::FLUSH_COST * S;
+}
+
+__global__ void k_tc_emit(const Chunk *__restrict__ chunks, const uint4 *__restrict__ qb,
+                          const uint32_t *__restrict__ kbpos, uint32_t nch,
+                          uint2 *__restrict__ kblk) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  const Chunk ch = chunks[c];
+  const uint4 q4 = qb[c];
+  const uint32_t b[5] = {ch.start, q4.x, q4.y, q4.z, q4.w};
+  uint32_t kq[4];
+  for (int q = 0; q < 4; ++q) kq[q] = (b[q + 1] - b[q] + tc::KB - 1) / tc::KB;
+  const uint32_t S = tc_subchunks(kq);
+  const uint32_t tbits = ch.tile << tc::TILE_SHIFT_META;
+  uint32_t k = kbpos[c];
+  for (uint32_t j = 0; j < S; ++j) {
+    uint32_t m[4], cnt[4], mx = 0;
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t done = j * tc::DRAIN_AT;
+      m[q] = kq[q] > done ? min(kq[q] - done, uint32_t(tc::DRAIN_AT)) : 0u;
+      cnt[q] = max(m[q], 1u);
+      mx = max(mx, cnt[q]);
+    }
+    for (uint32_t i = 0; i < mx; ++i)
+      for (uint32_t q = 0; q < 4; ++q) {
+        if (i >= cnt[q]) continue;
+        const uint32_t last = (i + 1 == cnt[q]) ? tc::META_LAST : 0u;
+        if (m[q] == 0) {
+          kblk[k++] = make_uint2(0u, (q << 5) | last | tbits);   // empty quadrant
+        } else {
+          const uint32_t st = b[q] + (j * tc::DRAIN_AT + i) * tc::KB;
+          const uint32_t np = min(uint32_t(tc::KB), b[q + 1] - st);
+          kblk[k++] = make_uint2(st, np | (q << 5) | last | tbits);
+        }
+      }
+  }
+}
+
+// CTA b takes records [range[b], range[b+1]), cut at chunk starts so that the
+// CTAs get about equal estimated cost (records + FLUSH_COST per sub-chunk).
+__global__ void k_tc_ranges(const uint32_t *__restrict__ kbpos, const uint32_t *__restrict__ cpos,
+                            uint32_t nch, uint32_t total, uint32_t ctotal, uint32_t groups,
+                            uint32_t *__restrict__ range) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > groups) return;
+  if (b == groups || b == 0) {
+    range[b] = (b == 0) ? 0u : total;
+    return;
+  }
+  const uint32_t target = uint32_t((uint64_t(b) * ctotal) / groups);
+  uint32_t lo = 0, hi = nch;   // first chunk with cost prefix >= target
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (cpos[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  range[b] = (lo < nch) ? kbpos[lo] : total;
+}
+
+size_t tc_kblock_workspace_bytes(uint32_t nch) {
+  return size_t(nch) * (sizeof(uint4) + 4 * sizeof(uint32_t)) + scan_workspace_bytes(nch) + 1024;
+}
+
+uint32_t tc_kblock_upper_bound(uint32_t npts, uint32_t nch) {
+  // per chunk of n points: K-blocks <= n/16 + 4, sub-chunks S <= (n/16 + 1)/24 + 1,
+  // and at most 4 empty records per sub-chunk
+  return npts / tc::KB + npts / (tc::KB * tc::DRAIN_AT) * 4 + 9 * nch + 16;
+}
+
+uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t groups, void *ws,
+                          uint2 *kblk, uint32_t *range, uint32_t *d_total, cudaStream_t st) {
+  const uint32_t nch = cl.nchunks;
+  DN_REQUIRE(nch > 0, ST_INTERNAL, "no chunks");
+  uint4 *qb = static_cast<uint4 *>(ws);
+  uint32_t *nrec = reinterpret_cast<uint32_t *>(qb + nch);
+  uint32_t *pos = nrec + nch;
+  uint32_t *cost = pos + nch;
+  uint32_t *cpos = cost + nch;
+  uint32_t *sws = reinterpret_cast<uint32_t *>(
+      (reinterpret_cast<uintptr_t>(cpos + nch) + 255) & ~uintptr_t(255));
+  const unsigned gb = (nch + 255) / 256;
+  k_tc_count<<<gb, 256, 0, st>>>(skeys, cl.chunks, nch, qb, nrec, cost);
+  DN_LAUNCHED();
+  exclusive_scan(nrec, pos, nch, sws, st);
+  exclusive_scan(cost, cpos, nch, sws, st);
+  k_tc_emit<<<gb, 256, 0, st>>>(cl.chunks, qb, pos, nch, kblk);
+  DN_LAUNCHED();
+  uint32_t h[4] = {0u, 0u, 0u, 0u};
+  DN_CUDA(cudaMemcpyAsync(&h[0], pos + nch - 1, 4, cudaMemcpyDeviceToHost, st));
+  DN_CUDA(cudaMemcpyAsync(&h[1], nrec + nch - 1, 4, cudaMemcpyDeviceToHost, st));
+  DN_CUDA(cudaMemcpyAsync(&h[2], cpos + nch - 1, 4, cudaMemcpyDeviceToHost, st));
+  DN_CUDA(cudaMemcpyAsync(&h[3], cost + nch - 1, 4, cudaMemcpyDeviceToHost, st));
+  DN_CUDA(cudaStreamSynchronize(st));
+  const uint32_t total = h[0] + h[1], ctotal = h[2] + h[3];
+  k_tc_ranges<<<(groups + 1 + 255) / 256, 256, 0, st>>>(pos, cpos, nch, total, ctotal, groups,
+                                                         range);
+  DN_LAUNCHED();
+  (void)d_total;
+  return total;
+}
+
+bool spread_tc_supported(const Geometry &g, bool calc_f64) {
+  return !calc_f64 && g.ndim == 2 && g.log2tile == 5 && g.W <= 8 &&
+         uint64_t(g.ntiles[0]) * uint64_t(g.ntiles[1]) < uint64_t(tc::MAX_TILES);
+}
+
+void launch_spread_tc(const PointsDesc &pts, const TcBlocks &tb, const Geometry &g,
+                      const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
+                      unsigned *absmax, int *err, cudaStream_t st) {
+  if (tb.groups == 0 || tb.total == 0) return;
   DN_REQUIRE(spread_tc_supported(g, false), ST_UNSUPPORTED,
              "tensor-core spreader: 2D single precision with support <= 8 only");
   DN_CUDA(cudaMemsetAsync(absmax, 0, sizeof(unsigned), st));
@@ -519,11 +871,11 @@ void launch_spread_tc(const PointsDesc &pts, const uint32_t *skeys, const ChunkL
 #define DN_TC(TC, WW)                                                                           \
   {                                                                                             \
     auto kern = k_spread_tc<TC, WW>;                                                            \
-    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
-                                 tc::SMEM_BYTES));                                              \
-    kern<<<cl.nchunks, TC_GROUPS * tc::THREADS, tc::SMEM_BYTES, st>>>(                                  \
-        pts, skeys, cl.chunks, g, kp, static_cast<const float2 *>(values), vs, absmax,          \
-        static_cast<float2 *>(grid), err);                                                      \
+    constexpr int smem = tc::smem_bytes<TC>();                                                  \
+    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));     \
+    kern<<<tb.groups, tc::THREADS, smem, st>>>(pts, tb.kblk, tb.range, g, kp,                   \
+                                               static_cast<const float2 *>(values), vs, absmax, \
+                                               static_cast<float2 *>(grid), err);               \
     DN_LAUNCHED();                                                                              \
     return;                                                                                     \
   }

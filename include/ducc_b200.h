@@ -131,6 +131,21 @@ int dnufft_plan_nu2u(dnufft_plan *plan, int forward, int verbosity,
 int dnufft_plan_u2nu(dnufft_plan *plan, int forward, int verbosity,
                      const dnufft_array *grid, dnufft_array *out, void *stream);
 
+/* Coordinate gradient of a type-2 transform (no counterpart in DUCC; it serves
+ * differentiation with respect to the points):
+ *   grad[j][d] = Re( conj(weights[j]) * d/dcoord[j][d] u2nu(grid, coord, forward)[j] )
+ * computed by interpolating the transformed grid with the derivative of the
+ * kernel.  weights: (M,) of the grid's dtype; grad: (M, ndim) real, the dtype
+ * of the coordinates.  With weights = dL/d(u2nu result) this is the
+ * coordinate part of the type-2 vector-Jacobian product; the type-1 one is
+ * grad[j][d] = Re(conj(points[j]) * d/dcoord u2nu(cotangent, coord, !forward)[j]),
+ * i.e. this call with grid = the cotangent and weights = the points. */
+int dnufft_u2nu_dcoord(const dnufft_array *grid, const dnufft_array *coord, int forward,
+                       double epsilon, const dnufft_array *weights, dnufft_array *grad,
+                       const dnufft_opts *opts, void *stream);
+int dnufft_plan_u2nu_dcoord(dnufft_plan *plan, int forward, const dnufft_array *grid,
+                            const dnufft_array *weights, dnufft_array *grad, void *stream);
+
 /* Replaces plan destruction (Julia nufft_delete_plan, julia/ducc_julia.cc:372-392). */
 int dnufft_plan_destroy(dnufft_plan *plan);
 

@@ -92,3 +92,19 @@ def test_tc_plan_permutation_is_duccs():
         assert O.l2error(r, g["nu2u"]) < float(g["eps"])
         r2 = p.u2nu(grid=g["grid_in"], forward=bool(g["forward"]))
         assert O.l2error(r2, g["u2nu"]) < float(g["eps"])
+
+
+def test_tc_one_tile_long_accumulation_chains():
+    """Every point in one tile quadrant: 4096-point chunks with 256 K-blocks
+    into one accumulator, so the chain bound (drain into FP32 shared memory)
+    is what keeps the error at the plain spreader's level."""
+    rng = np.random.default_rng(9)
+    M, shape = 300000, (64, 64)
+    coord = (0.3 + 1e-3 * rng.standard_normal((M, 2))).astype(np.float32)
+    vals = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)
+    a = run("tc", coord, vals, shape, 1e-6)
+    b = run("plain", coord, vals, shape, 1e-6)
+    p = O.Params(shape, 1e-6, True, M, True, 1)
+    ref = O.nu2u(p, coord, vals, True)
+    ea, eb = O.l2error(a, ref), O.l2error(b, ref)
+    assert ea < 3 * eb + 5e-7, (ea, eb)
