@@ -47,7 +47,8 @@ EXPORTS = [
     "dnufft_plan_create", "dnufft_plan_nu2u", "dnufft_plan_u2nu", "dnufft_plan_destroy",
     "dnufft_plan_get_info", "dnufft_plan_get_permutation", "dnufft_last_error",
     "dnufft_kernel_launches", "dnufft_profile_enable", "dnufft_profile_json",
-    "dnufft_nu2u_noalloc", "dnufft_noalloc_scratch_bytes",
+    "dnufft_nu2u_noalloc", "dnufft_noalloc_scratch_bytes", "dnufft_u2nu_dcoord",
+    "dnufft_plan_u2nu_dcoord",
 ]
 
 
@@ -73,6 +74,9 @@ def lib():
                                      ctypes.c_double, P(Opts), vp, P(vp)]
     for f in (L.dnufft_plan_nu2u, L.dnufft_plan_u2nu):
         f.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(Array), P(Array), vp]
+    L.dnufft_u2nu_dcoord.argtypes = [P(Array), P(Array), ctypes.c_int, ctypes.c_double, P(Array),
+                                     P(Array), P(Opts), vp]
+    L.dnufft_plan_u2nu_dcoord.argtypes = [vp, ctypes.c_int, P(Array), P(Array), P(Array), vp]
     L.dnufft_plan_destroy.argtypes = [vp]
     L.dnufft_plan_get_info.argtypes = [vp, P(PlanInfo)]
     L.dnufft_plan_get_permutation.argtypes = [vp, P(ctypes.c_uint32), vp]

@@ -74,7 +74,7 @@ constexpr int TMEM_COLS = 512;     // quadrant q, buffer b at column 128*q + 64*
 constexpr int PL = 40, PP = 41;    // FP32 plane rows, odd pitch
 constexpr int PLANE_FLOATS = PL * PP;
 constexpr int DRAIN_AT = 24;       // K-blocks per quadrant per sub-chunk (chain bound)
-constexpr uint32_t FLUSH_COST = 4; // CTA balancing: one sub-chunk flush ~ this many records
+constexpr uint32_t FLUSH_COST = 16;  // CTA balancing: one sub-chunk flush ~ this many records
 
 // warp roles
 constexpr int EPI_W0 = 0, N_EPI = 4;     // warps 0..3: tensor-memory lane quarters 0..3

@@ -16,7 +16,9 @@ precision, as in DUCC.  ``nthreads`` only feeds DUCC's parameter cost model, so
 the same (kernel, oversampled size) is chosen as DUCC would choose.
 
 Extensions beyond DUCC's signature (keyword-only, optional): ``spreader``
-('auto' | 'plain' | 'tc') and ``stream`` (a CUDA stream handle).
+('auto' | 'plain' | 'tc') and ``stream`` (a CUDA stream handle), and the
+coordinate-gradient transform ``u2nu_dcoord`` (function and plan method) used
+by ``ducc_b200.autograd``.
 """
 import ctypes
 import math
@@ -25,7 +27,7 @@ import numpy as np
 
 from . import _capi as C
 
-__all__ = ["nu2u", "u2nu", "bestEpsilon", "plan"]
+__all__ = ["nu2u", "u2nu", "u2nu_dcoord", "bestEpsilon", "plan"]
 
 
 def _np_complex_for(code):
@@ -112,6 +114,36 @@ def u2nu(*, grid, coord, forward, epsilon, nthreads=1, out=None, verbosity=0,
     return op.finish()
 
 
+def _dcoord_out(coord, out):
+    if out is not None:
+        return out
+    if C.is_torch(coord):
+        import torch
+        return torch.empty(tuple(coord.shape), dtype=coord.dtype, device=coord.device)
+    return np.empty(coord.shape, dtype=np.asarray(coord).dtype)
+
+
+def u2nu_dcoord(*, grid, coord, forward, epsilon, weights, nthreads=1, out=None,
+                sigma_min=1.2, sigma_max=2.51, periodicity=2 * math.pi, fft_order=False,
+                stream=None):
+    """Coordinate gradient of the type-2 transform contracted with ``weights``:
+    ``out[j, d] = Re(conj(weights[j]) * d/dcoord[j, d] u2nu(grid, coord)[j])``
+    (real, the coordinates' dtype).  No counterpart in DUCC."""
+    grid = _prepare_in(grid)
+    coord = _prepare_in(coord)
+    weights = _prepare_in(weights)
+    _check_types(grid, coord)
+    op = _OutProxy(_dcoord_out(coord, out))
+    ndim = len(grid.shape)
+    o = C.make_opts(False, nthreads, sigma_min, sigma_max, periodicity, fft_order, 0, "auto", ndim)
+    a_g, a_c, a_w, a_o = C.describe(grid), C.describe(coord), C.describe(weights), C.describe(op.buf)
+    C.check(C.lib().dnufft_u2nu_dcoord(ctypes.byref(a_g), ctypes.byref(a_c), 1 if forward else 0,
+                                       float(epsilon), ctypes.byref(a_w), ctypes.byref(a_o),
+                                       ctypes.byref(o),
+                                       C.stream_of(grid, coord, weights, op.buf, stream=stream)))
+    return op.finish()
+
+
 def bestEpsilon(*, ndim, singleprec, sigma_min=1.1, sigma_max=2.6):
     """Smallest achievable epsilon for the given dimensionality / precision."""
     r = ctypes.c_double()
@@ -191,6 +223,27 @@ class plan:
         return op.finish()
 
     # -- B200 extras
+    def u2nu_dcoord(self, *, forward, grid, weights, out=None, stream=None):
+        """Coordinate gradient of this plan's type-2 transform contracted with
+        ``weights`` (see the module-level ``u2nu_dcoord``)."""
+        grid = _prepare_in(grid)
+        weights = _prepare_in(weights)
+        if out is None:
+            ct = np.float64 if self._f64 else np.float32
+            if C.is_torch(grid):
+                import torch
+                out = torch.empty((self.npoints, len(self.grid_shape)),
+                                  dtype=torch.float64 if self._f64 else torch.float32,
+                                  device=grid.device)
+            else:
+                out = np.empty((self.npoints, len(self.grid_shape)), dtype=ct)
+        op = _OutProxy(out)
+        a_g, a_w, a_o = C.describe(grid), C.describe(weights), C.describe(op.buf)
+        C.check(C.lib().dnufft_plan_u2nu_dcoord(self._ptr, 1 if forward else 0, ctypes.byref(a_g),
+                                                ctypes.byref(a_w), ctypes.byref(a_o),
+                                                C.stream_of(grid, weights, op.buf, stream=stream)))
+        return op.finish()
+
     def info(self):
         """Kernel support, oversampled sizes etc. of this plan."""
         inf = C.PlanInfo()

@@ -495,6 +495,40 @@ def direct_u2nu(uniform, coord, forward, periodicity=2 * math.pi, fft_order=Fals
     return out
 
 
+def direct_u2nu_dcoord(uniform, coord, forward, weights, periodicity=2 * math.pi,
+                       fft_order=False, chunk=2048):
+    """FP64 direct coordinate gradient of the type-2 transform, contracted with
+    weights: out[j, d] = Re(conj(w_j) * d/dx_{j,d} sum_k u_k exp(s i K.x_j)),
+    K_d = k_d 2 pi / period_d.  DUCC has no counterpart; this is the derivative
+    of direct_u2nu, used to pin the library's derivative-kernel gradients."""
+    uniform = np.asarray(uniform).astype(np.complex128)
+    shape = uniform.shape
+    if fft_order:
+        uniform = np.fft.fftshift(uniform)
+    coord = np.asarray(coord, dtype=np.float64)
+    w = np.asarray(weights).astype(np.complex128)
+    ndim = len(shape)
+    if np.ndim(periodicity) == 0:
+        periodicity = [periodicity] * ndim
+    isign = -1 if forward else 1
+    ks = [(-(s // 2) + np.arange(s)) * (2 * math.pi / per) for s, per in zip(shape, periodicity)]
+    out = np.zeros(coord.shape, dtype=np.float64)
+    for lo in range(0, coord.shape[0], chunk):
+        c = coord[lo:lo + chunk]
+        facs = [np.exp(isign * 1j * np.outer(c[:, d], ks[d])) for d in range(ndim)]
+        dfacs = [f * (isign * 1j * ks[d])[None, :] for d, f in enumerate(facs)]
+        for d in range(ndim):
+            fs = [dfacs[e] if e == d else facs[e] for e in range(ndim)]
+            if ndim == 1:
+                v = fs[0] @ uniform
+            elif ndim == 2:
+                v = np.einsum("mi,mj,ij->m", fs[0], fs[1], uniform, optimize=True)
+            else:
+                v = np.einsum("mi,mj,mk,ijk->m", fs[0], fs[1], fs[2], uniform, optimize=True)
+            out[lo:lo + chunk, d] = (np.conj(w[lo:lo + chunk]) * v).real
+    return out
+
+
 def l2error(a, b):
     """sqrt(sum|a-b|^2 / max(sum|a|^2, sum|b|^2)) in long double (misc_pymod.cc:129-185)."""
     a = np.asarray(a).astype(np.clongdouble).ravel()
