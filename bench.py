@@ -4,7 +4,9 @@ Workload (one "step"): on a 4096x4096 grid, M=5e7 points drawn from a mixture
 of 16 Gaussians (sigma 0.3 rad, centres uniform in [-pi,pi)^2, wrapped),
 float32 coordinates, complex64 values N(0,1): a planned nu2u followed by a
 planned u2nu with the same plan (DUCC's ``plan.nu2u`` / ``plan.u2nu``).
-Throughput = points x transforms / time, in Mpts/s.
+Throughput = points x transforms / time, in Mpts/s.  The headline line uses
+the split-precision tensor-core spreader; the plain FP32 atomic spreader is
+timed on the same inputs and reported beside it (``alt_plain``).
 
 Arms
   default            this library on N GPUs (one process per GPU under
@@ -32,6 +34,10 @@ N_SIDE = 4096
 M_POINTS = 50_000_000
 EPS = 1e-6
 METRIC = "NUFFT Mpts/s 2D eps=1e-6: TC split-prec vs plain FP32 spreader, same B200"
+KERNEL_NAMES = {"tc": "k_spread_tc (split-precision tensor-core spreader)",
+                "plain": "k_spread (plain FP32 atomic spreader)",
+                "auto": "k_spread (plain FP32 atomic spreader)"}
+TRAFFIC_PER_LAUNCH = {}   # filled from the ncu captures under profiles/
 
 
 def clustered_coords(rng, m, ncl=16, sigma=0.3):
@@ -296,6 +302,14 @@ def run_ours(args, rank, world, local_rank):
     # (8 B) + permutation (4 B) per point, plus one write of the oversampled grid
     spread_bytes = m * (8 + 8 + 4) + nov[0] * nov[1] * 8
     achieved = spread_bytes / (sp_ms * 1e-3) / 1e9 if sp_ms > 0 else None
+    # DRAM bytes of one spreading launch from ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum), measured on the same kernel at a quarter of the
+    # workload (2048^2 grid, 1.25e7 points: same points per tile) and scaled
+    # by 4, since points and grid cells both scale by 4 (profiles/)
+    traffic = TRAFFIC_PER_LAUNCH.get(head)
+    # tensor pipe: each K-block record is at most one 128x48x16 MMA
+    recs = r["info"].get("tc_records", 0)
+    tc_flops = recs * 2 * 128 * 48 * 16
     cpu = None if args.no_cpu else cpu_baseline_leg(m, n, coord, vals, grid)
     line = {
         "metric": METRIC,
@@ -312,10 +326,14 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs and oversampled grid larger than L2 (no flush needed)",
                    "parallelism": "replicas" if world > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                     "kernel": "k_spread (plain FP32 spreader)", "peak_source": src,
+                     "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                     "kernel": KERNEL_NAMES[head], "peak_source": src,
                      "algorithmic_bytes_per_launch": spread_bytes,
-                     "avg_launch_ms": sp_ms},
+                     "avg_launch_ms": sp_ms,
+                     "tensor": None if not recs else {
+                         "executed_tflops": tc_flops / (sp_ms * 1e-3) / 1e12,
+                         "peak_tflops": bf16, "frac": tc_flops / (sp_ms * 1e-3) / 1e12 / bf16,
+                         "mma_per_launch": recs}},
         "stages_ms": {k: v[0] / max(v[1], 1) for k, v in r["prof"].items()},
         "plan_create_s": r["plan_s"],
         "interp_avg_ms": ip_ms,
@@ -340,7 +358,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--m", type=int, default=M_POINTS)
     ap.add_argument("--n", type=int, default=N_SIDE)
-    ap.add_argument("--spreaders", default="plain")
+    ap.add_argument("--spreaders", default="tc,plain")
     ap.add_argument("--param-threads", type=int, default=8,
                     help="nthreads fed to DUCC's parameter cost model (fixes W / sigma)")
     ap.add_argument("--no-e2e", action="store_true")

@@ -37,7 +37,8 @@ class PlanInfo(ctypes.Structure):
                 ("nuni", ctypes.c_int64 * 3), ("nover", ctypes.c_int64 * 3),
                 ("ofactor", ctypes.c_double), ("beta", ctypes.c_double), ("e0", ctypes.c_double),
                 ("npoints", ctypes.c_int64), ("coord_f64", ctypes.c_int32),
-                ("calc_f64", ctypes.c_int32)]
+                ("calc_f64", ctypes.c_int32), ("nchunks", ctypes.c_int64),
+                ("tc_records", ctypes.c_int64)]
 
 
 _lib = None

@@ -1125,6 +1125,8 @@ int dnufft_plan_get_info(const dnufft_plan *p, dnufft_plan_info *info) {
     info->npoints = p->s.npoints;
     info->coord_f64 = p->s.coord_f64;
     info->calc_f64 = p->s.calc_f64;
+    info->nchunks = p->ix.nchunks;
+    info->tc_records = p->ix.nkblk;
   })
 }
 

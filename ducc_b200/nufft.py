@@ -252,7 +252,8 @@ class plan:
         return {"ndim": nd, "supp": inf.supp, "kernel_index": inf.kernel_index,
                 "log2tile": inf.log2tile, "nuni": list(inf.nuni[:nd]),
                 "nover": list(inf.nover[:nd]), "ofactor": inf.ofactor, "beta": inf.beta,
-                "e0": inf.e0, "npoints": inf.npoints}
+                "e0": inf.e0, "npoints": inf.npoints, "nchunks": inf.nchunks,
+                "tc_records": inf.tc_records}
 
     def permutation(self):
         """The tile-order permutation of the points (DUCC's coord_idx)."""

@@ -83,6 +83,8 @@ typedef struct dnufft_plan_info {
   int64_t npoints;
   int32_t coord_f64;
   int32_t calc_f64;
+  int64_t nchunks;        /* tile chunks of the sorted points                    */
+  int64_t tc_records;     /* tensor-core plans: K-block records (<= 1 MMA each)  */
 } dnufft_plan_info;
 
 /* Fill *opts with the defaults of DUCC's functions (for_plan=0:
