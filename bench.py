@@ -37,7 +37,11 @@ METRIC = "NUFFT Mpts/s 2D eps=1e-6: TC split-prec vs plain FP32 spreader, same B
 KERNEL_NAMES = {"tc": "k_spread_tc (split-precision tensor-core spreader)",
                 "plain": "k_spread (plain FP32 atomic spreader)",
                 "auto": "k_spread (plain FP32 atomic spreader)"}
-TRAFFIC_PER_LAUNCH = {}   # filled from the ncu captures under profiles/
+# DRAM bytes per spreading launch at the full workload: ncu dram__bytes_read.sum
+# + dram__bytes_write.sum of one launch at 2048^2 / M=1.25e7 (the same points per
+# tile), times 4 (profiles/k_spread_*_2048sq_M12.5M.md)
+TRAFFIC_PER_LAUNCH = {"tc": 4 * (905.697280e6 + 120.017664e6),
+                      "plain": 4 * (878.126080e6 + 111.346432e6)}
 
 
 def clustered_coords(rng, m, ncl=16, sigma=0.3):
