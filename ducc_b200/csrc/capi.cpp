@@ -107,7 +107,7 @@ static void check_device_error(int *word, cudaStream_t st) {
   DN_CUDA(cudaStreamSynchronize(st));
   if (h != 0) {
     DN_CUDA(cudaMemsetAsync(word, 0, sizeof(int), st));
-    throw Error(ST_TIMEOUT, "a bounded device-side wait gave up (tensor-core spreader)");
+    throw Error(ST_TIMEOUT, "a bounded device-side wait gave up (tensor-core spreader or FFT)");
   }
 }
 
@@ -505,7 +505,7 @@ template <typename T>
 static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
                           const ChunkList &cl, const TcBlocks *tb, const View &points,
                           const View &out, bool forward, bool fft_order, StageTimer &tm,
-                          cudaStream_t st, DevBuf *ws = nullptr) {
+                          cudaStream_t st, DevBuf *ws = nullptr, DevBuf *wk = nullptr) {
   size_t cells = grid_cells(s.g);
   tm.mark("zeroing grid");
   DevBuf local;
@@ -525,53 +525,73 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
     DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
                "tensor-core spreader: single precision (complex64) only");
   }
+  int *err = device_error_word();
   if (use_tc) {
-    int *err = device_error_word();
     launch_spread_tc(pts, *tb, s.g, s.kpf, points.data, points.stride[0], grid.p,
                      reinterpret_cast<unsigned *>(err + 1), err, st);
-    check_device_error(err, st);
   } else {
     launch_spread<T>(pts, cl, s.g, kp, points.data, points.stride[0], 0, grid.p, 0, 1, st);
   }
   tm.mark("FFT + correction");
-  fft_nu2u_tail<T>(grid.p, s.g, dc.ax, forward, dc.cf, fft_order, out.data, out.stride, st);
+  DevBuf localw;
+  DevBuf &work = wk ? *wk : localw;
+  const size_t wb = fft_work_bytes(s.g, sizeof(T) * 2);
+  if (wb && !work.p) work = DevBuf(wb, st);
+  fft_nu2u_tail<T>(grid.p, s.g, dc.ax, forward, dc.cf, fft_order, out.data, out.stride, st,
+                   work.p, err);
   tm.mark("end");
+  check_device_error(err, st);
 }
 
 template <typename T>
 static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &pts,
                           const ChunkList &cl, const View &uni, const View &out, bool forward,
-                          bool fft_order, StageTimer &tm, cudaStream_t st, DevBuf *ws = nullptr) {
+                          bool fft_order, StageTimer &tm, cudaStream_t st, DevBuf *ws = nullptr,
+                          DevBuf *wk = nullptr) {
   size_t cells = grid_cells(s.g);
   DevBuf local;
   DevBuf &grid = ws ? *ws : local;
   if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
+  DevBuf localw;
+  DevBuf &work = wk ? *wk : localw;
+  const size_t wb = fft_work_bytes(s.g, sizeof(T) * 2);
+  if (wb && !work.p) work = DevBuf(wb, st);
+  int *err = device_error_word();
   tm.mark("correction + FFT");
-  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st);
+  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st,
+                   work.p, err);
   tm.mark("interpolation");
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
   launch_interp<T>(pts, cl, s.g, kp, grid.p, 0, out.data, out.stride[0], 0, 1, st);
   tm.mark("end");
+  check_device_error(err, st);
 }
 
 template <typename T>
 static void do_fft_dcoord(const Setup &s, const DevConst &dc, const PointsDesc &pts,
                           const ChunkList &cl, const View &uni, const View &wts,
                           const View &grad, bool forward, bool fft_order, StageTimer &tm,
-                          cudaStream_t st, DevBuf *ws = nullptr) {
+                          cudaStream_t st, DevBuf *ws = nullptr, DevBuf *wk = nullptr) {
   size_t cells = grid_cells(s.g);
   DevBuf local;
   DevBuf &grid = ws ? *ws : local;
   if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
+  DevBuf localw;
+  DevBuf &work = wk ? *wk : localw;
+  const size_t wb = fft_work_bytes(s.g, sizeof(T) * 2);
+  if (wb && !work.p) work = DevBuf(wb, st);
+  int *err = device_error_word();
   tm.mark("correction + FFT");
-  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st);
+  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st,
+                   work.p, err);
   tm.mark("derivative interpolation");
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
   launch_interp_dcoord<T>(pts, cl, s.g, kp, grid.p, wts.data, wts.stride[0], grad.data,
                           grad.stride[0], grad.stride[1], st);
   tm.mark("end");
+  check_device_error(err, st);
 }
 
 static void check_dcoord_args(const View &wts, const View &grad, int cdt, int coord_dt,
@@ -733,6 +753,7 @@ struct dnufft_plan {
   dnufft::Index ix;
   dnufft::DevBuf sorted_coord;
   dnufft::DevBuf grid;   // oversampled grid, allocated on first execution
+  dnufft::DevBuf work;   // FFT column-pass scratch (2D), allocated on first execution
   dnufft_opts o;
   int device = 0;
 };
@@ -797,6 +818,8 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
   if (!p->grid.p) {
     // allocated once, on first use, and made visible to every stream
     p->grid = DevBuf(grid_cells(s.g) * (f64 ? 16 : 8), st);
+    const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
+    if (wb) p->work = DevBuf(wb, st);
     DN_CUDA(cudaStreamSynchronize(st));
   }
   PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
@@ -806,12 +829,12 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
   if (type1) {
     const TcBlocks tb = p->ix.tc();
     const TcBlocks *sk = s.qbits ? &tb : nullptr;
-    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
-    else do_spread_fft<float>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
+    if (f64) do_spread_fft<double>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid, &p->work);
+    else do_spread_fft<float>(s, p->dc, pts, cl, sk, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid, &p->work);
     tm.report("nu2u (planned)");
   } else {
-    if (f64) do_fft_interp<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
-    else do_fft_interp<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid);
+    if (f64) do_fft_interp<double>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid, &p->work);
+    else do_fft_interp<float>(s, p->dc, pts, cl, si.dev, so.dev, forward != 0, fo, tm, st, &p->grid, &p->work);
     tm.report("u2nu (planned)");
   }
   so.finish();
@@ -836,14 +859,16 @@ static void plan_dcoord_impl(dnufft_plan *p, int forward, const dnufft_array *gr
   Staged su(uni, true, false, st), sw(wts, true, false, st), sg(grad, false, true, st);
   if (!p->grid.p) {
     p->grid = DevBuf(grid_cells(s.g) * (f64 ? 16 : 8), st);
+    const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
+    if (wb) p->work = DevBuf(wb, st);
     DN_CUDA(cudaStreamSynchronize(st));
   }
   PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
                  p->ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
   bool fo = p->o.fft_order != 0;
-  if (f64) do_fft_dcoord<double>(s, p->dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, fo, tm, st, &p->grid);
-  else do_fft_dcoord<float>(s, p->dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, fo, tm, st, &p->grid);
+  if (f64) do_fft_dcoord<double>(s, p->dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, fo, tm, st, &p->grid, &p->work);
+  else do_fft_dcoord<float>(s, p->dc, pts, cl, su.dev, sw.dev, sg.dev, forward != 0, fo, tm, st, &p->grid, &p->work);
   tm.report("u2nu_dcoord (planned)");
   sg.finish();
 }
@@ -1100,6 +1125,7 @@ int dnufft_plan_destroy(dnufft_plan *plan) {
       plan->ix.kblk.st = plan->ix.kbrange.st = st;
       plan->sorted_coord.st = st;
       plan->grid.st = st;
+      plan->work.st = st;
       for (int d = 0; d < 3; ++d) plan->dc.corfac[d].st = plan->dc.tw[d].st = st;
       delete plan;
       DN_CUDA(cudaDeviceSynchronize());

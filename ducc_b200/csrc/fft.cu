@@ -20,6 +20,7 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <cstring>
 
 namespace dnufft {
 
@@ -586,6 +587,437 @@ static bool run_lines2(cplx<T> *grid, LineSpec ls, const FFTAxisPlan &p, const U
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// FFT v3 for 2D grids.
+//
+// Rows (the contiguous axis): a persistent kernel, one CTA per SM, walks its
+// rows with three shared-memory line buffers: the next row is fetched by a TMA
+// bulk copy (cp.async.bulk, completion on an mbarrier) while the current one
+// runs its Stockham stages (ping-pong between the other two buffers), and the
+// result is written back by bulk stores.  Kept ranges (type 1 output, type 2
+// input) are copied as two ranges; 16-byte alignment is kept by moving ragged
+// end elements with ordinary loads and stores.
+//
+// Columns (the strided axis, length n = P*Q): the four-step method, as two
+// passes over blocks of C adjacent kept columns (C*8 or C*16 contiguous bytes
+// per row, so every access is coalesced):
+//   pass A: for each q < Q, the P-point DFTs over rows q + Q*p, times the
+//           twiddle w_n^(q*k1), into a compact work array (row q + Q*k1);
+//   pass B: for each k1 < P, the Q-point DFTs over the Q contiguous work rows
+//           Q*k1 + q; output element k = k1 + P*k2 (natural order), either the
+//           corrected, cropped uniform array (type 1) or the grid (type 2).
+// The small DFTs are the Stockham stages above on a [len][C] tile.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t fft_smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void fft_bar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(fft_smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void fft_bar_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fft_smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// bounded wait (a second of wall clock); false if the phase did not complete
+__device__ __forceinline__ bool fft_bar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t addr = fft_smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity), "r"(1000u)
+        : "memory");
+    if (ok) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (it == 0) t0 = t;
+    else if (t - t0 > 1000000000ull) return false;
+  }
+}
+
+__device__ __forceinline__ void fft_bulk_load(void *sdst, const void *gsrc, uint32_t bytes,
+                                              uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(fft_smem_u32(sdst)), "l"(gsrc), "r"(bytes), "r"(fft_smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fft_bulk_store(void *gdst, const void *ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
+               "r"(fft_smem_u32(ssrc)), "r"(bytes)
+               : "memory");
+}
+
+// 16-byte aligned part [a2, b2) of an element range [a, b) (esz = element bytes)
+__device__ __forceinline__ void fft_aligned(int a, int b, int esz, int &a2, int &b2) {
+  const int per = 16 / esz;   // elements per 16 bytes (2 for complex64, 1 for complex128)
+  a2 = (a + per - 1) / per * per;
+  b2 = b / per * per;
+  if (b2 < a2) b2 = a2;
+}
+
+template <typename T> constexpr int rows_threads() { return sizeof(T) == 4 ? 1024 : 512; }
+
+// One row = line of n contiguous elements at grid + row*rs.  Ranges: the whole
+// line, or the kept ranges [0, lo) and [hi0, n) (zeros in between on input).
+template <typename T>
+__global__ void __launch_bounds__(rows_threads<T>(), 1)
+    k_fft_rows(cplx<T> *__restrict__ grid, int64_t rs, int n, int nlines, int lo, int hi0,
+               int in_kept, int out_kept, StageInfo si, const cplx<T> *__restrict__ tw, bool fwd,
+               int *__restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bars[3];
+  __shared__ int stR[24], stNs[24], stT[24];
+  __shared__ uint32_t stM[24];
+  __shared__ int s_fail;
+  constexpr int ES = int(sizeof(cplx<T>));
+  cplx<T> *bufs = reinterpret_cast<cplx<T> *>(smraw);
+  const int nh = (n + 63) / 64 + 1;
+  cplx<T> *twl = bufs + 3 * n;
+  cplx<T> *twh = twl + 64;
+  const int tid = threadIdx.x;
+  if (tid < 24) {
+    stR[tid] = si.R[tid];
+    stNs[tid] = si.Ns[tid];
+    stT[tid] = si.tstep[tid];
+    stM[tid] = si.mul[tid];
+  }
+  for (int i = tid; i < 64; i += blockDim.x) twl[i] = (i < n) ? tw[i] : mkc<T>(T(1), T(0));
+  for (int i = tid; i < nh; i += blockDim.x) twh[i] = (64 * i < n) ? tw[64 * i] : mkc<T>(T(1), T(0));
+  if (tid == 0) {
+    for (int b = 0; b < 3; ++b) fft_bar_init(&bars[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  __syncthreads();
+  const int nr = in_kept ? 2 : 1;
+  // issue the bulk part of row L into buffer b (thread 0)
+  auto issue_load = [&](int L, int b) {
+    const cplx<T> *src = grid + int64_t(L) * rs;
+    cplx<T> *dst = bufs + b * n;
+    uint32_t bytes = 0;
+    int a2[2], b2[2];
+    for (int r = 0; r < nr; ++r) {
+      const int ra = in_kept ? (r == 0 ? 0 : hi0) : 0;
+      const int rb = in_kept ? (r == 0 ? lo : n) : n;
+      fft_aligned(ra, rb, ES, a2[r], b2[r]);
+      bytes += uint32_t(b2[r] - a2[r]) * ES;
+    }
+    fft_bar_expect(&bars[b], bytes);
+    for (int r = 0; r < nr; ++r)
+      if (b2[r] > a2[r])
+        fft_bulk_load(dst + a2[r], src + a2[r], uint32_t(b2[r] - a2[r]) * ES, &bars[b]);
+  };
+  int bi = 0, bt = 1, bf = 2;
+  uint32_t ph = 0;   // bit b: parity of the next completion of bars[b]
+  if (tid == 0 && int(blockIdx.x) < nlines) issue_load(blockIdx.x, bi);
+  for (int L = blockIdx.x; L < nlines; L += gridDim.x) {
+    const int Ln = L + gridDim.x;
+    if (tid == 0 && Ln < nlines) {
+      // buffer bf was the source of the previous row's bulk stores
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      issue_load(Ln, bf);
+    }
+    cplx<T> *in = bufs + bi * n;
+    const cplx<T> *src = grid + int64_t(L) * rs;
+    // ragged ends of the ranges and the zero middle (disjoint from the bulk part)
+    for (int r = 0; r < nr; ++r) {
+      const int ra = in_kept ? (r == 0 ? 0 : hi0) : 0;
+      const int rb = in_kept ? (r == 0 ? lo : n) : n;
+      int a2, b2;
+      fft_aligned(ra, rb, ES, a2, b2);
+      for (int k = ra + tid; k < a2; k += blockDim.x) in[k] = src[k];
+      for (int k = b2 + tid; k < rb; k += blockDim.x) in[k] = src[k];
+    }
+    if (in_kept)
+      for (int k = lo + tid; k < hi0; k += blockDim.x) in[k] = mkc<T>(T(0), T(0));
+    const bool ok = fft_bar_wait(&bars[bi], (ph >> bi) & 1u);
+    ph ^= 1u << bi;
+    if (__syncthreads_or(ok ? 0 : 1)) {
+      if (tid == 0) atomicExch(err, 1);
+      break;
+    }
+    cplx<T> *sa = in, *sb = bufs + bt * n;
+    for (int f = 0; f < si.nst; ++f) {
+      const int R = stR[f], Ns = stNs[f], ts = stT[f];
+      const uint32_t mul = stM[f];
+      switch (R) {
+        case 2: stage2<T, 2>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        case 3: stage2<T, 3>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        case 4: stage2<T, 4>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        case 5: stage2<T, 5>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        case 7: stage2<T, 7>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        case 8: stage2<T, 8>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        case 11: stage2<T, 11>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
+        default: break;
+      }
+      cplx<T> *t = sa;
+      sa = sb;
+      sb = t;
+    }
+    // result in sa; write it back (bulk part by thread 0, ragged ends by all)
+    cplx<T> *dst = grid + int64_t(L) * rs;
+    const int nro = out_kept ? 2 : 1;
+    for (int r = 0; r < nro; ++r) {
+      const int ra = out_kept ? (r == 0 ? 0 : hi0) : 0;
+      const int rb = out_kept ? (r == 0 ? lo : n) : n;
+      int a2, b2;
+      fft_aligned(ra, rb, ES, a2, b2);
+      for (int k = ra + tid; k < a2; k += blockDim.x) dst[k] = sa[k];
+      for (int k = b2 + tid; k < rb; k += blockDim.x) dst[k] = sa[k];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      for (int r = 0; r < nro; ++r) {
+        const int ra = out_kept ? (r == 0 ? 0 : hi0) : 0;
+        const int rb = out_kept ? (r == 0 ? lo : n) : n;
+        int a2, b2;
+        fft_aligned(ra, rb, ES, a2, b2);
+        if (b2 > a2) fft_bulk_store(dst + a2, sa + a2, uint32_t(b2 - a2) * ES);
+      }
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    // rotate: the prefetched buffer is next, the result buffer is busy storing
+    const int br = int((sa - bufs) / n);
+    const int bo = (br == bi) ? bt : bi;
+    bi = bf;
+    bt = bo;
+    bf = br;
+  }
+  if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  __syncthreads();
+}
+
+// Four-step column pass.  PASS 0 = A, 1 = B.  Columns: x in [0, N1) kept
+// columns (grid column kept_to_grid(x)); C = 1 << lc columns per CTA.
+struct ColSpec {
+  int n;        // column length (n0)
+  int P, Q;     // n = P*Q
+  int N1, n1;   // kept columns / row length of the grid
+  int lc;       // log2 columns per CTA
+  int in_mode;  // pass A: 0 grid, 1 uniform array (type 2); pass B: work
+  int out_mode; // pass A: work; pass B: 0 grid (natural order), 1 uniform array (type 1)
+};
+
+template <typename T, int PASS>
+__global__ void __launch_bounds__(256)
+    k_fft_colstep(cplx<T> *__restrict__ grid, cplx<T> *__restrict__ work, ColSpec cs,
+                  StageInfo si, const cplx<T> *__restrict__ tw, UniSpec u, bool fwd) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int C = 1 << cs.lc;
+  const int len = PASS == 0 ? cs.P : cs.Q;    // DFT length of this pass
+  const int tstr = PASS == 0 ? cs.Q : cs.P;   // sub-table stride into tw (length n)
+  const int nh = (len + 63) / 64 + 1;
+  cplx<T> *s = reinterpret_cast<cplx<T> *>(smraw);
+  cplx<T> *s2 = s + len * C;
+  cplx<T> *twl = s2 + len * C;
+  cplx<T> *twh = twl + 64;
+  __shared__ int stR[24], stNs[24], stT[24];
+  __shared__ uint32_t stM[24];
+  const int tid = threadIdx.x;
+  if (tid < 24) {
+    stR[tid] = si.R[tid];
+    stNs[tid] = si.Ns[tid];
+    stT[tid] = si.tstep[tid];
+    stM[tid] = si.mul[tid];
+  }
+  for (int i = tid; i < 64; i += blockDim.x)
+    twl[i] = (i < len) ? tw[i * tstr] : mkc<T>(T(1), T(0));
+  for (int i = tid; i < nh; i += blockDim.x)
+    twh[i] = (64 * i < len) ? tw[64 * i * tstr] : mkc<T>(T(1), T(0));
+  const int nblk = (cs.N1 + C - 1) >> cs.lc;
+  const int cb = blockIdx.x % nblk;      // column block
+  const int g = blockIdx.x / nblk;       // q (pass A) or k1 (pass B)
+  const int x0 = cb << cs.lc;
+  const int N0 = sel3(u.N, 0);
+  const int lo0 = (N0 + 1) / 2, hi00 = cs.n - N0 / 2;
+  // ---- load the [len][C] tile (element m of column c at s[m*C + c])
+  for (int idx = tid; idx < len * C; idx += blockDim.x) {
+    const int m = idx >> cs.lc, c = idx & (C - 1);
+    const int x = x0 + c;
+    cplx<T> v = mkc<T>(T(0), T(0));
+    if (x < cs.N1) {
+      if (PASS == 0) {
+        const int row = g + cs.Q * m;   // q + Q*p
+        if (cs.in_mode == 0) {
+          v = grid[int64_t(row) * cs.n1 + kept_to_grid(x, cs.N1, cs.n1)];
+        } else if (row < lo0 || row >= hi00) {
+          // gather the caller's uniform array with the correction factors
+          int iu0, icf0, iu1, icf1;
+          grid_to_uni(row, N0, cs.n, u.fft_order, iu0, icf0);
+          grid_to_uni(kept_to_grid(x, cs.N1, cs.n1), cs.N1, cs.n1, u.fft_order, iu1, icf1);
+          const cplx<T> xv = static_cast<const cplx<T> *>(u.ptr)[int64_t(iu0) * u.stride[0] +
+                                                                 int64_t(iu1) * u.stride[1]];
+          const T f = T(u.corfac[0][icf0] * u.corfac[1][icf1]);
+          v = mkc<T>(xv.x * f, xv.y * f);
+        }
+      } else {
+        v = work[int64_t(g * cs.Q + m) * cs.N1 + x];   // row Q*k1 + q
+      }
+    }
+    s[idx] = v;
+  }
+  __syncthreads();
+  cplx<T> *sa = s, *sb = s2;
+  for (int f = 0; f < si.nst; ++f) {
+    const int R = stR[f], Ns = stNs[f], ts = stT[f];
+    const uint32_t mul = stM[f];
+    switch (R) {
+      case 2: stage2<T, 2>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      case 3: stage2<T, 3>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      case 4: stage2<T, 4>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      case 5: stage2<T, 5>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      case 7: stage2<T, 7>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      case 8: stage2<T, 8>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      case 11: stage2<T, 11>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
+      default: break;
+    }
+    cplx<T> *t = sa;
+    sa = sb;
+    sb = t;
+  }
+  // ---- store
+  for (int idx = tid; idx < len * C; idx += blockDim.x) {
+    const int m = idx >> cs.lc, c = idx & (C - 1);
+    const int x = x0 + c;
+    if (x >= cs.N1) continue;
+    cplx<T> v = sa[idx];
+    if (PASS == 0) {
+      // twiddle w_n^(q*k1), then work row q + Q*k1
+      const int t = int((int64_t(g) * m) % cs.n);
+      cplx<T> w = tw[t];
+      if (!fwd) w.y = -w.y;
+      v = cmul<T>(v, w);
+      work[int64_t(g + cs.Q * m) * cs.N1 + x] = v;
+    } else {
+      const int k = g + cs.P * m;   // k1 + P*k2
+      const int gc = kept_to_grid(x, cs.N1, cs.n1);
+      if (cs.out_mode == 0) {
+        grid[int64_t(k) * cs.n1 + gc] = v;
+      } else if (k < lo0 || k >= hi00) {
+        int iu0, icf0, iu1, icf1;
+        grid_to_uni(k, N0, cs.n, u.fft_order, iu0, icf0);
+        grid_to_uni(gc, cs.N1, cs.n1, u.fft_order, iu1, icf1);
+        const T f = T(u.corfac[0][icf0] * u.corfac[1][icf1]);
+        static_cast<cplx<T> *>(u.ptr)[int64_t(iu0) * u.stride[0] + int64_t(iu1) * u.stride[1]] =
+            mkc<T>(v.x * f, v.y * f);
+      }
+    }
+  }
+}
+
+// n = P*Q with P, Q as close to sqrt(n) as the factors allow (both >= 8)
+static bool split_pq(int n, int &P, int &Q) {
+  int best = -1;
+  for (int p = 8; p * p <= n; ++p) {
+    if (n % p) continue;
+    const int q = n / p;
+    if (q < 8) continue;
+    best = p;   // largest p <= sqrt(n)
+  }
+  if (best < 0) return false;
+  P = best;
+  Q = n / best;
+  return P <= 1024 && Q <= 1024;
+}
+
+static StageInfo stages_for(int len) {
+  FFTAxisPlan p;
+  std::memset(&p, 0, sizeof(p));
+  p.n = len;
+  auto f = fft_factors(len);
+  p.nfac = int(f.size());
+  for (int i = 0; i < p.nfac; ++i) p.fac[i] = f[i];
+  return make_stages(p);
+}
+
+static int sm_count_dev() {
+  int dev = 0, nsm = 0;
+  DN_CUDA(cudaGetDevice(&dev));
+  DN_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  return nsm > 0 ? nsm : 1;
+}
+
+// persistent row FFTs; false if this size is not handled (the caller falls back)
+template <typename T>
+static bool run_rows_v3(cplx<T> *grid, int n, int nlines, int64_t rs, int Nk, bool in_kept,
+                        bool out_kept, const FFTAxisPlan &p, bool fwd, int *err,
+                        cudaStream_t st) {
+  if (err == nullptr || nlines <= 0) return false;
+  const int nh = (n + 63) / 64 + 1;
+  const size_t sm = size_t(3 * n + 64 + nh) * sizeof(cplx<T>);
+  if (sm > 220 * 1024 || n < 1024) return false;
+  for (int f = 0; f < p.nfac; ++f)
+    if (p.fac[f] > 11) return false;
+  const int lo = (Nk + 1) / 2, hi0 = n - Nk / 2;
+  StageInfo si = make_stages(p);
+  DN_CUDA(cudaFuncSetAttribute(k_fft_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  const int nb = std::min(nlines, sm_count_dev());
+  k_fft_rows<T><<<nb, rows_threads<T>(), sm, st>>>(grid, rs, n, nlines, lo, hi0, in_kept ? 1 : 0,
+                                                   out_kept ? 1 : 0, si,
+                                                   static_cast<const cplx<T> *>(p.tw), fwd, err);
+  DN_LAUNCHED();
+  return true;
+}
+
+// four-step column FFTs over the N1 kept columns of an n0 x n1 grid
+template <typename T>
+static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
+                        const FFTAxisPlan &p, const UniSpec &u, bool type1, bool fwd,
+                        cudaStream_t st) {
+  if (work == nullptr || n0 < 1024) return false;
+  int P, Q;
+  if (!split_pq(n0, P, Q)) return false;
+  const int lc = sizeof(T) == 4 ? 5 : 4;   // 32 (complex64) or 16 (complex128) columns
+  const int C = 1 << lc;
+  ColSpec cs;
+  cs.n = n0;
+  cs.P = P;
+  cs.Q = Q;
+  cs.N1 = N1;
+  cs.n1 = n1;
+  cs.lc = lc;
+  const cplx<T> *tw = static_cast<const cplx<T> *>(p.tw);
+  const int nblk = (N1 + C - 1) / C;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int len = pass == 0 ? P : Q;
+    const int nh = (len + 63) / 64 + 1;
+    const size_t sm = size_t(2 * len * C + 64 + nh) * sizeof(cplx<T>);
+    if (sm > 200 * 1024) return false;
+  }
+  cs.in_mode = type1 ? 0 : 1;
+  cs.out_mode = type1 ? 1 : 0;
+  {
+    const int nh = (P + 63) / 64 + 1;
+    const size_t sm = size_t(2 * P * C + 64 + nh) * sizeof(cplx<T>);
+    DN_CUDA(cudaFuncSetAttribute(k_fft_colstep<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sm)));
+    k_fft_colstep<T, 0><<<unsigned(nblk) * unsigned(Q), 256, sm, st>>>(grid, work, cs,
+                                                                       stages_for(P), tw, u, fwd);
+    DN_LAUNCHED();
+  }
+  {
+    const int nh = (Q + 63) / 64 + 1;
+    const size_t sm = size_t(2 * Q * C + 64 + nh) * sizeof(cplx<T>);
+    DN_CUDA(cudaFuncSetAttribute(k_fft_colstep<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sm)));
+    k_fft_colstep<T, 1><<<unsigned(nblk) * unsigned(P), 256, sm, st>>>(grid, work, cs,
+                                                                       stages_for(Q), tw, u, fwd);
+    DN_LAUNCHED();
+  }
+  return true;
+}
+
 template <typename T>
 static void run_lines(cplx<T> *grid, LineSpec ls, const FFTAxisPlan &p, const UniSpec &u,
                       bool fwd, cudaStream_t st) {
@@ -654,8 +1086,9 @@ static UniSpec mk_uni(void *ptr, const int64_t *stride, const Geometry &g,
 template <typename T>
 void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
                    const double *const corfac[3], bool fft_order, void *out,
-                   const int64_t *ostride, cudaStream_t st) {
+                   const int64_t *ostride, cudaStream_t st, void *workv, int *err) {
   cplx<T> *grid = static_cast<cplx<T> *>(gridv);
+  cplx<T> *work = static_cast<cplx<T> *>(workv);
   UniSpec u = mk_uni(out, ostride, g, corfac, fft_order);
   const int n0 = int(g.nover[0]);
   if (g.ndim == 1) {
@@ -664,11 +1097,13 @@ void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool f
     const int n1 = int(g.nover[1]);
     const int N1 = int(g.nuni[1]);
     // rows (axis 1), all n0 rows, keep N1 columns
-    run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_FULL, IO_KEPT), ax[1], u,
-                 fwd, st);
+    if (!run_rows_v3<T>(grid, n1, n0, n1, N1, false, true, ax[1], fwd, err, st))
+      run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_FULL, IO_KEPT), ax[1],
+                   u, fwd, st);
     // columns (axis 0) of the kept columns, correction + crop
-    run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_FULL, IO_UNI), ax[0], u,
-                 fwd, st);
+    if (!run_cols_v3<T>(grid, work, n0, n1, N1, ax[0], u, true, fwd, st))
+      run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_FULL, IO_UNI), ax[0],
+                   u, fwd, st);
   } else {
     const int n1 = int(g.nover[1]), n2 = int(g.nover[2]);
     const int N1 = int(g.nuni[1]), N2 = int(g.nuni[2]);
@@ -687,8 +1122,9 @@ void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool f
 template <typename T>
 void fft_u2nu_head(const void *uni, const int64_t *istride, const Geometry &g,
                    const FFTAxisPlan *ax, bool fwd, const double *const corfac[3],
-                   bool fft_order, void *gridv, cudaStream_t st) {
+                   bool fft_order, void *gridv, cudaStream_t st, void *workv, int *err) {
   cplx<T> *grid = static_cast<cplx<T> *>(gridv);
+  cplx<T> *work = static_cast<cplx<T> *>(workv);
   UniSpec u = mk_uni(const_cast<void *>(uni), istride, g, corfac, fft_order);
   const int n0 = int(g.nover[0]);
   if (g.ndim == 1) {
@@ -697,11 +1133,13 @@ void fft_u2nu_head(const void *uni, const int64_t *istride, const Geometry &g,
     const int n1 = int(g.nover[1]);
     const int N1 = int(g.nuni[1]);
     // columns (axis 0) of the kept columns: gather + correction + pad
-    run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_UNI, IO_FULL), ax[0], u,
-                 fwd, st);
+    if (!run_cols_v3<T>(grid, work, n0, n1, N1, ax[0], u, false, fwd, st))
+      run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_UNI, IO_FULL), ax[0],
+                   u, fwd, st);
     // rows (axis 1): only kept columns are non-zero
-    run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_KEPT, IO_FULL), ax[1], u,
-                 fwd, st);
+    if (!run_rows_v3<T>(grid, n1, n0, n1, N1, true, false, ax[1], fwd, err, st))
+      run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_KEPT, IO_FULL), ax[1],
+                   u, fwd, st);
   } else {
     const int n1 = int(g.nover[1]), n2 = int(g.nover[2]);
     const int N1 = int(g.nuni[1]), N2 = int(g.nuni[2]);
@@ -748,15 +1186,20 @@ void zero_strided(void *ptr, int ndim, const int64_t *shape, const int64_t *stri
 
 template void fft_nu2u_tail<float>(void *, const Geometry &, const FFTAxisPlan *, bool,
                                    const double *const[3], bool, void *, const int64_t *,
-                                   cudaStream_t);
+                                   cudaStream_t, void *, int *);
 template void fft_nu2u_tail<double>(void *, const Geometry &, const FFTAxisPlan *, bool,
                                     const double *const[3], bool, void *, const int64_t *,
-                                    cudaStream_t);
+                                    cudaStream_t, void *, int *);
 template void fft_u2nu_head<float>(const void *, const int64_t *, const Geometry &,
                                    const FFTAxisPlan *, bool, const double *const[3], bool,
-                                   void *, cudaStream_t);
+                                   void *, cudaStream_t, void *, int *);
 template void fft_u2nu_head<double>(const void *, const int64_t *, const Geometry &,
                                     const FFTAxisPlan *, bool, const double *const[3], bool,
-                                    void *, cudaStream_t);
+                                    void *, cudaStream_t, void *, int *);
+
+size_t fft_work_bytes(const Geometry &g, size_t esize) {
+  if (g.ndim != 2) return 0;
+  return size_t(g.nover[0]) * size_t(g.nuni[1]) * esize;
+}
 
 }  // namespace dnufft

@@ -93,17 +93,24 @@ struct FFTAxisPlan {
 
 // Type 1 tail: FFTs over the oversampled grid with output pruning, then
 // deconvolution + crop into the caller's uniform array (arbitrary strides).
+// work: n0 x N1 scratch for the four-step column passes of 2D grids
+// (fft_work_bytes; may be null: the single-pass column kernel is used); err:
+// device error word for the bounded waits of the persistent row kernel (null:
+// the row kernel is not used)
 template <typename T>
 void fft_nu2u_tail(void *grid, const Geometry &g, const FFTAxisPlan *ax, bool forward,
                    const double *const corfac[3], bool fft_order, void *out,
-                   const int64_t *ostride, cudaStream_t st);
+                   const int64_t *ostride, cudaStream_t st, void *work = nullptr,
+                   int *err = nullptr);
 
 // Type 2 head: deconvolution + zero-pad of the caller's uniform array into the
 // oversampled grid, then FFTs with input pruning.
 template <typename T>
 void fft_u2nu_head(const void *uni, const int64_t *istride, const Geometry &g,
                    const FFTAxisPlan *ax, bool forward, const double *const corfac[3],
-                   bool fft_order, void *grid, cudaStream_t st);
+                   bool fft_order, void *grid, cudaStream_t st, void *work = nullptr,
+                   int *err = nullptr);
+size_t fft_work_bytes(const Geometry &g, size_t esize);
 
 void zero_strided(void *ptr, int ndim, const int64_t *shape, const int64_t *stride, size_t esize,
                   cudaStream_t st);
