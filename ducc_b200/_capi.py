@@ -27,7 +27,7 @@ class Opts(ctypes.Structure):
                 ("sigma_max", ctypes.c_double), ("periodicity", ctypes.c_double * 3),
                 ("fft_order", ctypes.c_int32), ("verbosity", ctypes.c_int32),
                 ("spreader", ctypes.c_int32), ("simd_lanes", ctypes.c_int32),
-                ("force_kernel", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("force_kernel", ctypes.c_int32), ("log2tile", ctypes.c_int32),
                 ("force_nover", ctypes.c_int64 * 3)]
 
 
@@ -49,7 +49,8 @@ EXPORTS = [
     "dnufft_plan_get_info", "dnufft_plan_get_permutation", "dnufft_last_error",
     "dnufft_kernel_launches", "dnufft_profile_enable", "dnufft_profile_json",
     "dnufft_nu2u_noalloc", "dnufft_noalloc_scratch_bytes", "dnufft_u2nu_dcoord",
-    "dnufft_plan_u2nu_dcoord",
+    "dnufft_plan_u2nu_dcoord", "dnufft_batch_create", "dnufft_batch_nu2u", "dnufft_batch_u2nu",
+    "dnufft_batch_destroy", "dnufft_kernel_candidates",
 ]
 
 
@@ -79,6 +80,15 @@ def lib():
                                      P(Array), P(Opts), vp]
     L.dnufft_plan_u2nu_dcoord.argtypes = [vp, ctypes.c_int, P(Array), P(Array), P(Array), vp]
     L.dnufft_plan_destroy.argtypes = [vp]
+    L.dnufft_batch_create.argtypes = [ctypes.c_int, P(vp), P(ctypes.c_int32), vp, P(vp)]
+    for f in (L.dnufft_batch_nu2u, L.dnufft_batch_u2nu):
+        f.argtypes = [vp, ctypes.c_int, P(Array), P(Array), vp]
+    L.dnufft_batch_destroy.argtypes = [vp]
+    L.dnufft_kernel_candidates.argtypes = [ctypes.c_int, P(ctypes.c_int64), ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int32),
+                                           P(ctypes.c_double), P(ctypes.c_int64),
+                                           P(ctypes.c_int)]
     L.dnufft_plan_get_info.argtypes = [vp, P(PlanInfo)]
     L.dnufft_plan_get_permutation.argtypes = [vp, P(ctypes.c_uint32), vp]
     L.dnufft_last_error.restype = ctypes.c_char_p
@@ -162,7 +172,8 @@ def stream_of(*xs, stream=None):
 
 
 def make_opts(for_plan, nthreads=None, sigma_min=None, sigma_max=None, periodicity=None,
-              fft_order=False, verbosity=0, spreader="auto", ndim=1):
+              fft_order=False, verbosity=0, spreader="auto", ndim=1, force_kernel=None,
+              force_nover=None, log2tile=None):
     o = Opts()
     lib().dnufft_default_opts(ctypes.byref(o), 1 if for_plan else 0)
     if nthreads is not None:
@@ -187,4 +198,12 @@ def make_opts(for_plan, nthreads=None, sigma_min=None, sigma_max=None, periodici
     if spreader not in SPREAD:
         raise ValueError("spreader must be one of %s" % list(SPREAD))
     o.spreader = SPREAD[spreader]
+    if force_kernel is not None:
+        if force_nover is None or len(force_nover) != ndim:
+            raise ValueError("force_kernel needs force_nover with one size per axis")
+        o.force_kernel = int(force_kernel)
+        for d in range(ndim):
+            o.force_nover[d] = int(force_nover[d])
+    if log2tile is not None:
+        o.log2tile = int(log2tile)
     return o

@@ -328,6 +328,12 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
   g.W = ks.W;
   g.nsafe = (g.W + 1) / 2;
   g.log2tile = (ndim == 1) ? 9 : (ndim == 2 ? (calc_f64 ? 4 : 5) : 4);
+  if (o.log2tile != 0) {
+    DN_REQUIRE(ndim == 1 ? o.log2tile == 9
+                         : (ndim == 2 ? (o.log2tile == 4 || o.log2tile == 5) : o.log2tile == 4),
+               ST_BADARG, "log2tile must be 9 (1D), 4 or 5 (2D), 4 (3D)");
+    g.log2tile = o.log2tile;
+  }
   s.ofactor = ks.ofactor;
   s.beta = ks.beta * ks.W;
   s.e0 = ks.e0;
@@ -772,8 +778,8 @@ static void plan_create_impl(int nu2u, const dnufft_array *coord_, const int64_t
   bool f64 = coord.dtype == DNUFFT_F64;
   auto p = std::make_unique<dnufft_plan>();
   p->o = o;
-  DN_CUDA(cudaGetDevice(&p->device));
   p->s = make_setup(ndim, shape, uint64_t(coord.shape[0]), eps, nu2u != 0, f64, f64, o);
+  DN_CUDA(cudaGetDevice(&p->device));
   upload_consts(p->s, p->dc, st);
   if (p->s.npoints > 0) {
     Staged sc(coord, true, false, st);
@@ -1074,6 +1080,34 @@ int dnufft_best_epsilon(size_t ndim, int singleprec, double sigma_min, double si
   })
 }
 
+int dnufft_kernel_candidates(int ndim, const int64_t *shape, int singleprec, double epsilon,
+                             double sigma_min, double sigma_max, int max, int32_t *kernel_index,
+                             int32_t *supp, double *ofactor, int64_t *nover, int *count) {
+  DN_GUARD({
+    DN_REQUIRE(ndim >= 1 && ndim <= 3 && shape && count && max >= 0, dnufft::ST_BADARG,
+               "bad arguments");
+    auto idx = dnufft::available_kernels(epsilon, size_t(ndim), singleprec != 0, sigma_min,
+                                         sigma_max);
+    int c = 0;
+    for (size_t i : idx) {
+      if (c >= max) break;
+      const auto &k = dnufft::kernel_db()[i];
+      if (kernel_index) kernel_index[c] = int32_t(i);
+      if (supp) supp[c] = k.W;
+      if (ofactor) ofactor[c] = k.ofactor;
+      if (nover)
+        for (int d = 0; d < 3; ++d)
+          nover[3 * c + d] =
+              d < ndim ? int64_t(std::max<size_t>(
+                             2 * dnufft::good_size_complex(size_t(double(shape[d]) * k.ofactor * 0.5) + 1),
+                             16))
+                       : 1;
+      ++c;
+    }
+    *count = c;
+  })
+}
+
 int dnufft_nu2u(const dnufft_array *points, const dnufft_array *coord, int forward, double epsilon,
                 dnufft_array *out, const dnufft_opts *opts, void *stream) {
   DN_GUARD(dnufft::nu2u_impl(points, coord, forward, epsilon, out, opts,
@@ -1215,6 +1249,236 @@ const char *dnufft_profile_json(void) {
   js += "}";
   g_prof_json = js;
   return g_prof_json.c_str();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batches
+struct dnufft_batch {
+  std::vector<dnufft_plan *> plans;
+  std::vector<int> ntrans;
+  bool f64 = false;
+  int device = 0;
+  int max_ntrans = 1;
+  uint32_t nchunks = 0;
+  size_t sm_spread = 0, sm_interp = 0;
+  dnufft::DevBuf grids, insts, tab;
+  void *fftb = nullptr;
+  dnufft::BatchArray *htab = nullptr;    // pinned: [points | uniform] x nplans
+  cudaStream_t cap = nullptr;            // capture stream
+  cudaEvent_t done = nullptr;
+  cudaGraphExec_t exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [type][forward]
+  ~dnufft_batch() {
+    for (auto &e : exec)
+      for (auto &x : e)
+        if (x) cudaGraphExecDestroy(x);
+    if (done) {
+      cudaEventSynchronize(done);
+      cudaEventDestroy(done);
+    }
+    if (fftb) dnufft::fft_batch_destroy(fftb);
+    if (htab) cudaFreeHost(htab);
+    if (cap) cudaStreamDestroy(cap);
+    grids.st = insts.st = tab.st = nullptr;
+  }
+};
+
+namespace dnufft {
+
+template <typename T>
+static void batch_build(dnufft_batch *b, cudaStream_t st) {
+  const int n = int(b->plans.size());
+  const size_t nn = static_cast<size_t>(n);
+  std::vector<SpreadInst<T>> si(nn);
+  std::vector<FFTBatchInst> fi(nn);
+  size_t total = 0;
+  std::vector<size_t> off(nn);
+  for (int i = 0; i < n; ++i) {
+    const dnufft_plan *p = b->plans[size_t(i)];
+    off[size_t(i)] = total;
+    total += grid_cells(p->s.g) * size_t(b->ntrans[size_t(i)]) * sizeof(T) * 2;
+  }
+  b->grids = DevBuf(total, st);
+  uint32_t c0 = 0;
+  for (int i = 0; i < n; ++i) {
+    const dnufft_plan *p = b->plans[size_t(i)];
+    SpreadInst<T> &s = si[size_t(i)];
+    std::memset(&s, 0, sizeof(s));
+    s.pts = PointsDesc{p->sorted_coord.p, int64_t(2), 1, true, p->s.coord_f64,
+                       p->ix.perm.as<uint32_t>(), p->s.npoints};
+    s.chunks = p->ix.chunks.as<Chunk>();
+    s.g = p->s.g;
+    s.kp = *reinterpret_cast<const KernelPoly<T> *>(
+        sizeof(T) == 4 ? static_cast<const void *>(&p->s.kpf) : static_cast<const void *>(&p->s.kpd));
+    s.grid = static_cast<unsigned char *>(b->grids.p) + off[size_t(i)];
+    s.ntrans = b->ntrans[size_t(i)];
+    s.chunk0 = c0;
+    c0 += p->ix.nchunks;
+    b->sm_spread = std::max(b->sm_spread, spread_multi_smem<T>(p->s.g));
+    b->sm_interp = std::max(b->sm_interp, interp_multi_smem<T>(p->s.g));
+    FFTBatchInst &f = fi[size_t(i)];
+    f.g = p->s.g;
+    f.ax = p->dc.ax;
+    for (int d = 0; d < 3; ++d) f.corfac[d] = p->dc.cf[d];
+    f.grid = s.grid;
+    f.ntrans = s.ntrans;
+    f.fft_order = p->o.fft_order != 0;
+  }
+  b->nchunks = c0;
+  b->insts = DevBuf(si.size() * sizeof(SpreadInst<T>), st);
+  DN_CUDA(cudaMemcpyAsync(b->insts.p, si.data(), si.size() * sizeof(SpreadInst<T>),
+                          cudaMemcpyHostToDevice, st));
+  b->fftb = fft_batch_create<T>(fi, st);
+  DN_CUDA(cudaStreamSynchronize(st));
+}
+
+static void batch_create_impl(int nplans, dnufft_plan *const *plans, const int32_t *ntrans,
+                              cudaStream_t st, dnufft_batch **out) {
+  DN_REQUIRE(out && plans && nplans > 0, ST_BADARG, "batch: bad arguments");
+  auto b = std::make_unique<dnufft_batch>();
+  DN_CUDA(cudaGetDevice(&b->device));
+  for (int i = 0; i < nplans; ++i) {
+    dnufft_plan *p = plans[i];
+    DN_REQUIRE(p != nullptr, ST_BADARG, "batch: null plan");
+    DN_REQUIRE(p->s.g.ndim == 2, ST_UNSUPPORTED, "batch: 2D plans only");
+    DN_REQUIRE(p->s.npoints > 0, ST_BADARG, "batch: plans need at least one point");
+    DN_REQUIRE(p->device == b->device, ST_BADARG, "batch: plans of another device");
+    if (i == 0) b->f64 = p->s.calc_f64;
+    DN_REQUIRE(p->s.calc_f64 == b->f64, ST_BADARG, "batch: plans of one precision only");
+    const int nt = ntrans ? ntrans[i] : 1;
+    DN_REQUIRE(nt >= 1 && nt <= 65535, ST_BADARG, "batch: ntrans out of range");
+    b->plans.push_back(p);
+    b->ntrans.push_back(nt);
+    b->max_ntrans = std::max(b->max_ntrans, nt);
+  }
+  if (b->f64) batch_build<double>(b.get(), st);
+  else batch_build<float>(b.get(), st);
+  b->tab = DevBuf(size_t(2 * nplans) * sizeof(BatchArray), st);
+  DN_CUDA(cudaMallocHost(reinterpret_cast<void **>(&b->htab), size_t(2 * nplans) * sizeof(BatchArray)));
+  DN_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  DN_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+  DN_CUDA(cudaEventRecord(b->done, st));
+  DN_CUDA(cudaStreamSynchronize(st));
+  *out = b.release();
+}
+
+// describe instance i's arrays in the table: points (ntrans, M) and uniform (ntrans, N0, N1)
+static void batch_fill(dnufft_batch *b, bool type1, const dnufft_array *pts_,
+                       const dnufft_array *uni_) {
+  const int n = int(b->plans.size());
+  const int cdt = b->f64 ? DNUFFT_C128 : DNUFFT_C64;
+  for (int i = 0; i < n; ++i) {
+    const dnufft_plan *p = b->plans[size_t(i)];
+    const int nt = b->ntrans[size_t(i)];
+    View pv = view_of(pts_ + i, "points"), uv = view_of(uni_ + i, "uniform");
+    DN_REQUIRE(!pv.host && !uv.host, ST_BADARG, "batch: device arrays only");
+    DN_REQUIRE(pv.dtype == cdt && uv.dtype == cdt, ST_BADARG, "batch: dtype mismatch");
+    BatchArray &a = b->htab[i];
+    BatchArray &u = b->htab[n + i];
+    std::memset(&a, 0, sizeof(a));
+    std::memset(&u, 0, sizeof(u));
+    if (pv.ndim == 1) {
+      DN_REQUIRE(nt == 1 && uint64_t(pv.shape[0]) == p->s.npoints, ST_BADARG,
+                 "batch: points shape mismatch");
+      a.stride[1] = pv.stride[0];
+    } else {
+      DN_REQUIRE(pv.ndim == 2 && pv.shape[0] == nt && uint64_t(pv.shape[1]) == p->s.npoints,
+                 ST_BADARG, "batch: points shape mismatch");
+      a.stride[0] = pv.stride[0];
+      a.stride[1] = pv.stride[1];
+    }
+    a.ptr = pv.data;
+    const int base = (uv.ndim == 3) ? 1 : 0;
+    DN_REQUIRE((uv.ndim == 2 && nt == 1) || (uv.ndim == 3 && uv.shape[0] == nt), ST_BADARG,
+               "batch: uniform array shape mismatch");
+    DN_REQUIRE(uv.shape[base] == p->s.g.nuni[0] && uv.shape[base + 1] == p->s.g.nuni[1],
+               ST_BADARG, "batch: uniform array shape mismatch");
+    u.ptr = uv.data;
+    u.stride[0] = base ? uv.stride[0] : 0;
+    u.stride[1] = uv.stride[base];
+    u.stride[2] = uv.stride[base + 1];
+    (void)type1;
+  }
+}
+
+template <typename T>
+static void batch_record(dnufft_batch *b, int type, bool fwd, cudaStream_t cs) {
+  const int n = int(b->plans.size());
+  BatchArray *tab = b->tab.as<BatchArray>();
+  DN_CUDA(cudaMemcpyAsync(tab, b->htab, size_t(2 * n) * sizeof(BatchArray),
+                          cudaMemcpyHostToDevice, cs));
+  const SpreadInst<T> *insts = b->insts.as<const SpreadInst<T>>();
+  if (type == 0) {
+    size_t bytes = 0;
+    for (int i = 0; i < n; ++i)
+      bytes += grid_cells(b->plans[size_t(i)]->s.g) * size_t(b->ntrans[size_t(i)]) * sizeof(T) * 2;
+    DN_CUDA(cudaMemsetAsync(b->grids.p, 0, bytes, cs));
+    launch_spread_multi<T>(insts, n, b->nchunks, b->max_ntrans, b->sm_spread, tab, cs);
+    fft_batch_run<T>(b->fftb, 0, tab + n, fwd, cs);
+  } else {
+    fft_batch_run<T>(b->fftb, 1, tab + n, fwd, cs);
+    launch_interp_multi<T>(insts, n, b->nchunks, b->max_ntrans, b->sm_interp, tab, cs);
+  }
+}
+
+static void batch_exec_impl(dnufft_batch *b, bool type1, int forward, const dnufft_array *in,
+                            dnufft_array *out, cudaStream_t st) {
+  DN_REQUIRE(b && in && out, ST_BADARG, "batch: null argument");
+  int dev = 0;
+  DN_CUDA(cudaGetDevice(&dev));
+  DN_REQUIRE(dev == b->device, ST_BADARG, "batch: wrong current device");
+  // the previous call must have copied its argument table before it is reused
+  DN_CUDA(cudaEventSynchronize(b->done));
+  if (type1) batch_fill(b, true, in, out);
+  else batch_fill(b, false, out, in);
+  const int type = type1 ? 0 : 1, f = forward ? 1 : 0;
+  if (!b->exec[type][f]) {
+    cudaGraph_t graph = nullptr;
+    DN_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    try {
+      if (b->f64) batch_record<double>(b, type, forward != 0, b->cap);
+      else batch_record<float>(b, type, forward != 0, b->cap);
+    } catch (...) {
+      cudaStreamEndCapture(b->cap, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    DN_CUDA(cudaStreamEndCapture(b->cap, &graph));
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    DN_CUDA(e);
+    b->exec[type][f] = ex;
+  }
+  DN_CUDA(cudaGraphLaunch(b->exec[type][f], st));
+  note_launch(type1 ? 4 : 3);
+  DN_CUDA(cudaEventRecord(b->done, st));
+}
+
+}  // namespace dnufft
+
+extern "C" {
+
+int dnufft_batch_create(int nplans, dnufft_plan *const *plans, const int32_t *ntrans, void *stream,
+                        dnufft_batch **batch) {
+  DN_GUARD(dnufft::batch_create_impl(nplans, plans, ntrans, static_cast<cudaStream_t>(stream),
+                                     batch))
+}
+
+int dnufft_batch_nu2u(dnufft_batch *batch, int forward, const dnufft_array *points,
+                      dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::batch_exec_impl(batch, true, forward, points, out,
+                                   static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_batch_u2nu(dnufft_batch *batch, int forward, const dnufft_array *grids,
+                      dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::batch_exec_impl(batch, false, forward, grids, out,
+                                   static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_batch_destroy(dnufft_batch *batch) {
+  DN_GUARD({ delete batch; })
 }
 
 }  // extern "C"

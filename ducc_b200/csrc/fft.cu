@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <memory>
 
 namespace dnufft {
 
@@ -433,11 +434,13 @@ __device__ __forceinline__ void stage2(const cplx<T> *__restrict__ src, cplx<T> 
 template <typename T> constexpr int fft2_max_threads() { return sizeof(T) == 4 ? 1024 : 512; }
 constexpr int FFT2_MAXE = 12;   // elements per CTA <= FFT2_MAXE * threads
 
+// One block of lines (the body of k_fft_lines2, also run by the multi-job
+// kernel of batched transforms): lines blk*2^ls.nl ... of the pass ls.
 template <typename T>
-__global__ void __launch_bounds__(fft2_max_threads<T>())
-    k_fft_lines2(cplx<T> *__restrict__ grid, LineSpec ls, StageInfo si, const cplx<T> *__restrict__ tw,
-                 UniSpec u, bool fwd) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+__device__ __forceinline__ void fft_lines_block(cplx<T> *__restrict__ grid, const LineSpec &ls,
+                                                const StageInfo &si,
+                                                const cplx<T> *__restrict__ tw, const UniSpec &u,
+                                                bool fwd, int blk, unsigned char *smraw) {
   const int n = ls.n;
   const int lnl = ls.nl;   // log2 of lines per CTA
   const int nl = 1 << lnl;
@@ -457,7 +460,7 @@ __global__ void __launch_bounds__(fft2_max_threads<T>())
     stT[threadIdx.x] = si.tstep[threadIdx.x];
     stM[threadIdx.x] = si.mul[threadIdx.x];
   }
-  const int L0 = blockIdx.x << lnl;
+  const int L0 = blk << lnl;
   const int nloc = min(nl, ls.nlines - L0);
   const int N = sel3(u.N, ls.ax);
   const int lo = (N + 1) / 2, hi0 = n - N / 2;
@@ -540,6 +543,14 @@ __global__ void __launch_bounds__(fft2_max_threads<T>())
     for (int idx = threadIdx.x; idx < tot; idx += blockDim.x)
       store_elem(idx & (nl - 1), idx >> lnl, s[idx]);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(fft2_max_threads<T>())
+    k_fft_lines2(cplx<T> *__restrict__ grid, LineSpec ls, StageInfo si, const cplx<T> *__restrict__ tw,
+                 UniSpec u, bool fwd) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  fft_lines_block<T>(grid, ls, si, tw, u, fwd, blockIdx.x, smraw);
 }
 
 static StageInfo make_stages(const FFTAxisPlan &p) {
@@ -1151,6 +1162,193 @@ void fft_u2nu_head(const void *uni, const int64_t *istride, const Geometry &g,
                  u, fwd, st);
   }
 }
+
+// ---------------------------------------------------------------------------
+// Batched FFT passes: the line passes of many transforms (instances of
+// different sizes, several transforms each) in one launch.  A job is one pass
+// over the lines of one transform; CTA b runs block b - blk0[j] of job j (found
+// by binary search over the prefix of block counts).  The uniform array of a
+// job comes from the per-call table (pointer and strides of its instance, plus
+// the transform's offset), so a captured graph can be replayed on new arrays.
+// ---------------------------------------------------------------------------
+static bool lines2_config(int n, int64_t es, int nlines, size_t esz, int maxnt, int &lnl, int &nt,
+                          size_t &sm) {
+  const size_t maxsm = 200 * 1024;
+  if (n > FFT2_MAXE * maxnt || n >= (1 << 16)) return false;
+  lnl = 0;
+  const int want = (es == 1) ? 2048 : 8192;
+  if (size_t(2 * n) * esz > maxsm - 8192) return false;
+  while ((n << (lnl + 1)) <= want && (1 << (lnl + 1)) <= 16 && (1 << lnl) < nlines &&
+         size_t(n << (lnl + 2)) * esz <= maxsm / 2 && (n << (lnl + 1)) <= FFT2_MAXE * maxnt)
+    ++lnl;
+  const int total = n << lnl;
+  nt = 32 * ((total + FFT2_MAXE - 1) / FFT2_MAXE / 32 + 1);
+  nt = std::max(64, std::min(maxnt, nt));
+  if (total > FFT2_MAXE * nt) return false;
+  const int nh = (n + 63) / 64 + 1;
+  sm = size_t(2 * total + 64 + nh) * esz + size_t(1 << lnl) * 24;
+  return sm <= maxsm;
+}
+
+struct FFTJob {
+  LineSpec ls;
+  StageInfo si;
+  UniSpec u;          // ptr / stride[] filled from the per-call table at run time
+  const void *tw;
+  void *grid;         // this transform's oversampled grid
+  int inst;           // instance (row of the per-call table)
+  int t;              // transform of the instance
+};
+
+template <typename T>
+__global__ void __launch_bounds__(fft2_max_threads<T>())
+    k_fft_lines_multi(const FFTJob *__restrict__ jobs, const uint32_t *__restrict__ blk0, int njobs,
+                      const BatchArray *__restrict__ uni, bool fwd) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ FFTJob job;
+  __shared__ int s_j;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = njobs - 1;   // last job with blk0 <= blockIdx.x
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (blk0[mid] <= blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    s_j = lo;
+  }
+  __syncthreads();
+  const int j = s_j;
+  for (int i = threadIdx.x; i < int(sizeof(FFTJob) / 4); i += blockDim.x)
+    reinterpret_cast<uint32_t *>(&job)[i] = reinterpret_cast<const uint32_t *>(jobs + j)[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const BatchArray a = uni[job.inst];
+    job.u.ptr = static_cast<cplx<T> *>(a.ptr) + int64_t(job.t) * a.stride[0];
+    for (int d = 0; d < 3; ++d) job.u.stride[d] = a.stride[d + 1];
+  }
+  __syncthreads();
+  fft_lines_block<T>(static_cast<cplx<T> *>(job.grid), job.ls, job.si,
+                     static_cast<const cplx<T> *>(job.tw), job.u, fwd, int(blockIdx.x - blk0[j]),
+                     smraw);
+}
+
+// device buffer owned by a batch (synchronous allocation at batch creation)
+struct DevBufRaw {
+  void *p = nullptr;
+  DevBufRaw() = default;
+  DevBufRaw(const DevBufRaw &) = delete;
+  DevBufRaw &operator=(const DevBufRaw &) = delete;
+  void alloc(size_t bytes) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    if (bytes) DN_CUDA(cudaMalloc(&p, bytes));
+  }
+  ~DevBufRaw() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct FFTBatchPass {
+  DevBufRaw jobs, blk0;
+  int njobs = 0;
+  uint32_t nblocks = 0;
+  int nt = 64;
+  size_t sm = 0;
+};
+
+struct FFTBatchImpl {
+  bool f64 = false;
+  FFTBatchPass pass[2][2];   // [type 1 / type 2][first / second pass]
+};
+
+static void batch_pass_upload(FFTBatchPass &bp, const std::vector<FFTJob> &jobs,
+                              const std::vector<uint32_t> &blk0, cudaStream_t st) {
+  bp.njobs = int(jobs.size());
+  bp.jobs.alloc(jobs.size() * sizeof(FFTJob));
+  bp.blk0.alloc(blk0.size() * sizeof(uint32_t));
+  DN_CUDA(cudaMemcpyAsync(bp.jobs.p, jobs.data(), jobs.size() * sizeof(FFTJob),
+                          cudaMemcpyHostToDevice, st));
+  DN_CUDA(cudaMemcpyAsync(bp.blk0.p, blk0.data(), blk0.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice, st));
+}
+
+template <typename T>
+void *fft_batch_create(const std::vector<FFTBatchInst> &insts, cudaStream_t st) {
+  DN_REQUIRE(!insts.empty(), ST_BADARG, "empty batch");
+  auto impl = std::make_unique<FFTBatchImpl>();
+  impl->f64 = sizeof(T) == 8;
+  const int maxnt = fft2_max_threads<T>();
+  for (int type = 0; type < 2; ++type)
+    for (int ps = 0; ps < 2; ++ps) {
+      std::vector<FFTJob> jobs;
+      std::vector<uint32_t> blk0;
+      FFTBatchPass &bp = impl->pass[type][ps];
+      uint32_t nb = 0;
+      for (size_t i = 0; i < insts.size(); ++i) {
+        const FFTBatchInst &in = insts[i];
+        const Geometry &g = in.g;
+        DN_REQUIRE(g.ndim == 2, ST_UNSUPPORTED, "batched transforms: 2D only");
+        const int n0 = int(g.nover[0]), n1 = int(g.nover[1]), N1 = int(g.nuni[1]);
+        // type 1: rows (full -> kept), then kept columns (-> uniform)
+        // type 2: kept columns (uniform -> full), then rows (kept -> full)
+        const bool rows = (type == 0) == (ps == 0);
+        LineSpec ls = rows ? mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0,
+                                     type == 0 ? IO_FULL : IO_KEPT, type == 0 ? IO_KEPT : IO_FULL)
+                           : mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1,
+                                     type == 0 ? IO_FULL : IO_UNI, type == 0 ? IO_UNI : IO_FULL);
+        const FFTAxisPlan &ax = in.ax[rows ? 1 : 0];
+        int lnl, nt;
+        size_t sm;
+        DN_REQUIRE(lines2_config(ls.n, ls.es, ls.nlines, sizeof(cplx<T>), maxnt, lnl, nt, sm),
+                   ST_UNSUPPORTED, "batched transforms: oversampled grid too large");
+        ls.nl = lnl;
+        bp.nt = std::max(bp.nt, nt);
+        bp.sm = std::max(bp.sm, sm);
+        const uint32_t blocks = uint32_t((ls.nlines + (1 << lnl) - 1) >> lnl);
+        for (int t = 0; t < in.ntrans; ++t) {
+          FFTJob jb;
+          std::memset(&jb, 0, sizeof(jb));
+          jb.ls = ls;
+          jb.si = make_stages(ax);
+          const int64_t zero[3] = {0, 0, 0};
+          jb.u = mk_uni(nullptr, zero, g, in.corfac, in.fft_order);
+          jb.tw = ax.tw;
+          jb.grid = static_cast<cplx<T> *>(in.grid) + int64_t(t) * n0 * n1;
+          jb.inst = int(i);
+          jb.t = t;
+          jobs.push_back(jb);
+          blk0.push_back(nb);
+          nb += blocks;
+        }
+      }
+      bp.nblocks = nb;
+      batch_pass_upload(bp, jobs, blk0, st);
+    }
+  DN_CUDA(cudaStreamSynchronize(st));
+  return impl.release();
+}
+
+void fft_batch_destroy(void *h) { delete static_cast<FFTBatchImpl *>(h); }
+
+template <typename T>
+void fft_batch_run(void *h, int type, const BatchArray *uni, bool fwd, cudaStream_t st) {
+  FFTBatchImpl *impl = static_cast<FFTBatchImpl *>(h);
+  for (int ps = 0; ps < 2; ++ps) {
+    FFTBatchPass &bp = impl->pass[type][ps];
+    if (bp.nblocks == 0) continue;
+    DN_CUDA(cudaFuncSetAttribute(k_fft_lines_multi<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(bp.sm)));
+    k_fft_lines_multi<T><<<bp.nblocks, bp.nt, bp.sm, st>>>(
+        static_cast<const FFTJob *>(bp.jobs.p), static_cast<const uint32_t *>(bp.blk0.p),
+        bp.njobs, uni, fwd);
+    DN_LAUNCHED();
+  }
+}
+
+template void *fft_batch_create<float>(const std::vector<FFTBatchInst> &, cudaStream_t);
+template void *fft_batch_create<double>(const std::vector<FFTBatchInst> &, cudaStream_t);
+template void fft_batch_run<float>(void *, int, const BatchArray *, bool, cudaStream_t);
+template void fft_batch_run<double>(void *, int, const BatchArray *, bool, cudaStream_t);
 
 // zero a strided array of up to 3 dimensions (element size 8 or 16 bytes)
 template <typename E>

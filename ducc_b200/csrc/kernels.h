@@ -115,4 +115,49 @@ size_t fft_work_bytes(const Geometry &g, size_t esize);
 void zero_strided(void *ptr, int ndim, const int64_t *shape, const int64_t *stride, size_t esize,
                   cudaStream_t st);
 
+// ---- batched transforms (batch.cu, fft.cu)
+// caller's array of one instance in a per-call device table: stride[0] between
+// transforms, stride[1..] per axis (elements)
+struct BatchArray {
+  void *ptr;
+  int64_t stride[4];
+};
+
+struct FFTBatchInst {
+  Geometry g;
+  const FFTAxisPlan *ax;      // host copies (twiddle pointers are device memory)
+  const double *corfac[3];    // device
+  void *grid;                 // ntrans oversampled grids, back to back
+  int ntrans;
+  bool fft_order;
+};
+// line passes of all instances, one launch per pass; type 0 = type 1 tail
+// (rows, then kept columns with correction into the uniform arrays), type 1 =
+// type 2 head (columns from the uniform arrays, then rows)
+template <typename T>
+void *fft_batch_create(const std::vector<FFTBatchInst> &insts, cudaStream_t st);
+template <typename T>
+void fft_batch_run(void *h, int type, const BatchArray *uni, bool fwd, cudaStream_t st);
+void fft_batch_destroy(void *h);
+
+template <typename T> struct SpreadInst {
+  PointsDesc pts;
+  const Chunk *chunks;
+  Geometry g;
+  KernelPoly<T> kp;
+  void *grid;        // ntrans grids back to back
+  int ntrans;
+  uint32_t chunk0;   // first chunk of this instance in the launch
+};
+// one launch over the chunks of all instances (x) and their transforms (y);
+// vals: per-call table of the point arrays (type 1 input, type 2 output)
+template <typename T>
+void launch_spread_multi(const SpreadInst<T> *insts, int ninst, uint32_t nchunks, int max_ntrans,
+                         size_t smem, const BatchArray *vals, cudaStream_t st);
+template <typename T>
+void launch_interp_multi(const SpreadInst<T> *insts, int ninst, uint32_t nchunks, int max_ntrans,
+                         size_t smem, const BatchArray *vals, cudaStream_t st);
+template <typename T> size_t spread_multi_smem(const Geometry &g);
+template <typename T> size_t interp_multi_smem(const Geometry &g);
+
 }  // namespace dnufft

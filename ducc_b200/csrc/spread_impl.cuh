@@ -78,19 +78,17 @@ __device__ __forceinline__ void global_add(cplx<T> *p, T re, T im) {
   }
 }
 
+// One chunk of one transform (the body of k_spread; also used by the
+// multi-instance kernel of batched transforms).
 template <typename T, typename Tc, int NDIM, int W>
-__global__ void __launch_bounds__(SP_THREADS)
-    k_spread(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
-             const cplx<T> *__restrict__ values, int64_t vs, int64_t vtrans,
-             cplx<T> *__restrict__ grid, int64_t gtrans) {
+__device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk ch, const Geometry &g,
+                                             const KernelPoly<T> &kp,
+                                             const cplx<T> *__restrict__ values, int64_t vs,
+                                             cplx<T> *__restrict__ grid, unsigned char *smraw) {
   constexpr bool SMEM = BufferLayout<T>::smem(NDIM);
   constexpr int FP = (NDIM == 1) ? W : (NDIM == 2 ? W * W : W * W * W);
   constexpr int NIT = (FP + 31) / 32;
   constexpr int UNR = NIT <= 8 ? NIT : 4;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const Chunk ch = chunks[blockIdx.x];
-  values += int64_t(blockIdx.y) * vtrans;
-  grid += int64_t(blockIdx.y) * gtrans;
   const int S = (1 << g.log2tile) + W;
   int ncell = S;
   if (NDIM >= 2) ncell *= S;
@@ -205,14 +203,24 @@ __global__ void __launch_bounds__(SP_THREADS)
 
 template <typename T, typename Tc, int NDIM, int W>
 __global__ void __launch_bounds__(SP_THREADS)
-    k_interp(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
-             const cplx<T> *__restrict__ grid, int64_t gtrans, cplx<T> *__restrict__ out,
-             int64_t os, int64_t otrans) {
-  constexpr bool SMEM = BufferLayout<T>::smem(NDIM);
+    k_spread(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
+             const cplx<T> *__restrict__ values, int64_t vs, int64_t vtrans,
+             cplx<T> *__restrict__ grid, int64_t gtrans) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const Chunk ch = chunks[blockIdx.x];
-  grid += int64_t(blockIdx.y) * gtrans;
-  out += int64_t(blockIdx.y) * otrans;
+  spread_chunk<T, Tc, NDIM, W>(pts, chunks[blockIdx.x], g, kp,
+                               values + int64_t(blockIdx.y) * vtrans, vs,
+                               grid + int64_t(blockIdx.y) * gtrans, smraw);
+}
+
+// One chunk of one transform (the body of k_interp; also used by the
+// multi-instance kernel of batched transforms).
+template <typename T, typename Tc, int NDIM, int W>
+__device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk ch, const Geometry &g,
+                                             const KernelPoly<T> &kp,
+                                             const cplx<T> *__restrict__ grid,
+                                             cplx<T> *__restrict__ out, int64_t os,
+                                             unsigned char *smraw) {
+  constexpr bool SMEM = BufferLayout<T>::smem(NDIM);
   const int S = (1 << g.log2tile) + W;
   int ncell = S;
   if (NDIM >= 2) ncell *= S;
@@ -324,6 +332,16 @@ __global__ void __launch_bounds__(SP_THREADS)
     }
     out[int64_t(j) * os] = mkc<T>(ar, ai);
   }
+}
+
+template <typename T, typename Tc, int NDIM, int W>
+__global__ void __launch_bounds__(SP_THREADS)
+    k_interp(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
+             const cplx<T> *__restrict__ grid, int64_t gtrans, cplx<T> *__restrict__ out,
+             int64_t os, int64_t otrans) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  interp_chunk<T, Tc, NDIM, W>(pts, chunks[blockIdx.x], g, kp, grid + int64_t(blockIdx.y) * gtrans,
+                               out + int64_t(blockIdx.y) * otrans, os, smraw);
 }
 
 template <typename T, int NDIM, int W>

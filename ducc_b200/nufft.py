@@ -160,7 +160,7 @@ class plan:
 
     def __init__(self, *, nu2u, coord, grid_shape, epsilon, nthreads=0, sigma_min=1.1,
                  sigma_max=2.6, periodicity=2 * math.pi, fft_order=False, spreader="auto",
-                 stream=None):
+                 stream=None, force_kernel=None, force_nover=None, log2tile=None):
         self._ptr = None
         coord = _prepare_in(coord)
         if C.dtype_code(coord) not in (C.F32, C.F64):
@@ -174,7 +174,7 @@ class plan:
         self._f64 = C.dtype_code(coord) == C.F64
         self._torch_device = coord.device if C.is_torch(coord) else None
         o = C.make_opts(True, nthreads, sigma_min, sigma_max, periodicity, fft_order, 0,
-                        spreader, ndim)
+                        spreader, ndim, force_kernel, force_nover, log2tile)
         a_c = C.describe(coord)
         shp = (ctypes.c_int64 * 3)(*(shape + [1] * (3 - ndim)))
         ptr = ctypes.c_void_p()

@@ -64,7 +64,7 @@ typedef struct dnufft_opts {
   int32_t spreader;       /* DNUFFT_SPREAD_*                                     */
   int32_t simd_lanes;     /* SIMD width DUCC's cost model assumes (default 8)    */
   int32_t force_kernel;   /* >=0: use this kernel-table row instead of choosing  */
-  int32_t reserved0;
+  int32_t log2tile;       /* 0: DUCC's tile size; 2D/3D: 4 or 5, 1D: 9 (tuning) */
   int64_t force_nover[3]; /* with force_kernel: oversampled sizes                */
 } dnufft_opts;
 
@@ -176,6 +176,36 @@ int dnufft_nu2u_noalloc(const dnufft_array *points, const dnufft_array *coord, i
                         double epsilon, dnufft_array *out, const dnufft_opts *opts,
                         void *stream);
 size_t dnufft_noalloc_scratch_bytes(void);
+
+/* Batched transforms (no counterpart in DUCC): 2D plans of one precision,
+ * each with its own grid size, points, epsilon (kernel) and ntrans[i]
+ * transforms over its coordinates, executed together - one multi-instance
+ * launch per stage (grid zeroing, spreading or interpolation, the two FFT line
+ * passes with the correction), captured into a CUDA graph on the first call of
+ * each direction and sign and replayed afterwards.  The plans must outlive the
+ * batch.  Per call, points[i] is (ntrans[i], M_i) (or (M_i,) when ntrans[i] is
+ * 1) and the uniform array (ntrans[i], N0, N1) (or (N0, N1)); device arrays
+ * only, any strides.  Calls on one batch are serialised (each waits until the
+ * previous one has consumed its argument table). */
+typedef struct dnufft_batch dnufft_batch;
+int dnufft_batch_create(int nplans, dnufft_plan *const *plans, const int32_t *ntrans, void *stream,
+                        dnufft_batch **batch);
+int dnufft_batch_nu2u(dnufft_batch *batch, int forward, const dnufft_array *points,
+                      dnufft_array *out, void *stream);
+int dnufft_batch_u2nu(dnufft_batch *batch, int forward, const dnufft_array *grids,
+                      dnufft_array *out, void *stream);
+int dnufft_batch_destroy(dnufft_batch *batch);
+
+/* Candidate (kernel, oversampled size) pairs for an autotuner: for every
+ * kernel support W, the smallest oversampling factor in [sigma_min, sigma_max]
+ * whose kernel reaches epsilon (DUCC's getAvailableKernels,
+ * src/ducc0/math/gridding_kernel.h:420-444) and the oversampled sizes DUCC's
+ * findNufftParameters would use with it (nufft.h:177-178).  Writes up to max
+ * entries (nover: 3 per entry) and their number to *count.  Feed the choice
+ * back through dnufft_opts.force_kernel / force_nover. */
+int dnufft_kernel_candidates(int ndim, const int64_t *shape, int singleprec, double epsilon,
+                             double sigma_min, double sigma_max, int max, int32_t *kernel_index,
+                             int32_t *supp, double *ofactor, int64_t *nover, int *count);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *dnufft_last_error(void);

@@ -91,3 +91,28 @@ def test_parameter_choice_matches_oracle():
         row = O.kernel_db()[kidx]
         assert row[6] == sp
         assert len(nover) == len(shape)
+
+
+@pytest.mark.parametrize("shape,eps,single", [((4096, 4096), 1e-6, True), ((300, 200), 1e-4, True),
+                                              ((64, 80, 90), 1e-10, False), ((1000,), 1e-9, False)])
+def test_kernel_candidates_match_oracle(shape, eps, single):
+    """The autotuner's candidates: DUCC's available kernels (one per support,
+    smallest oversampling factor reaching eps) with DUCC's oversampled sizes."""
+    from ducc_b200 import autotune
+    from oracle import nufft_oracle as O
+    got = autotune.candidates(shape, eps, single, 1.1, 2.6)
+    ref = O.available_kernels(eps, len(shape), single, 1.1, 2.6)
+    assert [g[0] for g in got] == list(ref)
+    db = O.kernel_db()
+    for kidx, W, of, nov in got:
+        assert W == db[kidx][0] and of == db[kidx][1]
+        assert nov == [max(2 * O.good_size_complex(int(s * of * 0.5) + 1), 16) for s in shape]
+    # the model's own choice is one of the candidates
+    p = O.Params(shape, eps, single, 1000, True, 1)
+    assert p.kidx in [g[0] for g in got]
+
+
+def test_log2tile_option_checked():
+    with pytest.raises(RuntimeError, match="log2tile"):
+        nufft.plan(nu2u=True, coord=np.zeros((3, 2), np.float32), grid_shape=(16, 16),
+                   epsilon=1e-4, log2tile=7)
