@@ -166,6 +166,146 @@ def run_reference(args, rank):
     }))
 
 
+# ---------------------------------------------------------------- other workloads
+# Reported beside the headline (same JSON line, "workloads"): the batched,
+# differentiable and 3D double-precision transforms, each timed with CUDA
+# events on the current stream after warm-up.
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def workload_batched(dev, steps=5, warmup=2, ninst=64, seed=7):
+    """64 uneven 2D instances: side log-uniform in [64, 1024] (even), M
+    log-uniform in [1e3, 1e6] uniform points, ntrans in {1, 4}, eps in
+    {1e-4, 1e-6}, complex64; autotuned per instance; one batch (multi-instance
+    launches replayed from a CUDA graph) against the same plans run one by one."""
+    import torch
+    from ducc_b200 import autotune, batch, nufft
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    plans, nts, pts, outs, grids, pouts, total = [], [], [], [], [], [], 0
+    for _ in range(ninst):
+        side = int(round(np.exp(rng.uniform(np.log(64), np.log(1024))) / 2)) * 2
+        M = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        nt = int(rng.choice([1, 4]))
+        eps = float(rng.choice([1e-4, 1e-6]))
+        coord = torch.from_numpy(rng.uniform(-np.pi, np.pi, (M, 2)).astype(np.float32)).to(dev)
+        choice = autotune.tune(coord, (side, side), eps, ntrans=nt, reps=1)
+        plans.append(nufft.plan(nu2u=True, coord=coord, grid_shape=(side, side), epsilon=eps,
+                                **autotune.plan_kwargs(choice)))
+        nts.append(nt)
+        v = torch.randn((nt, M), dtype=torch.complex64, device=dev)
+        g = torch.randn((nt, side, side), dtype=torch.complex64, device=dev)
+        pts.append(v)
+        grids.append(g)
+        outs.append(torch.empty((nt, side, side), dtype=torch.complex64, device=dev))
+        pouts.append(torch.empty((nt, M), dtype=torch.complex64, device=dev))
+        total += M * nt
+    tune_s = time.perf_counter() - t0
+    b = batch.Batch(plans, ntrans=nts)
+
+    def batched():
+        b.nu2u(points=pts, out=outs, forward=True)
+        b.u2nu(grids=grids, out=pouts, forward=False)
+
+    def one_by_one():
+        for p, nt, v, o, g, po in zip(plans, nts, pts, outs, grids, pouts):
+            for t in range(nt):
+                p.nu2u(points=v[t], forward=True, out=o[t])
+                p.u2nu(grid=g[t], forward=False, out=po[t])
+
+    res = {}
+    for name, fn in (("batched", batched), ("one_by_one", one_by_one)):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        res[name] = e0.elapsed_time(e1) / steps
+    return {"metric": "Mpts/s (points x transforms x 2 / time)",
+            "value": 2 * total / (res["batched"] * 1e-3) / 1e6,
+            "ms_per_step": res["batched"], "one_by_one_ms": res["one_by_one"],
+            "one_by_one_value": 2 * total / (res["one_by_one"] * 1e-3) / 1e6,
+            "instances": ninst, "points_x_ntrans": total, "autotune_s": tune_s,
+            "config": "64 uneven 2D instances (side 64..1024, M 1e3..1e6, ntrans 1/4, "
+                      "eps 1e-4/1e-6), complex64, step = batched nu2u + u2nu"}
+
+
+def workload_autograd(dev, steps=5, warmup=2, seed=8):
+    """1024^2 complex64 image, radial trajectory 2048 spokes x 2048 samples,
+    float32 coordinates, eps 1e-6: forward u2nu + backward (image and
+    coordinate gradients) of L = ||u2nu(img) - y||^2."""
+    import torch
+    from ducc_b200 import autograd as AG
+    rng = np.random.default_rng(seed)
+    N, ns = 1024, 2048
+    ang = np.pi * np.arange(ns) / ns
+    rad = np.linspace(-np.pi, np.pi, ns, endpoint=False)
+    x = np.stack([np.outer(np.cos(ang), rad).ravel(), np.outer(np.sin(ang), rad).ravel()], 1)
+    coord = torch.from_numpy(x.astype(np.float32)).to(dev).requires_grad_()
+    img = torch.randn((N, N), dtype=torch.complex64, device=dev).requires_grad_()
+    with torch.no_grad():
+        y = AG.u2nu(img + 0.3 * torch.randn_like(img), coord, epsilon=1e-6)
+
+    def step():
+        img.grad = None
+        coord.grad = None
+        loss = (AG.u2nu(img, coord, epsilon=1e-6) - y).abs().pow(2).sum()
+        loss.backward()
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    return {"metric": "ms per forward + backward", "value": ms,
+            "mpts_per_s": ns * ns / (ms * 1e-3) / 1e6,
+            "config": "1024^2 c64 image, 2048x2048 radial f32 coords, eps 1e-6; step = plan + "
+                      "u2nu + adjoint nu2u + derivative-kernel coordinate gradient"}
+
+
+def workload_3d(dev, steps=3, warmup=1, seed=9):
+    """3D type 2 on a 256^3 grid, M = 2e7 uniform points: float64 coordinates
+    and complex128 modes at eps 1e-10, and float32 / complex64 at eps 1e-5."""
+    import torch
+    from ducc_b200 import nufft
+    rng = np.random.default_rng(seed)
+    N, M = 256, 20_000_000
+    out = {}
+    for name, cdt, ct, eps in (("fp64_eps1e-10", np.float64, torch.complex128, 1e-10),
+                               ("fp32_eps1e-5", np.float32, torch.complex64, 1e-5)):
+        coord = torch.from_numpy(rng.uniform(-np.pi, np.pi, (M, 3)).astype(cdt)).to(dev)
+        grid = torch.randn((N, N, N), dtype=ct, device=dev)
+        pts = torch.empty(M, dtype=ct, device=dev)
+        p = nufft.plan(nu2u=False, coord=coord, grid_shape=(N, N, N), epsilon=eps, nthreads=8)
+        for _ in range(warmup):
+            p.u2nu(grid=grid, forward=True, out=pts)
+        torch.cuda.synchronize(dev)
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            p.u2nu(grid=grid, forward=True, out=pts)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms": ms, "mpts_per_s": M / (ms * 1e-3) / 1e6, "supp": p.info()["supp"],
+                     "nover": p.info()["nover"]}
+        del p, coord, grid, pts
+        torch.cuda.empty_cache()
+    out["config"] = "3D type 2, 256^3 modes, M=2e7 uniform points, planned u2nu"
+    return out
+
+
 # ---------------------------------------------------------------- our arm
 def cpu_baseline_leg(m, n, coord, vals, grid, budget_s=30.0):
     """DUCC's CPU NUFFT on the host cores, bounded to ~budget_s seconds."""
@@ -315,6 +455,18 @@ def run_ours(args, rank, world, local_rank):
     recs = r["info"].get("tc_records", 0)
     tc_flops = recs * 2 * 128 * 48 * 16
     cpu = None if args.no_cpu else cpu_baseline_leg(m, n, coord, vals, grid)
+    workloads = None
+    if not args.no_extra and world == 1:
+        del d_coord, d_vals, d_grid, d_out_grid, d_out_pts
+        torch.cuda.empty_cache()
+        workloads = {}
+        for name, fn in (("batched_uneven_2d", workload_batched),
+                         ("radial_autograd_2d", workload_autograd),
+                         ("type2_3d_256", workload_3d)):
+            try:
+                workloads[name] = fn(dev)
+            except Exception as e:   # reported, never fatal for the headline line
+                workloads[name] = {"error": str(e)[:200]}
     line = {
         "metric": METRIC,
         "value": world * 2 * m / (ms * 1e-3) / 1e6,
@@ -345,6 +497,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(r["launches"]),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "workloads": workloads,
     }
     for other in args.spreaders[1:]:
         o = results[other]
@@ -367,6 +520,8 @@ def main():
                     help="nthreads fed to DUCC's parameter cost model (fixes W / sigma)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the batched / autograd / 3D workloads")
     args = ap.parse_args()
     args.spreaders = args.spreaders.split(",")
     rank = int(os.environ.get("RANK", 0))
