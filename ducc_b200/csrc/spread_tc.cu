@@ -31,10 +31,10 @@
 //                        placement; MN-major operand tiles in 2 stages;
 //   MMA warp (1)       : one thread issues the MMAs of a round into the
 //                        accumulator of each K-block's quadrant and commits;
-//   epilogue warps (4) : read finished accumulators from tensor memory, add
-//                        them into FP32 shared-memory planes (no atomics), and
-//                        at the end of a chunk add the planes to the grid with
-//                        float2 atomics.
+//   epilogue warps (4) : read finished accumulators from tensor memory and add
+//                        them into FP32 shared-memory planes (no atomics);
+//   flusher warps (4)  : add a finished sub-chunk's planes (double-buffered)
+//                        to the grid with float2 atomics and zero them.
 // Tensor memory holds two accumulator sets (2 x 4 quadrants x 64 columns), so
 // the MMA thread continues with the next chunk while the epilogue drains the
 // previous one.  An accumulator is also handed to the epilogue once any of its
@@ -61,7 +61,8 @@ namespace tc {
 constexpr int KB = 16;             // points per MMA (K)
 constexpr int ROUND = 8;           // K-blocks per round (one operand stage)
 constexpr int NST = 3;             // operand stages
-constexpr int NPRE = 16;           // point-data ring slots (rounds)
+// point-data ring slots (rounds): fewer for float64 coordinates (larger slots)
+template <typename Tc> constexpr int npre() { return sizeof(Tc) == 8 ? 12 : 16; }
 constexpr int A_BYTES = 4096;      // 128 x 16 fp16, MN-major, no swizzle
 constexpr int B_BYTES = 1536;      // 48 x 16 fp16, MN-major, no swizzle
 constexpr int A_LBO = 2048;        // between the two K-groups of 8 points
@@ -80,9 +81,10 @@ constexpr uint32_t FLUSH_COST = 16;  // CTA balancing: one sub-chunk flush ~ thi
 constexpr int EPI_W0 = 0, N_EPI = 4;     // warps 0..3: tensor-memory lane quarters 0..3
 constexpr int MMA_W0 = 4, N_MMA = 4;     // warp 4+q issues the MMAs of quadrant q
 constexpr int LOAD_W0 = 8, N_LOAD = 4;
-constexpr int BUILD_W0 = 12, N_BUILD = 12;
-constexpr int WARPS = BUILD_W0 + N_BUILD;   // 24
-constexpr int THREADS = 32 * WARPS;         // 768
+constexpr int FLUSH_W0 = 12, N_FLUSH = 4;   // planes -> grid
+constexpr int BUILD_W0 = 16, N_BUILD = 12;
+constexpr int WARPS = BUILD_W0 + N_BUILD;   // 28
+constexpr int THREADS = 32 * WARPS;         // 896
 constexpr int BUILDERS = 32 * N_BUILD;      // 384 = 3 groups x 128 point slots
 
 // K-block record in global memory: {first sorted point index, meta}
@@ -292,8 +294,11 @@ template <typename Tc> struct PreLayout {
   static constexpr int BYTES = VAL + ROUND * KB * 8;
 };
 
+// two sets of the four planes: the epilogue fills one while the flusher warps
+// add the other to the grid
+constexpr int PLANE_SET_BYTES = 4 * PLANE_FLOATS * 4;
 template <typename Tc> constexpr int smem_bytes() {
-  return NST * STAGE_BYTES + 4 * PLANE_FLOATS * 4 + NPRE * PreLayout<Tc>::BYTES;
+  return NST * STAGE_BYTES + 2 * PLANE_SET_BYTES + npre<Tc>() * PreLayout<Tc>::BYTES;
 }
 
 }  // namespace tc
@@ -321,10 +326,13 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
   using namespace tc;
   static_assert(W <= 8, "tensor-core spreader handles supports up to 8");
   using PL_ = PreLayout<Tc>;
+  constexpr int NPRE = npre<Tc>();
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   __shared__ uint64_t full_bar[NST], empty_bar[NST];
   __shared__ uint64_t pre_full[NPRE], pre_empty[NPRE];
   __shared__ uint64_t acc_full[4][2], acc_empty[4][2], done_bar;
+  __shared__ uint64_t pl_full[2], pl_empty[2];   // plane sets: epilogue <-> flusher
+  __shared__ uint2 pl_info[2];                   // {tile, dirty quadrants | exit bit 8}
   __shared__ uint2 acc_info[4][2];   // {flags (1 dirty, 2 exit), tile}
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
@@ -341,8 +349,8 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
   const float unscale = ldexpf(1.f, e2 - 28);
 
   unsigned char *stages = tc_smem;
-  float *planes = reinterpret_cast<float *>(tc_smem + NST * STAGE_BYTES);
-  unsigned char *pre = tc_smem + NST * STAGE_BYTES + 4 * PLANE_FLOATS * 4;
+  float *planes = reinterpret_cast<float *>(tc_smem + NST * STAGE_BYTES);   // 2 sets
+  unsigned char *pre = tc_smem + NST * STAGE_BYTES + 2 * PLANE_SET_BYTES;
 
   if (warp == MMA_W0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -364,13 +372,17 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         mbar_init(&acc_empty[q][b], 32 * N_EPI);
       }
     mbar_init(&done_bar, N_MMA);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&pl_full[b], 1);
+      mbar_init(&pl_empty[b], 32 * N_FLUSH);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
   }
   // zero the operand stages (A rows 96..127 are never written again) and planes
   {
     const uint32_t zb = smem_u32(tc_smem);
-    const int nvec = (NST * STAGE_BYTES + 4 * PLANE_FLOATS * 4) / 16;
+    const int nvec = (NST * STAGE_BYTES + 2 * PLANE_SET_BYTES) / 16;
     for (int i = tid; i < nvec; i += THREADS) st_v4(zb + uint32_t(i) * 16u, 0u, 0u, 0u, 0u);
   }
   fence_proxy_async();
@@ -532,7 +544,7 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
       fence_proxy_async();
       mbar_arrive(&full_bar[s]);
     }
-  } else if (warp >= MMA_W0) {
+  } else if (warp >= MMA_W0 && warp < MMA_W0 + N_MMA) {
     // ------------------------------------------------------------ MMA issue
     // Warp 4+q issues every MMA into quadrant q's accumulators (so MMAs into
     // one accumulator keep their order), four issuers in parallel.  Event k of
@@ -602,22 +614,23 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
       mbar_wait(&done_bar, 0u, abortp, err);
     }
     __syncwarp();
-  } else {
+  } else if (warp < EPI_W0 + N_EPI) {
     // ------------------------------------------------------------ epilogue
     // One event per quadrant per sub-chunk, taken in quadrant order: the
-    // accumulators are added into the FP32 planes (part p of tensor-memory
-    // lane L = 24p + u is row u of plane p), then the sub-chunk's planes are
-    // added to the grid and zeroed.
+    // accumulators are added into the FP32 planes of set k & 1 (part p of
+    // tensor-memory lane L = 24p + u is row u of plane p), which then go to
+    // the flusher warps.
     const int L = tid;                   // tensor-memory lane 0..127
     const int p = L / 24, u = L - 24 * (L / 24);
-    float *plane = planes + (p < 4 ? p : 0) * PLANE_FLOATS;
-    const int S = 32 + W;
-    const int nu = int(g.nover[0]), nv = int(g.nover[1]);
     for (uint32_t k = 0;; ++k) {
       const uint32_t buf = k & 1, par = (k >> 1) & 1;
+      // plane set k & 1 must have been flushed and zeroed (sub-chunk k - 2)
+      bool stop = false;
+      if (k >= 2)
+        stop = !__all_sync(0xffffffffu, mbar_wait(&pl_empty[buf], ((k >> 1) - 1) & 1u, abortp, err));
+      float *plane = planes + buf * (4 * PLANE_FLOATS) + (p < 4 ? p : 0) * PLANE_FLOATS;
       // 'stop' (a failed wait or the exit record) is uniform in a warp, and
       // made uniform across the four warps at each named barrier
-      bool stop = false;
       uint32_t tile = 0, dq = 0;   // dq: dirty quadrants
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) {
@@ -657,17 +670,38 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         tc_fence_before();
         mbar_arrive(&acc_empty[q][buf]);
       }
-      if (named_bar_or(1, 32 * N_EPI, stop)) break;
-      // sub-chunk complete: planes -> grid, and zero them for the next one
-      const int tu = int(tile) / ntv, tv = int(tile) - tu * ntv;
+      const bool fin = named_bar_or(1, 32 * N_EPI, stop);
+      // hand plane set k & 1 to the flusher (or tell it to stop)
+      if (L == 0) {
+        pl_info[buf] = make_uint2(tile, fin ? 0x100u : dq);
+        mbar_arrive(&pl_full[buf]);
+      }
+      if (fin) break;
+    }
+  }
+  if (warp >= FLUSH_W0 && warp < FLUSH_W0 + N_FLUSH) {
+    // ------------------------------------------------------------ flusher
+    // Sub-chunk k's planes (set k & 1) -> grid with float2 atomics, zeroing
+    // them for sub-chunk k + 2.  Only the dirty quadrants' windows hold data.
+    const int L = tid - FLUSH_W0 * 32;
+    const int S = 32 + W;
+    const int nu = int(g.nover[0]), nv = int(g.nover[1]);
+    for (uint32_t k = 0;; ++k) {
+      const uint32_t buf = k & 1;
+      if (!mbar_wait(&pl_full[buf], (k >> 1) & 1u, abortp, err)) break;
+      const uint2 info = pl_info[buf];
+      if (info.y & 0x100u) break;
+      const uint32_t dq = info.y;
+      const float *pls = planes + buf * (4 * PLANE_FLOATS);
+      float *plw = planes + buf * (4 * PLANE_FLOATS);
+      const int tu = int(info.x) / ntv, tv = int(info.x) - tu * ntv;
       const int b0u = (tu << 5) - g.nsafe, b0v = (tv << 5) - g.nsafe;
-      // only the windows of the dirty quadrants hold data: their bounding box
       const int r0 = (dq & 3u) ? 0 : 16, r1 = min((dq & 12u) ? 40 : 24, S);
       const int c0 = (dq & 5u) ? 0 : 16, c1 = min((dq & 10u) ? 40 : 24, S);
       // thread -> one column of the box and every nph-th row: the column's
       // wrapped index once, rows wrapped incrementally, no divisions per cell
-      const int bw = c1 - c0, nph = (32 * N_EPI) / bw;
-      if (L < nph * bw) {
+      const int bw = c1 - c0, nph = (32 * N_FLUSH) / bw;
+      if (dq != 0 && L < nph * bw) {
         const int col = c0 + L % bw;
         const int gv = wrapi(b0v + col, nv);
         int a = r0 + L / bw;
@@ -675,19 +709,19 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
 #pragma unroll 4
         for (; a < r1; a += nph) {
           const int o = a * PP + col;
-          const float re = planes[o] + planes[2 * PLANE_FLOATS + o];
-          const float im = planes[PLANE_FLOATS + o] + planes[3 * PLANE_FLOATS + o];
-          planes[o] = 0.f;
-          planes[PLANE_FLOATS + o] = 0.f;
-          planes[2 * PLANE_FLOATS + o] = 0.f;
-          planes[3 * PLANE_FLOATS + o] = 0.f;
+          const float re = pls[o] + pls[2 * PLANE_FLOATS + o];
+          const float im = pls[PLANE_FLOATS + o] + pls[3 * PLANE_FLOATS + o];
+          plw[o] = 0.f;
+          plw[PLANE_FLOATS + o] = 0.f;
+          plw[2 * PLANE_FLOATS + o] = 0.f;
+          plw[3 * PLANE_FLOATS + o] = 0.f;
           if (re != 0.f || im != 0.f)
             atomicAdd(grid + int64_t(gu) * nv + gv, make_float2(re * unscale, im * unscale));
           gu += nph;
           gu -= (gu >= nu) ? nu : 0;
         }
       }
-      named_bar(1, 32 * N_EPI);
+      mbar_arrive(&pl_empty[buf]);
     }
   }
 
