@@ -26,9 +26,9 @@
 //   loader warps (4)   : K-block records, permutation, then cp.async of the
 //                        coordinates and values of one round (8 K-blocks) into
 //                        a 16-slot ring;
-//   builder warps (12) : 3 threads per point (A rows of Re(c)ku, of Im(c)ku,
-//                        B row of kv): fold, Horner weights, FP16 hi/lo split,
-//                        placement; MN-major operand tiles in 2 stages;
+//   builder warps (8)  : 2 threads per point (A column: Re(c)ku and Im(c)ku, B
+//                        row: kv): fold, Horner weights, FP16 hi/lo split,
+//                        placement; MN-major operand tiles in 3 stages;
 //   MMA warp (1)       : one thread issues the MMAs of a round into the
 //                        accumulator of each K-block's quadrant and commits;
 //   epilogue warps (4) : read finished accumulators from tensor memory and add
@@ -82,10 +82,10 @@ constexpr int EPI_W0 = 0, N_EPI = 4;     // warps 0..3: tensor-memory lane quart
 constexpr int MMA_W0 = 4, N_MMA = 4;     // warp 4+q issues the MMAs of quadrant q
 constexpr int LOAD_W0 = 8, N_LOAD = 4;
 constexpr int FLUSH_W0 = 12, N_FLUSH = 4;   // planes -> grid
-constexpr int BUILD_W0 = 16, N_BUILD = 12;
-constexpr int WARPS = BUILD_W0 + N_BUILD;   // 28
-constexpr int THREADS = 32 * WARPS;         // 896
-constexpr int BUILDERS = 32 * N_BUILD;      // 384 = 3 groups x 128 point slots
+constexpr int BUILD_W0 = 16, N_BUILD = 8;
+constexpr int WARPS = BUILD_W0 + N_BUILD;   // 24
+constexpr int THREADS = 32 * WARPS;         // 768
+constexpr int BUILDERS = 32 * N_BUILD;      // 256 = 2 groups x 128 point slots
 
 // K-block record in global memory: {first sorted point index, meta}
 //   meta bits 0-4 points (0..16), 5-6 quadrant, 7 last record of its quadrant
@@ -469,10 +469,12 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (warp >= BUILD_W0) {
     // ------------------------------------------------------------ builders
+    // Two threads per point: group 0 builds the point's A column (ku times
+    // Re(c) and Im(c), hi and lo: four parts), group 1 its B row (kv, hi and lo).
     const int bt = tid - BUILD_W0 * 32;
-    const int grp = bt >> 7;   // 0: Re A rows, 1: Im A rows, 2: B row
+    const int grp = bt >> 7;   // 0: A column, 1: B row
     const int slot = bt & 127, kbl = slot >> 4, e = slot & 15;
-    const int d = (grp == 2) ? 1 : 0;
+    const int d = grp;
     for (int r = 0; r < nrounds; ++r) {
       const int ps = r % NPRE;
       if (!mbar_wait(&pre_full[ps], uint32_t((r / NPRE) & 1), abortp, err)) break;
@@ -481,16 +483,22 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
       const int np = int(kr.meta & 31u);
       const bool valid = e < np;
       Tc x = Tc(0);
-      float sc = 0.f;
+      float s0 = 0.f, s1 = 0.f;
       if (valid) {
         x = reinterpret_cast<const Tc *>(sl + PL_::COORD)[2 * slot + d];
-        const float2 v = reinterpret_cast<const float2 *>(sl + PL_::VAL)[slot];
-        sc = (grp == 0) ? v.x * sA : ((grp == 1) ? v.y * sA : sB);
+        if (grp == 0) {
+          const float2 v = reinterpret_cast<const float2 *>(sl + PL_::VAL)[slot];
+          s0 = v.x * sA;
+          s1 = v.y * sA;
+        } else {
+          s0 = sB;
+        }
       }
       mbar_arrive(&pre_empty[ps]);
-      uint32_t hw[2][4];
+      // part words: A: 0 Re hi, 1 Im hi, 2 Re lo, 3 Im lo; B: 0 hi, 1 lo
+      uint32_t hw[4][4];
 #pragma unroll
-      for (int w = 0; w < 4; ++w) hw[0][w] = hw[1][w] = 0u;
+      for (int w = 0; w < 4; ++w) hw[0][w] = hw[1][w] = hw[2][w] = hw[3][w] = 0u;
       int off = 0;
       if (valid) {
         int i0;
@@ -499,10 +507,19 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         off = i0 - (d ? kr.b0v : kr.b0u);
         float k[W];
         kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fr), k);
+        if (grp == 0) {
 #pragma unroll
-        for (int w = 0; w < 4; ++w)
-          split2((2 * w < W) ? k[2 * w] * sc : 0.f, (2 * w + 1 < W) ? k[2 * w + 1] * sc : 0.f,
-                 hw[0][w], hw[1][w]);
+          for (int w = 0; w < 4; ++w) {
+            const float k0 = (2 * w < W) ? k[2 * w] : 0.f, k1 = (2 * w + 1 < W) ? k[2 * w + 1] : 0.f;
+            split2(k0 * s0, k1 * s0, hw[0][w], hw[2][w]);
+            split2(k0 * s1, k1 * s1, hw[1][w], hw[3][w]);
+          }
+        } else {
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            split2((2 * w < W) ? k[2 * w] * s0 : 0.f, (2 * w + 1 < W) ? k[2 * w + 1] * s0 : 0.f,
+                   hw[0][w], hw[1][w]);
+        }
       }
       const int s = r % NST;
       if (r >= NST &&
@@ -512,22 +529,17 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         unsigned char *stA = stages + s * STAGE_BYTES;
         const int c0 = off >> 3;   // 0 or 1: taps in chunks c0, c0+1 of the part
         const int cz = (c0 == 0) ? 2 : 0;
-        uint32_t base, pstep;
-        if (grp < 2) {
-          // A column of point e: part p (rows 24p..24p+23); group g owns
-          // parts g (hi) and g+2 (lo)
-          base = smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO +
-                 uint32_t(grp * PART) * SBO;
-          pstep = uint32_t(2 * PART) * SBO;
-        } else {
-          // B row of point e: part h columns 24h..24h+23
-          base = smem_u32(stA + ROUND * A_BYTES + kbl * B_BYTES) + (e & 7) * 16 +
-                 (e >> 3) * B_LBO;
-          pstep = uint32_t(PART) * SBO;
-        }
+        // A column of point e: part p at rows 24p..24p+23; B row of point e:
+        // part h at columns 24h..24h+23
+        const uint32_t base =
+            grp == 0 ? smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO
+                     : smem_u32(stA + ROUND * A_BYTES + kbl * B_BYTES) + (e & 7) * 16 +
+                           (e >> 3) * B_LBO;
+        const int nparts = grp == 0 ? 4 : 2;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const uint32_t pb = base + uint32_t(h) * pstep;
+        for (int h = 0; h < 4; ++h) {
+          if (h >= nparts) break;
+          const uint32_t pb = base + uint32_t(h * PART) * SBO;
           if (valid) {
             uint32_t z[8];
             place8(hw[h], off & 7, z);
