@@ -214,6 +214,15 @@ __global__ void __launch_bounds__(SP_THREADS)
 
 // One chunk of one transform (the body of k_interp; also used by the
 // multi-instance kernel of batched transforms).
+// scratch of the bank-balanced interpolation order (after the tile buffer)
+template <typename T> struct InterpOrder {
+  static constexpr int NSLOT = 128 / int(sizeof(cplx<T>));   // 8-/16-byte bank slots
+  static constexpr int IB = 1024;                             // points per sorted batch
+  // slot counters, then per-point records: output index, first cell, kernel
+  // argument per axis
+  static constexpr size_t bytes(int ndim) { return NSLOT * 4 + IB * (8 + ndim * sizeof(T)); }
+};
+
 template <typename T, typename Tc, int NDIM, int W>
 __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk ch, const Geometry &g,
                                              const KernelPoly<T> &kp,
@@ -245,8 +254,7 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
     }
     __syncthreads();
   }
-  const uint32_t end = ch.start + ch.count;
-  for (uint32_t i = ch.start + threadIdx.x; i < end; i += SP_THREADS) {
+  auto point = [&](uint32_t i) {
     Tc x[NDIM];
     uint32_t j = load_point<Tc, NDIM>(pts, i, x);
     T w[NDIM][W];
@@ -331,11 +339,151 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
       }
     }
     out[int64_t(j) * os] = mkc<T>(ar, ai);
+  };
+  const uint32_t end = ch.start + ch.count;
+  if constexpr (!SMEM) {
+    for (uint32_t i = ch.start + threadIdx.x; i < end; i += SP_THREADS) point(i);
+  } else {
+    // Bank-balanced order.  At a given step of the footprint loop all lanes of
+    // a warp read at the same offset from their point's first cell, so the
+    // bank conflicts of that read depend only on the first cells' banks.  Each
+    // batch of IB points is folded once (coalesced coordinate reads), its
+    // records (output index, first cell, kernel arguments) kept in registers,
+    // counting-sorted by bank slot of the first cell (cell index mod 128 bytes
+    // / cell size, NSLOT slots) and written to shared memory so that, at step
+    // r, lane NSLOT*h + l of a warp takes sorted entry p*q + r with
+    // p = l*(32/NSLOT) + h (q = ceil(n/32)) from word r*32 + p: the NSLOT lanes
+    // of one 128-byte wavefront group (a half-warp for 8-byte cells, a
+    // quarter-warp for 16-byte ones) take entries spread over the whole sorted
+    // list, one per slot for uniformly spread points, and all lanes read their
+    // records without conflicts.  Every point is still computed by one thread
+    // in a fixed order, so results do not depend on the assignment.
+    using IO = InterpOrder<T>;
+    constexpr int NSLOT = IO::NSLOT, IB = IO::IB, PER = IB / SP_THREADS;
+    int *s_cnt = reinterpret_cast<int *>(smraw + size_t(ncell) * sizeof(cplx<T>));
+    uint32_t *r_j = reinterpret_cast<uint32_t *>(s_cnt + NSLOT);
+    int *r_base = reinterpret_cast<int *>(r_j + IB);
+    T *r_t = reinterpret_cast<T *>(r_base + IB);   // [NDIM][IB]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t s0 = ch.start; s0 < end; s0 += IB) {
+      const int nb = int(min(uint32_t(IB), end - s0));
+      const int q = (nb + 31) >> 5;
+      if (threadIdx.x < NSLOT) s_cnt[threadIdx.x] = 0;
+      __syncthreads();
+      uint32_t pj[PER];
+      int pb[PER];
+      T pt[PER][NDIM];
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int li = k * SP_THREADS + int(threadIdx.x);
+        pb[k] = -1;
+        if (li < nb) {
+          Tc x[NDIM];
+          pj[k] = load_point<Tc, NDIM>(pts, s0 + uint32_t(li), x);
+          int base = 0;
+#pragma unroll
+          for (int d = 0; d < NDIM; ++d) {
+            int i0;
+            double frac;
+            fold<Tc>(x[d], g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], i0, frac);
+            pt[k][d] = T(double(W - 1) - 2.0 * frac);
+            base = base * S + (i0 - b0[d]);
+          }
+          pb[k] = base;
+          atomicAdd(&s_cnt[base & (NSLOT - 1)], 1);
+        }
+      }
+      __syncthreads();
+      if (warp == 0) {   // exclusive prefix over the slots
+        const int c = lane < NSLOT ? s_cnt[lane] : 0;
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        __syncwarp();
+        if (lane < NSLOT) s_cnt[lane] = incl - c;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        if (pb[k] >= 0) {
+          const int e = atomicAdd(&s_cnt[pb[k] & (NSLOT - 1)], 1);
+          const int w = (e % q) * 32 + e / q;
+          r_j[w] = pj[k];
+          r_base[w] = pb[k];
+#pragma unroll
+          for (int d = 0; d < NDIM; ++d) r_t[d * IB + w] = pt[k][d];
+        }
+      }
+      __syncthreads();
+      const int pl = (lane % NSLOT) * (32 / NSLOT) + lane / NSLOT;
+      for (int r = warp; r < q; r += SP_WARPS) {
+        if (pl * q + r >= nb) continue;
+        const int w = r * 32 + pl;
+        const uint32_t j = r_j[w];
+        const cplx<T> *p0 = buf + r_base[w];
+        T wt[NDIM][W];
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) kernel_weights<T, W>(kp, r_t[d * IB + w], wt[d]);
+        T ar = 0, ai = 0;
+        if constexpr (NDIM == 1) {
+#pragma unroll
+          for (int a = 0; a < W; ++a) {
+            cplx<T> gv = p0[a];
+            ar += wt[0][a] * gv.x;
+            ai += wt[0][a] * gv.y;
+          }
+        } else if constexpr (NDIM == 2) {
+#pragma unroll
+          for (int a = 0; a < W; ++a) {
+            const cplx<T> *row = p0 + a * S;
+            T rr = 0, ri = 0;
+#pragma unroll
+            for (int b = 0; b < W; ++b) {
+              cplx<T> gv = row[b];
+              rr += wt[1][b] * gv.x;
+              ri += wt[1][b] * gv.y;
+            }
+            ar += wt[0][a] * rr;
+            ai += wt[0][a] * ri;
+          }
+        } else {
+#pragma unroll 1
+          for (int a = 0; a < W; ++a) {
+            T pr = 0, pi = 0;
+#pragma unroll
+            for (int b = 0; b < W; ++b) {
+              const cplx<T> *row = p0 + (a * S + b) * S;
+              T rr = 0, ri = 0;
+#pragma unroll
+              for (int e = 0; e < W; ++e) {
+                cplx<T> gv = row[e];
+                rr += wt[2][e] * gv.x;
+                ri += wt[2][e] * gv.y;
+              }
+              pr += wt[1][b] * rr;
+              pi += wt[1][b] * ri;
+            }
+            ar += wt[0][a] * pr;
+            ai += wt[0][a] * pi;
+          }
+        }
+        out[int64_t(j) * os] = mkc<T>(ar, ai);
+      }
+      __syncthreads();
+    }
   }
 }
 
+// five CTAs per SM for single-precision 1D/2D (fits 48 registers without spills)
+template <typename T, int NDIM> constexpr int interp_min_ctas() {
+  return (sizeof(T) == 4 && NDIM < 3) ? 5 : 1;
+}
+
 template <typename T, typename Tc, int NDIM, int W>
-__global__ void __launch_bounds__(SP_THREADS)
+__global__ void __launch_bounds__(SP_THREADS, interp_min_ctas<T, NDIM>())
     k_interp(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
              const cplx<T> *__restrict__ grid, int64_t gtrans, cplx<T> *__restrict__ out,
              int64_t os, int64_t otrans) {
@@ -361,7 +509,7 @@ size_t interp_smem_bytes(const Geometry &g) {
   int S = (1 << g.log2tile) + W;
   size_t ncell = size_t(S);
   for (int d = 1; d < NDIM; ++d) ncell *= size_t(S);
-  return BufferLayout<T>::smem(NDIM) ? ncell * sizeof(cplx<T>) : 0;
+  return BufferLayout<T>::smem(NDIM) ? ncell * sizeof(cplx<T>) + InterpOrder<T>::bytes(NDIM) : 0;
 }
 
 template <typename T, typename Tc, int NDIM, int W>
