@@ -21,7 +21,11 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 
 namespace dnufft {
 
@@ -398,6 +402,12 @@ __device__ __forceinline__ void dft_const(cplx<T> (&a)[R], bool fwd) {
   }
 }
 
+}  // namespace dnufft
+
+#include "fft_pencil.cuh"
+
+namespace dnufft {
+
 template <typename T>
 __device__ __forceinline__ cplx<T> tw2(const cplx<T> *twh, const cplx<T> *twl, int t, bool fwd) {
   cplx<T> w = cmul<T>(twh[t >> 6], twl[t & 63]);
@@ -676,36 +686,50 @@ __device__ __forceinline__ void fft_aligned(int a, int b, int esz, int &a2, int 
   if (b2 < a2) b2 = a2;
 }
 
-template <typename T> constexpr int rows_threads() { return sizeof(T) == 4 ? 1024 : 512; }
+#ifndef ROWS_MAXR_F
+#define ROWS_MAXR_F 25
+#define ROWS_MAXR_D 16
+#define COLS_MAXR_F 12
+#define COLS_MAXR_D 11
+#endif
+// every prime factor the planner allows (up to 11) must fit one pass
+static_assert(ROWS_MAXR_F >= 11 && ROWS_MAXR_D >= 11 && COLS_MAXR_F >= 11 && COLS_MAXR_D >= 11,
+              "pencil radix bound below the largest prime factor");
+
+// largest pencil radix of the row and column passes (register budgets of their
+// CTAs: 512 / 256 threads per SM for rows, several 256-thread CTAs for columns)
+template <typename T> constexpr int rows_maxr() { return sizeof(T) == 4 ? ROWS_MAXR_F : ROWS_MAXR_D; }
+template <typename T> constexpr int cols_maxr() { return sizeof(T) == 4 ? COLS_MAXR_F : COLS_MAXR_D; }
+// column CTAs per SM the register allocation must allow (64 / 80 registers)
+template <typename T> constexpr int cols_min_ctas() { return sizeof(T) == 4 ? 4 : 3; }
+template <typename T> constexpr int rows_threads() { return 512; }
 
 // One row = line of n contiguous elements at grid + row*rs.  Ranges: the whole
 // line, or the kept ranges [0, lo) and [hi0, n) (zeros in between on input).
-template <typename T>
+// Two row buffers: the current row is transformed in place while the next one
+// arrives by TMA bulk copy into the other; the result is written back by bulk
+// stores from the current buffer, which becomes the prefetch target of the
+// row after next once those stores have read it.
+template <typename T, bool FWD>
 __global__ void __launch_bounds__(rows_threads<T>(), 1)
     k_fft_rows(cplx<T> *__restrict__ grid, int64_t rs, int n, int nlines, int lo, int hi0,
-               int in_kept, int out_kept, StageInfo si, const cplx<T> *__restrict__ tw, bool fwd,
+               int in_kept, int out_kept, PencilPlan pp, const cplx<T> *__restrict__ tw,
                int *__restrict__ err) {
   extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bars[3];
-  __shared__ int stR[24], stNs[24], stT[24];
-  __shared__ uint32_t stM[24];
+  __shared__ uint64_t bars[2];
+  __shared__ PencilPlan spp;
   __shared__ int s_fail;
   constexpr int ES = int(sizeof(cplx<T>));
   cplx<T> *bufs = reinterpret_cast<cplx<T> *>(smraw);
   const int nh = (n + 63) / 64 + 1;
-  cplx<T> *twl = bufs + 3 * n;
+  cplx<T> *twl = bufs + 2 * n;
   cplx<T> *twh = twl + 64;
   const int tid = threadIdx.x;
-  if (tid < 24) {
-    stR[tid] = si.R[tid];
-    stNs[tid] = si.Ns[tid];
-    stT[tid] = si.tstep[tid];
-    stM[tid] = si.mul[tid];
-  }
+  if (tid == 0) spp = pp;
   for (int i = tid; i < 64; i += blockDim.x) twl[i] = (i < n) ? tw[i] : mkc<T>(T(1), T(0));
   for (int i = tid; i < nh; i += blockDim.x) twh[i] = (64 * i < n) ? tw[64 * i] : mkc<T>(T(1), T(0));
   if (tid == 0) {
-    for (int b = 0; b < 3; ++b) fft_bar_init(&bars[b], 1);
+    for (int b = 0; b < 2; ++b) fft_bar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
   }
@@ -728,7 +752,7 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
       if (b2[r] > a2[r])
         fft_bulk_load(dst + a2[r], src + a2[r], uint32_t(b2[r] - a2[r]) * ES, &bars[b]);
   };
-  int bi = 0, bt = 1, bf = 2;
+  int bi = 0, bf = 1;
   uint32_t ph = 0;   // bit b: parity of the next completion of bars[b]
   if (tid == 0 && int(blockIdx.x) < nlines) issue_load(blockIdx.x, bi);
   for (int L = blockIdx.x; L < nlines; L += gridDim.x) {
@@ -757,24 +781,9 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
       if (tid == 0) atomicExch(err, 1);
       break;
     }
-    cplx<T> *sa = in, *sb = bufs + bt * n;
-    for (int f = 0; f < si.nst; ++f) {
-      const int R = stR[f], Ns = stNs[f], ts = stT[f];
-      const uint32_t mul = stM[f];
-      switch (R) {
-        case 2: stage2<T, 2>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        case 3: stage2<T, 3>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        case 4: stage2<T, 4>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        case 5: stage2<T, 5>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        case 7: stage2<T, 7>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        case 8: stage2<T, 8>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        case 11: stage2<T, 11>(sa, sb, n, 0, Ns, mul, ts, twh, twl, fwd); break;
-        default: break;
-      }
-      cplx<T> *t = sa;
-      sa = sb;
-      sb = t;
-    }
+    // all passes in place in the input buffer
+    pencil_fft_inplace<T, FWD, rows_maxr<T>()>(in, spp, twh, twl);
+    const cplx<T> *sa = in;
     // result in sa; write it back (bulk part by thread 0, ragged ends by all)
     cplx<T> *dst = grid + int64_t(L) * rs;
     const int nro = out_kept ? 2 : 1;
@@ -798,16 +807,15 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
       }
       asm volatile("cp.async.bulk.commit_group;" ::: "memory");
     }
-    // rotate: the prefetched buffer is next, the result buffer is busy storing
-    const int br = int((sa - bufs) / n);
-    const int bo = (br == bi) ? bt : bi;
+    // the prefetched buffer is next; this one is busy storing
+    const int t = bi;
     bi = bf;
-    bt = bo;
-    bf = br;
+    bf = t;
   }
   if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   __syncthreads();
 }
+
 
 // Four-step column pass.  PASS 0 = A, 1 = B.  Columns: x in [0, N1) kept
 // columns (grid column kept_to_grid(x)); C = 1 << lc columns per CTA.
@@ -820,10 +828,10 @@ struct ColSpec {
   int out_mode; // pass A: work; pass B: 0 grid (natural order), 1 uniform array (type 1)
 };
 
-template <typename T, int PASS>
-__global__ void __launch_bounds__(256)
+template <typename T, int PASS, bool FWD>
+__global__ void __launch_bounds__(256, cols_min_ctas<T>())
     k_fft_colstep(cplx<T> *__restrict__ grid, cplx<T> *__restrict__ work, ColSpec cs,
-                  StageInfo si, const cplx<T> *__restrict__ tw, UniSpec u, bool fwd) {
+                  PencilPlan pp, const cplx<T> *__restrict__ tw, UniSpec u) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int C = 1 << cs.lc;
   const int len = PASS == 0 ? cs.P : cs.Q;    // DFT length of this pass
@@ -833,15 +841,9 @@ __global__ void __launch_bounds__(256)
   cplx<T> *s2 = s + len * C;
   cplx<T> *twl = s2 + len * C;
   cplx<T> *twh = twl + 64;
-  __shared__ int stR[24], stNs[24], stT[24];
-  __shared__ uint32_t stM[24];
+  __shared__ PencilPlan spp;
   const int tid = threadIdx.x;
-  if (tid < 24) {
-    stR[tid] = si.R[tid];
-    stNs[tid] = si.Ns[tid];
-    stT[tid] = si.tstep[tid];
-    stM[tid] = si.mul[tid];
-  }
+  if (tid == 0) spp = pp;
   for (int i = tid; i < 64; i += blockDim.x)
     twl[i] = (i < len) ? tw[i * tstr] : mkc<T>(T(1), T(0));
   for (int i = tid; i < nh; i += blockDim.x)
@@ -879,24 +881,8 @@ __global__ void __launch_bounds__(256)
     s[idx] = v;
   }
   __syncthreads();
-  cplx<T> *sa = s, *sb = s2;
-  for (int f = 0; f < si.nst; ++f) {
-    const int R = stR[f], Ns = stNs[f], ts = stT[f];
-    const uint32_t mul = stM[f];
-    switch (R) {
-      case 2: stage2<T, 2>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      case 3: stage2<T, 3>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      case 4: stage2<T, 4>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      case 5: stage2<T, 5>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      case 7: stage2<T, 7>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      case 8: stage2<T, 8>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      case 11: stage2<T, 11>(sa, sb, len, cs.lc, Ns, mul, ts, twh, twl, fwd); break;
-      default: break;
-    }
-    cplx<T> *t = sa;
-    sa = sb;
-    sb = t;
-  }
+  pencil_fft<T, FWD, cols_maxr<T>()>(s, s2, C, cs.lc, spp, twh, twl);
+  const cplx<T> *sa = s2;
   // ---- store
   for (int idx = tid; idx < len * C; idx += blockDim.x) {
     const int m = idx >> cs.lc, c = idx & (C - 1);
@@ -904,10 +890,9 @@ __global__ void __launch_bounds__(256)
     if (x >= cs.N1) continue;
     cplx<T> v = sa[idx];
     if (PASS == 0) {
-      // twiddle w_n^(q*k1), then work row q + Q*k1
-      const int t = int((int64_t(g) * m) % cs.n);
-      cplx<T> w = tw[t];
-      if (!fwd) w.y = -w.y;
+      // twiddle w_n^(q*k1) (q*k1 < Q*P = n), then work row q + Q*k1
+      cplx<T> w = tw[g * m];
+      if (!FWD) w.y = -w.y;
       v = cmul<T>(v, w);
       work[int64_t(g + cs.Q * m) * cs.N1 + x] = v;
     } else {
@@ -942,14 +927,70 @@ static bool split_pq(int n, int &P, int &Q) {
   return P <= 1024 && Q <= 1024;
 }
 
-static StageInfo stages_for(int len) {
-  FFTAxisPlan p;
-  std::memset(&p, 0, sizeof(p));
-  p.n = len;
-  auto f = fft_factors(len);
-  p.nfac = int(f.size());
-  for (int i = 0; i < p.nfac; ++i) p.fac[i] = f[i];
-  return make_stages(p);
+// Radix sequence of the pencil passes for a line of length n: the fewest
+// passes with radices of a register DFT up to maxr; among those, an odd last
+// radix and an odd product of the radices before the last two (the strides of
+// the last pass's shared-memory reads and writes of rows, conflict-free when
+// odd), then the smallest largest radix.  maxlast bounds the groups of the
+// last pass (n / R_L), which the in-place row transform gives one thread each.
+// Cached per (n, maxr, maxlast).
+static bool make_pencil(int n, int maxr, int maxlast, PencilPlan &pp) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int>, std::pair<bool, PencilPlan>> cache;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({n, maxr, maxlast});
+    if (it != cache.end()) {
+      pp = it->second.second;
+      return it->second.first;
+    }
+  }
+  static const int rad[] = {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 14,
+                            15, 16, 18, 20, 21, 22, 24, 25, 27, 28, 30, 32};
+  std::vector<int> cur, best;
+  long best_score = -1;
+  std::function<void(int)> rec = [&](int rem) {
+    if (rem == 1) {
+      const int L = int(cur.size());
+      if (n / cur[L - 1] > maxlast) return;
+      int mx = 0, pre = 1;
+      for (int i = 0; i < L; ++i) mx = std::max(mx, cur[i]);
+      for (int i = 0; i + 2 < L; ++i) pre *= cur[i];
+      const int conflicts = (cur[L - 1] % 2 == 0) + (pre % 2 == 0);
+      const long score = long(L) * 1000000 + conflicts * 10000 + mx * 10 + (cur[0] % 2 == 0);
+      if (best_score < 0 || score < best_score) {
+        best_score = score;
+        best = cur;
+      }
+      return;
+    }
+    if (int(cur.size()) == PEN_MAXL) return;
+    for (int r : rad) {
+      if (r > maxr || rem % r) continue;
+      cur.push_back(r);
+      rec(rem / r);
+      cur.pop_back();
+    }
+  };
+  if (n >= 2) rec(n);
+  std::memset(&pp, 0, sizeof(pp));
+  const bool ok = !best.empty();
+  if (ok) {
+    pp.n = n;
+    pp.L = int(best.size());
+    int m = n, P = 1;
+    for (int i = 0; i < pp.L; ++i) {
+      pp.R[i] = best[i];
+      m /= best[i];
+      pp.m[i] = m;
+      pp.P[i] = P;
+      pp.mmul[i] = m <= 1 ? 0u : uint32_t(((uint64_t(1) << 32) + uint64_t(m) - 1) / uint64_t(m));
+      P *= best[i];
+    }
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  cache[{n, maxr, maxlast}] = {ok, pp};
+  return ok;
 }
 
 static int sm_count_dev() {
@@ -966,17 +1007,17 @@ static bool run_rows_v3(cplx<T> *grid, int n, int nlines, int64_t rs, int Nk, bo
                         cudaStream_t st) {
   if (err == nullptr || nlines <= 0) return false;
   const int nh = (n + 63) / 64 + 1;
-  const size_t sm = size_t(3 * n + 64 + nh) * sizeof(cplx<T>);
-  if (sm > 220 * 1024 || n < 1024) return false;
-  for (int f = 0; f < p.nfac; ++f)
-    if (p.fac[f] > 11) return false;
+  const size_t sm = size_t(2 * n + 64 + nh) * sizeof(cplx<T>);
+  if (sm > 224 * 1024 || n < 1024) return false;
+  PencilPlan pp;
+  if (!make_pencil(n, rows_maxr<T>(), rows_threads<T>(), pp)) return false;
   const int lo = (Nk + 1) / 2, hi0 = n - Nk / 2;
-  StageInfo si = make_stages(p);
-  DN_CUDA(cudaFuncSetAttribute(k_fft_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  auto kern = fwd ? k_fft_rows<T, true> : k_fft_rows<T, false>;
+  DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   const int nb = std::min(nlines, sm_count_dev());
-  k_fft_rows<T><<<nb, rows_threads<T>(), sm, st>>>(grid, rs, n, nlines, lo, hi0, in_kept ? 1 : 0,
-                                                   out_kept ? 1 : 0, si,
-                                                   static_cast<const cplx<T> *>(p.tw), fwd, err);
+  kern<<<nb, rows_threads<T>(), sm, st>>>(grid, rs, n, nlines, lo, hi0, in_kept ? 1 : 0,
+                                          out_kept ? 1 : 0, pp, static_cast<const cplx<T> *>(p.tw),
+                                          err);
   DN_LAUNCHED();
   return true;
 }
@@ -989,6 +1030,9 @@ static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
   if (work == nullptr || n0 < 1024) return false;
   int P, Q;
   if (!split_pq(n0, P, Q)) return false;
+  PencilPlan ppP, ppQ;
+  if (!make_pencil(P, cols_maxr<T>(), 1 << 30, ppP) || !make_pencil(Q, cols_maxr<T>(), 1 << 30, ppQ))
+    return false;
   const int lc = sizeof(T) == 4 ? 5 : 4;   // 32 (complex64) or 16 (complex128) columns
   const int C = 1 << lc;
   ColSpec cs;
@@ -1011,19 +1055,17 @@ static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
   {
     const int nh = (P + 63) / 64 + 1;
     const size_t sm = size_t(2 * P * C + 64 + nh) * sizeof(cplx<T>);
-    DN_CUDA(cudaFuncSetAttribute(k_fft_colstep<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sm)));
-    k_fft_colstep<T, 0><<<unsigned(nblk) * unsigned(Q), 256, sm, st>>>(grid, work, cs,
-                                                                       stages_for(P), tw, u, fwd);
+    auto kern = fwd ? k_fft_colstep<T, 0, true> : k_fft_colstep<T, 0, false>;
+    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    kern<<<unsigned(nblk) * unsigned(Q), 256, sm, st>>>(grid, work, cs, ppP, tw, u);
     DN_LAUNCHED();
   }
   {
     const int nh = (Q + 63) / 64 + 1;
     const size_t sm = size_t(2 * Q * C + 64 + nh) * sizeof(cplx<T>);
-    DN_CUDA(cudaFuncSetAttribute(k_fft_colstep<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sm)));
-    k_fft_colstep<T, 1><<<unsigned(nblk) * unsigned(P), 256, sm, st>>>(grid, work, cs,
-                                                                       stages_for(Q), tw, u, fwd);
+    auto kern = fwd ? k_fft_colstep<T, 1, true> : k_fft_colstep<T, 1, false>;
+    DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    kern<<<unsigned(nblk) * unsigned(P), 256, sm, st>>>(grid, work, cs, ppQ, tw, u);
     DN_LAUNCHED();
   }
   return true;
