@@ -38,10 +38,10 @@ KERNEL_NAMES = {"tc": "k_spread_tc (split-precision tensor-core spreader)",
                 "plain": "k_spread (plain FP32 atomic spreader)",
                 "auto": "k_spread (plain FP32 atomic spreader)"}
 # DRAM bytes per spreading launch at the full workload: ncu dram__bytes_read.sum
-# + dram__bytes_write.sum of one launch at 2048^2 / M=1.25e7 (the same points per
-# tile), times 4 (profiles/k_spread_*_2048sq_M12.5M.md)
-TRAFFIC_PER_LAUNCH = {"tc": 4 * (905.697280e6 + 120.017664e6),
-                      "plain": 4 * (878.126080e6 + 111.346432e6)}
+# + dram__bytes_write.sum (a one-pass metric set) of launches of this bench's
+# default command (profiles/launches_bench_4096sq_M5e7.md)
+TRAFFIC_PER_LAUNCH = {"tc": 6460321536.0 + 528613120.0,
+                      "plain": 6345106944.0 + 451456000.0}
 
 
 def clustered_coords(rng, m, ncl=16, sigma=0.3):

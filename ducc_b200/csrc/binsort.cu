@@ -15,6 +15,8 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <algorithm>
+
 namespace dnufft {
 
 // ---------------------------------------------------------------- keys
@@ -247,6 +249,16 @@ size_t radix_workspace_bytes(uint32_t n, int keybits) {
          + scan_workspace_bytes(hn) + 1024;
 }
 
+// element-wise copy of the sorted pairs back (the ping-pong halves of the
+// workspace are only 4-byte aligned)
+__global__ void k_copy_pairs(const uint32_t *__restrict__ ka, const uint32_t *__restrict__ va,
+                             uint32_t *__restrict__ kb, uint32_t *__restrict__ vb, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    kb[i] = ka[i];
+    vb[i] = va[i];
+  }
+}
+
 // Sorts (keys, vals) in place by the low 'keybits' bits of keys, stably.
 void radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t n, int keybits, void *ws,
                       cudaStream_t st) {
@@ -289,8 +301,11 @@ void radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t n, int keybits, v
     std::swap(va, vb);
   }
   if (ka != keys) {
-    DN_CUDA(cudaMemcpyAsync(keys, ka, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
-    DN_CUDA(cudaMemcpyAsync(vals, va, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+    // a kernel, not a device-to-device memcpy: a copy engine may be busy with a
+    // host transfer of the same call on another stream
+    const unsigned nb = unsigned(std::min<uint64_t>((uint64_t(n) + 255) / 256, 148 * 16));
+    k_copy_pairs<<<nb, 256, 0, st>>>(ka, va, keys, vals, n);
+    DN_LAUNCHED();
   }
 }
 

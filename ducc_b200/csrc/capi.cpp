@@ -37,6 +37,7 @@ namespace dnufft {
 
 constexpr uint32_t CHUNK = 1024;       // points per chunk (one CTA)
 constexpr uint32_t CHUNK_TC = 4096;    // tensor-core plans: fewer, longer chunks
+constexpr double TC_AUTO_DENSITY = 0.5;   // points per uniform mode from which 'auto' picks TC
 
 // ---------------------------------------------------------------- device buffers
 // Keep memory freed with cudaFreeAsync in the device's default pool instead of
@@ -221,14 +222,49 @@ static int64_t nelem(const View &v) {
   return s;
 }
 
+// A second stream of an unplanned call on host arrays: host->device copies
+// (and work that needs only them) run there while the caller's stream builds
+// the index, forked from and joined back into the caller's stream by events.
+struct SideStream {
+  cudaStream_t main, s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  explicit SideStream(cudaStream_t m) : main(m) {
+    DN_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DN_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    DN_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  }
+  // the side stream continues after everything queued on the main stream so far
+  void start() {
+    DN_CUDA(cudaEventRecord(fork, main));
+    DN_CUDA(cudaStreamWaitEvent(s, fork, 0));
+  }
+  // the main stream continues after everything queued on the side stream so far
+  void merge() {
+    DN_CUDA(cudaEventRecord(join, s));
+    DN_CUDA(cudaStreamWaitEvent(main, join, 0));
+  }
+  ~SideStream() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+  }
+};
+
 // Device-side copy of a host array (inputs copied in, outputs copied back).
+// The buffer is allocated on the caller's stream; with a side stream, the
+// input copy runs there (after the caller's stream's work so far).
 struct Staged {
   View dev;
   DevBuf buf;
   const View *orig = nullptr;
   bool is_output = false;
   cudaStream_t st;
-  Staged(const View &v, bool input, bool output, cudaStream_t s) : st(s) {
+  cudaStream_t side = nullptr;
+  Staged(const View &v, bool input, bool output, cudaStream_t s, SideStream *ss = nullptr)
+      : st(s) {
     dev = v;
     orig = &v;
     is_output = output && v.host;
@@ -237,7 +273,19 @@ struct Staged {
     buf = DevBuf(bytes, s);
     dev.data = buf.p;
     dev.host = false;
-    if (input && bytes) DN_CUDA(cudaMemcpyAsync(buf.p, v.data, bytes, cudaMemcpyHostToDevice, s));
+    if (!input || !bytes) return;
+    if (ss) {
+      ss->start();
+      side = ss->s;
+      DN_CUDA(cudaMemcpyAsync(buf.p, v.data, bytes, cudaMemcpyHostToDevice, side));
+    } else {
+      DN_CUDA(cudaMemcpyAsync(buf.p, v.data, bytes, cudaMemcpyHostToDevice, s));
+    }
+  }
+  ~Staged() {
+    // an exception may leave a side-stream copy in flight: finish it before
+    // the buffer returns to the caller's stream's pool
+    if (side) cudaStreamSynchronize(side);
   }
   void finish() {
     if (!is_output) return;
@@ -378,6 +426,14 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
     s.tile_shift = 3 * g.ssmall;
     s.max_tiles = prod;
   }
+  // automatic choice for type 1: the tensor-core spreader where it is the
+  // faster one (measured on B200 from 256^2 to 4096^2 grids, uniform and
+  // clustered points: from about half a point per uniform mode up; below that
+  // its per-tile set-up and flush cost more than the plain atomics)
+  if (s.spreader == DNUFFT_SPREAD_AUTO && gridding && ndim == 2 && !calc_f64 &&
+      spread_tc_supported(g, calc_f64) &&
+      double(npoints) >= TC_AUTO_DENSITY * double(nuni[0]) * double(nuni[1]))
+    s.spreader = DNUFFT_SPREAD_TC;
   if (s.spreader == DNUFFT_SPREAD_TC && spread_tc_supported(g, calc_f64)) {
     s.qbits = true;
     maxkey <<= 2;
@@ -545,15 +601,19 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
   if (wb && !work.p) work = DevBuf(wb, st);
   fft_nu2u_tail<T>(grid.p, s.g, dc.ax, forward, dc.cf, fft_order, out.data, out.stride, st,
                    work.p, err);
-  tm.mark("end");
+  tm.mark("output copy");   // last mark of a planned call; an unplanned call copies out next
   check_device_error(err, st);
 }
 
+// With a side stream, the FFT pass runs there and st waits for it before the
+// interpolation; the caller provides the grid and work buffers, allocated on
+// st before the side stream was last started (so the FFT does not wait for
+// whatever st queued after that, e.g. the index build).
 template <typename T>
 static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &pts,
                           const ChunkList &cl, const View &uni, const View &out, bool forward,
                           bool fft_order, StageTimer &tm, cudaStream_t st, DevBuf *ws = nullptr,
-                          DevBuf *wk = nullptr) {
+                          DevBuf *wk = nullptr, SideStream *side = nullptr) {
   size_t cells = grid_cells(s.g);
   DevBuf local;
   DevBuf &grid = ws ? *ws : local;
@@ -564,13 +624,20 @@ static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &
   if (wb && !work.p) work = DevBuf(wb, st);
   int *err = device_error_word();
   tm.mark("correction + FFT");
-  fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st,
-                   work.p, err);
+  if (side) {
+    DN_REQUIRE(ws && wk, ST_INTERNAL, "side-stream FFT without preallocated buffers");
+    fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p,
+                     side->s, work.p, err);
+    side->merge();
+  } else {
+    fft_u2nu_head<T>(uni.data, uni.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st,
+                     work.p, err);
+  }
   tm.mark("interpolation");
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
   launch_interp<T>(pts, cl, s.g, kp, grid.p, 0, out.data, out.stride[0], 0, 1, st);
-  tm.mark("end");
+  tm.mark("output copy");
   check_device_error(err, st);
 }
 
@@ -650,18 +717,28 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
                        coord.dtype == DNUFFT_F64, o);
   StageTimer tm(o.verbosity > 0, st);
   if (o.verbosity > 0) report_sizes(s, true);
-  Staged sp(points, true, false, st), sc(coord, true, false, st), so(out, false, true, st);
+  // constants first (small pageable copies, which would otherwise queue behind
+  // the large transfers on the copy engine)
+  tm.mark("upload constants");
+  DevConst dc;
+  if (s.npoints) upload_consts(s, dc, st);
+  tm.mark("coordinates host->device");
+  // host arrays: the coordinates next; the point values follow on a side
+  // stream while this stream builds the index
+  SideStream side(st);
+  Staged sc(coord, true, false, st);
+  Staged sp(points, true, false, st, points.host ? &side : nullptr), so(out, false, true, st);
   if (s.npoints == 0) {
+    side.merge();
     zero_view(so.dev, st);
     so.finish();
     return;
   }
-  tm.mark("upload constants");
-  DevConst dc;
-  upload_consts(s, dc, st);
   tm.mark("building index");
   Index ix;
   build_index(s, sc.dev, ix, st);
+  tm.mark("wait for values copy");
+  side.merge();
   PointsDesc pts{sc.dev.data, sc.dev.stride[0], sc.dev.stride[1], false, s.coord_f64,
                  ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
@@ -672,8 +749,9 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
   else
     do_spread_fft<float>(s, dc, pts, cl, &tb, sp.dev, so.dev, forward != 0,
                          o.fft_order != 0, tm, st);
-  tm.report("nu2u");
   so.finish();
+  tm.mark("end");
+  tm.report("nu2u");
 }
 
 static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int forward,
@@ -694,10 +772,20 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
   StageTimer tm(o.verbosity > 0, st);
   if (o.verbosity > 0) report_sizes(s, false);
   if (s.npoints == 0) return;
-  Staged su(uni, true, false, st), sc(coord, true, false, st), so(out, false, true, st);
   tm.mark("upload constants");
   DevConst dc;
   upload_consts(s, dc, st);
+  tm.mark("coordinates host->device");
+  // host arrays: the coordinates first; the uniform grid follows on a side
+  // stream, which also runs the FFT pass, while this stream builds the index
+  SideStream side(st);
+  Staged sc(coord, true, false, st), so(out, false, true, st);
+  Staged su(uni, true, false, st, uni.host ? &side : nullptr);
+  const size_t esz = f64 ? 16 : 8;
+  DevBuf grid(grid_cells(s.g) * esz, st), work;
+  const size_t wb = fft_work_bytes(s.g, esz);
+  if (wb) work = DevBuf(wb, st);
+  side.start();   // the FFT pass may use the buffers from here on
   tm.mark("building index");
   Index ix;
   build_index(s, sc.dev, ix, st);
@@ -705,11 +793,14 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
                  ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
   if (f64)
-    do_fft_interp<double>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
+    do_fft_interp<double>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st,
+                          &grid, &work, &side);
   else
-    do_fft_interp<float>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st);
-  tm.report("u2nu");
+    do_fft_interp<float>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st,
+                         &grid, &work, &side);
   so.finish();
+  tm.mark("end");
+  tm.report("u2nu");
 }
 
 static void u2nu_dcoord_impl(const dnufft_array *grid_, const dnufft_array *coord_, int forward,
@@ -991,6 +1082,9 @@ static void nu2u_scratch_impl(const dnufft_array *points_, const dnufft_array *c
   dnufft_opts o = resolved(opts_, false);
   DN_REQUIRE(o.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
              "the no-allocation entry point uses the plain spreader only");
+  // plain keys and chunks below (no tensor-core quadrant bits): 'auto' must
+  // not resolve to the tensor-core setup here
+  o.spreader = DNUFFT_SPREAD_PLAIN;
   View points = view_of(points_, "points"), coord = view_of(coord_, "coord"),
        out = view_of(out_, "out");
   DN_REQUIRE(!points.host && !coord.host && !out.host, ST_BADARG,

@@ -42,7 +42,9 @@ extern "C" {
 #define DNUFFT_C128 4
 
 /* spreader selection (type 1) */
-#define DNUFFT_SPREAD_AUTO 0   /* tensor-core form where it applies, else plain */
+/* AUTO: the tensor-core form for 2D complex64 type 1 with at least 0.5 points
+   per uniform mode (where it is measured faster), else plain */
+#define DNUFFT_SPREAD_AUTO 0
 #define DNUFFT_SPREAD_PLAIN 1  /* per-point FP32/FP64 atomics in shared memory   */
 #define DNUFFT_SPREAD_TC 2     /* split-precision FP16 tcgen05 tile contraction  */
 
