@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(256, cols_min_ctas<T>())
   const int N0 = sel3(u.N, 0);
   const int lo0 = (N0 + 1) / 2, hi00 = cs.n - N0 / 2;
   // ---- load the [len][C] tile (element m of column c at s[m*C + c])
-  for (int idx = tid; idx < len * C; idx += blockDim.x) {
+  auto load_elem = [&](int idx) -> cplx<T> {
     const int m = idx >> cs.lc, c = idx & (C - 1);
     const int x = x0 + c;
     cplx<T> v = mkc<T>(T(0), T(0));
@@ -878,7 +878,24 @@ __global__ void __launch_bounds__(256, cols_min_ctas<T>())
         v = work[int64_t(g * cs.Q + m) * cs.N1 + x];   // row Q*k1 + q
       }
     }
-    s[idx] = v;
+    return v;
+  };
+  {
+    constexpr int LB = 8;   // loads in flight per thread
+    const int tot = len * C;
+    for (int b0 = tid; b0 < tot; b0 += LB * int(blockDim.x)) {
+      cplx<T> v[LB];
+#pragma unroll
+      for (int u2 = 0; u2 < LB; ++u2) {
+        const int idx = b0 + u2 * int(blockDim.x);
+        v[u2] = idx < tot ? load_elem(idx) : mkc<T>(T(0), T(0));
+      }
+#pragma unroll
+      for (int u2 = 0; u2 < LB; ++u2) {
+        const int idx = b0 + u2 * int(blockDim.x);
+        if (idx < tot) s[idx] = v[u2];
+      }
+    }
   }
   __syncthreads();
   pencil_fft<T, FWD, cols_maxr<T>()>(s, s2, C, cs.lc, spp, twh, twl);

@@ -238,7 +238,9 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
   tile_origin<NDIM>(ch.tile, g, b0);
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
   if constexpr (SMEM) {
-    for (int c = threadIdx.x; c < ncell; c += SP_THREADS) {
+    // tile + halo, LB loads in flight per thread before their stores
+    constexpr int LB = 8;
+    auto cell = [&](int c) -> cplx<T> {
       int gi[NDIM];
       int rem = c;
 #pragma unroll
@@ -250,7 +252,20 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
 #pragma unroll
       for (int d = 0; d < NDIM; ++d)
         gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
-      buf[c] = grid[gidx];
+      return grid[gidx];
+    };
+    for (int c0 = threadIdx.x; c0 < ncell; c0 += LB * SP_THREADS) {
+      cplx<T> v[LB];
+#pragma unroll
+      for (int u = 0; u < LB; ++u) {
+        const int c = c0 + u * SP_THREADS;
+        v[u] = c < ncell ? cell(c) : mkc<T>(T(0), T(0));
+      }
+#pragma unroll
+      for (int u = 0; u < LB; ++u) {
+        const int c = c0 + u * SP_THREADS;
+        if (c < ncell) buf[c] = v[u];
+      }
     }
     __syncthreads();
   }
