@@ -225,21 +225,27 @@ static int64_t nelem(const View &v) {
 // A second stream of an unplanned call on host arrays: host->device copies
 // (and work that needs only them) run there while the caller's stream builds
 // the index, forked from and joined back into the caller's stream by events.
+// Created only for calls with host arrays (device-array calls, e.g. recorded
+// into a stream capture, keep to the caller's stream); inactive otherwise.
 struct SideStream {
   cudaStream_t main, s = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
-  explicit SideStream(cudaStream_t m) : main(m) {
+  SideStream(cudaStream_t m, bool use) : main(m) {
+    if (!use) return;
     DN_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     DN_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     DN_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
   }
+  bool active() const { return s != nullptr; }
   // the side stream continues after everything queued on the main stream so far
   void start() {
+    if (!s) return;
     DN_CUDA(cudaEventRecord(fork, main));
     DN_CUDA(cudaStreamWaitEvent(s, fork, 0));
   }
   // the main stream continues after everything queued on the side stream so far
   void merge() {
+    if (!s) return;
     DN_CUDA(cudaEventRecord(join, s));
     DN_CUDA(cudaStreamWaitEvent(main, join, 0));
   }
@@ -274,7 +280,7 @@ struct Staged {
     dev.data = buf.p;
     dev.host = false;
     if (!input || !bytes) return;
-    if (ss) {
+    if (ss && ss->active()) {
       ss->start();
       side = ss->s;
       DN_CUDA(cudaMemcpyAsync(buf.p, v.data, bytes, cudaMemcpyHostToDevice, side));
@@ -725,9 +731,9 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
   tm.mark("coordinates host->device");
   // host arrays: the coordinates next; the point values follow on a side
   // stream while this stream builds the index
-  SideStream side(st);
+  SideStream side(st, points.host);
   Staged sc(coord, true, false, st);
-  Staged sp(points, true, false, st, points.host ? &side : nullptr), so(out, false, true, st);
+  Staged sp(points, true, false, st, &side), so(out, false, true, st);
   if (s.npoints == 0) {
     side.merge();
     zero_view(so.dev, st);
@@ -778,9 +784,9 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
   tm.mark("coordinates host->device");
   // host arrays: the coordinates first; the uniform grid follows on a side
   // stream, which also runs the FFT pass, while this stream builds the index
-  SideStream side(st);
+  SideStream side(st, uni.host);
   Staged sc(coord, true, false, st), so(out, false, true, st);
-  Staged su(uni, true, false, st, uni.host ? &side : nullptr);
+  Staged su(uni, true, false, st, &side);
   const size_t esz = f64 ? 16 : 8;
   DevBuf grid(grid_cells(s.g) * esz, st), work;
   const size_t wb = fft_work_bytes(s.g, esz);
@@ -794,10 +800,10 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
   ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
   if (f64)
     do_fft_interp<double>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st,
-                          &grid, &work, &side);
+                          &grid, &work, side.active() ? &side : nullptr);
   else
     do_fft_interp<float>(s, dc, pts, cl, su.dev, so.dev, forward != 0, o.fft_order != 0, tm, st,
-                         &grid, &work, &side);
+                         &grid, &work, side.active() ? &side : nullptr);
   so.finish();
   tm.mark("end");
   tm.report("u2nu");

@@ -714,20 +714,27 @@ template <typename T, bool FWD>
 __global__ void __launch_bounds__(rows_threads<T>(), 1)
     k_fft_rows(cplx<T> *__restrict__ grid, int64_t rs, int n, int nlines, int lo, int hi0,
                int in_kept, int out_kept, PencilPlan pp, const cplx<T> *__restrict__ tw,
-               int *__restrict__ err) {
+               int full_tw, int *__restrict__ err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bars[2];
   __shared__ PencilPlan spp;
   __shared__ int s_fail;
   constexpr int ES = int(sizeof(cplx<T>));
   cplx<T> *bufs = reinterpret_cast<cplx<T> *>(smraw);
+  // twiddles: the full table of n roots after the buffers where it fits
+  // (full_tw), else the two-level one
   const int nh = (n + 63) / 64 + 1;
   cplx<T> *twl = bufs + 2 * n;
-  cplx<T> *twh = twl + 64;
+  cplx<T> *twh = full_tw ? nullptr : twl + 64;
   const int tid = threadIdx.x;
   if (tid == 0) spp = pp;
-  for (int i = tid; i < 64; i += blockDim.x) twl[i] = (i < n) ? tw[i] : mkc<T>(T(1), T(0));
-  for (int i = tid; i < nh; i += blockDim.x) twh[i] = (64 * i < n) ? tw[64 * i] : mkc<T>(T(1), T(0));
+  if (full_tw) {
+    for (int i = tid; i < n; i += blockDim.x) twl[i] = tw[i];
+  } else {
+    for (int i = tid; i < 64; i += blockDim.x) twl[i] = (i < n) ? tw[i] : mkc<T>(T(1), T(0));
+    for (int i = tid; i < nh; i += blockDim.x)
+      twh[i] = (64 * i < n) ? tw[64 * i] : mkc<T>(T(1), T(0));
+  }
   if (tid == 0) {
     for (int b = 0; b < 2; ++b) fft_bar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -836,18 +843,14 @@ __global__ void __launch_bounds__(256, cols_min_ctas<T>())
   const int C = 1 << cs.lc;
   const int len = PASS == 0 ? cs.P : cs.Q;    // DFT length of this pass
   const int tstr = PASS == 0 ? cs.Q : cs.P;   // sub-table stride into tw (length n)
-  const int nh = (len + 63) / 64 + 1;
   cplx<T> *s = reinterpret_cast<cplx<T> *>(smraw);
   cplx<T> *s2 = s + len * C;
-  cplx<T> *twl = s2 + len * C;
-  cplx<T> *twh = twl + 64;
+  cplx<T> *twl = s2 + len * C;   // the len roots of this pass (every tstr-th of tw)
+  const cplx<T> *twh = nullptr;
   __shared__ PencilPlan spp;
   const int tid = threadIdx.x;
   if (tid == 0) spp = pp;
-  for (int i = tid; i < 64; i += blockDim.x)
-    twl[i] = (i < len) ? tw[i * tstr] : mkc<T>(T(1), T(0));
-  for (int i = tid; i < nh; i += blockDim.x)
-    twh[i] = (64 * i < len) ? tw[64 * i * tstr] : mkc<T>(T(1), T(0));
+  for (int i = tid; i < len; i += blockDim.x) twl[i] = tw[i * tstr];
   const int nblk = (cs.N1 + C - 1) >> cs.lc;
   const int cb = blockIdx.x % nblk;      // column block
   const int g = blockIdx.x / nblk;       // q (pass A) or k1 (pass B)
@@ -1024,7 +1027,9 @@ static bool run_rows_v3(cplx<T> *grid, int n, int nlines, int64_t rs, int Nk, bo
                         cudaStream_t st) {
   if (err == nullptr || nlines <= 0) return false;
   const int nh = (n + 63) / 64 + 1;
-  const size_t sm = size_t(2 * n + 64 + nh) * sizeof(cplx<T>);
+  const size_t smfull = size_t(3 * n) * sizeof(cplx<T>);
+  const int full_tw = smfull <= 224 * 1024 ? 1 : 0;
+  const size_t sm = full_tw ? smfull : size_t(2 * n + 64 + nh) * sizeof(cplx<T>);
   if (sm > 224 * 1024 || n < 1024) return false;
   PencilPlan pp;
   if (!make_pencil(n, rows_maxr<T>(), rows_threads<T>(), pp)) return false;
@@ -1034,7 +1039,7 @@ static bool run_rows_v3(cplx<T> *grid, int n, int nlines, int64_t rs, int Nk, bo
   const int nb = std::min(nlines, sm_count_dev());
   kern<<<nb, rows_threads<T>(), sm, st>>>(grid, rs, n, nlines, lo, hi0, in_kept ? 1 : 0,
                                           out_kept ? 1 : 0, pp, static_cast<const cplx<T> *>(p.tw),
-                                          err);
+                                          full_tw, err);
   DN_LAUNCHED();
   return true;
 }
@@ -1063,23 +1068,20 @@ static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
   const int nblk = (N1 + C - 1) / C;
   for (int pass = 0; pass < 2; ++pass) {
     const int len = pass == 0 ? P : Q;
-    const int nh = (len + 63) / 64 + 1;
-    const size_t sm = size_t(2 * len * C + 64 + nh) * sizeof(cplx<T>);
+    const size_t sm = size_t(2 * len * C + len) * sizeof(cplx<T>);
     if (sm > 200 * 1024) return false;
   }
   cs.in_mode = type1 ? 0 : 1;
   cs.out_mode = type1 ? 1 : 0;
   {
-    const int nh = (P + 63) / 64 + 1;
-    const size_t sm = size_t(2 * P * C + 64 + nh) * sizeof(cplx<T>);
+    const size_t sm = size_t(2 * P * C + P) * sizeof(cplx<T>);
     auto kern = fwd ? k_fft_colstep<T, 0, true> : k_fft_colstep<T, 0, false>;
     DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     kern<<<unsigned(nblk) * unsigned(Q), 256, sm, st>>>(grid, work, cs, ppP, tw, u);
     DN_LAUNCHED();
   }
   {
-    const int nh = (Q + 63) / 64 + 1;
-    const size_t sm = size_t(2 * Q * C + 64 + nh) * sizeof(cplx<T>);
+    const size_t sm = size_t(2 * Q * C + Q) * sizeof(cplx<T>);
     auto kern = fwd ? k_fft_colstep<T, 1, true> : k_fft_colstep<T, 1, false>;
     DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     kern<<<unsigned(nblk) * unsigned(P), 256, sm, st>>>(grid, work, cs, ppQ, tw, u);
