@@ -569,18 +569,13 @@ static void report_sizes(const Setup &s, bool gridding) {
 }
 
 // ---------------------------------------------------------------- transforms
+// Spreading of the points of pts (values at `values` with stride vs) into the
+// oversampled grid: the tensor-core spreader where the setup chose it, else
+// the plain one.
 template <typename T>
-static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
-                          const ChunkList &cl, const TcBlocks *tb, const View &points,
-                          const View &out, bool forward, bool fft_order, StageTimer &tm,
-                          cudaStream_t st, DevBuf *ws = nullptr, DevBuf *wk = nullptr) {
-  size_t cells = grid_cells(s.g);
-  tm.mark("zeroing grid");
-  DevBuf local;
-  DevBuf &grid = ws ? *ws : local;
-  if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
-  DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * sizeof(T) * 2, st));
-  tm.mark("spreading");
+static void spread_points(const Setup &s, const PointsDesc &pts, const ChunkList &cl,
+                          const TcBlocks *tb, const void *values, int64_t vs, void *grid, int *err,
+                          cudaStream_t st) {
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
   bool use_tc = false;
@@ -593,13 +588,28 @@ static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &
     DN_REQUIRE(s.spreader != DNUFFT_SPREAD_TC, ST_UNSUPPORTED,
                "tensor-core spreader: single precision (complex64) only");
   }
-  int *err = device_error_word();
   if (use_tc) {
-    launch_spread_tc(pts, *tb, s.g, s.kpf, points.data, points.stride[0], grid.p,
-                     reinterpret_cast<unsigned *>(err + 1), err, st);
+    launch_spread_tc(pts, *tb, s.g, s.kpf, values, vs, grid, reinterpret_cast<unsigned *>(err + 1),
+                     err, st);
   } else {
-    launch_spread<T>(pts, cl, s.g, kp, points.data, points.stride[0], 0, grid.p, 0, 1, st);
+    launch_spread<T>(pts, cl, s.g, kp, values, vs, 0, grid, 0, 1, st);
   }
+}
+
+template <typename T>
+static void do_spread_fft(const Setup &s, const DevConst &dc, const PointsDesc &pts,
+                          const ChunkList &cl, const TcBlocks *tb, const View &points,
+                          const View &out, bool forward, bool fft_order, StageTimer &tm,
+                          cudaStream_t st, DevBuf *ws = nullptr, DevBuf *wk = nullptr) {
+  size_t cells = grid_cells(s.g);
+  tm.mark("zeroing grid");
+  DevBuf local;
+  DevBuf &grid = ws ? *ws : local;
+  if (!grid.p) grid = DevBuf(cells * sizeof(T) * 2, st);
+  DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * sizeof(T) * 2, st));
+  tm.mark("spreading");
+  int *err = device_error_word();
+  spread_points<T>(s, pts, cl, tb, points.data, points.stride[0], grid.p, err, st);
   tm.mark("FFT + correction");
   DevBuf localw;
   DevBuf &work = wk ? *wk : localw;
@@ -705,6 +715,180 @@ static dnufft_opts resolved(const dnufft_opts *o, bool for_plan) {
   return r;
 }
 
+// ---------------------------------------------------------------- pipelined host calls
+// Unplanned calls whose points come from host memory are bound by the PCIe
+// transfers (about 55 GB/s each way).  Large ones are cut into groups of
+// consecutive points (in the caller's order).  Every group is sorted and spread
+// on its own (type 1: spreading adds into one grid) or sorted and interpolated
+// on its own (type 2: its results are one contiguous range), so the
+// host->device copy of the next groups, and for type 2 the device->host copy of
+// the finished groups' results, overlap the work on the current one.  Kernel,
+// oversampled grid and FFT are those of the whole problem.
+constexpr uint32_t PIPE_MIN_POINTS = 1u << 22;     // pipelined from 4M points
+constexpr uint32_t PIPE_GROUP_POINTS = 12500000u;  // about this many per group
+
+static int pipe_groups(uint32_t M) {
+  if (M < PIPE_MIN_POINTS) return 1;
+  const int G = int((uint64_t(M) + PIPE_GROUP_POINTS - 1) / PIPE_GROUP_POINTS);
+  return std::max(2, std::min(8, G));
+}
+
+struct EventSet {
+  std::vector<cudaEvent_t> ev;
+  explicit EventSet(int n) : ev(size_t(n), nullptr) {
+    for (auto &e : ev) DN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  ~EventSet() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+// first point of group gi of G over M points
+static uint64_t group_start(uint32_t M, int G, int gi) { return uint64_t(M) * uint64_t(gi) / uint64_t(G); }
+
+// coordinates (C-contiguous (M, d) device copy) of points [a, b)
+static View coord_range(const View &coord, void *dev, uint64_t a, uint64_t b, size_t cb) {
+  View v = coord;
+  v.data = static_cast<char *>(dev) + a * size_t(coord.shape[1]) * cb;
+  v.shape[0] = int64_t(b - a);
+  v.host = false;
+  return v;
+}
+
+template <typename T>
+static void nu2u_pipelined(const Setup &s, const View &points, const View &coord, const View &out,
+                           bool forward, bool fft_order, StageTimer &tm, cudaStream_t st) {
+  const uint32_t M = s.npoints;
+  const size_t nd = size_t(coord.shape[1]);
+  const size_t cb = s.coord_f64 ? 8 : 4, vb = sizeof(T) * 2;
+  const int G = pipe_groups(M);
+  tm.mark("upload constants");
+  DevConst dc;
+  upload_consts(s, dc, st);
+  DevBuf dcoord(size_t(M) * nd * cb, st), dvals(size_t(M) * vb, st);
+  const size_t cells = grid_cells(s.g);
+  DevBuf grid(cells * vb, st), work;
+  const size_t wb = fft_work_bytes(s.g, vb);
+  if (wb) work = DevBuf(wb, st);
+  Staged so(out, false, true, st);
+  DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * vb, st));
+  EventSet copied(G);
+  // declared after the buffers: destroyed (after synchronising) before them
+  SideStream up(st, true);
+  up.start();
+  for (int gi = 0; gi < G; ++gi) {
+    const uint64_t a = group_start(M, G, gi), b = group_start(M, G, gi + 1);
+    DN_CUDA(cudaMemcpyAsync(static_cast<char *>(dcoord.p) + a * nd * cb,
+                            static_cast<const char *>(coord.data) + a * nd * cb, (b - a) * nd * cb,
+                            cudaMemcpyHostToDevice, up.s));
+    DN_CUDA(cudaMemcpyAsync(static_cast<char *>(dvals.p) + a * vb,
+                            static_cast<const char *>(points.data) + a * vb, (b - a) * vb,
+                            cudaMemcpyHostToDevice, up.s));
+    DN_CUDA(cudaEventRecord(copied.ev[gi], up.s));
+  }
+  tm.mark("groups: index + spreading");
+  int *err = device_error_word();
+  for (int gi = 0; gi < G; ++gi) {
+    const uint64_t a = group_start(M, G, gi), b = group_start(M, G, gi + 1);
+    DN_CUDA(cudaStreamWaitEvent(st, copied.ev[gi], 0));
+    Setup sg = s;
+    sg.npoints = uint32_t(b - a);
+    const View cv = coord_range(coord, dcoord.p, a, b, cb);
+    Index ix;
+    build_index(sg, cv, ix, st);
+    PointsDesc pts{cv.data, cv.stride[0], cv.stride[1], false, s.coord_f64,
+                   ix.perm.as<uint32_t>(), sg.npoints};
+    ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+    const TcBlocks tb = ix.tc();
+    spread_points<T>(sg, pts, cl, &tb, static_cast<char *>(dvals.p) + a * vb, 1, grid.p, err, st);
+  }
+  tm.mark("FFT + correction");
+  fft_nu2u_tail<T>(grid.p, s.g, dc.ax, forward, dc.cf, fft_order, so.dev.data, so.dev.stride, st,
+                   work.p, err);
+  tm.mark("output copy");
+  check_device_error(err, st);
+  so.finish();
+}
+
+template <typename T>
+static void u2nu_pipelined(const Setup &s, const View &uni, const View &coord, const View &out,
+                           bool forward, bool fft_order, StageTimer &tm, cudaStream_t st) {
+  const uint32_t M = s.npoints;
+  const size_t nd = size_t(coord.shape[1]);
+  const size_t cb = s.coord_f64 ? 8 : 4, vb = sizeof(T) * 2;
+  const int G = pipe_groups(M);
+  tm.mark("upload constants");
+  DevConst dc;
+  upload_consts(s, dc, st);
+  DevBuf dcoord(size_t(M) * nd * cb, st), duni, dout;
+  const size_t ubytes = size_t(nelem(uni)) * vb;
+  if (uni.host) duni = DevBuf(ubytes, st);
+  if (out.host) dout = DevBuf(size_t(M) * vb, st);
+  DevBuf grid(grid_cells(s.g) * vb, st), work;
+  const size_t wb = fft_work_bytes(s.g, vb);
+  if (wb) work = DevBuf(wb, st);
+  View uv = uni, ov = out;
+  if (uni.host) {
+    uv.data = duni.p;
+    uv.host = false;
+  }
+  if (out.host) {
+    ov.data = dout.p;
+    ov.host = false;
+  }
+  EventSet copied(G + 1), done(G);
+  // declared after the buffers: destroyed (after synchronising) before them
+  SideStream up(st, true), down(st, out.host);
+  up.start();
+  down.start();
+  // the uniform grid first, then the coordinates group by group
+  if (uni.host) DN_CUDA(cudaMemcpyAsync(duni.p, uni.data, ubytes, cudaMemcpyHostToDevice, up.s));
+  DN_CUDA(cudaEventRecord(copied.ev[G], up.s));
+  for (int gi = 0; gi < G; ++gi) {
+    const uint64_t a = group_start(M, G, gi), b = group_start(M, G, gi + 1);
+    DN_CUDA(cudaMemcpyAsync(static_cast<char *>(dcoord.p) + a * nd * cb,
+                            static_cast<const char *>(coord.data) + a * nd * cb, (b - a) * nd * cb,
+                            cudaMemcpyHostToDevice, up.s));
+    DN_CUDA(cudaEventRecord(copied.ev[gi], up.s));
+  }
+  int *err = device_error_word();
+  tm.mark("correction + FFT");
+  DN_CUDA(cudaStreamWaitEvent(st, copied.ev[G], 0));
+  fft_u2nu_head<T>(uv.data, uv.stride, s.g, dc.ax, forward, dc.cf, fft_order, grid.p, st, work.p,
+                   err);
+  tm.mark("groups: index + interpolation");
+  const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
+      sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
+  for (int gi = 0; gi < G; ++gi) {
+    const uint64_t a = group_start(M, G, gi), b = group_start(M, G, gi + 1);
+    DN_CUDA(cudaStreamWaitEvent(st, copied.ev[gi], 0));
+    Setup sg = s;
+    sg.npoints = uint32_t(b - a);
+    const View cv = coord_range(coord, dcoord.p, a, b, cb);
+    Index ix;
+    build_index(sg, cv, ix, st);
+    PointsDesc pts{cv.data, cv.stride[0], cv.stride[1], false, s.coord_f64,
+                   ix.perm.as<uint32_t>(), sg.npoints};
+    ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
+    launch_interp<T>(pts, cl, s.g, kp, grid.p, 0,
+                     static_cast<char *>(ov.data) + a * size_t(ov.stride[0]) * vb, ov.stride[0], 0,
+                     1, st);
+    if (out.host) {
+      // the finished range goes back while the next groups are interpolated
+      DN_CUDA(cudaEventRecord(done.ev[gi], st));
+      DN_CUDA(cudaStreamWaitEvent(down.s, done.ev[gi], 0));
+      DN_CUDA(cudaMemcpyAsync(static_cast<char *>(out.data) + a * vb,
+                              static_cast<const char *>(dout.p) + a * vb, (b - a) * vb,
+                              cudaMemcpyDeviceToHost, down.s));
+    }
+  }
+  tm.mark("output copy");
+  down.merge();
+  check_device_error(err, st);
+  DN_CUDA(cudaStreamSynchronize(st));
+}
+
 static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, int forward,
                       double eps, dnufft_array *out_, const dnufft_opts *opts_, cudaStream_t st) {
   dnufft_opts o = resolved(opts_, false);
@@ -723,6 +907,15 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
                        coord.dtype == DNUFFT_F64, o);
   StageTimer tm(o.verbosity > 0, st);
   if (o.verbosity > 0) report_sizes(s, true);
+  if (points.host && coord.host && pipe_groups(s.npoints) > 1) {
+    if (f64)
+      nu2u_pipelined<double>(s, points, coord, out, forward != 0, o.fft_order != 0, tm, st);
+    else
+      nu2u_pipelined<float>(s, points, coord, out, forward != 0, o.fft_order != 0, tm, st);
+    tm.mark("end");
+    tm.report("nu2u");
+    return;
+  }
   // constants first (small pageable copies, which would otherwise queue behind
   // the large transfers on the copy engine)
   tm.mark("upload constants");
@@ -778,6 +971,15 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
   StageTimer tm(o.verbosity > 0, st);
   if (o.verbosity > 0) report_sizes(s, false);
   if (s.npoints == 0) return;
+  if (coord.host && pipe_groups(s.npoints) > 1) {
+    if (f64)
+      u2nu_pipelined<double>(s, uni, coord, out, forward != 0, o.fft_order != 0, tm, st);
+    else
+      u2nu_pipelined<float>(s, uni, coord, out, forward != 0, o.fft_order != 0, tm, st);
+    tm.mark("end");
+    tm.report("u2nu");
+    return;
+  }
   tm.mark("upload constants");
   DevConst dc;
   upload_consts(s, dc, st);

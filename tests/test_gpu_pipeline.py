@@ -1,0 +1,58 @@
+"""Unplanned calls on large host arrays run pipelined: the points are cut into
+groups whose host->device copies (and, for type 2, device->host copies of the
+results) overlap the sorting and spreading / interpolation of the other
+groups.  Checked against the same calls on device arrays (one group, no
+overlap), in complex64 (tensor-core spreader chosen by 'auto' at this density)
+and complex128, both signs, and against the direct NUDFT on a sample of
+modes / points.
+"""
+import numpy as np
+import pytest
+
+from ducc_b200 import nufft
+from oracle import nufft_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+M = 5_000_000          # above the pipelining threshold (4M points): 2 groups
+SHAPE = (320, 288)
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_pipelined_host_calls_match_device_calls(single):
+    import torch
+    rng = np.random.default_rng(11)
+    cdt, vdt = (np.float32, np.complex64) if single else (np.float64, np.complex128)
+    eps = 1e-5 if single else 1e-10
+    coord = rng.uniform(-np.pi, np.pi, (M, 2)).astype(cdt)
+    vals = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(vdt)
+    grid = (rng.standard_normal(SHAPE) + 1j * rng.standard_normal(SHAPE)).astype(vdt)
+    dc, dv, dg = (torch.from_numpy(x).cuda() for x in (coord, vals, grid))
+    tol = 2e-6 if single else 1e-12
+    for forward in (True, False):
+        # type 1
+        h_out = np.zeros(SHAPE, vdt)
+        nufft.nu2u(points=vals, coord=coord, forward=forward, epsilon=eps, out=h_out)
+        d_out = torch.zeros(SHAPE, dtype=dv.dtype, device="cuda")
+        nufft.nu2u(points=dv, coord=dc, forward=forward, epsilon=eps, out=d_out)
+        assert O.l2error(h_out, d_out.cpu().numpy()) < tol
+        # a few modes against the direct sum over all points
+        s = -1 if forward else 1
+        ku = np.array([0, 1])
+        kv = np.arange(8) - 4
+        ex = np.zeros((2, 8), np.complex128)
+        for i in range(0, M, 1000000):
+            cc = coord[i:i + 1000000].astype(np.float64)
+            ex += np.einsum("m,mi,mj->ij", vals[i:i + 1000000].astype(np.complex128),
+                            np.exp(s * 1j * np.outer(cc[:, 0], ku)),
+                            np.exp(s * 1j * np.outer(cc[:, 1], kv)), optimize=True)
+        got = h_out[SHAPE[0] // 2:SHAPE[0] // 2 + 2, SHAPE[1] // 2 - 4:SHAPE[1] // 2 + 4]
+        assert O.l2error(got, ex) < 2 * eps
+        # type 2
+        h_pts = np.empty(M, vdt)
+        nufft.u2nu(grid=grid, coord=coord, forward=forward, epsilon=eps, out=h_pts)
+        d_pts = nufft.u2nu(grid=dg, coord=dc, forward=forward, epsilon=eps)
+        assert O.l2error(h_pts, d_pts.cpu().numpy()) < tol
+        idx = rng.choice(M, 500, replace=False)
+        ref = O.direct_u2nu(grid, coord[idx], forward)
+        assert O.l2error(h_pts[idx], ref) < 2 * eps
