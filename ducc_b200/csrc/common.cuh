@@ -209,4 +209,13 @@ __device__ __forceinline__ int wrapi(int i, int n) {
   return i < 0 ? i + n : i;
 }
 
+// periodic wrap of i in [-n, 2n) without a division
+__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// floor(x / d) for d >= 2 and x * d < 2^32 by a multiply-high with m = ceil(2^32 / d)
+__host__ __device__ __forceinline__ uint32_t fastdiv_magic(uint32_t d) {
+  return uint32_t(((uint64_t(1) << 32) + d - 1) / d);
+}
+__device__ __forceinline__ uint32_t fastdiv(uint32_t x, uint32_t m) { return __umulhi(x, m); }
+
 }  // namespace dnufft

@@ -239,19 +239,30 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
   if constexpr (SMEM) {
     // tile + halo, LB loads in flight per thread before their stores
+    // cell -> tile coordinates by multiply-high division (cells < S^3, so
+    // cell * S < 2^32), periodic wrap without a division where every axis is
+    // at least 2S long (a tile origin lies in [-W/2, n + W), so its cells'
+    // indices stay in [-n, 2n))
     constexpr int LB = 8;
+    const uint32_t mS = fastdiv_magic(uint32_t(S));
+    bool fastwrap = true;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) fastwrap = fastwrap && int(g.nover[d]) >= 2 * S;
     auto cell = [&](int c) -> cplx<T> {
       int gi[NDIM];
-      int rem = c;
+      uint32_t rem = uint32_t(c);
 #pragma unroll
       for (int d = NDIM - 1; d >= 0; --d) {
-        gi[d] = rem % S;
-        rem /= S;
+        const uint32_t qd = fastdiv(rem, mS);
+        gi[d] = int(rem - qd * uint32_t(S));
+        rem = qd;
       }
       int64_t gidx = 0;
 #pragma unroll
-      for (int d = 0; d < NDIM; ++d)
-        gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
+      for (int d = 0; d < NDIM; ++d) {
+        const int nd = int(g.nover[d]);
+        gidx = gidx * nd + (fastwrap ? wrap1(b0[d] + gi[d], nd) : wrapi(b0[d] + gi[d], nd));
+      }
       return grid[gidx];
     };
     for (int c0 = threadIdx.x; c0 < ncell; c0 += LB * SP_THREADS) {
@@ -383,6 +394,7 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
     for (uint32_t s0 = ch.start; s0 < end; s0 += IB) {
       const int nb = int(min(uint32_t(IB), end - s0));
       const int q = (nb + 31) >> 5;
+      const uint32_t mq = q > 1 ? fastdiv_magic(uint32_t(q)) : 0u;
       if (threadIdx.x < NSLOT) s_cnt[threadIdx.x] = 0;
       __syncthreads();
       uint32_t pj[PER];
@@ -425,7 +437,8 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
       for (int k = 0; k < PER; ++k) {
         if (pb[k] >= 0) {
           const int e = atomicAdd(&s_cnt[pb[k] & (NSLOT - 1)], 1);
-          const int w = (e % q) * 32 + e / q;
+          const int eq = q > 1 ? int(fastdiv(uint32_t(e), mq)) : e;   // e / q (e < 1024)
+          const int w = (e - eq * q) * 32 + eq;
           r_j[w] = pj[k];
           r_base[w] = pb[k];
 #pragma unroll
