@@ -34,21 +34,11 @@ __global__ void __launch_bounds__(SP_THREADS)
   int b0[NDIM];
   tile_origin<NDIM>(ch.tile, g, b0);
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
+  const uint32_t mS = fastdiv_magic(uint32_t(S));
+  const bool fastwrap = fast_wrap_ok<NDIM>(g, S);
   if constexpr (SMEM) {
-    for (int c = threadIdx.x; c < ncell; c += SP_THREADS) {
-      int gi[NDIM];
-      int rem = c;
-#pragma unroll
-      for (int d = NDIM - 1; d >= 0; --d) {
-        gi[d] = rem % S;
-        rem /= S;
-      }
-      int64_t gidx = 0;
-#pragma unroll
-      for (int d = 0; d < NDIM; ++d)
-        gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
-      buf[c] = grid[gidx];
-    }
+    for (int c = threadIdx.x; c < ncell; c += SP_THREADS)
+      buf[c] = grid[cell_index<NDIM>(c, S, mS, fastwrap, b0, g)];
     __syncthreads();
   }
   T dscale[NDIM];
@@ -107,7 +97,8 @@ __global__ void __launch_bounds__(SP_THREADS)
           if constexpr (SMEM) {
             row = buf + ((o[0] + a) * S + (o[1] + b)) * S + o[2];
           } else {
-            int iu = wrapi(b0[0] + o[0] + a, nu), iv = wrapi(b0[1] + o[1] + b, nv);
+            const int iu = fastwrap ? wrap1(b0[0] + o[0] + a, nu) : wrapi(b0[0] + o[0] + a, nu);
+            const int iv = fastwrap ? wrap1(b0[1] + o[1] + b, nv) : wrapi(b0[1] + o[1] + b, nv);
             row = grid + (int64_t(iu) * nv + iv) * nw;
           }
           T rr = 0, ri = 0, dr = 0, di = 0;
@@ -115,7 +106,7 @@ __global__ void __launch_bounds__(SP_THREADS)
           for (int e = 0; e < W; ++e) {
             cplx<T> gv;
             if constexpr (SMEM) gv = row[e];
-            else gv = __ldg(row + wrapi(b0[2] + o[2] + e, nw));
+            else gv = __ldg(row + (fastwrap ? wrap1(b0[2] + o[2] + e, nw) : wrapi(b0[2] + o[2] + e, nw)));
             rr += w[2][e] * gv.x;
             ri += w[2][e] * gv.y;
             dr += dw[2][e] * gv.x;

@@ -78,6 +78,38 @@ __device__ __forceinline__ void global_add(cplx<T> *p, T re, T im) {
   }
 }
 
+// Periodic wrap without a division is valid where every axis is at least 2S
+// long: a tile origin lies in [-W/2, n + W), so its cells' indices stay in
+// [-n, 2n).
+template <int NDIM> __device__ __forceinline__ bool fast_wrap_ok(const Geometry &g, int S) {
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) ok = ok && int(g.nover[d]) >= 2 * S;
+  return ok;
+}
+
+// grid index of tile cell c (row-major in S^NDIM, c * S < 2^32; mS =
+// fastdiv_magic(S)) for the tile at origin b0, wrapped periodically
+template <int NDIM>
+__device__ __forceinline__ int64_t cell_index(int c, int S, uint32_t mS, bool fastwrap,
+                                              const int (&b0)[NDIM], const Geometry &g) {
+  int gi[NDIM];
+  uint32_t rem = uint32_t(c);
+#pragma unroll
+  for (int d = NDIM - 1; d >= 0; --d) {
+    const uint32_t qd = fastdiv(rem, mS);
+    gi[d] = int(rem - qd * uint32_t(S));
+    rem = qd;
+  }
+  int64_t gidx = 0;
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) {
+    const int nd = int(g.nover[d]);
+    gidx = gidx * nd + (fastwrap ? wrap1(b0[d] + gi[d], nd) : wrapi(b0[d] + gi[d], nd));
+  }
+  return gidx;
+}
+
 // One chunk of one transform (the body of k_spread; also used by the
 // multi-instance kernel of batched transforms).
 template <typename T, typename Tc, int NDIM, int W>
@@ -95,6 +127,8 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
   if (NDIM >= 3) ncell *= S;
   int b0[NDIM];
   tile_origin<NDIM>(ch.tile, g, b0);
+  const uint32_t mS = fastdiv_magic(uint32_t(S));
+  const bool fastwrap = fast_wrap_ok<NDIM>(g, S);
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned char *stage = smraw + (SMEM ? size_t(ncell) * sizeof(cplx<T>) : 0);
@@ -162,18 +196,7 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
             atomicAdd(&buf[cell].y, im);
           } else {
             // direct global accumulation at wrapped positions
-            int gi[NDIM];
-            int rem = cell;
-#pragma unroll
-            for (int d = NDIM - 1; d >= 0; --d) {
-              gi[d] = rem % S;
-              rem /= S;
-            }
-            int64_t gidx = 0;
-#pragma unroll
-            for (int d = 0; d < NDIM; ++d)
-              gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
-            global_add<T>(grid + gidx, re, im);
+            global_add<T>(grid + cell_index<NDIM>(cell, S, mS, fastwrap, b0, g), re, im);
           }
         }
       }
@@ -185,18 +208,7 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
     for (int c = threadIdx.x; c < ncell; c += SP_THREADS) {
       cplx<T> v = buf[c];
       if (v.x == T(0) && v.y == T(0)) continue;
-      int gi[NDIM];
-      int rem = c;
-#pragma unroll
-      for (int d = NDIM - 1; d >= 0; --d) {
-        gi[d] = rem % S;
-        rem /= S;
-      }
-      int64_t gidx = 0;
-#pragma unroll
-      for (int d = 0; d < NDIM; ++d)
-        gidx = gidx * g.nover[d] + wrapi(b0[d] + gi[d], int(g.nover[d]));
-      global_add<T>(grid + gidx, v.x, v.y);
+      global_add<T>(grid + cell_index<NDIM>(c, S, mS, fastwrap, b0, g), v.x, v.y);
     }
   }
 }
@@ -239,32 +251,11 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
   if constexpr (SMEM) {
     // tile + halo, LB loads in flight per thread before their stores
-    // cell -> tile coordinates by multiply-high division (cells < S^3, so
-    // cell * S < 2^32), periodic wrap without a division where every axis is
-    // at least 2S long (a tile origin lies in [-W/2, n + W), so its cells'
-    // indices stay in [-n, 2n))
+    // cell -> grid index by multiply-high division and division-free wrap
     constexpr int LB = 8;
     const uint32_t mS = fastdiv_magic(uint32_t(S));
-    bool fastwrap = true;
-#pragma unroll
-    for (int d = 0; d < NDIM; ++d) fastwrap = fastwrap && int(g.nover[d]) >= 2 * S;
-    auto cell = [&](int c) -> cplx<T> {
-      int gi[NDIM];
-      uint32_t rem = uint32_t(c);
-#pragma unroll
-      for (int d = NDIM - 1; d >= 0; --d) {
-        const uint32_t qd = fastdiv(rem, mS);
-        gi[d] = int(rem - qd * uint32_t(S));
-        rem = qd;
-      }
-      int64_t gidx = 0;
-#pragma unroll
-      for (int d = 0; d < NDIM; ++d) {
-        const int nd = int(g.nover[d]);
-        gidx = gidx * nd + (fastwrap ? wrap1(b0[d] + gi[d], nd) : wrapi(b0[d] + gi[d], nd));
-      }
-      return grid[gidx];
-    };
+    const bool fastwrap = fast_wrap_ok<NDIM>(g, S);
+    auto cell = [&](int c) -> cplx<T> { return grid[cell_index<NDIM>(c, S, mS, fastwrap, b0, g)]; };
     for (int c0 = threadIdx.x; c0 < ncell; c0 += LB * SP_THREADS) {
       cplx<T> v[LB];
 #pragma unroll
@@ -338,16 +329,19 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
         }
       } else {
         const int nu = int(g.nover[0]), nv = int(g.nover[1]), nw = int(g.nover[2]);
+        // indices stay in [-n, 2n) where every axis is at least 2S long
+        const bool fw = nu >= 2 * S && nv >= 2 * S && nw >= 2 * S;
+        auto wr = [fw](int i, int n) { return fw ? wrap1(i, n) : wrapi(i, n); };
         int iw[W];
 #pragma unroll
-        for (int e = 0; e < W; ++e) iw[e] = wrapi(b0[2] + o[2] + e, nw);
+        for (int e = 0; e < W; ++e) iw[e] = wr(b0[2] + o[2] + e, nw);
 #pragma unroll 1
         for (int a = 0; a < W; ++a) {
-          int iu = wrapi(b0[0] + o[0] + a, nu);
+          int iu = wr(b0[0] + o[0] + a, nu);
           T pr = 0, pi = 0;
 #pragma unroll
           for (int b = 0; b < W; ++b) {
-            int iv = wrapi(b0[1] + o[1] + b, nv);
+            int iv = wr(b0[1] + o[1] + b, nv);
             const cplx<T> *row = grid + (int64_t(iu) * nv + iv) * nw;
             T rr = 0, ri = 0;
 #pragma unroll
