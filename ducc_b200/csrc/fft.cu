@@ -17,6 +17,7 @@
 //    the correction factors and zero-pads in shared memory, so the oversampled
 //    grid is never zeroed or written before the first FFT.
 #include "common.cuh"
+#include "fft_pencil_plan.h"
 #include "kernels.h"
 
 #include <algorithm>
@@ -334,6 +335,7 @@ struct StageInfo {
   int Ns[24];
   int tstep[24];
   uint32_t mul[24];   // ceil(2^32 / Ns)
+  PencilPlan pen;     // pencil passes of the line kernels (pen.L == 0: the stages above)
 };
 
 // cos / sin of 2*pi*k/R, k < R, for the odd radices 3, 5, 7, 11 (rows 0..3)
@@ -442,6 +444,9 @@ __device__ __forceinline__ void stage2(const cplx<T> *__restrict__ src, cplx<T> 
 }
 
 template <typename T> constexpr int fft2_max_threads() { return sizeof(T) == 4 ? 1024 : 512; }
+// largest pencil radix of the line kernels (64 / 128 registers at 1024 / 512
+// threads)
+template <typename T> constexpr int lines_maxr() { return sizeof(T) == 4 ? 12 : 16; }
 constexpr int FFT2_MAXE = 12;   // elements per CTA <= FFT2_MAXE * threads
 
 // One block of lines (the body of k_fft_lines2, also run by the multi-job
@@ -464,12 +469,14 @@ __device__ __forceinline__ void fft_lines_block(cplx<T> *__restrict__ grid, cons
   double *lfac = reinterpret_cast<double *>(luoff + nl);
   __shared__ int stR[24], stNs[24], stT[24];
   __shared__ uint32_t stM[24];
+  __shared__ PencilPlan spen;
   if (threadIdx.x < 24) {
     stR[threadIdx.x] = si.R[threadIdx.x];
     stNs[threadIdx.x] = si.Ns[threadIdx.x];
     stT[threadIdx.x] = si.tstep[threadIdx.x];
     stM[threadIdx.x] = si.mul[threadIdx.x];
   }
+  if (threadIdx.x == 0) spen = si.pen;
   const int L0 = blk << lnl;
   const int nloc = min(nl, ls.nlines - L0);
   const int N = sel3(u.N, ls.ax);
@@ -526,6 +533,14 @@ __device__ __forceinline__ void fft_lines_block(cplx<T> *__restrict__ grid, cons
       s[idx] = load_elem(idx & (nl - 1), idx >> lnl);
   }
   __syncthreads();
+  if (spen.L > 0) {
+    // pencil passes (result in s2)
+    if (fwd)
+      pencil_fft<T, true, lines_maxr<T>()>(s, s2, nl, lnl, spen, twh, twl);
+    else
+      pencil_fft<T, false, lines_maxr<T>()>(s, s2, nl, lnl, spen, twh, twl);
+    s = s2;
+  } else {
   cplx<T> *src = s, *dst = s2;
   for (int f = 0; f < si.nst; ++f) {
     const int R = stR[f], Ns = stNs[f], ts = stT[f];
@@ -545,6 +560,7 @@ __device__ __forceinline__ void fft_lines_block(cplx<T> *__restrict__ grid, cons
     dst = t;
   }
   s = src;
+  }
   if (ls.es == 1) {
     for (int l = 0; l < nl; ++l)
       for (int k = threadIdx.x; k < n; k += blockDim.x) store_elem(l, k, s[(k << lnl) + l]);
@@ -563,8 +579,14 @@ __global__ void __launch_bounds__(fft2_max_threads<T>())
   fft_lines_block<T>(grid, ls, si, tw, u, fwd, blockIdx.x, smraw);
 }
 
-static StageInfo make_stages(const FFTAxisPlan &p) {
+static bool make_pencil(int n, int maxr, int maxlast, PencilPlan &pp);
+
+// Radix-by-radix stage table of an axis, plus the pencil passes with radices up
+// to pen_maxr where such a plan exists (pen_maxr == 0: none).
+static StageInfo make_stages(const FFTAxisPlan &p, int pen_maxr) {
   StageInfo si;
+  std::memset(&si, 0, sizeof(si));
+  if (pen_maxr > 0 && !make_pencil(p.n, pen_maxr, 1 << 30, si.pen)) si.pen.L = 0;
   si.nst = p.nfac;
   int Ns = 1;
   for (int f = 0; f < p.nfac; ++f) {
@@ -600,7 +622,7 @@ static bool run_lines2(cplx<T> *grid, LineSpec ls, const FFTAxisPlan &p, const U
   size_t sm = size_t(2 * total + 64 + nh) * sizeof(cplx<T>) + size_t(1 << lnl) * 24;
   if (sm > maxsm) return false;
   ls.nl = lnl;
-  StageInfo si = make_stages(p);
+  StageInfo si = make_stages(p, lines_maxr<T>());
   DN_CUDA(cudaFuncSetAttribute(k_fft_lines2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   unsigned nb = unsigned((ls.nlines + (1 << lnl) - 1) >> lnl);
   k_fft_lines2<T><<<nb, nt, sm, st>>>(grid, ls, si, static_cast<const cplx<T> *>(p.tw), u, fwd);
@@ -1370,7 +1392,7 @@ void *fft_batch_create(const std::vector<FFTBatchInst> &insts, cudaStream_t st) 
           FFTJob jb;
           std::memset(&jb, 0, sizeof(jb));
           jb.ls = ls;
-          jb.si = make_stages(ax);
+          jb.si = make_stages(ax, lines_maxr<T>());
           const int64_t zero[3] = {0, 0, 0};
           jb.u = mk_uni(nullptr, zero, g, in.corfac, in.fft_order);
           jb.tw = ax.tw;
