@@ -330,6 +330,17 @@ def cpu_baseline_leg(m, n, coord, vals, grid, budget_s=30.0):
                       % (m, reps)}
 
 
+def max_over_ranks(value, dev, dist):
+    """The largest of every rank's value (the job's time is its slowest rank)."""
+    if not dist:
+        return value
+    import torch
+    import torch.distributed as td
+    t = torch.tensor([float(value)], device=dev)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from ducc_b200 import nufft
@@ -386,11 +397,7 @@ def run_ours(args, rank, world, local_rank):
         prof = json.loads(C.lib().dnufft_profile_json().decode())
         C.lib().dnufft_profile_enable(0)
         clocks = clk.stop()
-        ms = ev0.elapsed_time(ev1) / args.steps
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            td.all_reduce(t, op=td.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dev, dist)
         results[spreader] = {"ms": ms, "plan_s": plan_s, "prof": prof, "clocks": clocks,
                              "launches": launches, "info": plan.info()}
         del plan
@@ -418,11 +425,7 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(k):
             e2e_step()
         barrier()
-        et = (time.perf_counter() - t0) / k
-        if dist:
-            t = torch.tensor([et], device=dev)
-            td.all_reduce(t, op=td.ReduceOp.MAX)
-            et = float(t.item())
+        et = max_over_ranks((time.perf_counter() - t0) / k, dev, dist)
         e2e = {"value": world * 2 * m / et / 1e6, "unit": "Mpts/s",
                "h2d_bytes_per_step": int(2 * coord.nbytes + vals.nbytes + grid.nbytes),
                "d2h_bytes_per_step": int(n * n * 8 + m * 8),
