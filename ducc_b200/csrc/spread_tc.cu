@@ -629,21 +629,23 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
   } else if (warp < EPI_W0 + N_EPI) {
     // ------------------------------------------------------------ epilogue
     // One event per quadrant per sub-chunk, taken in quadrant order: the
-    // accumulators are added into the FP32 planes of set k & 1 (part p of
-    // tensor-memory lane L = 24p + u is row u of plane p), which then go to
-    // the flusher warps.
+    // accumulators are added into the FP32 planes of the current plane set
+    // (part p of tensor-memory lane L = 24p + u is row u of plane p).
+    // Consecutive sub-chunks of the same tile keep adding into the same set
+    // (sub-chunks bound the tensor-memory accumulation chains, not the FP32
+    // planes); when the tile changes, the set goes to the flusher warps and the
+    // epilogue continues in the other one.  Hand-off h uses set h & 1.
     const int L = tid;                   // tensor-memory lane 0..127
     const int p = L / 24, u = L - 24 * (L / 24);
+    uint32_t h = 0;                      // plane sets handed to the flusher so far
+    bool have = false;                   // set h & 1 holds data of tile cur_tile
+    uint32_t cur_tile = 0, cur_dq = 0;   // cur_dq: dirty quadrants of the set
     for (uint32_t k = 0;; ++k) {
-      const uint32_t buf = k & 1, par = (k >> 1) & 1;
-      // plane set k & 1 must have been flushed and zeroed (sub-chunk k - 2)
-      bool stop = false;
-      if (k >= 2)
-        stop = !__all_sync(0xffffffffu, mbar_wait(&pl_empty[buf], ((k >> 1) - 1) & 1u, abortp, err));
-      float *plane = planes + buf * (4 * PLANE_FLOATS) + (p < 4 ? p : 0) * PLANE_FLOATS;
+      const uint32_t buf = k & 1, par = (k >> 1) & 1;   // tensor-memory buffer of sub-chunk k
       // 'stop' (a failed wait or the exit record) is uniform in a warp, and
-      // made uniform across the four warps at each named barrier
-      uint32_t tile = 0, dq = 0;   // dq: dirty quadrants
+      // made uniform across the four warps at each named barrier; the
+      // hand-off decisions depend only on acc_info, the same for all warps
+      bool stop = false;
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) {
         // rows 16..23 are shared by both halves of the quadrants
@@ -660,9 +662,28 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
           stop = true;
           continue;
         }
-        tile = info.y;
-        dq |= (info.x & 1u) << q;
+        if (q == 0 && have && info.y != cur_tile) {
+          // a new tile: every warp finished adding into the current set at the
+          // previous sub-chunk's barrier; hand it over and move to the other
+          // set once the flusher has released it (hand-off h - 2)
+          if (L == 0) {
+            pl_info[h & 1] = make_uint2(cur_tile, cur_dq);
+            mbar_arrive(&pl_full[h & 1]);
+          }
+          ++h;
+          have = false;
+          cur_dq = 0;
+          if (h >= 2 &&
+              !__all_sync(0xffffffffu, mbar_wait(&pl_empty[h & 1], ((h >> 1) - 1) & 1u, abortp, err))) {
+            stop = true;
+            continue;
+          }
+        }
+        cur_tile = info.y;
+        have = true;
+        cur_dq |= (info.x & 1u) << q;
         if (info.x & 1u) {
+          float *plane = planes + (h & 1) * (4 * PLANE_FLOATS) + (p < 4 ? p : 0) * PLANE_FLOATS;
           uint32_t d0[16], d1[16], d2[16];
           const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + uint32_t(128 * q + 64 * buf);
           tmem_ld16(ta, d0);
@@ -683,18 +704,29 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         mbar_arrive(&acc_empty[q][buf]);
       }
       const bool fin = named_bar_or(1, 32 * N_EPI, stop);
-      // hand plane set k & 1 to the flusher (or tell it to stop)
-      if (L == 0) {
-        pl_info[buf] = make_uint2(tile, fin ? 0x100u : dq);
-        mbar_arrive(&pl_full[buf]);
+      if (fin) {
+        // hand over the last data, then tell the flusher to stop (in a set it
+        // has released)
+        if (have) {
+          if (L == 0) {
+            pl_info[h & 1] = make_uint2(cur_tile, cur_dq);
+            mbar_arrive(&pl_full[h & 1]);
+          }
+          ++h;
+          if (h >= 2) mbar_wait(&pl_empty[h & 1], ((h >> 1) - 1) & 1u, abortp, err);
+        }
+        if (L == 0) {
+          pl_info[h & 1] = make_uint2(0u, 0x100u);
+          mbar_arrive(&pl_full[h & 1]);
+        }
+        break;
       }
-      if (fin) break;
     }
   }
   if (warp >= FLUSH_W0 && warp < FLUSH_W0 + N_FLUSH) {
     // ------------------------------------------------------------ flusher
-    // Sub-chunk k's planes (set k & 1) -> grid with float2 atomics, zeroing
-    // them for sub-chunk k + 2.  Only the dirty quadrants' windows hold data.
+    // Hand-off k's planes (set k & 1) -> grid with float2 atomics, zeroing
+    // them for hand-off k + 2.  Only the dirty quadrants' windows hold data.
     const int L = tid - FLUSH_W0 * 32;
     const int S = 32 + W;
     const int nu = int(g.nover[0]), nv = int(g.nover[1]);
