@@ -56,3 +56,27 @@ def test_pipelined_host_calls_match_device_calls(single):
         idx = rng.choice(M, 500, replace=False)
         ref = O.direct_u2nu(grid, coord[idx], forward)
         assert O.l2error(h_pts[idx], ref) < 2 * eps
+
+
+def test_pipelined_mixed_host_and_device_arrays():
+    """Host coordinates with device grids / outputs (the pipeline then uploads
+    only the coordinates), and host values with a device output."""
+    import torch
+    rng = np.random.default_rng(12)
+    eps = 1e-5
+    coord = rng.uniform(-np.pi, np.pi, (M, 2)).astype(np.float32)
+    vals = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)
+    grid = (rng.standard_normal(SHAPE) + 1j * rng.standard_normal(SHAPE)).astype(np.complex64)
+    dc, dv, dg = (torch.from_numpy(x).cuda() for x in (coord, vals, grid))
+    # type 2: host coordinates, device grid and output (strided output view)
+    big = torch.zeros(2 * M, dtype=torch.complex64, device="cuda")
+    nufft.u2nu(grid=dg, coord=coord, forward=True, epsilon=eps, out=big[::2])
+    ref = nufft.u2nu(grid=dg, coord=dc, forward=True, epsilon=eps)
+    assert O.l2error(big[::2].cpu().numpy(), ref.cpu().numpy()) < 2e-6
+    assert float(big[1::2].abs().max()) == 0.0
+    # type 1: host coordinates and values, device output
+    d_out = torch.zeros(SHAPE, dtype=torch.complex64, device="cuda")
+    nufft.nu2u(points=vals, coord=coord, forward=False, epsilon=eps, out=d_out)
+    ref1 = torch.zeros(SHAPE, dtype=torch.complex64, device="cuda")
+    nufft.nu2u(points=dv, coord=dc, forward=False, epsilon=eps, out=ref1)
+    assert O.l2error(d_out.cpu().numpy(), ref1.cpu().numpy()) < 2e-6
