@@ -50,7 +50,7 @@ EXPORTS = [
     "dnufft_kernel_launches", "dnufft_profile_enable", "dnufft_profile_json",
     "dnufft_nu2u_noalloc", "dnufft_noalloc_scratch_bytes", "dnufft_u2nu_dcoord",
     "dnufft_plan_u2nu_dcoord", "dnufft_batch_create", "dnufft_batch_nu2u", "dnufft_batch_u2nu",
-    "dnufft_batch_destroy", "dnufft_kernel_candidates",
+    "dnufft_batch_destroy", "dnufft_kernel_candidates", "dnufft_selftest_wait_timeout",
 ]
 
 
@@ -96,6 +96,7 @@ def lib():
     L.dnufft_profile_enable.argtypes = [ctypes.c_int]
     L.dnufft_profile_enable.restype = None
     L.dnufft_profile_json.restype = ctypes.c_char_p
+    L.dnufft_selftest_wait_timeout.argtypes = [ctypes.c_int64, vp]
     _lib = L
     return L
 

@@ -1531,6 +1531,17 @@ const char *dnufft_last_error(void) { return g_last_error.c_str(); }
 
 uint64_t dnufft_kernel_launches(void) { return dnufft::launch_count(); }
 
+int dnufft_selftest_wait_timeout(int64_t limit_ns, void *stream) {
+  DN_GUARD({
+    DN_REQUIRE(limit_ns > 0 && limit_ns <= 1000000000, dnufft::ST_BADARG,
+               "limit must be in (0, 1 s]");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int *err = dnufft::device_error_word();
+    dnufft::launch_wait_selftest(err, (unsigned long long)limit_ns, st);
+    dnufft::check_device_error(err, st);
+  })
+}
+
 void dnufft_profile_enable(int enable) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   g_prof_on = enable != 0;

@@ -64,6 +64,8 @@ void launch_interp_dcoord(const PointsDesc &pts, const ChunkList &cl, const Geom
                           int64_t ws, void *grad, int64_t gs0, int64_t gs1, cudaStream_t st);
 
 // ---- split-precision tensor-core spreader (spread_tc.cu): 2D, complex64
+// failure-path self-test of the bounded device waits (sets word *err)
+void launch_wait_selftest(int *err, unsigned long long limit_ns, cudaStream_t st);
 bool spread_tc_supported(const Geometry &g, bool calc_f64);
 // K-block list of a (tile, quadrant)-sorted point set: records {first sorted
 // point, meta} of <= 16 points of one quadrant of one chunk, and the K-block

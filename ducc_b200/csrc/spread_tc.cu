@@ -154,8 +154,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Bounded wait for the phase with the given parity.  Gives up (returning
 // false) when another role has raised the abort flag, or after WAIT_NS, in
 // which case it raises the flag and the device error word itself.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                          int *err) {
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, uint32_t parity,
+                                              volatile int *abort_flag, int *err,
+                                              unsigned long long limit_ns) {
   const uint32_t addr = smem_u32(bar);
   if (mbar_try(addr, parity)) return true;
   const unsigned long long t0 = global_ns();
@@ -163,13 +164,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     if (mbar_try(addr, parity)) return true;
     if ((it & 3u) == 0) {
       if (*abort_flag) return false;
-      if (global_ns() - t0 > WAIT_NS) {
+      if (global_ns() - t0 > limit_ns) {
         *abort_flag = 1;
         atomicExch(err, 1);
         return false;
       }
     }
   }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                          int *err) {
+  return mbar_wait_for(bar, parity, abort_flag, err, WAIT_NS);
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
@@ -927,6 +933,27 @@ uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t g
   DN_LAUNCHED();
   (void)d_total;
   return total;
+}
+
+// Self-test of the failure path of the bounded waits: one warp waits, with the
+// spreader's wait routine and a short limit, on an mbarrier that nothing
+// arrives at; the routine gives up, raises the abort flag and sets the error
+// word, which the host turns into DNUFFT_ERR_TIMEOUT.  No fault, no hang.
+__global__ void k_wait_selftest(int *err, unsigned long long limit_ns) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  tc::mbar_wait_for(&bar, 0u, &abort_flag, err, limit_ns);
+}
+
+void launch_wait_selftest(int *err, unsigned long long limit_ns, cudaStream_t st) {
+  k_wait_selftest<<<1, 32, 0, st>>>(err, limit_ns);
+  DN_LAUNCHED();
 }
 
 bool spread_tc_supported(const Geometry &g, bool calc_f64) {

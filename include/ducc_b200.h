@@ -220,6 +220,12 @@ uint64_t dnufft_kernel_launches(void);
  * stage times): while enabled, every transform records CUDA events between its
  * stages and accumulates the elapsed time per stage.  Enabling clears the
  * totals.  dnufft_profile_json() returns {"<transform>/<stage>": [ms, calls]}. */
+/* Test hook for the failure path of the bounded device-side waits: runs the
+   tensor-core spreader's wait routine, with the given limit, on a barrier that
+   nothing arrives at.  Returns DNUFFT_ERR_TIMEOUT (the context stays usable).
+   No DUCC counterpart. */
+int dnufft_selftest_wait_timeout(int64_t limit_ns, void *stream);
+
 void dnufft_profile_enable(int enable);
 const char *dnufft_profile_json(void);
 
