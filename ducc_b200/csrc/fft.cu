@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
     k_fft_rows(cplx<T> *__restrict__ grid, int64_t rs, int n, int nlines, int lo, int hi0,
                int in_kept, int out_kept, PencilPlan pp, const cplx<T> *__restrict__ tw,
                int full_tw, int *__restrict__ err) {
-  extern __shared__ __align__(128) unsigned char smraw[];
+  extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ uint64_t bars[2];
   __shared__ PencilPlan spp;
   __shared__ int s_fail;
@@ -879,76 +879,81 @@ __global__ void __launch_bounds__(256, cols_min_ctas<T>())
   const int x0 = cb << cs.lc;
   const int N0 = sel3(u.N, 0);
   const int lo0 = (N0 + 1) / 2, hi00 = cs.n - N0 / 2;
-  // ---- load the [len][C] tile (element m of column c at s[m*C + c])
-  auto load_elem = [&](int idx) -> cplx<T> {
-    const int m = idx >> cs.lc, c = idx & (C - 1);
-    const int x = x0 + c;
+  // ---- load the [len][C] tile (element m of column c at s[m*C + c]).  Every
+  // thread keeps one column c (blockDim is a multiple of C) and walks rows
+  // m = m0, m0 + mstep, ...: the column's grid index, row pointers and the
+  // column part of the uniform index are computed once.
+  const int c = tid & (C - 1), m0 = tid >> cs.lc, mstep = int(blockDim.x) >> cs.lc;
+  const int x = x0 + c;
+  const bool colok = x < cs.N1;
+  const int gx = colok ? kept_to_grid(x, cs.N1, cs.n1) : 0;
+  const cplx<T> *uptr = static_cast<const cplx<T> *>(u.ptr);
+  int iu1 = 0, icf1 = 0;
+  double cf1 = 0.0;
+  if (colok && ((PASS == 0 && cs.in_mode != 0) || (PASS == 1 && cs.out_mode != 0))) {
+    grid_to_uni(gx, cs.N1, cs.n1, u.fft_order, iu1, icf1);
+    cf1 = u.corfac[1][icf1];
+  }
+  auto load_m = [&](int m) -> cplx<T> {
     cplx<T> v = mkc<T>(T(0), T(0));
-    if (x < cs.N1) {
-      if (PASS == 0) {
-        const int row = g + cs.Q * m;   // q + Q*p
-        if (cs.in_mode == 0) {
-          v = grid[int64_t(row) * cs.n1 + kept_to_grid(x, cs.N1, cs.n1)];
-        } else if (row < lo0 || row >= hi00) {
-          // gather the caller's uniform array with the correction factors
-          int iu0, icf0, iu1, icf1;
-          grid_to_uni(row, N0, cs.n, u.fft_order, iu0, icf0);
-          grid_to_uni(kept_to_grid(x, cs.N1, cs.n1), cs.N1, cs.n1, u.fft_order, iu1, icf1);
-          const cplx<T> xv = static_cast<const cplx<T> *>(u.ptr)[int64_t(iu0) * u.stride[0] +
-                                                                 int64_t(iu1) * u.stride[1]];
-          const T f = T(u.corfac[0][icf0] * u.corfac[1][icf1]);
-          v = mkc<T>(xv.x * f, xv.y * f);
-        }
-      } else {
-        v = work[int64_t(g * cs.Q + m) * cs.N1 + x];   // row Q*k1 + q
+    if (!colok) return v;
+    if (PASS == 0) {
+      const int row = g + cs.Q * m;   // q + Q*p
+      if (cs.in_mode == 0) {
+        v = grid[int64_t(row) * cs.n1 + gx];
+      } else if (row < lo0 || row >= hi00) {
+        // gather the caller's uniform array with the correction factors
+        int iu0, icf0;
+        grid_to_uni(row, N0, cs.n, u.fft_order, iu0, icf0);
+        const cplx<T> xv = uptr[int64_t(iu0) * u.stride[0] + int64_t(iu1) * u.stride[1]];
+        const T f = T(u.corfac[0][icf0] * cf1);
+        v = mkc<T>(xv.x * f, xv.y * f);
       }
+    } else {
+      v = work[int64_t(g * cs.Q + m) * cs.N1 + x];   // row Q*k1 + q
     }
     return v;
   };
   {
     constexpr int LB = 8;   // loads in flight per thread
-    const int tot = len * C;
-    for (int b0 = tid; b0 < tot; b0 += LB * int(blockDim.x)) {
+    for (int mb = m0; mb < len; mb += LB * mstep) {
       cplx<T> v[LB];
 #pragma unroll
       for (int u2 = 0; u2 < LB; ++u2) {
-        const int idx = b0 + u2 * int(blockDim.x);
-        v[u2] = idx < tot ? load_elem(idx) : mkc<T>(T(0), T(0));
+        const int m = mb + u2 * mstep;
+        v[u2] = m < len ? load_m(m) : mkc<T>(T(0), T(0));
       }
 #pragma unroll
       for (int u2 = 0; u2 < LB; ++u2) {
-        const int idx = b0 + u2 * int(blockDim.x);
-        if (idx < tot) s[idx] = v[u2];
+        const int m = mb + u2 * mstep;
+        if (m < len) s[m * C + c] = v[u2];
       }
     }
   }
   __syncthreads();
   pencil_fft<T, FWD, cols_maxr<T>()>(s, s2, C, cs.lc, spp, twh, twl);
   const cplx<T> *sa = s2;
-  // ---- store
-  for (int idx = tid; idx < len * C; idx += blockDim.x) {
-    const int m = idx >> cs.lc, c = idx & (C - 1);
-    const int x = x0 + c;
-    if (x >= cs.N1) continue;
-    cplx<T> v = sa[idx];
-    if (PASS == 0) {
-      // twiddle w_n^(q*k1) (q*k1 < Q*P = n), then work row q + Q*k1
-      cplx<T> w = tw[g * m];
-      if (!FWD) w.y = -w.y;
-      v = cmul<T>(v, w);
-      work[int64_t(g + cs.Q * m) * cs.N1 + x] = v;
-    } else {
-      const int k = g + cs.P * m;   // k1 + P*k2
-      const int gc = kept_to_grid(x, cs.N1, cs.n1);
-      if (cs.out_mode == 0) {
-        grid[int64_t(k) * cs.n1 + gc] = v;
-      } else if (k < lo0 || k >= hi00) {
-        int iu0, icf0, iu1, icf1;
-        grid_to_uni(k, N0, cs.n, u.fft_order, iu0, icf0);
-        grid_to_uni(gc, cs.N1, cs.n1, u.fft_order, iu1, icf1);
-        const T f = T(u.corfac[0][icf0] * u.corfac[1][icf1]);
-        static_cast<cplx<T> *>(u.ptr)[int64_t(iu0) * u.stride[0] + int64_t(iu1) * u.stride[1]] =
-            mkc<T>(v.x * f, v.y * f);
+  // ---- store (same column per thread)
+  if (colok) {
+    for (int m = m0; m < len; m += mstep) {
+      cplx<T> v = sa[m * C + c];
+      if (PASS == 0) {
+        // twiddle w_n^(q*k1) (q*k1 < Q*P = n), then work row q + Q*k1
+        cplx<T> w = tw[g * m];
+        if (!FWD) w.y = -w.y;
+        v = cmul<T>(v, w);
+        work[int64_t(g + cs.Q * m) * cs.N1 + x] = v;
+      } else {
+        const int k = g + cs.P * m;   // k1 + P*k2
+        if (cs.out_mode == 0) {
+          grid[int64_t(k) * cs.n1 + gx] = v;
+        } else if (k < lo0 || k >= hi00) {
+          int iu0, icf0;
+          grid_to_uni(k, N0, cs.n, u.fft_order, iu0, icf0);
+          const T f = T(u.corfac[0][icf0] * cf1);
+          static_cast<cplx<T> *>(u.ptr)[int64_t(iu0) * u.stride[0] + int64_t(iu1) * u.stride[1]] =
+              mkc<T>(v.x * f, v.y * f);
+        }
       }
     }
   }
