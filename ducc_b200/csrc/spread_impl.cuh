@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(SP_THREADS)
 // scratch of the bank-balanced interpolation order (after the tile buffer)
 template <typename T> struct InterpOrder {
   static constexpr int NSLOT = 128 / int(sizeof(cplx<T>));   // 8-/16-byte bank slots
-  static constexpr int IB = 1024;                             // points per sorted batch
+  static constexpr int IB = 512;                             // points per sorted batch
   // slot counters, then per-point records: output index, first cell, kernel
   // argument per axis
   static constexpr size_t bytes(int ndim) { return NSLOT * 4 + IB * (8 + ndim * sizeof(T)); }
@@ -431,7 +431,7 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
       for (int k = 0; k < PER; ++k) {
         if (pb[k] >= 0) {
           const int e = atomicAdd(&s_cnt[pb[k] & (NSLOT - 1)], 1);
-          const int eq = q > 1 ? int(fastdiv(uint32_t(e), mq)) : e;   // e / q (e < 1024)
+          const int eq = q > 1 ? int(fastdiv(uint32_t(e), mq)) : e;   // e / q (e < IB)
           const int w = (e - eq * q) * 32 + eq;
           r_j[w] = pj[k];
           r_base[w] = pb[k];
@@ -499,9 +499,9 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
   }
 }
 
-// five CTAs per SM for single-precision 1D/2D (fits 48 registers without spills)
+// six CTAs per SM for single-precision 1D/2D (fits 40 registers)
 template <typename T, int NDIM> constexpr int interp_min_ctas() {
-  return (sizeof(T) == 4 && NDIM < 3) ? 5 : 1;
+  return (sizeof(T) == 4 && NDIM < 3) ? 6 : 1;
 }
 
 template <typename T, typename Tc, int NDIM, int W>
