@@ -786,11 +786,6 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
   if (tid == 0 && int(blockIdx.x) < nlines) issue_load(blockIdx.x, bi);
   for (int L = blockIdx.x; L < nlines; L += gridDim.x) {
     const int Ln = L + gridDim.x;
-    if (tid == 0 && Ln < nlines) {
-      // buffer bf was the source of the previous row's bulk stores
-      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-      issue_load(Ln, bf);
-    }
     cplx<T> *in = bufs + bi * n;
     const cplx<T> *src = grid + int64_t(L) * rs;
     // ragged ends of the ranges and the zero middle (disjoint from the bulk part)
@@ -810,22 +805,20 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
       if (tid == 0) atomicExch(err, 1);
       break;
     }
-    // all passes in place in the input buffer
+    // every thread has finished the previous row (its ragged output copies
+    // read buffer bf): prefetch the next row there once the previous row's
+    // bulk stores have read it
+    if (tid == 0 && Ln < nlines) {
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      issue_load(Ln, bf);
+    }
+    // all passes in place in the input buffer (each thread fences its
+    // shared-memory writes for the bulk stores before the final barrier)
     pencil_fft_inplace<T, FWD, rows_maxr<T>()>(in, spp, twh, twl);
     const cplx<T> *sa = in;
     // result in sa; write it back (bulk part by thread 0, ragged ends by all)
     cplx<T> *dst = grid + int64_t(L) * rs;
     const int nro = out_kept ? 2 : 1;
-    for (int r = 0; r < nro; ++r) {
-      const int ra = out_kept ? (r == 0 ? 0 : hi0) : 0;
-      const int rb = out_kept ? (r == 0 ? lo : n) : n;
-      int a2, b2;
-      fft_aligned(ra, rb, ES, a2, b2);
-      for (int k = ra + tid; k < a2; k += blockDim.x) dst[k] = sa[k];
-      for (int k = b2 + tid; k < rb; k += blockDim.x) dst[k] = sa[k];
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
     if (tid == 0) {
       for (int r = 0; r < nro; ++r) {
         const int ra = out_kept ? (r == 0 ? 0 : hi0) : 0;
@@ -835,6 +828,14 @@ __global__ void __launch_bounds__(rows_threads<T>(), 1)
         if (b2 > a2) fft_bulk_store(dst + a2, sa + a2, uint32_t(b2 - a2) * ES);
       }
       asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    for (int r = 0; r < nro; ++r) {
+      const int ra = out_kept ? (r == 0 ? 0 : hi0) : 0;
+      const int rb = out_kept ? (r == 0 ? lo : n) : n;
+      int a2, b2;
+      fft_aligned(ra, rb, ES, a2, b2);
+      for (int k = ra + tid; k < a2; k += blockDim.x) dst[k] = sa[k];
+      for (int k = b2 + tid; k < rb; k += blockDim.x) dst[k] = sa[k];
     }
     // the prefetched buffer is next; this one is busy storing
     const int t = bi;
