@@ -524,13 +524,53 @@ __device__ __forceinline__ void fft_lines_block(cplx<T> *__restrict__ grid, cons
     T f = T(lfac[l] * cfa[icf]);
     static_cast<cplx<T> *>(u.ptr)[luoff[l] + int64_t(iu) * ust] = mkc<T>(x.x * f, x.y * f);
   };
-  if (ls.es == 1) {
-    for (int l = 0; l < nl; ++l)
-      for (int k = threadIdx.x; k < n; k += blockDim.x) s[(k << lnl) + l] = load_elem(l, k);
-  } else {
+  {
+    // LB loads in flight per thread before their shared-memory stores;
+    // contiguous lines walk each line with consecutive threads (coalesced).
+    // Each thread keeps its (line, element) position and steps it by the
+    // block size (no division per element).
+    constexpr int LB = 8;
     const int tot = n << lnl;
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x)
-      s[idx] = load_elem(idx & (nl - 1), idx >> lnl);
+    const int nt = int(blockDim.x);
+    int fl, fk;   // position of flat index f = threadIdx.x (+ multiples of nt)
+    if (ls.es == 1) {
+      fl = int(threadIdx.x) / n;
+      fk = int(threadIdx.x) - fl * n;
+    } else {
+      fl = int(threadIdx.x) & (nl - 1);
+      fk = int(threadIdx.x) >> lnl;
+    }
+    const int dl = ls.es == 1 ? nt / n : (nt & (nl - 1));
+    const int dk = ls.es == 1 ? nt - (nt / n) * n : (nt >> lnl);
+    for (int b0 = threadIdx.x; b0 < tot; b0 += LB * nt) {
+      cplx<T> v[LB];
+      int dst[LB];
+#pragma unroll
+      for (int u2 = 0; u2 < LB; ++u2) {
+        const bool in = b0 + u2 * nt < tot;
+        dst[u2] = (fk << lnl) + fl;
+        v[u2] = in ? load_elem(fl, fk) : mkc<T>(T(0), T(0));
+        // advance by nt in the flat order
+        if (ls.es == 1) {
+          fk += dk;
+          fl += dl;
+          if (fk >= n) {
+            fk -= n;
+            ++fl;
+          }
+        } else {
+          fl += dl;
+          fk += dk;
+          if (fl >= nl) {
+            fl -= nl;
+            ++fk;
+          }
+        }
+      }
+#pragma unroll
+      for (int u2 = 0; u2 < LB; ++u2)
+        if (b0 + u2 * nt < tot) s[dst[u2]] = v[u2];
+    }
   }
   __syncthreads();
   if (spen.L > 0) {
