@@ -352,10 +352,57 @@ size_t chunk_workspace_bytes(uint32_t n) {
   return 2 * size_t(n) * sizeof(uint32_t) + scan_workspace_bytes(n) + 1024;
 }
 
+// ---------------------------------------------------------------- small read-backs
+// A few 32-bit device words are read back by a one-warp kernel that stores
+// them into mapped pinned host memory, then the stream is synchronised.  A
+// device->host memcpy of the same words would queue on the device->host copy
+// engine behind large result copies that other streams issued earlier (the
+// pipelined host calls copy 100 MB result ranges back while the next groups
+// are sorted), and the sort would wait for them; a kernel's stores to host
+// memory do not.
+struct WordSrcs {
+  const uint32_t *p[8];
+};
+
+__global__ void k_read_words(WordSrcs s, int n, volatile uint32_t *dst) {
+  const int i = threadIdx.x;
+  if (i < n) dst[i] = *s.p[i];
+  __threadfence_system();
+}
+
+void read_words(const uint32_t *const *src, int n, uint32_t *out, cudaStream_t st) {
+  DN_REQUIRE(n >= 1 && n <= 8, ST_INTERNAL, "read_words: 1 to 8 words");
+  // one mapped buffer per host thread and device (calls of one thread are
+  // sequential; calls from several threads use separate buffers)
+  static thread_local uint32_t *host[64] = {nullptr};
+  static thread_local uint32_t *mapped[64] = {nullptr};
+  int dev = 0;
+  DN_CUDA(cudaGetDevice(&dev));
+  DN_REQUIRE(dev >= 0 && dev < 64, ST_INTERNAL, "device index out of range");
+  if (!host[dev]) {
+    void *h = nullptr;
+    DN_CUDA(cudaHostAlloc(&h, 8 * sizeof(uint32_t), cudaHostAllocMapped | cudaHostAllocPortable));
+    void *d = nullptr;
+    DN_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+    host[dev] = static_cast<uint32_t *>(h);
+    mapped[dev] = static_cast<uint32_t *>(d);
+  }
+  WordSrcs s{};
+  for (int i = 0; i < n; ++i) s.p[i] = src[i];
+  k_read_words<<<1, 32, 0, st>>>(s, n, mapped[dev]);
+  DN_LAUNCHED();
+  DN_CUDA(cudaStreamSynchronize(st));
+  const volatile uint32_t *h = host[dev];
+  for (int i = 0; i < n; ++i) out[i] = h[i];
+}
+
 // Builds the chunk list from sorted keys; returns the number of chunks (the
-// count is copied to the host, which synchronises the stream once).
+// count is read back to the host, which synchronises the stream once: through
+// mapped host memory, or with zero_copy false, which allocates nothing, by a
+// device->host copy).
 uint32_t build_chunks(const uint32_t *skeys, uint32_t n, int tile_shift, uint32_t chunk,
-                      Chunk *chunks, uint32_t *d_count, void *ws, cudaStream_t st) {
+                      Chunk *chunks, uint32_t *d_count, void *ws, cudaStream_t st,
+                      bool zero_copy) {
   if (n == 0) return 0;
   uint32_t *flags = static_cast<uint32_t *>(ws);
   uint32_t *pos = flags + n;
@@ -372,8 +419,13 @@ uint32_t build_chunks(const uint32_t *skeys, uint32_t n, int tile_shift, uint32_
   k_chunk_counts<<<g, 256, 0, st>>>(chunks, d_count, n);
   DN_LAUNCHED();
   uint32_t h = 0;
-  DN_CUDA(cudaMemcpyAsync(&h, d_count, 4, cudaMemcpyDeviceToHost, st));
-  DN_CUDA(cudaStreamSynchronize(st));
+  if (zero_copy) {
+    const uint32_t *src[1] = {d_count};
+    read_words(src, 1, &h, st);
+  } else {
+    DN_CUDA(cudaMemcpyAsync(&h, d_count, 4, cudaMemcpyDeviceToHost, st));
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
   return h;
 }
 

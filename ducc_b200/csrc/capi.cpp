@@ -103,9 +103,9 @@ static void check_device_error(int *word, cudaStream_t st) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   DN_CUDA(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) return;
-  int h = 0;
-  DN_CUDA(cudaMemcpyAsync(&h, word, sizeof(int), cudaMemcpyDeviceToHost, st));
-  DN_CUDA(cudaStreamSynchronize(st));
+  uint32_t h = 0;
+  const uint32_t *src[1] = {reinterpret_cast<const uint32_t *>(word)};
+  read_words(src, 1, &h, st);
   if (h != 0) {
     DN_CUDA(cudaMemsetAsync(word, 0, sizeof(int), st));
     throw Error(ST_TIMEOUT, "a bounded device-side wait gave up (tensor-core spreader or FFT)");
@@ -725,7 +725,7 @@ static dnufft_opts resolved(const dnufft_opts *o, bool for_plan) {
 // the finished groups' results, overlap the work on the current one.  Kernel,
 // oversampled grid and FFT are those of the whole problem.
 constexpr uint32_t PIPE_MIN_POINTS = 1u << 22;     // pipelined from 4M points
-constexpr uint32_t PIPE_GROUP_POINTS = 12500000u;  // about this many per group
+constexpr uint32_t PIPE_GROUP_POINTS = 8500000u;   // about this many per group
 
 static int pipe_groups(uint32_t M) {
   if (M < PIPE_MIN_POINTS) return 1;
@@ -772,11 +772,12 @@ static void nu2u_pipelined(const Setup &s, const View &points, const View &coord
   const size_t wb = fft_work_bytes(s.g, vb);
   if (wb) work = DevBuf(wb, st);
   Staged so(out, false, true, st);
-  DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * vb, st));
   EventSet copied(G);
   // declared after the buffers: destroyed (after synchronising) before them
   SideStream up(st, true);
   up.start();
+  // zeroed on the caller's stream while the first groups are copied in
+  DN_CUDA(cudaMemsetAsync(grid.p, 0, cells * vb, st));
   for (int gi = 0; gi < G; ++gi) {
     const uint64_t a = group_start(M, G, gi), b = group_start(M, G, gi + 1);
     DN_CUDA(cudaMemcpyAsync(static_cast<char *>(dcoord.p) + a * nd * cb,
@@ -1272,7 +1273,8 @@ static void nu2u_scratch_typed(const Setup &s, const View &points, const View &c
   // the stream, after which the host constant buffers may be released)
   launch_fold_keys(s.coord_f64, coord.data, coord.stride[0], coord.stride[1], M, g, keys, perm, st);
   radix_sort_pairs(keys, perm, M, s.keybits, rws, st);
-  uint32_t nch = build_chunks(keys, M, s.tile_shift, s.chunk, chunks, count, cws, st);
+  uint32_t nch = build_chunks(keys, M, s.tile_shift, s.chunk, chunks, count, cws, st,
+                              /*zero_copy=*/false);
   PointsDesc pts{coord.data, coord.stride[0], coord.stride[1], false, s.coord_f64, perm, M};
   ChunkList cl{chunks, nch};
   // the scratch keeps the previous call's contents: the grid must start at zero

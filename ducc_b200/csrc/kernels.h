@@ -19,7 +19,10 @@ void radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t n, int keybits, v
                       cudaStream_t st);
 size_t chunk_workspace_bytes(uint32_t n);
 uint32_t build_chunks(const uint32_t *skeys, uint32_t n, int tile_shift, uint32_t chunk,
-                      Chunk *chunks, uint32_t *d_count, void *ws, cudaStream_t st);
+                      Chunk *chunks, uint32_t *d_count, void *ws, cudaStream_t st,
+                      bool zero_copy = true);
+// reads n (1..8) device words into out through mapped host memory; synchronises st
+void read_words(const uint32_t *const *src, int n, uint32_t *out, cudaStream_t st);
 void launch_gather_coords(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
                           int ndim, const uint32_t *perm, uint32_t n, void *out,
                           cudaStream_t st);

@@ -922,11 +922,8 @@ uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t g
   k_tc_emit<<<gb, 256, 0, st>>>(cl.chunks, qb, pos, nch, kblk);
   DN_LAUNCHED();
   uint32_t h[4] = {0u, 0u, 0u, 0u};
-  DN_CUDA(cudaMemcpyAsync(&h[0], pos + nch - 1, 4, cudaMemcpyDeviceToHost, st));
-  DN_CUDA(cudaMemcpyAsync(&h[1], nrec + nch - 1, 4, cudaMemcpyDeviceToHost, st));
-  DN_CUDA(cudaMemcpyAsync(&h[2], cpos + nch - 1, 4, cudaMemcpyDeviceToHost, st));
-  DN_CUDA(cudaMemcpyAsync(&h[3], cost + nch - 1, 4, cudaMemcpyDeviceToHost, st));
-  DN_CUDA(cudaStreamSynchronize(st));
+  const uint32_t *src[4] = {pos + nch - 1, nrec + nch - 1, cpos + nch - 1, cost + nch - 1};
+  read_words(src, 4, h, st);
   const uint32_t total = h[0] + h[1], ctotal = h[2] + h[3];
   k_tc_ranges<<<(groups + 1 + 255) / 256, 256, 0, st>>>(pos, cpos, nch, total, ctotal, groups,
                                                          range);
