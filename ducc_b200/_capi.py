@@ -51,6 +51,7 @@ EXPORTS = [
     "dnufft_nu2u_noalloc", "dnufft_noalloc_scratch_bytes", "dnufft_u2nu_dcoord",
     "dnufft_plan_u2nu_dcoord", "dnufft_batch_create", "dnufft_batch_nu2u", "dnufft_batch_u2nu",
     "dnufft_batch_destroy", "dnufft_kernel_candidates", "dnufft_selftest_wait_timeout",
+    "dnufft_plan_spread", "dnufft_plan_grid_to_uniform", "dnufft_find_parameters",
 ]
 
 
@@ -80,6 +81,12 @@ def lib():
                                      P(Array), P(Opts), vp]
     L.dnufft_plan_u2nu_dcoord.argtypes = [vp, ctypes.c_int, P(Array), P(Array), P(Array), vp]
     L.dnufft_plan_destroy.argtypes = [vp]
+    L.dnufft_plan_spread.argtypes = [vp, P(Array), P(Array), vp]
+    L.dnufft_plan_grid_to_uniform.argtypes = [vp, ctypes.c_int, P(Array), P(Array), vp]
+    L.dnufft_find_parameters.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int64),
+                                         ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
+                                         ctypes.c_int, P(Opts), P(ctypes.c_int32),
+                                         P(ctypes.c_int64)]
     L.dnufft_batch_create.argtypes = [ctypes.c_int, P(vp), P(ctypes.c_int32), vp, P(vp)]
     for f in (L.dnufft_batch_nu2u, L.dnufft_batch_u2nu):
         f.argtypes = [vp, ctypes.c_int, P(Array), P(Array), vp]

@@ -1179,6 +1179,99 @@ static void plan_dcoord_impl(dnufft_plan *p, int forward, const dnufft_array *gr
   sg.finish();
 }
 
+// ---------------------------------------------------------------- split type 1
+// A type-1 transform whose points are split over several GPUs (one process
+// each): every rank spreads its own points into a full oversampled grid
+// (plan_spread), the caller sums the grids over the ranks (one all-reduce),
+// and the sum goes through the FFT and the correction (plan_grid_to_uniform).
+// Spreading is linear in the values, so the summed grid is the grid of all
+// points.  The oversampled grid is a C-contiguous device array of the plan's
+// data type and oversampled shape.
+static View over_grid_view(const dnufft_plan *p, const dnufft_array *grid_) {
+  const Setup &s = p->s;
+  View g = view_of(grid_, "grid");
+  DN_REQUIRE(!g.host, ST_BADARG, "the oversampled grid must be a device array");
+  DN_REQUIRE(g.dtype == (s.calc_f64 ? DNUFFT_C128 : DNUFFT_C64), ST_BADARG,
+             "the oversampled grid must have the plan's data type");
+  DN_REQUIRE(g.ndim == s.g.ndim, ST_BADARG, "oversampled grid dimensions mismatch");
+  int64_t cs = 1;
+  for (int d = s.g.ndim - 1; d >= 0; --d) {
+    DN_REQUIRE(g.shape[d] == int64_t(s.g.nover[d]), ST_BADARG,
+               "the oversampled grid must have the plan's oversampled sizes");
+    DN_REQUIRE(g.stride[d] == cs, ST_BADARG, "the oversampled grid must be C-contiguous");
+    cs *= g.shape[d];
+  }
+  return g;
+}
+
+static void plan_spread_impl(dnufft_plan *p, const dnufft_array *points_, dnufft_array *grid_,
+                             cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  const bool f64 = s.calc_f64;
+  View points = view_of(points_, "points");
+  DN_REQUIRE(points.dtype == (f64 ? DNUFFT_C128 : DNUFFT_C64), ST_BADARG,
+             f64 ? "a float64-coordinate plan needs complex128 data"
+                 : "a float32-coordinate plan needs complex64 data");
+  DN_REQUIRE(points.ndim == 1 && uint64_t(points.shape[0]) == s.npoints, ST_BADARG,
+             "number of points mismatch");
+  const View grid = over_grid_view(p, grid_);
+  DN_CUDA(cudaMemsetAsync(grid.data, 0, grid_cells(s.g) * (f64 ? 16 : 8), st));
+  if (s.npoints > 0) {
+    Staged sp(points, true, false, st);
+    PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
+                   p->ix.perm.as<uint32_t>(), s.npoints};
+    ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
+    const TcBlocks tb = p->ix.tc();
+    const TcBlocks *sk = s.qbits ? &tb : nullptr;
+    int *err = device_error_word();
+    if (f64) spread_points<double>(s, pts, cl, sk, sp.dev.data, sp.dev.stride[0], grid.data, err, st);
+    else spread_points<float>(s, pts, cl, sk, sp.dev.data, sp.dev.stride[0], grid.data, err, st);
+    check_device_error(err, st);
+  }
+}
+
+static void plan_grid_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array *grid_,
+                                      dnufft_array *out_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  const bool f64 = s.calc_f64;
+  const View grid = over_grid_view(p, grid_);
+  View out = view_of(out_, "out");
+  DN_REQUIRE(out.dtype == grid.dtype, ST_BADARG, "out must have the plan's data type");
+  DN_REQUIRE(out.ndim == s.g.ndim, ST_BADARG, "uniform grid dimensions mismatch");
+  for (int d = 0; d < s.g.ndim; ++d)
+    DN_REQUIRE(out.shape[d] == s.g.nuni[d], ST_BADARG, "uniform grid dimensions mismatch");
+  Staged so(out, false, true, st);
+  const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
+  if (wb && !p->work.p) {
+    p->work = DevBuf(wb, st);
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
+  int *err = device_error_word();
+  const bool fo = p->o.fft_order != 0;
+  if (f64)
+    fft_nu2u_tail<double>(grid.data, s.g, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
+                          so.dev.stride, st, p->work.p, err);
+  else
+    fft_nu2u_tail<float>(grid.data, s.g, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
+                         so.dev.stride, st, p->work.p, err);
+  check_device_error(err, st);
+  so.finish();
+}
+
+static void find_parameters_impl(int nu2u, int ndim, const int64_t *shape, uint64_t npoints,
+                                 double eps, int calc_f64, int coord_f64, const dnufft_opts *opts_,
+                                 int32_t *kidx, int64_t *nover) {
+  DN_REQUIRE(shape != nullptr && kidx != nullptr && nover != nullptr, ST_BADARG,
+             "null argument");
+  DN_REQUIRE(ndim >= 1 && ndim <= 3, ST_BADARG, "unsupported dimensionality");
+  const dnufft_opts o = resolved(opts_, true);
+  const Setup s = make_setup(ndim, shape, npoints, eps, nu2u != 0, calc_f64 != 0, coord_f64 != 0, o);
+  *kidx = s.kidx;
+  for (int d = 0; d < 3; ++d) nover[d] = d < ndim ? int64_t(s.g.nover[d]) : 1;
+}
+
 // ---------------------------------------------------------------- scratch-only type 1
 // A type-1 transform whose every temporary (correction factors, twiddles,
 // tile keys and permutation, sort / chunk workspaces, chunk list, oversampled
@@ -1453,6 +1546,24 @@ int dnufft_plan_u2nu_dcoord(dnufft_plan *plan, int forward, const dnufft_array *
                             const dnufft_array *weights, dnufft_array *grad, void *stream) {
   DN_GUARD(dnufft::plan_dcoord_impl(plan, forward, grid, weights, grad,
                                     static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_spread(dnufft_plan *plan, const dnufft_array *points, dnufft_array *grid,
+                       void *stream) {
+  DN_GUARD(dnufft::plan_spread_impl(plan, points, grid, static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_grid_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
+                                dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::plan_grid_to_uniform_impl(plan, forward, grid, out,
+                                             static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_find_parameters(int nu2u, int ndim, const int64_t *grid_shape, uint64_t npoints,
+                           double epsilon, int calc_f64, int coord_f64, const dnufft_opts *opts,
+                           int32_t *kernel_index, int64_t *nover) {
+  DN_GUARD(dnufft::find_parameters_impl(nu2u, ndim, grid_shape, npoints, epsilon, calc_f64,
+                                        coord_f64, opts, kernel_index, nover))
 }
 
 int dnufft_plan_destroy(dnufft_plan *plan) {

@@ -27,7 +27,7 @@ import numpy as np
 
 from . import _capi as C
 
-__all__ = ["nu2u", "u2nu", "u2nu_dcoord", "bestEpsilon", "plan"]
+__all__ = ["nu2u", "u2nu", "u2nu_dcoord", "bestEpsilon", "plan", "find_parameters"]
 
 
 def _np_complex_for(code):
@@ -152,6 +152,28 @@ def bestEpsilon(*, ndim, singleprec, sigma_min=1.1, sigma_max=2.6):
     return r.value
 
 
+def find_parameters(*, nu2u, grid_shape, npoints, epsilon, singleprec, coord_single=None,
+                    nthreads=0, sigma_min=1.1, sigma_max=2.6):
+    """(kernel-table row, oversampled shape) that DUCC's parameter choice gives
+    for a transform of ``npoints`` points (findNufftParameters,
+    src/ducc0/nufft/nufft.h:155-216; plan defaults).  Processes that split the
+    points of one transform pass the total count and plan with
+    ``force_kernel`` / ``force_nover``.  Runs on the host only."""
+    shape = [int(x) for x in grid_shape]
+    ndim = len(shape)
+    if coord_single is None:
+        coord_single = singleprec
+    o = C.make_opts(True, nthreads, sigma_min, sigma_max, 2 * math.pi, False, 0, "auto", ndim)
+    shp = (ctypes.c_int64 * 3)(*(shape + [1] * (3 - ndim)))
+    kidx = ctypes.c_int32()
+    nover = (ctypes.c_int64 * 3)()
+    C.check(C.lib().dnufft_find_parameters(1 if nu2u else 0, ndim, shp, int(npoints),
+                                           float(epsilon), 0 if singleprec else 1,
+                                           0 if coord_single else 1, ctypes.byref(o),
+                                           ctypes.byref(kidx), nover))
+    return kidx.value, [int(nover[d]) for d in range(ndim)]
+
+
 class plan:
     """NUFFT plan for fixed coordinates (DUCC's ``ducc0.nufft.plan``).
 
@@ -242,6 +264,40 @@ class plan:
         C.check(C.lib().dnufft_plan_u2nu_dcoord(self._ptr, 1 if forward else 0, ctypes.byref(a_g),
                                                 ctypes.byref(a_w), ctypes.byref(a_o),
                                                 C.stream_of(grid, weights, op.buf, stream=stream)))
+        return op.finish()
+
+    # -- type 1 in two halves (one transform's points split over several GPUs)
+    def spread(self, *, points, out=None, stream=None):
+        """Spread this plan's points with the values ``points`` into an
+        oversampled grid: a C-contiguous CUDA tensor of the plan's data type and
+        oversampled shape (``info()["nover"]``), zeroed first and returned.
+        Summing such grids over plans of disjoint point sets and passing the sum
+        to ``grid_to_uniform`` gives the type 1 of all points (the plans must
+        share kernel and oversampled sizes, see ``find_parameters``)."""
+        import torch
+        points = _prepare_in(points)
+        if out is None:
+            dev = points.device if C.is_torch(points) else (
+                self._torch_device or torch.device("cuda", torch.cuda.current_device()))
+            out = torch.empty(tuple(self.info()["nover"]),
+                              dtype=torch.complex128 if self._f64 else torch.complex64,
+                              device=dev)
+        a_p, a_g = C.describe(points), C.describe(out)
+        C.check(C.lib().dnufft_plan_spread(self._ptr, ctypes.byref(a_p), ctypes.byref(a_g),
+                                           C.stream_of(points, out, stream=stream)))
+        return out
+
+    def grid_to_uniform(self, *, forward, grid, out=None, stream=None):
+        """FFT and correction of an oversampled grid (as from ``spread``, maybe
+        summed over several plans; it is overwritten) into the uniform grid
+        ``out`` (allocated like ``nu2u``'s when None); returns ``out``."""
+        if out is None:
+            out = self._alloc(grid, self.grid_shape)
+        op = _OutProxy(out)
+        a_g, a_o = C.describe(grid), C.describe(op.buf)
+        C.check(C.lib().dnufft_plan_grid_to_uniform(self._ptr, 1 if forward else 0,
+                                                    ctypes.byref(a_g), ctypes.byref(a_o),
+                                                    C.stream_of(grid, op.buf, stream=stream)))
         return op.finish()
 
     def info(self):

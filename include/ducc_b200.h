@@ -150,6 +150,34 @@ int dnufft_u2nu_dcoord(const dnufft_array *grid, const dnufft_array *coord, int 
 int dnufft_plan_u2nu_dcoord(dnufft_plan *plan, int forward, const dnufft_array *grid,
                             const dnufft_array *weights, dnufft_array *grad, void *stream);
 
+/* Type 1 in two halves, for one transform whose points are split over several
+ * GPUs (no counterpart in DUCC, whose transforms run on one node's threads):
+ * each process makes a plan of its own points (with the kernel and
+ * oversampled sizes of the whole transform, see dnufft_find_parameters),
+ * dnufft_plan_spread writes the spread of its points into an oversampled grid
+ * (zeroed first), the caller sums these grids over the processes (one
+ * all-reduce), and dnufft_plan_grid_to_uniform runs the FFT and the
+ * correction of the summed grid (which it overwrites) into out.  Spreading is
+ * linear in the values, so the result is the type 1 of all points.  grid: a
+ * C-contiguous device array of the plan's data type with the plan's
+ * oversampled shape (dnufft_plan_info.nover).  The two halves are
+ * src/ducc0/nufft/nufft.h:1279-1285 (zeroing and spreading) and :1286-1312
+ * (FFT and correction) of DUCC's 2D nonuni2uni (1D and 3D alike). */
+int dnufft_plan_spread(dnufft_plan *plan, const dnufft_array *points, dnufft_array *grid,
+                       void *stream);
+int dnufft_plan_grid_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
+                                dnufft_array *out, void *stream);
+
+/* Kernel-table row and oversampled sizes (nover[0..2], 1 beyond ndim) that
+ * DUCC's parameter choice gives for a transform of npoints points; its cost
+ * model depends on npoints and opts->nthreads, so processes sharing one
+ * transform pass the global count and plan with force_kernel / force_nover.
+ * opts: plan defaults when NULL.  Replaces findNufftParameters
+ * (src/ducc0/nufft/nufft.h:155-216). */
+int dnufft_find_parameters(int nu2u, int ndim, const int64_t *grid_shape, uint64_t npoints,
+                           double epsilon, int calc_f64, int coord_f64, const dnufft_opts *opts,
+                           int32_t *kernel_index, int64_t *nover);
+
 /* Replaces plan destruction (Julia nufft_delete_plan, julia/ducc_julia.cc:372-392). */
 int dnufft_plan_destroy(dnufft_plan *plan);
 

@@ -1,0 +1,133 @@
+"""Type 1 in two halves (plan.spread + plan.grid_to_uniform), the pieces of a
+transform whose points are split over several GPUs: the halves against the
+plan's one-piece type 1, two shards whose summed grids give the transform of
+all points (checked against the one-piece transform and direct sums), the
+sharded plan over a one-rank NCCL group, and argument errors.
+"""
+import numpy as np
+import pytest
+
+from ducc_b200 import nufft
+from oracle import nufft_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(ndim, M, single, seed):
+    rng = np.random.default_rng(seed)
+    coord = rng.uniform(-np.pi, np.pi, (M, ndim))
+    vals = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    if single:
+        return coord.astype(np.float32), vals.astype(np.complex64)
+    return coord, vals
+
+
+CASES = [((256, 240), 400_000, True, 1e-6),     # tensor-core spreader ('auto')
+         ((96, 80), 30_000, True, 1e-5),        # plain
+         ((96, 80), 30_000, False, 1e-11),
+         ((400,), 20_000, False, 1e-10),
+         ((24, 20, 16), 20_000, True, 1e-5)]
+
+
+@pytest.mark.parametrize("shape,M,single,eps", CASES)
+def test_halves_equal_one_piece(shape, M, single, eps):
+    import torch
+    coord, vals = _problem(len(shape), M, single, 3)
+    dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+    p = nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=eps)
+    for forward in (True, False):
+        ref = p.nu2u(points=dv, forward=forward).cpu().numpy()
+        g = p.spread(points=dv)
+        assert tuple(g.shape) == tuple(p.info()["nover"]) and g.is_contiguous()
+        got = p.grid_to_uniform(forward=forward, grid=g).cpu().numpy()
+        # same kernels; float atomics may add in another order
+        assert O.l2error(got, ref) < (1e-6 if single else 1e-14)
+
+
+@pytest.mark.parametrize("shape,M,single,eps", CASES)
+def test_two_shards_sum_to_whole(shape, M, single, eps):
+    import torch
+    coord, vals = _problem(len(shape), M, single, 4)
+    k, n = nufft.find_parameters(nu2u=True, grid_shape=shape, npoints=M, epsilon=eps,
+                                 singleprec=single)
+    cut = M // 3
+    parts = []
+    for sl in (slice(0, cut), slice(cut, M)):
+        dc = torch.from_numpy(np.ascontiguousarray(coord[sl])).cuda()
+        parts.append((nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=eps,
+                                 force_kernel=k, force_nover=n),
+                      torch.from_numpy(np.ascontiguousarray(vals[sl])).cuda()))
+    whole = nufft.plan(nu2u=True, coord=torch.from_numpy(coord).cuda(), grid_shape=shape,
+                       epsilon=eps, force_kernel=k, force_nover=n)
+    g = parts[0][0].spread(points=parts[0][1])
+    g += parts[1][0].spread(points=parts[1][1])
+    got = parts[0][0].grid_to_uniform(forward=True, grid=g).cpu().numpy()
+    ref = whole.nu2u(points=torch.from_numpy(vals).cuda(), forward=True).cpu().numpy()
+    assert O.l2error(got, ref) < (2e-6 if single else 1e-13)
+    # against the direct sum over a sample of points (all modes)
+    sub = slice(0, 2000)
+    p_sub = nufft.plan(nu2u=True, coord=torch.from_numpy(np.ascontiguousarray(coord[sub])).cuda(),
+                       grid_shape=shape, epsilon=eps, force_kernel=k, force_nover=n)
+    ga = p_sub.spread(points=torch.from_numpy(np.ascontiguousarray(vals[sub])).cuda())
+    got_sub = p_sub.grid_to_uniform(forward=True, grid=ga).cpu().numpy()
+    exact = O.direct_nu2u(coord[sub].astype(np.float64), vals[sub].astype(np.complex128), shape,
+                          True)
+    assert O.l2error(got_sub, exact) < 4 * eps
+
+
+def test_sharded_plan_one_rank_nccl():
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    td.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                          world_size=1, timeout=datetime.timedelta(seconds=60),
+                          device_id=torch.device("cuda", torch.cuda.current_device()))
+    try:
+        shape, M, eps = (128, 112), 60_000, 1e-6
+        coord, vals = _problem(2, M, True, 5)
+        dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+        sp = D.ShardedPlan(nu2u=True, coord=dc, grid_shape=shape, epsilon=eps)
+        k, n = nufft.find_parameters(nu2u=True, grid_shape=shape, npoints=M, epsilon=eps,
+                                     singleprec=True)
+        assert sp.kernel_index == k and list(sp.nover) == list(n) and sp.npoints_total == M
+        got = sp.nu2u(forward=False, points=dv).cpu().numpy()
+        ref = nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=eps, force_kernel=k,
+                         force_nover=n).nu2u(points=dv, forward=False).cpu().numpy()
+        assert O.l2error(got, ref) < 1e-6
+        grid = torch.from_numpy((np.random.default_rng(6).standard_normal(shape)
+                                 + 0j).astype(np.complex64)).cuda()
+        pts = sp.u2nu(forward=True, grid=grid).cpu().numpy()
+        idx = np.arange(0, M, 97)
+        exact = O.direct_u2nu(grid.cpu().numpy().astype(np.complex128),
+                              coord[idx].astype(np.float64), True)
+        assert O.l2error(pts[idx], exact) < 4 * eps
+        td.barrier()
+    finally:
+        td.destroy_process_group()
+
+
+def test_split_type1_argument_errors():
+    import torch
+    coord, vals = _problem(2, 5000, True, 7)
+    dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+    p = nufft.plan(nu2u=True, coord=dc, grid_shape=(64, 64), epsilon=1e-5)
+    nover = tuple(p.info()["nover"])
+    with pytest.raises(RuntimeError, match="oversampled sizes"):
+        p.spread(points=dv, out=torch.empty((nover[0], nover[1] + 2), dtype=torch.complex64,
+                                            device="cuda"))
+    with pytest.raises(RuntimeError, match="C-contiguous"):
+        big = torch.empty((nover[1], nover[0]), dtype=torch.complex64, device="cuda")
+        p.spread(points=dv, out=big.t())
+    with pytest.raises(RuntimeError, match="data type"):
+        p.spread(points=dv, out=torch.empty(nover, dtype=torch.complex128, device="cuda"))
+    with pytest.raises(RuntimeError, match="device array"):
+        p.grid_to_uniform(forward=True, grid=np.zeros(nover, np.complex64))
+    with pytest.raises(RuntimeError, match="number of points"):
+        p.spread(points=dv[:100])

@@ -1,0 +1,109 @@
+"""Host side of one transform split over several ranks (ducc_b200.distributed),
+on the CPU: the parameter choice of the whole transform (the library's
+restatement of DUCC's findNufftParameters against the oracle's), its
+agreement over two `gloo` ranks, and the grid sum of the type-1 exchange.
+Without a GPU the oracle's FP64 spreading, FFT and correction stand in for
+the two CUDA halves of the type 1 (plan.spread / plan.grid_to_uniform, which
+the GPU tests check against the library's own one-piece transform), so what
+runs here is exactly the collective logic: count agreement, broadcast of the
+parameters, the all-reduce of the complex grid, and that the sum of the
+per-rank grids gives the transform of all points.
+"""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from ducc_b200 import nufft
+from oracle import nufft_oracle as O
+
+
+@pytest.mark.parametrize("shape,M,eps,single", [
+    ((4096, 4096), 50_000_000, 1e-6, True),
+    ((4096, 4096), 1_000_000, 1e-6, True),
+    ((256, 256), 200_000, 1e-6, False),
+    ((300,), 5_000, 1e-9, False),
+    ((48, 40, 32), 100_000, 1e-5, True),
+    ((64, 64, 64), 2_000_000, 1e-10, False),
+])
+def test_find_parameters_matches_oracle(shape, M, eps, single):
+    for nthreads in (1, 8):
+        k, n = nufft.find_parameters(nu2u=True, grid_shape=shape, npoints=M, epsilon=eps,
+                                     singleprec=single, nthreads=nthreads)
+        ko, no = O.find_parameters(eps, 1.1, 2.6, list(shape), M, True, nthreads, single)
+        assert k == ko and list(n) == list(no)
+
+
+def _free_port():
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+SHAPE = (40, 36)
+EPS = 1e-9
+M_RANK = (700, 1100)   # uneven shards
+
+
+def _inputs():
+    rng = np.random.default_rng(21)
+    M = sum(M_RANK)
+    coord = rng.uniform(-np.pi, np.pi, (M, 2))
+    vals = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    return coord, vals
+
+
+def _worker(rank, world, port, outdir):
+    import datetime
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    td.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                          world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        coord, vals = _inputs()
+        a = sum(M_RANK[:rank])
+        mine = slice(a, a + M_RANK[rank])
+        kidx, nover, total = D.global_parameters(nu2u=True, grid_shape=SHAPE,
+                                                 npoints_local=M_RANK[rank], epsilon=EPS,
+                                                 singleprec=False, nthreads=4)
+        p = O.Params(SHAPE, EPS, False, total, True, force=(kidx, nover))
+        # this rank's half of the type 1: its points spread on the oversampled grid
+        g = torch.from_numpy(O.spread(p, coord[mine], vals[mine]))
+        D.sum_grids(g)
+        # the other half from the summed grid: FFT + correction of the oracle
+        full = O._fft(g.numpy(), True)
+        out = np.zeros(SHAPE, np.complex128)
+        maps = O._index_maps(p, False)
+        fac = np.ones(())
+        for d, (icf, iu, ig) in enumerate(maps):
+            shp = [1, 1]
+            shp[d] = -1
+            fac = fac * p.corfac[d][icf].reshape(shp)
+        out[np.ix_(maps[0][1], maps[1][1])] = full[np.ix_(maps[0][2], maps[1][2])] * fac
+        ref = O.nu2u(p, coord, vals, True)
+        err = O.l2error(out, ref)
+        td.barrier()
+    finally:
+        td.destroy_process_group()
+    with open(os.path.join(outdir, "rank%d.json" % rank), "w") as f:
+        json.dump({"kidx": kidx, "nover": nover, "total": total, "err": err}, f)
+
+
+def test_two_gloo_ranks_type1_exchange(tmp_path):
+    import torch.multiprocessing as mp
+    world = 2
+    mp.spawn(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    res = [json.load(open(tmp_path / ("rank%d.json" % r))) for r in range(world)]
+    k, n = nufft.find_parameters(nu2u=True, grid_shape=SHAPE, npoints=sum(M_RANK), epsilon=EPS,
+                                 singleprec=False, nthreads=4)
+    for r in res:
+        assert r["total"] == sum(M_RANK)
+        assert r["kidx"] == k and r["nover"] == list(n)
+        # the summed shard grids give the transform of all points (FP64 sums
+        # in another order)
+        assert r["err"] < 1e-13
