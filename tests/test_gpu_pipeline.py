@@ -80,3 +80,33 @@ def test_pipelined_mixed_host_and_device_arrays():
     ref1 = torch.zeros(SHAPE, dtype=torch.complex64, device="cuda")
     nufft.nu2u(points=dv, coord=dc, forward=False, epsilon=eps, out=ref1)
     assert O.l2error(d_out.cpu().numpy(), ref1.cpu().numpy()) < 2e-6
+
+
+@pytest.mark.parametrize("shape,single", [((3000,), False), ((40, 36, 32), True),
+                                          ((24, 20, 18), False)])
+def test_pipelined_1d_3d(shape, single):
+    """The pipelined host path in 1D and 3D (4.5M points: two groups) against
+    the device-array path and direct sums on samples."""
+    import torch
+    rng = np.random.default_rng(13)
+    M = 4_500_000
+    nd = len(shape)
+    cdt, vdt = (np.float32, np.complex64) if single else (np.float64, np.complex128)
+    eps = 1e-5 if single else 1e-10
+    coord = rng.uniform(-np.pi, np.pi, (M, nd)).astype(cdt)
+    vals = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(vdt)
+    grid = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(vdt)
+    dc, dv, dg = (torch.from_numpy(x).cuda() for x in (coord, vals, grid))
+    tol = 2e-6 if single else 1e-12
+    h_out = np.zeros(shape, vdt)
+    nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=eps, out=h_out)
+    d_out = torch.zeros(shape, dtype=dv.dtype, device="cuda")
+    nufft.nu2u(points=dv, coord=dc, forward=True, epsilon=eps, out=d_out)
+    assert O.l2error(h_out, d_out.cpu().numpy()) < tol
+    h_pts = np.empty(M, vdt)
+    nufft.u2nu(grid=grid, coord=coord, forward=False, epsilon=eps, out=h_pts)
+    d_pts = nufft.u2nu(grid=dg, coord=dc, forward=False, epsilon=eps)
+    assert O.l2error(h_pts, d_pts.cpu().numpy()) < tol
+    idx = rng.choice(M, 300, replace=False)
+    ref = O.direct_u2nu(grid, coord[idx], False)
+    assert O.l2error(h_pts[idx], ref) < 2 * eps

@@ -131,3 +131,24 @@ def test_split_type1_argument_errors():
         p.grid_to_uniform(forward=True, grid=np.zeros(nover, np.complex64))
     with pytest.raises(RuntimeError, match="number of points"):
         p.spread(points=dv[:100])
+
+
+def test_empty_shard_contributes_zero():
+    """A rank without points: its plan spreads a zero grid, and the sum with a
+    shard holding every point is that shard's transform."""
+    import torch
+    shape, eps = (64, 48), 1e-6
+    coord, vals = _problem(2, 20_000, True, 8)
+    k, n = nufft.find_parameters(nu2u=True, grid_shape=shape, npoints=20_000, epsilon=eps,
+                                 singleprec=True)
+    empty = nufft.plan(nu2u=True, coord=torch.zeros((0, 2), dtype=torch.float32, device="cuda"),
+                       grid_shape=shape, epsilon=eps, force_kernel=k, force_nover=n)
+    full = nufft.plan(nu2u=True, coord=torch.from_numpy(coord).cuda(), grid_shape=shape,
+                      epsilon=eps, force_kernel=k, force_nover=n)
+    g0 = empty.spread(points=torch.zeros(0, dtype=torch.complex64, device="cuda"))
+    assert float(g0.abs().max()) == 0.0
+    dv = torch.from_numpy(vals).cuda()
+    g = full.spread(points=dv) + g0
+    got = empty.grid_to_uniform(forward=True, grid=g).cpu().numpy()
+    ref = full.nu2u(points=dv, forward=True).cpu().numpy()
+    assert O.l2error(got, ref) < 1e-6
