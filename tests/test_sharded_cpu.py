@@ -107,3 +107,26 @@ def test_two_gloo_ranks_type1_exchange(tmp_path):
         # the summed shard grids give the transform of all points (FP64 sums
         # in another order)
         assert r["err"] < 1e-13
+
+
+def test_find_parameters_argument_errors():
+    import ctypes
+
+    from ducc_b200 import _capi as C
+    L = C.lib()
+    o = C.make_opts(True, 0, 1.1, 2.6, 2 * np.pi, False, 0, "auto", 2)
+    shp = (ctypes.c_int64 * 3)(64, 64, 1)
+    k = ctypes.c_int32()
+    n = (ctypes.c_int64 * 3)()
+    assert L.dnufft_find_parameters(1, 4, shp, 1000, 1e-6, 1, 1, ctypes.byref(o),
+                                    ctypes.byref(k), n) == 1
+    assert b"dimensionality" in L.dnufft_last_error()
+    assert L.dnufft_find_parameters(1, 2, shp, 1000, -1.0, 1, 1, ctypes.byref(o),
+                                    ctypes.byref(k), n) == 1
+    assert b"epsilon" in L.dnufft_last_error()
+    # below the reachable accuracy of single precision
+    assert L.dnufft_find_parameters(1, 2, shp, 1000, 1e-9, 0, 0, ctypes.byref(o),
+                                    ctypes.byref(k), n) == 2
+    with pytest.raises(RuntimeError):
+        nufft.find_parameters(nu2u=True, grid_shape=(64, 64), npoints=10, epsilon=1e-9,
+                              singleprec=True)
