@@ -1260,6 +1260,64 @@ static void plan_grid_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array 
   so.finish();
 }
 
+// The 2D type-1 FFT in two halves, for the exchange in which every rank sums
+// one slab of rows of the spread grids (a reduce-scatter), transforms those
+// rows, and the ranks gather the kept columns for the column pass.
+static View rows_view(const dnufft_plan *p, const dnufft_array *rows_) {
+  const Setup &s = p->s;
+  DN_REQUIRE(s.g.ndim == 2, ST_UNSUPPORTED, "row and column halves: 2D plans only");
+  View r = view_of(rows_, "rows");
+  DN_REQUIRE(!r.host, ST_BADARG, "the rows must be a device array");
+  DN_REQUIRE(r.dtype == (s.calc_f64 ? DNUFFT_C128 : DNUFFT_C64), ST_BADARG,
+             "the rows must have the plan's data type");
+  DN_REQUIRE(r.ndim == 2 && r.shape[1] == int64_t(s.g.nover[1]) &&
+                 r.shape[0] <= int64_t(s.g.nover[0]),
+             ST_BADARG, "rows: (at most nover[0], nover[1]) cells expected");
+  DN_REQUIRE(r.shape[0] <= 1 || r.stride[0] == r.shape[1], ST_BADARG,
+             "the rows must be C-contiguous");
+  DN_REQUIRE(r.stride[1] == 1, ST_BADARG, "the rows must be C-contiguous");
+  return r;
+}
+
+static void plan_rows_fft_impl(dnufft_plan *p, int forward, dnufft_array *rows_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const View r = rows_view(p, rows_);
+  if (r.shape[0] == 0) return;
+  int *err = device_error_word();
+  if (p->s.calc_f64)
+    fft_nu2u_rows<double>(r.data, int(r.shape[0]), p->s.g, p->dc.ax, forward != 0, st, err);
+  else
+    fft_nu2u_rows<float>(r.data, int(r.shape[0]), p->s.g, p->dc.ax, forward != 0, st, err);
+  check_device_error(err, st);
+}
+
+static void plan_cols_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array *grid_,
+                                      dnufft_array *out_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  DN_REQUIRE(s.g.ndim == 2, ST_UNSUPPORTED, "row and column halves: 2D plans only");
+  const bool f64 = s.calc_f64;
+  const View grid = over_grid_view(p, grid_);
+  View out = view_of(out_, "out");
+  DN_REQUIRE(out.dtype == grid.dtype, ST_BADARG, "out must have the plan's data type");
+  DN_REQUIRE(out.ndim == 2 && out.shape[0] == s.g.nuni[0] && out.shape[1] == s.g.nuni[1],
+             ST_BADARG, "uniform grid dimensions mismatch");
+  Staged so(out, false, true, st);
+  const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
+  if (wb && !p->work.p) {
+    p->work = DevBuf(wb, st);
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
+  const bool fo = p->o.fft_order != 0;
+  if (f64)
+    fft_nu2u_cols<double>(grid.data, s.g, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
+                          so.dev.stride, st, p->work.p);
+  else
+    fft_nu2u_cols<float>(grid.data, s.g, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
+                         so.dev.stride, st, p->work.p);
+  so.finish();
+}
+
 static void find_parameters_impl(int nu2u, int ndim, const int64_t *shape, uint64_t npoints,
                                  double eps, int calc_f64, int coord_f64, const dnufft_opts *opts_,
                                  int32_t *kidx, int64_t *nover) {
@@ -1556,6 +1614,16 @@ int dnufft_plan_spread(dnufft_plan *plan, const dnufft_array *points, dnufft_arr
 int dnufft_plan_grid_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
                                 dnufft_array *out, void *stream) {
   DN_GUARD(dnufft::plan_grid_to_uniform_impl(plan, forward, grid, out,
+                                             static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_rows_fft(dnufft_plan *plan, int forward, dnufft_array *rows, void *stream) {
+  DN_GUARD(dnufft::plan_rows_fft_impl(plan, forward, rows, static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_cols_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
+                                dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::plan_cols_to_uniform_impl(plan, forward, grid, out,
                                              static_cast<cudaStream_t>(stream)))
 }
 

@@ -1223,6 +1223,41 @@ static UniSpec mk_uni(void *ptr, const int64_t *stride, const Geometry &g,
   return u;
 }
 
+// 2D type 1, first half: FFTs along axis 1 of nrows consecutive rows (any
+// rows of the oversampled grid: they are independent), writing only the N1
+// kept columns, in place.
+template <typename T>
+void fft_nu2u_rows(void *rowsv, int nrows, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
+                   cudaStream_t st, int *err) {
+  cplx<T> *rows = static_cast<cplx<T> *>(rowsv);
+  const int n1 = int(g.nover[1]);
+  const int N1 = int(g.nuni[1]);
+  if (nrows <= 0) return;
+  if (!run_rows_v3<T>(rows, n1, nrows, n1, N1, false, true, ax[1], fwd, err, st)) {
+    static const int64_t zs[3] = {0, 0, 0};
+    const double *const nocf[3] = {nullptr, nullptr, nullptr};
+    const UniSpec u = mk_uni(nullptr, zs, g, nocf, false);
+    run_lines<T>(rows, mk_spec(n1, 1, 1, nrows, 1, n1, 0, -1, -1, 0, 0, IO_FULL, IO_KEPT), ax[1],
+                 u, fwd, st);
+  }
+}
+
+// 2D type 1, second half: FFTs along axis 0 of the N1 kept columns (every row
+// already transformed along axis 1), correction and crop into out.
+template <typename T>
+void fft_nu2u_cols(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
+                   const double *const corfac[3], bool fft_order, void *out,
+                   const int64_t *ostride, cudaStream_t st, void *workv) {
+  cplx<T> *grid = static_cast<cplx<T> *>(gridv);
+  cplx<T> *work = static_cast<cplx<T> *>(workv);
+  const UniSpec u = mk_uni(out, ostride, g, corfac, fft_order);
+  const int n0 = int(g.nover[0]), n1 = int(g.nover[1]);
+  const int N1 = int(g.nuni[1]);
+  if (!run_cols_v3<T>(grid, work, n0, n1, N1, ax[0], u, true, fwd, st))
+    run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_FULL, IO_UNI), ax[0], u,
+                 fwd, st);
+}
+
 template <typename T>
 void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
                    const double *const corfac[3], bool fft_order, void *out,
@@ -1234,16 +1269,10 @@ void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool f
   if (g.ndim == 1) {
     run_lines<T>(grid, mk_spec(n0, 0, 1, 1, 1, 0, 0, -1, -1, 0, 0, IO_FULL, IO_UNI), ax[0], u, fwd, st);
   } else if (g.ndim == 2) {
-    const int n1 = int(g.nover[1]);
-    const int N1 = int(g.nuni[1]);
-    // rows (axis 1), all n0 rows, keep N1 columns
-    if (!run_rows_v3<T>(grid, n1, n0, n1, N1, false, true, ax[1], fwd, err, st))
-      run_lines<T>(grid, mk_spec(n1, 1, 1, n0, 1, n1, 0, -1, -1, 0, 0, IO_FULL, IO_KEPT), ax[1],
-                   u, fwd, st);
-    // columns (axis 0) of the kept columns, correction + crop
-    if (!run_cols_v3<T>(grid, work, n0, n1, N1, ax[0], u, true, fwd, st))
-      run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_FULL, IO_UNI), ax[0],
-                   u, fwd, st);
+    // rows (axis 1), all n0 rows, keep N1 columns; then the kept columns
+    // (axis 0), correction + crop
+    fft_nu2u_rows<T>(grid, n0, g, ax, fwd, st, err);
+    fft_nu2u_cols<T>(grid, g, ax, fwd, corfac, fft_order, out, ostride, st, work);
   } else {
     const int n1 = int(g.nover[1]), n2 = int(g.nover[2]);
     const int N1 = int(g.nuni[1]), N2 = int(g.nuni[2]);
@@ -1517,6 +1546,16 @@ template void fft_nu2u_tail<float>(void *, const Geometry &, const FFTAxisPlan *
 template void fft_nu2u_tail<double>(void *, const Geometry &, const FFTAxisPlan *, bool,
                                     const double *const[3], bool, void *, const int64_t *,
                                     cudaStream_t, void *, int *);
+template void fft_nu2u_rows<float>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
+                                   cudaStream_t, int *);
+template void fft_nu2u_rows<double>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
+                                    cudaStream_t, int *);
+template void fft_nu2u_cols<float>(void *, const Geometry &, const FFTAxisPlan *, bool,
+                                   const double *const[3], bool, void *, const int64_t *,
+                                   cudaStream_t, void *);
+template void fft_nu2u_cols<double>(void *, const Geometry &, const FFTAxisPlan *, bool,
+                                    const double *const[3], bool, void *, const int64_t *,
+                                    cudaStream_t, void *);
 template void fft_u2nu_head<float>(const void *, const int64_t *, const Geometry &,
                                    const FFTAxisPlan *, bool, const double *const[3], bool,
                                    void *, cudaStream_t, void *, int *);

@@ -108,6 +108,17 @@ void fft_nu2u_tail(void *grid, const Geometry &g, const FFTAxisPlan *ax, bool fo
                    const int64_t *ostride, cudaStream_t st, void *work = nullptr,
                    int *err = nullptr);
 
+// The two halves of the 2D type-1 tail: row FFTs (axis 1, kept columns written
+// in place) over nrows consecutive rows of the oversampled grid, and column
+// FFTs of the kept columns with correction and crop into out.
+template <typename T>
+void fft_nu2u_rows(void *rows, int nrows, const Geometry &g, const FFTAxisPlan *ax, bool forward,
+                   cudaStream_t st, int *err);
+template <typename T>
+void fft_nu2u_cols(void *grid, const Geometry &g, const FFTAxisPlan *ax, bool forward,
+                   const double *const corfac[3], bool fft_order, void *out,
+                   const int64_t *ostride, cudaStream_t st, void *work);
+
 // Type 2 head: deconvolution + zero-pad of the caller's uniform array into the
 // oversampled grid, then FFTs with input pruning.
 template <typename T>

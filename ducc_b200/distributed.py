@@ -2,11 +2,17 @@
 GPU, ``torch.distributed``; NCCL over NVLink between GPUs).
 
 Type 1 (``ShardedPlan.nu2u``): every rank spreads its own points into a full
-oversampled grid (``plan.spread``), the grids are summed over the ranks with
-one all-reduce (``sum_grids``), and every rank runs the FFT and the
-correction of the sum (``plan.grid_to_uniform``), so each holds the whole
-uniform result.  Spreading is linear in the values, so the summed grid is the
-grid of all points: the single real exchange step of the transform.
+oversampled grid (``plan.spread``); spreading is linear in the values, so the
+sum of these grids over the ranks is the grid of all points, and summing them
+is the real exchange step of the transform.  In 2D (``type1_by_slabs``) each
+rank receives the sum of one slab of rows only (a reduce-scatter), transforms
+those rows along axis 1 (``plan.rows_fft``), and the ranks gather the kept
+columns of all rows (an all-gather of the N1 of n1 columns) for the column
+pass, correction and crop, which every rank runs (``plan.cols_to_uniform``).
+Against summing whole grids (``sum_grids`` + ``plan.grid_to_uniform``, the
+1D / 3D path) this moves (1 + N1/n1) instead of 2 grids' worth of bytes per
+rank and splits the row FFTs over the ranks.  Every rank holds the whole
+uniform result.
 
 Type 2 (``ShardedPlan.u2nu``): every rank has the whole uniform grid and
 interpolates its own points; nothing crosses between ranks.
@@ -24,7 +30,8 @@ import math
 
 from . import nufft
 
-__all__ = ["global_parameters", "sum_grids", "ShardedPlan"]
+__all__ = ["global_parameters", "sum_grids", "reduce_scatter_rows", "gather_kept_columns",
+           "type1_by_slabs", "ShardedPlan"]
 
 
 def _count_device(group):
@@ -71,6 +78,72 @@ def sum_grids(grid, group=None):
     return grid
 
 
+def reduce_scatter_rows(grid, group=None):
+    """Sum a complex (world * r, ...) grid over the ranks of the group and
+    return this rank's r rows of the sum (rank k: rows k*r .. k*r + r - 1)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    if grid.shape[0] % world or not grid.is_contiguous():
+        raise ValueError("reduce_scatter_rows: a contiguous grid of world * r rows expected")
+    out = torch.empty((grid.shape[0] // world,) + tuple(grid.shape[1:]), dtype=grid.dtype,
+                      device=grid.device)
+    dist.reduce_scatter_tensor(torch.view_as_real(out), torch.view_as_real(grid),
+                               op=dist.ReduceOp.SUM, group=group)
+    return out
+
+
+def _kept(n, N):
+    """(first, last) counts of the kept indices of an axis: [0, (N+1)//2) and
+    [n - N//2, n)."""
+    return (N + 1) // 2, N // 2
+
+
+def gather_kept_columns(rows, nkept, group=None):
+    """All-gather the kept columns of every rank's (r, n1) rows: returns a
+    (world * r, nkept) array, the first (nkept+1)//2 and the last nkept//2
+    columns of each row, packed."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    n1 = rows.shape[1]
+    lo, hi = _kept(n1, nkept)
+    packed = torch.cat([rows[:, :lo], rows[:, n1 - hi:]], dim=1).contiguous()
+    out = torch.empty((world * rows.shape[0], nkept), dtype=rows.dtype, device=rows.device)
+    dist.all_gather_into_tensor(torch.view_as_real(out), torch.view_as_real(packed),
+                                group=group)
+    return out
+
+
+def type1_by_slabs(*, spread_into, rows_fft, cols_to_uniform, nover, nkept, dtype, device,
+                   group=None):
+    """The slab exchange of a 2D type 1 with the local steps passed in:
+    ``spread_into(buf)`` writes this rank's spread grid into ``buf`` (an
+    (nover[0], nover[1]) C-contiguous tensor), ``rows_fft(rows)`` transforms
+    rows along axis 1 in place, ``cols_to_uniform(grid)`` runs the column pass,
+    correction and crop of the assembled grid and returns the uniform result.
+    Collective over the group."""
+    import torch
+    import torch.distributed as dist
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    n0, n1 = int(nover[0]), int(nover[1])
+    r = -(-n0 // world)
+    buf = torch.empty((r * world, n1), dtype=dtype, device=device)
+    grid = buf[:n0]
+    spread_into(grid)
+    buf[n0:].zero_()
+    slab = reduce_scatter_rows(buf, group)
+    nr = max(0, min(r, n0 - rank * r))
+    if nr:
+        rows_fft(slab[:nr])
+    kept = gather_kept_columns(slab, nkept, group)
+    lo, hi = _kept(n1, nkept)
+    grid[:, :lo] = kept[:n0, :lo]
+    if hi:
+        grid[:, n1 - hi:] = kept[:n0, lo:]
+    return cols_to_uniform(grid)
+
+
 class ShardedPlan:
     """Plan of this rank's points of one transform split over the ranks of a
     process group.  Arguments as ``ducc_b200.nufft.plan``; ``coord`` holds only
@@ -100,10 +173,29 @@ class ShardedPlan:
                                force_kernel=kidx, force_nover=nover)
         self.grid_shape = tuple(int(x) for x in grid_shape)
         self.npoints = coord.shape[0]
+        self.device = coord.device
 
-    def nu2u(self, *, forward, points, out=None):
+    def nu2u(self, *, forward, points, out=None, exchange=None):
         """Type 1 of all ranks' points (collective); every rank gets the whole
-        uniform grid in ``out``."""
+        uniform grid in ``out``.  ``exchange``: 'slabs' (2D default: reduce-
+        scatter of row slabs, row FFTs split over the ranks, all-gather of the
+        kept columns) or 'grid' (all-reduce of whole grids, any dimension)."""
+        import torch
+        if exchange is None:
+            exchange = "slabs" if len(self.grid_shape) == 2 else "grid"
+        if exchange == "slabs":
+            if len(self.grid_shape) != 2:
+                raise ValueError("the slab exchange is for 2D transforms")
+            dtype = torch.complex128 if self.plan._f64 else torch.complex64
+            return type1_by_slabs(
+                spread_into=lambda buf: self.plan.spread(points=points, out=buf),
+                rows_fft=lambda rows: self.plan.rows_fft(forward=forward, rows=rows),
+                cols_to_uniform=lambda g: self.plan.cols_to_uniform(forward=forward, grid=g,
+                                                                    out=out),
+                nover=self.nover, nkept=self.grid_shape[1], dtype=dtype,
+                device=self.device, group=self.group)
+        if exchange != "grid":
+            raise ValueError("exchange must be 'slabs' or 'grid'")
         g = self.plan.spread(points=points)
         sum_grids(g, self.group)
         return self.plan.grid_to_uniform(forward=forward, grid=g, out=out)

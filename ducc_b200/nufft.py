@@ -300,6 +300,29 @@ class plan:
                                                     C.stream_of(grid, op.buf, stream=stream)))
         return op.finish()
 
+    def rows_fft(self, *, forward, rows, stream=None):
+        """2D type 1: FFT along axis 1 of a slab of rows of an oversampled grid
+        (a C-contiguous CUDA tensor of shape (r, nover[1])), in place; only the
+        kept columns (the first (N1+1)//2 and the last N1//2) are written.
+        Returns ``rows``."""
+        a_r = C.describe(rows)
+        C.check(C.lib().dnufft_plan_rows_fft(self._ptr, 1 if forward else 0, ctypes.byref(a_r),
+                                             C.stream_of(rows, stream=stream)))
+        return rows
+
+    def cols_to_uniform(self, *, forward, grid, out=None, stream=None):
+        """2D type 1: column FFTs of the kept columns of an oversampled grid
+        whose rows ``rows_fft`` has transformed (overwritten), correction and
+        crop into ``out``; returns ``out``."""
+        if out is None:
+            out = self._alloc(grid, self.grid_shape)
+        op = _OutProxy(out)
+        a_g, a_o = C.describe(grid), C.describe(op.buf)
+        C.check(C.lib().dnufft_plan_cols_to_uniform(self._ptr, 1 if forward else 0,
+                                                    ctypes.byref(a_g), ctypes.byref(a_o),
+                                                    C.stream_of(grid, op.buf, stream=stream)))
+        return op.finish()
+
     def info(self):
         """Kernel support, oversampled sizes etc. of this plan."""
         inf = C.PlanInfo()

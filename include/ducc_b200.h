@@ -168,6 +168,20 @@ int dnufft_plan_spread(dnufft_plan *plan, const dnufft_array *points, dnufft_arr
 int dnufft_plan_grid_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
                                 dnufft_array *out, void *stream);
 
+/* The FFT half of a 2D type 1 split once more, for an exchange that moves
+ * fewer bytes than summing whole grids: each process sums one slab of rows of
+ * the spread grids (a reduce-scatter), dnufft_plan_rows_fft transforms those
+ * rows along axis 1 in place (rows: a C-contiguous device array of (r,
+ * nover[1]) cells, any r <= nover[0]; only the nuni[1] kept columns, the first
+ * (nuni[1]+1)/2 and the last nuni[1]/2, are written), the processes gather
+ * the kept columns of all rows into an oversampled grid, and
+ * dnufft_plan_cols_to_uniform runs the column FFTs, the correction and the
+ * crop into out (the grid is overwritten; its other columns are not read).
+ * src/ducc0/nufft/nufft.h:1290 (rows) and :1291-1312 (columns, correction). */
+int dnufft_plan_rows_fft(dnufft_plan *plan, int forward, dnufft_array *rows, void *stream);
+int dnufft_plan_cols_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
+                                dnufft_array *out, void *stream);
+
 /* Kernel-table row and oversampled sizes (nover[0..2], 1 beyond ndim) that
  * DUCC's parameter choice gives for a transform of npoints points; its cost
  * model depends on npoints and opts->nthreads, so processes sharing one

@@ -152,3 +152,78 @@ def test_empty_shard_contributes_zero():
     got = empty.grid_to_uniform(forward=True, grid=g).cpu().numpy()
     ref = full.nu2u(points=dv, forward=True).cpu().numpy()
     assert O.l2error(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("shape", [(300, 260), (1100, 1000)])   # line kernels / row + four-step kernels
+@pytest.mark.parametrize("single,eps", [(True, 1e-6), (False, 1e-11)])
+def test_row_slabs_then_columns_equal_one_piece(single, eps, shape):
+    """The 2D FFT half split into row slabs (each transformed on its own) and
+    the column pass equals the plan's one-piece type 1."""
+    import torch
+    coord, vals = _problem(2, 200_000, single, 9)
+    dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+    p = nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=eps)
+    for forward in (True, False):
+        ref = p.nu2u(points=dv, forward=forward).cpu().numpy()
+        g = p.spread(points=dv)
+        cut = g.shape[0] // 3
+        p.rows_fft(forward=forward, rows=g[:cut])
+        p.rows_fft(forward=forward, rows=g[cut:])
+        got = p.cols_to_uniform(forward=forward, grid=g).cpu().numpy()
+        # two separate spreads: atomic additions in another order
+        assert O.l2error(got, ref) < (1e-6 if single else 1e-13)
+
+
+def test_sharded_plan_exchanges_agree():
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    td.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                          world_size=1, timeout=datetime.timedelta(seconds=60),
+                          device_id=torch.device("cuda", torch.cuda.current_device()))
+    try:
+        coord, vals = _problem(2, 80_000, True, 10)
+        dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+        sp = D.ShardedPlan(nu2u=True, coord=dc, grid_shape=(160, 144), epsilon=1e-6)
+        a = sp.nu2u(forward=True, points=dv, exchange="slabs").cpu().numpy()
+        b = sp.nu2u(forward=True, points=dv, exchange="grid").cpu().numpy()
+        assert O.l2error(a, b) < 1e-6
+        exact = O.direct_nu2u(coord[:3000].astype(np.float64), vals[:3000].astype(np.complex128),
+                              (160, 144), True)
+        sub = D.ShardedPlan(nu2u=True, coord=dc[:3000].contiguous(), grid_shape=(160, 144),
+                            epsilon=1e-6)
+        assert O.l2error(sub.nu2u(forward=True, points=dv[:3000].contiguous()).cpu().numpy(),
+                         exact) < 4e-6
+        td.barrier()
+    finally:
+        td.destroy_process_group()
+
+
+def test_rows_cols_argument_errors():
+    import torch
+    coord, vals = _problem(3, 5000, True, 11)
+    p3 = nufft.plan(nu2u=True, coord=torch.from_numpy(coord).cuda(), grid_shape=(16, 16, 16),
+                    epsilon=1e-5)
+    n3 = tuple(p3.info()["nover"])
+    with pytest.raises(RuntimeError, match="2D plans only"):
+        p3.rows_fft(forward=True, rows=torch.zeros((n3[0], n3[1] * n3[2]), dtype=torch.complex64,
+                                                   device="cuda"))
+    coord2, _ = _problem(2, 5000, True, 12)
+    p = nufft.plan(nu2u=True, coord=torch.from_numpy(coord2).cuda(), grid_shape=(64, 64),
+                   epsilon=1e-5)
+    n = tuple(p.info()["nover"])
+    with pytest.raises(RuntimeError, match="cells expected"):
+        p.rows_fft(forward=True, rows=torch.zeros((4, n[1] + 1), dtype=torch.complex64,
+                                                  device="cuda"))
+    with pytest.raises(RuntimeError, match="device array"):
+        p.rows_fft(forward=True, rows=np.zeros((4, n[1]), np.complex64))
+    with pytest.raises(RuntimeError, match="oversampled sizes"):
+        p.cols_to_uniform(forward=True, grid=torch.zeros((n[0] - 1, n[1]), dtype=torch.complex64,
+                                                         device="cuda"))

@@ -130,3 +130,69 @@ def test_find_parameters_argument_errors():
     with pytest.raises(RuntimeError):
         nufft.find_parameters(nu2u=True, grid_shape=(64, 64), npoints=10, epsilon=1e-9,
                               singleprec=True)
+
+
+def _slab_worker(rank, world, port, outdir):
+    import datetime
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    td.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                          world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        coord, vals = _inputs()
+        cuts = [0, 500, 1300, sum(M_RANK)]
+        mine = slice(cuts[rank], cuts[rank + 1])
+        kidx, nover, total = D.global_parameters(nu2u=True, grid_shape=SHAPE,
+                                                 npoints_local=cuts[rank + 1] - cuts[rank],
+                                                 epsilon=EPS, singleprec=False, nthreads=4)
+        p = O.Params(SHAPE, EPS, False, total, True, force=(kidx, nover))
+        maps = O._index_maps(p, False)
+        fac = np.ones(())
+        for d, (icf, iu, ig) in enumerate(maps):
+            shp = [1, 1]
+            shp[d] = -1
+            fac = fac * p.corfac[d][icf].reshape(shp)
+        rows_done = []
+
+        def spread_into(buf):
+            buf.copy_(torch.from_numpy(O.spread(p, coord[mine], vals[mine])))
+
+        def rows_fft(rows):
+            rows_done.append(rows.shape[0])
+            rows.copy_(torch.from_numpy(np.fft.fft(rows.numpy(), axis=1)))
+
+        def cols_to_uniform(g):
+            full = np.fft.fft(g.numpy(), axis=0)
+            out = np.zeros(SHAPE, np.complex128)
+            out[np.ix_(maps[0][1], maps[1][1])] = full[np.ix_(maps[0][2], maps[1][2])] * fac
+            return out
+
+        got = D.type1_by_slabs(spread_into=spread_into, rows_fft=rows_fft,
+                               cols_to_uniform=cols_to_uniform, nover=nover,
+                               nkept=SHAPE[1], dtype=torch.complex128,
+                               device=torch.device("cpu"))
+        err = O.l2error(got, O.nu2u(p, coord, vals, True))
+        td.barrier()
+    finally:
+        td.destroy_process_group()
+    with open(os.path.join(outdir, "rank%d.json" % rank), "w") as f:
+        json.dump({"err": err, "rows": rows_done, "nover": nover}, f)
+
+
+def test_three_gloo_ranks_type1_slab_exchange(tmp_path):
+    """Reduce-scatter of row slabs (88 oversampled rows over three ranks: the
+    last slab holds padding rows), row FFTs per slab, all-gather of the kept
+    columns, column pass on every rank: the type 1 of all points everywhere."""
+    import torch.multiprocessing as mp
+    world = 3
+    mp.spawn(_slab_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    res = [json.load(open(tmp_path / ("rank%d.json" % r))) for r in range(world)]
+    n0 = res[0]["nover"][0]
+    r = -(-n0 // world)
+    assert sum(sum(x["rows"]) for x in res) == n0      # every row transformed once
+    assert res[0]["rows"] == [r]
+    for x in res:
+        assert x["err"] < 1e-13
