@@ -177,12 +177,16 @@ class ShardedPlan:
 
     def nu2u(self, *, forward, points, out=None, exchange=None):
         """Type 1 of all ranks' points (collective); every rank gets the whole
-        uniform grid in ``out``.  ``exchange``: 'slabs' (2D default: reduce-
-        scatter of row slabs, row FFTs split over the ranks, all-gather of the
-        kept columns) or 'grid' (all-reduce of whole grids, any dimension)."""
+        uniform grid in ``out``.  ``exchange``: 'slabs' (the 2D default on
+        several ranks: reduce-scatter of row slabs, row FFTs split over the
+        ranks, all-gather of the kept columns) or 'grid' (all-reduce of whole
+        grids, any dimension; the default otherwise)."""
         import torch
+        import torch.distributed as dist
         if exchange is None:
-            exchange = "slabs" if len(self.grid_shape) == 2 else "grid"
+            # one rank: nothing to exchange, and the grid path adds no copies
+            multi = dist.get_world_size(self.group) > 1
+            exchange = "slabs" if len(self.grid_shape) == 2 and multi else "grid"
         if exchange == "slabs":
             if len(self.grid_shape) != 2:
                 raise ValueError("the slab exchange is for 2D transforms")
