@@ -1297,7 +1297,22 @@ static void plan_cols_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array 
   const Setup &s = p->s;
   DN_REQUIRE(s.g.ndim == 2, ST_UNSUPPORTED, "row and column halves: 2D plans only");
   const bool f64 = s.calc_f64;
-  const View grid = over_grid_view(p, grid_);
+  // the whole oversampled grid, or its kept columns packed ((n0, N1): the
+  // column pass then sees a grid of row length N1, whose kept columns are all
+  // of its columns, with the same output and correction indices)
+  Geometry gc = s.g;
+  View grid = view_of(grid_, "grid");
+  if (grid.ndim == 2 && grid.shape[0] == int64_t(s.g.nover[0]) &&
+      grid.shape[1] == int64_t(s.g.nuni[1]) && s.g.nuni[1] != s.g.nover[1]) {
+    DN_REQUIRE(!grid.host, ST_BADARG, "the oversampled grid must be a device array");
+    DN_REQUIRE(grid.dtype == (f64 ? DNUFFT_C128 : DNUFFT_C64), ST_BADARG,
+               "the oversampled grid must have the plan's data type");
+    DN_REQUIRE(grid.stride[1] == 1 && grid.stride[0] == grid.shape[1], ST_BADARG,
+               "the oversampled grid must be C-contiguous");
+    gc.nover[1] = s.g.nuni[1];
+  } else {
+    grid = over_grid_view(p, grid_);
+  }
   View out = view_of(out_, "out");
   DN_REQUIRE(out.dtype == grid.dtype, ST_BADARG, "out must have the plan's data type");
   DN_REQUIRE(out.ndim == 2 && out.shape[0] == s.g.nuni[0] && out.shape[1] == s.g.nuni[1],
@@ -1310,10 +1325,10 @@ static void plan_cols_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array 
   }
   const bool fo = p->o.fft_order != 0;
   if (f64)
-    fft_nu2u_cols<double>(grid.data, s.g, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
+    fft_nu2u_cols<double>(grid.data, gc, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
                           so.dev.stride, st, p->work.p);
   else
-    fft_nu2u_cols<float>(grid.data, s.g, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
+    fft_nu2u_cols<float>(grid.data, gc, p->dc.ax, forward != 0, p->dc.cf, fo, so.dev.data,
                          so.dev.stride, st, p->work.p);
   so.finish();
 }

@@ -120,9 +120,9 @@ def type1_by_slabs(*, spread_into, rows_fft, cols_to_uniform, nover, nkept, dtyp
     """The slab exchange of a 2D type 1 with the local steps passed in:
     ``spread_into(buf)`` writes this rank's spread grid into ``buf`` (an
     (nover[0], nover[1]) C-contiguous tensor), ``rows_fft(rows)`` transforms
-    rows along axis 1 in place, ``cols_to_uniform(grid)`` runs the column pass,
-    correction and crop of the assembled grid and returns the uniform result.
-    Collective over the group."""
+    rows along axis 1 in place, ``cols_to_uniform(kept)`` runs the column pass,
+    correction and crop of the gathered kept columns (packed, (nover[0],
+    nkept)) and returns the uniform result.  Collective over the group."""
     import torch
     import torch.distributed as dist
     world, rank = dist.get_world_size(group), dist.get_rank(group)
@@ -137,11 +137,8 @@ def type1_by_slabs(*, spread_into, rows_fft, cols_to_uniform, nover, nkept, dtyp
     if nr:
         rows_fft(slab[:nr])
     kept = gather_kept_columns(slab, nkept, group)
-    lo, hi = _kept(n1, nkept)
-    grid[:, :lo] = kept[:n0, :lo]
-    if hi:
-        grid[:, n1 - hi:] = kept[:n0, lo:]
-    return cols_to_uniform(grid)
+    # the column pass takes the kept columns packed: no copy back into the grid
+    return cols_to_uniform(kept[:n0])
 
 
 class ShardedPlan:

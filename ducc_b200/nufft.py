@@ -312,8 +312,10 @@ class plan:
 
     def cols_to_uniform(self, *, forward, grid, out=None, stream=None):
         """2D type 1: column FFTs of the kept columns of an oversampled grid
-        whose rows ``rows_fft`` has transformed (overwritten), correction and
-        crop into ``out``; returns ``out``."""
+        whose rows ``rows_fft`` has transformed, correction and crop into
+        ``out``; returns ``out``.  ``grid``: the whole (nover[0], nover[1])
+        grid or its kept columns packed, (nover[0], N1) (the first (N1+1)//2
+        and the last N1//2 of each row); it is overwritten."""
         if out is None:
             out = self._alloc(grid, self.grid_shape)
         op = _OutProxy(out)

@@ -174,9 +174,12 @@ int dnufft_plan_grid_to_uniform(dnufft_plan *plan, int forward, dnufft_array *gr
  * rows along axis 1 in place (rows: a C-contiguous device array of (r,
  * nover[1]) cells, any r <= nover[0]; only the nuni[1] kept columns, the first
  * (nuni[1]+1)/2 and the last nuni[1]/2, are written), the processes gather
- * the kept columns of all rows into an oversampled grid, and
- * dnufft_plan_cols_to_uniform runs the column FFTs, the correction and the
- * crop into out (the grid is overwritten; its other columns are not read).
+ * the kept columns of all rows, and dnufft_plan_cols_to_uniform runs the
+ * column FFTs, the correction and the crop into out.  Its grid is either the
+ * whole oversampled grid with the kept columns in place (other columns are
+ * not read) or the kept columns packed, a C-contiguous (nover[0], nuni[1])
+ * array (the first (nuni[1]+1)/2 and the last nuni[1]/2 of every row side by
+ * side); it is overwritten.
  * src/ducc0/nufft/nufft.h:1290 (rows) and :1291-1312 (columns, correction). */
 int dnufft_plan_rows_fft(dnufft_plan *plan, int forward, dnufft_array *rows, void *stream);
 int dnufft_plan_cols_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,

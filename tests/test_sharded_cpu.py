@@ -164,8 +164,13 @@ def _slab_worker(rank, world, port, outdir):
             rows_done.append(rows.shape[0])
             rows.copy_(torch.from_numpy(np.fft.fft(rows.numpy(), axis=1)))
 
-        def cols_to_uniform(g):
-            full = np.fft.fft(g.numpy(), axis=0)
+        def cols_to_uniform(kept):
+            # packed kept columns back to their grid positions, then the columns
+            lo, hi = (SHAPE[1] + 1) // 2, SHAPE[1] // 2
+            g = np.zeros(tuple(nover), np.complex128)
+            g[:, :lo] = kept.numpy()[:, :lo]
+            g[:, nover[1] - hi:] = kept.numpy()[:, lo:]
+            full = np.fft.fft(g, axis=0)
             out = np.zeros(SHAPE, np.complex128)
             out[np.ix_(maps[0][1], maps[1][1])] = full[np.ix_(maps[0][2], maps[1][2])] * fac
             return out
