@@ -201,3 +201,31 @@ def test_three_gloo_ranks_type1_slab_exchange(tmp_path):
     assert res[0]["rows"] == [r]
     for x in res:
         assert x["err"] < 1e-13
+
+
+def test_exchange_helpers_one_rank():
+    """The packing of the kept columns (first (N+1)//2 and last N//2 of each
+    row) and the row-count check of the reduce-scatter, on a one-rank group."""
+    import datetime
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    td.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0,
+                          world_size=1, timeout=datetime.timedelta(seconds=30))
+    try:
+        g = torch.arange(6 * 10, dtype=torch.float64).reshape(6, 10).to(torch.complex128)
+        assert torch.equal(D.reduce_scatter_rows(g.clone()), g)
+        for nk in (1, 4, 5, 10):
+            k = D.gather_kept_columns(g, nk)
+            lo, hi = (nk + 1) // 2, nk // 2
+            assert k.shape == (6, nk)
+            assert torch.equal(k[:, :lo], g[:, :lo])
+            assert torch.equal(k[:, lo:], g[:, 10 - hi:])
+        with pytest.raises(ValueError):
+            D.reduce_scatter_rows(g[:, ::2])          # not contiguous
+        s = torch.ones(4, 3, dtype=torch.complex64)
+        assert torch.equal(D.sum_grids(s), torch.ones(4, 3, dtype=torch.complex64))
+    finally:
+        td.destroy_process_group()
