@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "dnufft_internal.h"
 #include "kernels.h"
 
@@ -114,14 +116,23 @@ static void check_device_error(int *word, cudaStream_t st) {
 
 // ---------------------------------------------------------------- stage timers
 // CUDA-event stage profile printed under verbosity>0 (the counterpart of DUCC's
-// TimerHierarchy report, src/ducc0/infra/timers.h:69-266).
+// TimerHierarchy report, src/ducc0/infra/timers.h:69-266), with one NVTX range
+// per stage.
 struct StageTimer {
   bool on;
   bool print;
   cudaStream_t st;
   std::vector<std::pair<std::string, cudaEvent_t>> marks;
+  bool range_open = false;   // an NVTX range named after the current stage
   StageTimer(bool on_, cudaStream_t s) : on(on_ || g_prof_on), print(on_), st(s) {}
+  // Starts stage `name`: closes the previous stage's NVTX range and opens one
+  // for this stage (host-side ranges around the launches of each stage, for
+  // a timeline tool; without one attached they cost a function call), and
+  // records a CUDA event when timing is on.
   void mark(const char *name) {
+    if (range_open) nvtxRangePop();
+    nvtxRangePushA(name);
+    range_open = true;
     if (!on) return;
     cudaEvent_t e;
     DN_CUDA(cudaEventCreate(&e));
@@ -150,6 +161,7 @@ struct StageTimer {
     if (print) std::fflush(stdout);
   }
   ~StageTimer() {
+    if (range_open) nvtxRangePop();
     for (auto &m : marks) cudaEventDestroy(m.second);
   }
 };

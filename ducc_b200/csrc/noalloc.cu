@@ -1,15 +1,20 @@
 // Type-1 NUFFT entry point that allocates nothing.
 //
 // Some callers cannot allocate device memory while they run a transform:
-// code that records work into a CUDA stream capture (cudaMalloc is not a
-// stream operation and is refused there), callbacks and plugins that run
-// inside another framework which owns the whole device memory pool, and
-// services that reserve a fixed memory budget up front and forbid allocation
-// afterwards (cudaMalloc may also synchronise the device and stall other
-// streams).  For them dnufft_nu2u_noalloc takes every temporary of the
-// transform from one fixed area compiled into this library: a file-scope
-// device array of NOALLOC_SCRATCH_BYTES bytes, which every GPU that loads the
-// library holds until the process exits.
+// callbacks and plugins that run inside another framework which owns the
+// whole device memory pool, and services that reserve a fixed memory budget
+// up front and forbid allocation afterwards (cudaMalloc may also synchronise
+// the device and stall other streams).  For them dnufft_nu2u_noalloc takes
+// every temporary of the transform from one fixed area compiled into this
+// library: a file-scope device array of NOALLOC_SCRATCH_BYTES bytes, which
+// every GPU that loads the library holds until the process exits.
+//
+// The call waits on its stream once, part-way through, to read the number of
+// point chunks back to the host (a 4-byte copy into a host variable), and it
+// uploads the correction factors from host vectors; the host thread therefore
+// returns only after the sort has run on the GPU.
+#include <cuda_runtime.h>
+
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -38,7 +43,10 @@ std::mutex g_mu;
 void *g_scratch_ptr[MAX_DEVICES] = {nullptr};
 
 // Device address of the scratch area on the current device, looked up once
-// per device (with that device current) on its first call.
+// per device (with that device current) on its first call and kept for the
+// life of the process: after cudaDeviceReset (or a reset of the primary
+// context) the kept address is stale, so a process that resets a device must
+// not call this entry point on it again.
 int scratch_address(void **ptr) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

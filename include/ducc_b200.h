@@ -208,17 +208,21 @@ int dnufft_plan_get_info(const dnufft_plan *plan, dnufft_plan_info *info);
 int dnufft_plan_get_permutation(const dnufft_plan *plan, uint32_t *out, void *stream);
 
 /* Type 1 like dnufft_nu2u, for callers that cannot allocate device memory
- * while they run it: code recording into a CUDA stream capture, plugins inside
- * a framework that owns the whole device memory pool, and services with a fixed
- * memory budget.  It has no counterpart in the reference (DUCC allocates its
- * temporaries on the host heap).  Every temporary comes from one area of
- * dnufft_noalloc_scratch_bytes() bytes (32 MiB) compiled into the library and
- * held by every GPU that loads it until the process exits; problems that need
- * more are rejected with DNUFFT_ERR_BADARG before any launch.  All arrays must
- * be device arrays.  The first call on a device looks up the area's address,
- * so make it before any stream capture.  All calls share the one area and it
- * keeps the previous call's contents: calls that can overlap on the GPU (other
- * streams, other host threads) race, so serialise them.  Plain spreader only. */
+ * while they run it: plugins inside a framework that owns the whole device
+ * memory pool, and services with a fixed memory budget.  It has no counterpart
+ * in the reference (DUCC allocates its temporaries on the host heap).  Every
+ * temporary comes from one area of dnufft_noalloc_scratch_bytes() bytes
+ * (32 MiB) compiled into the library and held by every GPU that loads it until
+ * the process exits; problems that need more are rejected with
+ * DNUFFT_ERR_BADARG before any launch.  All arrays must be device arrays.
+ * The first call on a device looks up the area's address and keeps it for the
+ * life of the process, so make that first call before any stream capture, and
+ * do not call this entry point on a device after resetting it.  The call waits
+ * on its stream once, part-way through, to read the number of point chunks
+ * back to the host.  All calls share the one area and it keeps the previous
+ * call's contents: calls that can overlap on the GPU (other streams, other
+ * host threads) race, so serialise them.  Plain spreader only; 2D rows run in
+ * the line FFT kernel. */
 int dnufft_nu2u_noalloc(const dnufft_array *points, const dnufft_array *coord, int forward,
                         double epsilon, dnufft_array *out, const dnufft_opts *opts,
                         void *stream);

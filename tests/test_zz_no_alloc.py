@@ -80,3 +80,41 @@ def test_noalloc_rejects_oversized_problem():
     status, _ = call(L.dnufft_nu2u_noalloc, coord, vals, (4096, 4096), 1e-5)
     assert status == 1
     assert b"no-allocation scratch" in L.dnufft_last_error()
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The property the entry point exists for: a call whose problem is new in
+    size (more points, so more scratch than any call before it) leaves the
+    device's free memory unchanged.  Every device array of the test is
+    allocated first, and one warm-up call loads the kernels the timed calls
+    use (loading kernel code takes device memory once)."""
+    import torch
+    L = C.lib()
+    shape, eps = (96, 80), 1e-5
+    arrays = []
+    for seed, M in ((5, 20000), (6, 70000)):
+        coord, vals = problem(seed, M, shape, np.float32, np.complex64)
+        dc = torch.from_numpy(coord).cuda()
+        dv = torch.from_numpy(vals).cuda()
+        out = torch.empty(shape, dtype=torch.complex64, device="cuda")
+        arrays.append((dc, dv, out))
+    opts = C.make_opts(False, ndim=2)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def run(dc, dv, out):
+        a_p, a_c, a_o = C.describe(dv), C.describe(dc), C.describe(out)
+        s = L.dnufft_nu2u_noalloc(ctypes.byref(a_p), ctypes.byref(a_c), 1, eps,
+                                  ctypes.byref(a_o), ctypes.byref(opts), st)
+        torch.cuda.synchronize()
+        return s
+
+    assert run(*arrays[0]) == 0, L.dnufft_last_error()
+    free0, _ = torch.cuda.mem_get_info()
+    assert run(*arrays[1]) == 0, L.dnufft_last_error()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    # and the larger call is still right
+    coord, vals = problem(6, 70000, shape, np.float32, np.complex64)
+    s1, ref = call(L.dnufft_nu2u, coord, vals, shape, eps)
+    assert s1 == 0
+    assert O.l2error(arrays[1][2].cpu().numpy(), ref) < eps
