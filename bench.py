@@ -3,17 +3,25 @@
 Workload (one "step"): on a 4096x4096 grid, M=5e7 points drawn from a mixture
 of 16 Gaussians (sigma 0.3 rad, centres uniform in [-pi,pi)^2, wrapped),
 float32 coordinates, complex64 values N(0,1): a planned nu2u followed by a
-planned u2nu with the same plan (DUCC's ``plan.nu2u`` / ``plan.u2nu``).
-Throughput = points x transforms / time, in Mpts/s.  The headline line uses
-the split-precision tensor-core spreader; the plain FP32 atomic spreader is
-timed on the same inputs and reported beside it (``alt_plain``).
+planned u2nu with the same plan (DUCC's ``plan.nu2u`` / ``plan.u2nu``; the
+plan, which bins and sorts the fixed coordinates, is built before the timed
+region in both arms).  Throughput = points x transforms / time, in Mpts/s.
+The headline line uses the split-precision tensor-core spreader; the plain
+FP32 atomic spreader is timed on the same inputs and reported beside it
+(``alt_plain``), and both are checked against DUCC's FP64 transforms
+(``errors``).
 
 Arms
   default            this library on N GPUs (one process per GPU under
                      torchrun; each rank runs its own seeded instance: weak
                      scaling, no collective on the data path)
   --impl reference   DUCC's own CPU NUFFT (built from source into oracle/_ref)
-                     on the host cores, rank 0 only
+                     on the host cores, rank 0 only, same plan-based step
+
+Both arms print the same ``config`` and feed the same ``nthreads`` value to
+DUCC's parameter cost model (``--param-threads``, default: the host's thread
+count, which is also the thread count of the reference arm), so they choose
+the same kernel support and oversampled grid.
 
 Prints one JSON line (rank 0).
 """
@@ -33,15 +41,25 @@ sys.path.insert(0, ROOT)
 N_SIDE = 4096
 M_POINTS = 50_000_000
 EPS = 1e-6
+ERR_SUBSET = 100_000      # type-2 error: DUCC FP64 evaluated on this many points
 METRIC = "NUFFT Mpts/s 2D eps=1e-6: TC split-prec vs plain FP32 spreader, same B200"
-KERNEL_NAMES = {"tc": "k_spread_tc (split-precision tensor-core spreader)",
-                "plain": "k_spread (plain FP32 atomic spreader)",
-                "auto": "k_spread (plain FP32 atomic spreader)"}
-# DRAM bytes per spreading launch at the full workload: ncu dram__bytes_read.sum
-# + dram__bytes_write.sum (a one-pass metric set) of launches of this bench's
-# default command (profiles/launches_bench_4096sq_M5e7.md)
-TRAFFIC_PER_LAUNCH = {"tc": 6460321536.0 + 528613120.0,
-                      "plain": 6345106944.0 + 451456000.0}
+
+# Counter-based figures of the dominant launches, from the ncu summaries under
+# profiles/ (named there), for the workload they were captured on.  They are
+# attached to the line only when the run's workload is that one.
+PROFILED = {
+    "workload": (4096, 50_000_000),
+    # dram__bytes_read.sum + dram__bytes_write.sum of one spreading launch
+    # (profiles/launches_bench_4096sq_M5e7.md, one-pass metrics, full workload)
+    "spread_dram_bytes": {"tc": 6460321536.0 + 528613120.0,
+                          "plain": 6345106944.0 + 451456000.0},
+    # shared-memory wavefronts of one launch (l1tex__data_pipe_lsu_wavefronts_
+    # mem_shared_op_atom.sum for the plain spreader, ..._op_ld.sum for the
+    # interpolation), captured at 2048^2 / M=1.25e7 (profiles/k_spread_plain_
+    # 2048sq_M12.5M.md, profiles/k_interp_2048sq_M12.5M.md) and scaled by 4:
+    # the points and the grid cells both grow by 4 at the same points per tile
+    "smem_wavefronts": {"plain_spread": 4 * 210563619.0, "interp": 4 * 86883694.0},
+}
 
 
 def clustered_coords(rng, m, ncl=16, sigma=0.3):
@@ -124,6 +142,19 @@ def peaks():
         return 6650.0, 1590.0, "fallback"
 
 
+# ---------------------------------------------------------------- shared by both arms
+def bench_config(args):
+    """The workload description; identical in both arms' lines."""
+    return {"workload": "2D type-1 + type-2 NUFFT, 4096x4096 grid, M=5e7 clustered points "
+                        "(16 Gaussians, sigma 0.3), f32 coords, c64, eps=1e-6",
+            "grid": [args.n, args.n], "npoints": args.m, "eps": EPS,
+            "coord_dtype": "float32", "value_dtype": "complex64",
+            "step": "plan.nu2u(forward=True) + plan.u2nu(forward=False), one plan built "
+                    "before the timed region",
+            "param_threads": args.param_threads,
+            "l2": "inputs and oversampled grid larger than L2 (no flush needed)"}
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, rank):
     if rank != 0:
@@ -136,15 +167,19 @@ def run_reference(args, rank):
         return
     m, n = args.m, args.n
     coord, vals, grid = make_inputs(1234, m, n)
-    nthr = os.cpu_count()
+    nthr = args.param_threads
+    choice = R.params_probe(shape=[n, n], npoints=m, epsilon=EPS, singleprec=True,
+                            gridding=True, nthreads=nthr, sigma_min=1.1, sigma_max=2.6)
     out = np.empty((n, n), np.complex64)
+    pts = np.empty(m, np.complex64)
+    t0 = time.perf_counter()
+    plan = R.nufft.plan(nu2u=True, coord=coord, grid_shape=(n, n), epsilon=EPS, nthreads=nthr)
+    plan_s = time.perf_counter() - t0
 
     def step():
-        R.nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=EPS, nthreads=nthr, out=out)
-        R.nufft.u2nu(grid=grid, coord=coord, forward=False, epsilon=EPS, nthreads=nthr)
+        plan.nu2u(points=vals, forward=True, out=out)
+        plan.u2nu(grid=grid, forward=False, out=pts)
 
-    plan_t0 = time.perf_counter()
-    del plan_t0
     for _ in range(args.warmup):
         step()
     t0 = time.perf_counter()
@@ -152,16 +187,27 @@ def run_reference(args, rank):
         step()
     dt = (time.perf_counter() - t0) / args.steps
     v = 2 * m / dt / 1e6
+    # DUCC's functions without a plan (each call bins and sorts), for reference
+    t0 = time.perf_counter()
+    R.nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=EPS, nthreads=nthr, out=out)
+    R.nufft.u2nu(grid=grid, coord=coord, forward=False, epsilon=EPS, nthreads=nthr, out=pts)
+    du = time.perf_counter() - t0
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "Mpts/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-        "config": {"workload": "2D type-1 + type-2 NUFFT, 4096x4096 grid, M=5e7 clustered "
-                               "points (16 Gaussians, sigma 0.3), f32 coords, c64, eps=1e-6",
-                   "grid": [n, n], "npoints": m, "call": "ducc0.nufft.nu2u + u2nu (unplanned)"},
+        "vs_baseline": None, "dtype": "c64 (f32 arithmetic)", "data": "synthetic",
+        "config": bench_config(args),
+        "parallelism": "%d host threads" % nthr,
+        "call": "ducc0.nufft.plan(nu2u=True, coord, grid_shape, epsilon, nthreads) "
+                ".nu2u + .u2nu (DUCC's own CPU NUFFT, built from source)",
+        "ducc_choice": {"kernel_index": choice["kernel_index"], "supp": choice["W"],
+                        "ofactor": choice["ofactor"], "nover": choice["nover"]},
+        "plan_create_s": plan_s,
+        "unplanned": {"value": 2 * m / du / 1e6, "ms_per_step": du * 1e3,
+                      "call": "ducc0.nufft.nu2u + u2nu", "steps": 1},
         "cpu_baseline": {"value": v, "unit": "Mpts/s", "cores": nthr, "kind": "reference",
-                         "sample": "full workload, %d step(s)" % args.steps},
+                         "sample": "the full workload, %d planned step(s)" % args.steps},
         "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -307,27 +353,65 @@ def workload_3d(dev, steps=3, warmup=1, seed=9):
 
 
 # ---------------------------------------------------------------- our arm
-def cpu_baseline_leg(m, n, coord, vals, grid, budget_s=30.0):
-    """DUCC's CPU NUFFT on the host cores, bounded to ~budget_s seconds."""
+def cpu_baseline_leg(args, coord, vals, grid, budget_s=20.0):
+    """DUCC's CPU NUFFT on the host cores (same planned step, same inputs),
+    bounded to about budget_s seconds.  Returns the baseline entry and DUCC's
+    own single-precision outputs (kept for the error report)."""
     from oracle import ref
     R = ref.load()
     if R is None:
-        return None
-    nthr = os.cpu_count()
+        return None, None
+    m, n, nthr = args.m, args.n, args.param_threads
     out = np.empty((n, n), np.complex64)
+    pts = np.empty(m, np.complex64)
+    plan = R.nufft.plan(nu2u=True, coord=coord, grid_shape=(n, n), epsilon=EPS, nthreads=nthr)
     t0 = time.perf_counter()
-    R.nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=EPS, nthreads=nthr, out=out)
-    R.nufft.u2nu(grid=grid, coord=coord, forward=False, epsilon=EPS, nthreads=nthr)
+    plan.nu2u(points=vals, forward=True, out=out)
+    plan.u2nu(grid=grid, forward=False, out=pts)
     first = time.perf_counter() - t0
     reps = max(1, min(3, int(budget_s / max(first, 1e-3)) - 1))
     t0 = time.perf_counter()
     for _ in range(reps):
-        R.nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=EPS, nthreads=nthr, out=out)
-        R.nufft.u2nu(grid=grid, coord=coord, forward=False, epsilon=EPS, nthreads=nthr)
+        plan.nu2u(points=vals, forward=True, out=out)
+        plan.u2nu(grid=grid, forward=False, out=pts)
     dt = (time.perf_counter() - t0) / reps
-    return {"value": 2 * m / dt / 1e6, "unit": "Mpts/s", "cores": nthr, "kind": "reference",
-            "sample": "the full workload (nu2u + u2nu, unplanned, M=%d), 1 warm-up + %d timed"
-                      % (m, reps)}
+    return ({"value": 2 * m / dt / 1e6, "unit": "Mpts/s", "cores": nthr, "kind": "reference",
+             "sample": "the full workload (plan.nu2u + plan.u2nu, M=%d), 1 warm-up + %d timed"
+                       % (m, reps)},
+            (out, pts))
+
+
+def error_report(args, coord, vals, grid, err_idx, ours, ducc_f32):
+    """Relative L2 errors (DUCC's l2error) of the type-1 outputs over the whole
+    grid and of the type-2 outputs at err_idx, against DUCC's FP64 transforms
+    (float64 coordinates, complex128 data, eps=1e-13) of the same inputs."""
+    from oracle import ref
+    from oracle.nufft_oracle import l2error
+    R = ref.load()
+    if R is None:
+        return None
+    n, nthr = args.n, args.param_threads
+    t0 = time.perf_counter()
+    c64 = coord.astype(np.float64)
+    ref1 = np.empty((n, n), np.complex128)
+    R.nufft.nu2u(points=vals.astype(np.complex128), coord=c64, forward=True, epsilon=1e-13,
+                 nthreads=nthr, out=ref1)
+    ref2 = R.nufft.u2nu(grid=grid.astype(np.complex128), coord=c64[err_idx], forward=False,
+                        epsilon=1e-13, nthreads=nthr)
+    del c64
+    rep = {"reference": "DUCC FP64 nu2u / u2nu (float64 coords, complex128, eps=1e-13)",
+           "type1_points": args.m, "type2_points": int(len(err_idx)),
+           "type1": {}, "type2": {}}
+    for sp, (g, p) in ours.items():
+        rep["type1"][sp] = l2error(g, ref1)
+        rep["type2"][sp] = l2error(p, ref2)
+    if ducc_f32 is not None:
+        rep["type1"]["ducc_f32"] = l2error(ducc_f32[0], ref1)
+        rep["type2"]["ducc_f32"] = l2error(ducc_f32[1][err_idx], ref2)
+    if "tc" in ours and "plain" in ours:
+        rep["type1_tc_over_plain"] = rep["type1"]["tc"] / rep["type1"]["plain"]
+    rep["seconds"] = time.perf_counter() - t0
+    return rep
 
 
 def max_over_ranks(value, dev, dist):
@@ -339,6 +423,83 @@ def max_over_ranks(value, dev, dist):
     t = torch.tensor([float(value)], device=dev)
     td.all_reduce(t, op=td.ReduceOp.MAX)
     return float(t.item())
+
+
+def _stage_ms(prof):
+    return {k: v[0] / max(v[1], 1) for k, v in prof.items()}
+
+
+def kernel_rooflines(stages, spreader, info, m, n, recs, hbm, bf16, sm_mhz, peak_src):
+    """One entry per kernel of the step: its bound resource, the achieved rate
+    from its CUDA-event time inside the timed region and the fraction of that
+    resource's peak.  Algorithmic bytes assume complex64 values (8 B), float32
+    coordinates (4 B per axis) and a uint32 permutation."""
+    n0, n1 = info["nover"]
+    N0, N1 = n, n
+    cells, kept = n0 * n1, n0 * N1
+    out = {}
+
+    def hbm_entry(key, nbytes, bound="hbm"):
+        ms = stages.get(key)
+        if not ms:
+            return None
+        ach = nbytes / (ms * 1e-3) / 1e9
+        return {"bound": bound, "avg_launch_ms": ms, "algorithmic_bytes": nbytes,
+                "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "peak_source": peak_src}
+
+    pts_bytes = m * (8 + 8 + 4)   # sorted coords, values (gathered), permutation
+    out["zeroing grid (memset)"] = hbm_entry("nu2u (planned)/zeroing grid", cells * 8)
+    sp = stages.get("nu2u (planned)/spreading")
+    if sp:
+        if spreader == "tc":
+            fl = recs * 2 * 128 * 48 * 16
+            ach = fl / (sp * 1e-3) / 1e12
+            e = {"bound": "tensor", "avg_launch_ms": sp, "executed_flops": fl,
+                 "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
+                 "peak_source": peak_src,
+                 "note": "one 128x48x16 FP16 MMA per K-block record (<= 16 points)"}
+        else:
+            wf = PROFILED["smem_wavefronts"]["plain_spread"]
+            e = {"bound": "smem", "avg_launch_ms": sp}
+            if (n, m) == PROFILED["workload"] and sm_mhz:
+                ach = wf / (sp * 1e-3)
+                pk = 148 * sm_mhz * 1e6
+                e.update({"achieved": ach, "peak": pk, "unit": "wavefronts/s",
+                          "frac": ach / pk, "wavefronts_per_launch": wf,
+                          "note": "shared-memory atomic wavefronts (ncu count, profiles/); "
+                                  "peak one wavefront per SM per clock at the sampled clock"})
+        h = pts_bytes + cells * 8
+        e["hbm_view"] = {"algorithmic_bytes": h,
+                         "achieved_gbs": h / (sp * 1e-3) / 1e9,
+                         "frac": h / (sp * 1e-3) / 1e9 / hbm}
+        out["k_spread_tc" if spreader == "tc" else "k_spread"] = e
+    for key, nb in (("nu2u (planned)/FFT rows (k_fft_rows)", (cells + kept) * 8),
+                    ("nu2u (planned)/FFT columns A (k_fft_colstep)", 2 * kept * 8),
+                    ("nu2u (planned)/FFT columns B, correction + crop (k_fft_colstep)",
+                     (kept + N0 * N1) * 8),
+                    ("u2nu (planned)/FFT columns A, correction + pad (k_fft_colstep)",
+                     (N0 * N1 + kept) * 8),
+                    ("u2nu (planned)/FFT columns B (k_fft_colstep)", 2 * kept * 8),
+                    ("u2nu (planned)/FFT rows, kept columns in (k_fft_rows)",
+                     (kept + cells) * 8)):
+        e = hbm_entry(key, nb)
+        if e:
+            out[key] = e
+    ip = stages.get("u2nu (planned)/interpolation")
+    if ip:
+        h = pts_bytes + cells * 8
+        e = hbm_entry("u2nu (planned)/interpolation", h)
+        e["bound"] = "smem"
+        if (n, m) == PROFILED["workload"] and sm_mhz:
+            wf = PROFILED["smem_wavefronts"]["interp"]
+            e["smem_view"] = {"wavefronts_per_launch": wf,
+                              "achieved": wf / (ip * 1e-3), "peak": 148 * sm_mhz * 1e6,
+                              "unit": "wavefronts/s",
+                              "frac": wf / (ip * 1e-3) / (148 * sm_mhz * 1e6),
+                              "note": "shared-memory load wavefronts (ncu count, profiles/)"}
+        out["k_interp"] = e
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -353,6 +514,8 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as td
     m, n = args.m, args.n
     coord, vals, grid = make_inputs(1234 + rank, m, n)
+    err_idx = np.sort(np.random.default_rng(99).choice(m, min(ERR_SUBSET, m), replace=False))
+    d_err_idx = torch.from_numpy(err_idx.astype(np.int64)).to(dev)
     d_coord = torch.from_numpy(coord).to(dev)
     d_vals = torch.from_numpy(vals).to(dev)
     d_grid = torch.from_numpy(grid).to(dev)
@@ -365,7 +528,7 @@ def run_ours(args, rank, world, local_rank):
             td.barrier()
         torch.cuda.synchronize(dev)
 
-    results = {}
+    results, kept = {}, {}
     for spreader in args.spreaders:
         t0 = time.perf_counter()
         plan = nufft.plan(nu2u=True, coord=d_coord, grid_shape=(n, n), epsilon=EPS,
@@ -400,64 +563,92 @@ def run_ours(args, rank, world, local_rank):
         ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dev, dist)
         results[spreader] = {"ms": ms, "plan_s": plan_s, "prof": prof, "clocks": clocks,
                              "launches": launches, "info": plan.info()}
+        # this arm's outputs of the last timed step, for the error report
+        kept[spreader] = (d_out_grid.cpu().numpy(), d_out_pts[d_err_idx].cpu().numpy())
         del plan
 
-    # end-to-end through the public API with host (pinned) buffers: unplanned
-    # nu2u + u2nu, host->device and device->host copies inside the timed region
-    e2e = None
+    head = args.spreaders[0]
+    e2e = e2e_unplanned = None
     if not args.no_e2e:
         h_coord = torch.from_numpy(coord).pin_memory().numpy()
         h_vals = torch.from_numpy(vals).pin_memory().numpy()
         h_grid = torch.from_numpy(grid).pin_memory().numpy()
         h_out = torch.empty((n, n), dtype=torch.complex64).pin_memory().numpy()
         h_pts = torch.empty(m, dtype=torch.complex64).pin_memory().numpy()
+        k = max(1, min(args.steps, 5))
+
+        # the same planned step through the public API on pinned host arrays:
+        # every step copies its values / uniform grid in and its results out
+        hplan = nufft.plan(nu2u=True, coord=h_coord, grid_shape=(n, n), epsilon=EPS,
+                           nthreads=args.param_threads, spreader=head)
 
         def e2e_step():
+            hplan.nu2u(points=h_vals, forward=True, out=h_out)
+            hplan.u2nu(grid=h_grid, forward=False, out=h_pts)
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            e2e_step()
+        barrier()
+        et = max_over_ranks((time.perf_counter() - t0) / k, dev, dist)
+        del hplan
+        e2e = {"value": world * 2 * m / et / 1e6, "unit": "Mpts/s",
+               "h2d_bytes_per_step": int(vals.nbytes + grid.nbytes),
+               "d2h_bytes_per_step": int(n * n * 8 + m * 8),
+               "call": "ducc_b200.nufft.plan(coord on the host).nu2u + .u2nu on pinned host "
+                       "numpy arrays (plan built before the timed region)",
+               "ms_per_step": et * 1e3}
+
+        # unplanned functions (each call uploads and sorts the coordinates)
+        def e2e_unplanned_step():
             nufft.nu2u(points=h_vals, coord=h_coord, forward=True, epsilon=EPS,
                        nthreads=args.param_threads, out=h_out)
             nufft.u2nu(grid=h_grid, coord=h_coord, forward=False, epsilon=EPS,
                        nthreads=args.param_threads, out=h_pts)
 
-        e2e_step()
+        e2e_unplanned_step()
         barrier()
         t0 = time.perf_counter()
-        k = max(1, min(args.steps, 5))
         for _ in range(k):
-            e2e_step()
+            e2e_unplanned_step()
         barrier()
         et = max_over_ranks((time.perf_counter() - t0) / k, dev, dist)
-        e2e = {"value": world * 2 * m / et / 1e6, "unit": "Mpts/s",
-               "h2d_bytes_per_step": int(2 * coord.nbytes + vals.nbytes + grid.nbytes),
-               "d2h_bytes_per_step": int(n * n * 8 + m * 8),
-               "call": "ducc_b200.nufft.nu2u + u2nu (unplanned) on pinned host numpy arrays",
-               "ms_per_step": et * 1e3}
+        e2e_unplanned = {"value": world * 2 * m / et / 1e6, "unit": "Mpts/s",
+                         "h2d_bytes_per_step": int(2 * coord.nbytes + vals.nbytes + grid.nbytes),
+                         "d2h_bytes_per_step": int(n * n * 8 + m * 8),
+                         "call": "ducc_b200.nufft.nu2u + u2nu (unplanned) on pinned host "
+                                 "numpy arrays", "ms_per_step": et * 1e3}
 
     if rank != 0:
         return
     hbm, bf16, src = peaks()
-    head = args.spreaders[0]
     r = results[head]
     ms = r["ms"]
-    # dominant kernel: the spreader of the planned type-1 transform
-    sp = r["prof"].get("nu2u (planned)/spreading", [0.0, 0])
-    ip = r["prof"].get("u2nu (planned)/interpolation", [0.0, 0])
-    sp_ms = sp[0] / max(sp[1], 1)
-    ip_ms = ip[0] / max(ip[1], 1)
-    W = r["info"]["supp"]
-    nov = r["info"]["nover"]
-    # algorithmic bytes of one spreading launch: sorted coords (8 B) + values
-    # (8 B) + permutation (4 B) per point, plus one write of the oversampled grid
-    spread_bytes = m * (8 + 8 + 4) + nov[0] * nov[1] * 8
-    achieved = spread_bytes / (sp_ms * 1e-3) / 1e9 if sp_ms > 0 else None
-    # DRAM bytes of one spreading launch from ncu (dram__bytes_read.sum +
-    # dram__bytes_write.sum), measured on the same kernel at a quarter of the
-    # workload (2048^2 grid, 1.25e7 points: same points per tile) and scaled
-    # by 4, since points and grid cells both scale by 4 (profiles/)
-    traffic = TRAFFIC_PER_LAUNCH.get(head)
-    # tensor pipe: each K-block record is at most one 128x48x16 MMA
+    stages = _stage_ms(r["prof"])
+    sm_mhz = r["clocks"].get("sm_mhz")
     recs = r["info"].get("tc_records", 0)
-    tc_flops = recs * 2 * 128 * 48 * 16
-    cpu = None if args.no_cpu else cpu_baseline_leg(m, n, coord, vals, grid)
+    rl = kernel_rooflines(stages, head, r["info"], m, n, recs, hbm, bf16, sm_mhz, src)
+    for other in args.spreaders[1:]:
+        o = results[other]
+        rl.update({k: v for k, v in kernel_rooflines(
+            _stage_ms(o["prof"]), other, o["info"], m, n, o["info"].get("tc_records", 0),
+            hbm, bf16, o["clocks"].get("sm_mhz"), src).items() if k.startswith("k_spread")})
+    # the headline roofline: the dominant kernel, the spreader of the head arm
+    sp_key = "k_spread_tc" if head == "tc" else "k_spread"
+    spr = rl.get(sp_key, {})
+    roofline = {k: spr.get(k) for k in ("bound", "achieved", "peak", "unit", "frac")}
+    roofline.update({"kernel": sp_key, "avg_launch_ms": spr.get("avg_launch_ms"),
+                     "peak_source": src, "hbm_view": spr.get("hbm_view")})
+    # DRAM bytes of one launch from ncu (PROFILED), only for the profiled workload
+    roofline["traffic"] = (PROFILED["spread_dram_bytes"].get(head)
+                           if (n, m) == PROFILED["workload"] else None)
+    roofline["traffic_source"] = "profiles/launches_bench_4096sq_M5e7.md"
+
+    cpu, ducc_out = (None, None) if args.no_cpu else cpu_baseline_leg(args, coord, vals, grid)
+    errors = None if args.no_errors else error_report(args, coord, vals, grid, err_idx, kept,
+                                                      ducc_out)
     workloads = None
     if not args.no_extra and world == 1:
         del d_coord, d_vals, d_grid, d_out_grid, d_out_pts
@@ -477,36 +668,26 @@ def run_ours(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (f32 arithmetic)", "data": "synthetic",
-        "config": {"workload": "2D type-1 + type-2 NUFFT, 4096x4096 grid, M=5e7 clustered "
-                               "points (16 Gaussians, sigma 0.3), f32 coords, c64, eps=1e-6",
-                   "grid": [n, n], "npoints": m, "eps": EPS, "spreader": head,
-                   "kernel_support": W, "oversampled": nov,
-                   "step": "plan.nu2u + plan.u2nu, inputs resident in HBM",
-                   "l2": "inputs and oversampled grid larger than L2 (no flush needed)",
-                   "parallelism": "replicas" if world > 1 else "1 GPU"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-                     "kernel": KERNEL_NAMES[head], "peak_source": src,
-                     "algorithmic_bytes_per_launch": spread_bytes,
-                     "avg_launch_ms": sp_ms,
-                     "tensor": None if not recs else {
-                         "executed_tflops": tc_flops / (sp_ms * 1e-3) / 1e12,
-                         "peak_tflops": bf16, "frac": tc_flops / (sp_ms * 1e-3) / 1e12 / bf16,
-                         "mma_per_launch": recs}},
-        "stages_ms": {k: v[0] / max(v[1], 1) for k, v in r["prof"].items()},
+        "config": bench_config(args),
+        "parallelism": "replicas" if world > 1 else "1 GPU",
+        "spreader": head, "kernel_support": r["info"]["supp"], "oversampled": r["info"]["nover"],
+        "roofline": roofline,
+        "kernels": rl,
+        "stages_ms": stages,
         "plan_create_s": r["plan_s"],
-        "interp_avg_ms": ip_ms,
         "clocks": r["clocks"],
         "gpu_launches": int(r["launches"]),
         "e2e": e2e,
+        "e2e_unplanned": e2e_unplanned,
         "cpu_baseline": cpu,
+        "errors": errors,
         "workloads": workloads,
     }
     for other in args.spreaders[1:]:
         o = results[other]
         line["alt_" + other] = {"value": world * 2 * m / (o["ms"] * 1e-3) / 1e6,
-                                "ms_per_step": o["ms"],
-                                "stages_ms": {k: v[0] / max(v[1], 1) for k, v in o["prof"].items()}}
+                                "ms_per_step": o["ms"], "stages_ms": _stage_ms(o["prof"]),
+                                "clocks": o["clocks"]}
     print(json.dumps(line))
 
 
@@ -519,10 +700,13 @@ def main():
     ap.add_argument("--m", type=int, default=M_POINTS)
     ap.add_argument("--n", type=int, default=N_SIDE)
     ap.add_argument("--spreaders", default="tc,plain")
-    ap.add_argument("--param-threads", type=int, default=8,
-                    help="nthreads fed to DUCC's parameter cost model (fixes W / sigma)")
+    ap.add_argument("--param-threads", type=int, default=os.cpu_count(),
+                    help="nthreads fed to DUCC's parameter cost model in both arms (and the "
+                         "reference arm's thread count)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-errors", action="store_true",
+                    help="skip the FP64 error report (DUCC on the host)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched / autograd / 3D workloads")
     args = ap.parse_args()

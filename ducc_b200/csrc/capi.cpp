@@ -124,7 +124,16 @@ struct StageTimer {
   cudaStream_t st;
   std::vector<std::pair<std::string, cudaEvent_t>> marks;
   bool range_open = false;   // an NVTX range named after the current stage
-  StageTimer(bool on_, cudaStream_t s) : on(on_ || g_prof_on), print(on_), st(s) {}
+  StageTimer *outer;         // the timer this one hides (nested transforms)
+  StageTimer(bool on_, cudaStream_t s) : on(on_ || g_prof_on), print(on_), st(s) {
+    outer = current();
+    current() = this;
+  }
+  // the innermost timer alive on this host thread (target of stage_mark)
+  static StageTimer *&current() {
+    static thread_local StageTimer *cur = nullptr;
+    return cur;
+  }
   // Starts stage `name`: closes the previous stage's NVTX range and opens one
   // for this stage (host-side ranges around the launches of each stage, for
   // a timeline tool; without one attached they cost a function call), and
@@ -161,10 +170,15 @@ struct StageTimer {
     if (print) std::fflush(stdout);
   }
   ~StageTimer() {
+    current() = outer;
     if (range_open) nvtxRangePop();
     for (auto &m : marks) cudaEventDestroy(m.second);
   }
 };
+
+void stage_mark(const char *name) {
+  if (StageTimer *t = StageTimer::current()) t->mark(name);
+}
 
 // ---------------------------------------------------------------- array views
 struct View {

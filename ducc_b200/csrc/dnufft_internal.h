@@ -42,6 +42,12 @@ uint64_t launch_count();
 // check a launch and count it
 #define DN_LAUNCHED() do { ::dnufft::cuda_check(cudaGetLastError(), "kernel launch"); ::dnufft::note_launch(); } while (0)
 
+// Starts a named sub-stage of the transform running on this host thread (one
+// NVTX range, and one CUDA event in the stage profile when that is on); used
+// between the launches of a multi-kernel stage such as the 2D FFT so that
+// each kernel gets its own time.  No effect outside a transform.
+void stage_mark(const char *name);
+
 // ---------------------------------------------------------------- planner
 struct KernelShape {
   int W;

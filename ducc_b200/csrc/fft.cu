@@ -1105,6 +1105,7 @@ static bool run_rows_v3(cplx<T> *grid, int n, int nlines, int64_t rs, int Nk, bo
   auto kern = fwd ? k_fft_rows<T, true> : k_fft_rows<T, false>;
   DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   const int nb = std::min(nlines, sm_count_dev());
+  stage_mark(out_kept ? "FFT rows (k_fft_rows)" : "FFT rows, kept columns in (k_fft_rows)");
   kern<<<nb, rows_threads<T>(), sm, st>>>(grid, rs, n, nlines, lo, hi0, in_kept ? 1 : 0,
                                           out_kept ? 1 : 0, pp, static_cast<const cplx<T> *>(p.tw),
                                           full_tw, err);
@@ -1145,6 +1146,8 @@ static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
     const size_t sm = size_t(2 * P * C + P) * sizeof(cplx<T>);
     auto kern = fwd ? k_fft_colstep<T, 0, true> : k_fft_colstep<T, 0, false>;
     DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    stage_mark(type1 ? "FFT columns A (k_fft_colstep)"
+                     : "FFT columns A, correction + pad (k_fft_colstep)");
     kern<<<unsigned(nblk) * unsigned(Q), 256, sm, st>>>(grid, work, cs, ppP, tw, u);
     DN_LAUNCHED();
   }
@@ -1152,6 +1155,8 @@ static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
     const size_t sm = size_t(2 * Q * C + Q) * sizeof(cplx<T>);
     auto kern = fwd ? k_fft_colstep<T, 1, true> : k_fft_colstep<T, 1, false>;
     DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    stage_mark(type1 ? "FFT columns B, correction + crop (k_fft_colstep)"
+                     : "FFT columns B (k_fft_colstep)");
     kern<<<unsigned(nblk) * unsigned(P), 256, sm, st>>>(grid, work, cs, ppQ, tw, u);
     DN_LAUNCHED();
   }

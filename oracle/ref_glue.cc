@@ -11,6 +11,7 @@
 //                                        :892-907, :1364-1381, :1862-1892
 //   - bucket_sort2                      src/ducc0/infra/bucket_sort.h:170
 //   - findNufftParameters               src/ducc0/nufft/nufft.h:155-208
+//                                        (also alone: params_probe)
 //   - selectKernel / getCoeffs          src/ducc0/math/gridding_kernel.cc:28-76,1552
 //   - Nufft_ancestor ctor corfac        src/ducc0/nufft/nufft.h:426-431
 //
@@ -148,6 +149,27 @@ py::dict index_probe(const py::array &coord, const std::vector<size_t> &shape,
   MR_fail("unsupported probe combination");
   }
 
+// DUCC's parameter choice alone (findNufftParameters, nufft.h:155-216) for a
+// transform of npoints points: kernel row, support, oversampling factor and
+// oversampled sizes, without building a plan.
+py::dict params_probe(const std::vector<size_t> &shape, size_t npoints, double epsilon,
+  bool singleprec, bool gridding, size_t nthreads, double sigma_min, double sigma_max)
+  {
+  auto [kidx, dims] = singleprec ?
+    detail_nufft::findNufftParameters<float,float>(epsilon, sigma_min, sigma_max,
+      shape, npoints, gridding, adjust_nthreads(nthreads)) :
+    detail_nufft::findNufftParameters<double,double>(epsilon, sigma_min, sigma_max,
+      shape, npoints, gridding, adjust_nthreads(nthreads));
+  const auto &kp = getKernel(kidx);
+  py::dict res;
+  res["kernel_index"] = kidx;
+  res["W"] = kp.W;
+  res["ofactor"] = kp.ofactor;
+  res["nover"] = std::vector<size_t>(dims.begin(), dims.end());
+  res["nthreads_used"] = adjust_nthreads(nthreads);
+  return res;
+  }
+
 // Kernel DB rows, for pinning the product's embedded parameter table.
 py::list kernel_db()
   {
@@ -188,6 +210,9 @@ PYBIND11_MODULE(MODNAME, m)
         "shape"_a, "epsilon"_a, "singleprec"_a, "gridding"_a, "nthreads"_a=1,
         "sigma_min"_a=1.2, "sigma_max"_a=2.51, "periodicity"_a,
         "fft_order"_a=false);
+  m.def("params_probe", &probe::params_probe, py::kw_only(), "shape"_a, "npoints"_a,
+        "epsilon"_a, "singleprec"_a, "gridding"_a, "nthreads"_a=1, "sigma_min"_a=1.2,
+        "sigma_max"_a=2.51);
   m.def("kernel_db", &probe::kernel_db);
   m.def("kernel_row", &probe::kernel_row);
   m.def("good_size", &probe::good_size);

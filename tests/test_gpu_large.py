@@ -1,0 +1,230 @@
+"""Accuracy at the benchmark's full sizes, against DUCC's own FP64 transforms.
+
+DUCC's CPU NUFFT (built from its sources into oracle/_ref) computes the
+references in float64 / complex128 at eps=1e-13, far below the tolerances:
+
+* 2D, 4096^2, M=5e7 points from 16 Gaussians (the bench workload), float32
+  coordinates, complex64, eps=1e-6: type 1 with both spreaders over the whole
+  grid (relative L2 below 1e-6, and the tensor-core spreader within 1.1x of
+  the plain FP32 spreader's error), type 2 on a fixed subset of 1e5 of the
+  5e7 outputs (type-2 outputs are independent per point, so DUCC evaluates
+  only those points);
+* 3D type 2, 256^3, M=2e7 uniform points: float64 at eps=1e-10 and float32 /
+  complex64 at eps=1e-5, by the same subset;
+* the tile permutation bit-exact against DUCC's (build_index + bucket_sort2,
+  nufft.h:1364-1381, bucket_sort.h:170) at 256^2 / M=2e5 and on the
+  clustered 4096^2 workload with M=2e6, where several radix passes and chunk
+  splits are exercised;
+* the 64 uneven instances of the batched benchmark, with the autotuner's
+  choices, instance by instance and transform by transform;
+* the tensor-core spreader on values whose magnitudes span eight decades.
+
+DUCC's relative L2 error is python/misc_pymod.cc:129-185 (oracle.l2error).
+"""
+import numpy as np
+import pytest
+
+import bench
+from ducc_b200 import autotune, batch, nufft
+from oracle import nufft_oracle as O
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+NTHR = 16
+
+
+def ducc():
+    R = ref.load()
+    if R is None:
+        pytest.skip("DUCC's CPU NUFFT is not built (oracle/_ref)")
+    return R
+
+
+def to_dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+@pytest.fixture(scope="module")
+def cfg2():
+    """The bench workload and DUCC's FP64 type 1 of it."""
+    R = ducc()
+    n, m = bench.N_SIDE, bench.M_POINTS
+    coord, vals, grid = bench.make_inputs(1234, m, n)
+    c64 = coord.astype(np.float64)
+    ref1 = np.empty((n, n), np.complex128)
+    R.nufft.nu2u(points=vals.astype(np.complex128), coord=c64, forward=True, epsilon=1e-13,
+                 nthreads=NTHR, out=ref1)
+    idx = np.sort(np.random.default_rng(99).choice(m, 100_000, replace=False))
+    ref2 = R.nufft.u2nu(grid=grid.astype(np.complex128), coord=c64[idx], forward=False,
+                        epsilon=1e-13, nthreads=NTHR)
+    return {"coord": coord, "vals": vals, "grid": grid, "ref1": ref1, "idx": idx,
+            "ref2": ref2, "n": n, "m": m}
+
+
+def test_cfg2_full_size_both_spreaders_vs_ducc_fp64(cfg2):
+    import torch
+    n = cfg2["n"]
+    dc, dv = to_dev(cfg2["coord"]), to_dev(cfg2["vals"])
+    errs = {}
+    for sp in ("plain", "tc"):
+        p = nufft.plan(nu2u=True, coord=dc, grid_shape=(n, n), epsilon=1e-6, nthreads=NTHR,
+                       spreader=sp)
+        out = torch.empty((n, n), dtype=torch.complex64, device="cuda")
+        p.nu2u(points=dv, forward=True, out=out)
+        errs[sp] = O.l2error(out.cpu().numpy(), cfg2["ref1"])
+        if sp == "tc":
+            assert p.info()["tc_records"] > 0
+        del p, out
+    assert errs["plain"] < 1e-6, errs
+    assert errs["tc"] < 1e-6, errs
+    assert errs["tc"] <= 1.1 * errs["plain"], errs
+
+
+def test_cfg2_type2_subset_vs_ducc_fp64(cfg2):
+    n = cfg2["n"]
+    dc = to_dev(cfg2["coord"])
+    p = nufft.plan(nu2u=False, coord=dc, grid_shape=(n, n), epsilon=1e-6, nthreads=NTHR)
+    res = p.u2nu(grid=to_dev(cfg2["grid"]), forward=False)
+    got = res[to_dev(cfg2["idx"].astype(np.int64))].cpu().numpy()
+    assert O.l2error(got, cfg2["ref2"]) < 1e-6
+
+
+def test_cfg2_unplanned_host_arrays_vs_ducc_fp64(cfg2):
+    """The public functions on host arrays (the pipelined upload path)."""
+    n = cfg2["n"]
+    out = np.empty((n, n), np.complex64)
+    nufft.nu2u(points=cfg2["vals"], coord=cfg2["coord"], forward=True, epsilon=1e-6,
+               nthreads=NTHR, out=out)
+    assert O.l2error(out, cfg2["ref1"]) < 1e-6
+    res = nufft.u2nu(grid=cfg2["grid"], coord=cfg2["coord"], forward=False, epsilon=1e-6,
+                     nthreads=NTHR)
+    assert O.l2error(res[cfg2["idx"]], cfg2["ref2"]) < 1e-6
+
+
+def test_permutation_bit_exact_clustered_4096(cfg2):
+    R = ducc()
+    m = 2_000_000
+    coord = np.ascontiguousarray(cfg2["coord"][:m])
+    pr = R.index_probe(coord=coord, shape=[4096, 4096], epsilon=1e-6, singleprec=True,
+                       gridding=True, nthreads=NTHR, sigma_min=1.2, sigma_max=2.51,
+                       periodicity=[2 * np.pi] * 2, fft_order=False)
+    p = nufft.plan(nu2u=True, coord=to_dev(coord), grid_shape=(4096, 4096), epsilon=1e-6,
+                   nthreads=NTHR, sigma_min=1.2, sigma_max=2.51, spreader="plain")
+    assert p.info()["nover"] == [int(x) for x in pr["nover"]]
+    assert np.array_equal(p.permutation(), pr["coord_idx"])
+
+
+def test_permutation_bit_exact_cfg1():
+    R = ducc()
+    rng = np.random.default_rng(11)
+    coord = rng.uniform(-np.pi, np.pi, (200_000, 2))
+    pr = R.index_probe(coord=coord, shape=[256, 256], epsilon=1e-6, singleprec=False,
+                       gridding=True, nthreads=1, sigma_min=1.2, sigma_max=2.51,
+                       periodicity=[2 * np.pi] * 2, fft_order=False)
+    p = nufft.plan(nu2u=True, coord=coord, grid_shape=(256, 256), epsilon=1e-6, nthreads=1,
+                   sigma_min=1.2, sigma_max=2.51)
+    assert p.info()["supp"] == int(pr["W"])
+    assert np.array_equal(p.permutation(), pr["coord_idx"])
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_cfg3_type2_256cube_subset_vs_ducc_fp64(single):
+    import torch
+    R = ducc()
+    rng = np.random.default_rng(9)
+    N, M = 256, 20_000_000
+    cdt, ct, eps = (np.float32, torch.complex64, 1e-5) if single else \
+        (np.float64, torch.complex128, 1e-10)
+    coord = rng.uniform(-np.pi, np.pi, (M, 3)).astype(cdt)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    grid = torch.randn((N, N, N), dtype=ct, device="cuda", generator=g)
+    p = nufft.plan(nu2u=False, coord=to_dev(coord), grid_shape=(N, N, N), epsilon=eps,
+                   nthreads=NTHR)
+    res = p.u2nu(grid=grid, forward=True)
+    idx = np.sort(rng.choice(M, 100_000, replace=False))
+    got = res[to_dev(idx.astype(np.int64))].cpu().numpy()
+    del res, p
+    ref2 = R.nufft.u2nu(grid=grid.cpu().numpy().astype(np.complex128),
+                        coord=coord[idx].astype(np.float64), forward=True, epsilon=1e-13,
+                        nthreads=NTHR)
+    assert O.l2error(got, ref2) < eps
+
+
+def test_cfg4_64_uneven_instances_vs_ducc():
+    """The batched benchmark's 64 instances (same generator and seed), autotuned,
+    run as one batch; every transform within 2*eps of DUCC's FP64 one (DUCC's
+    2D tolerance against the exact sum, python/test/test_nufft.py:140)."""
+    import torch
+    R = ducc()
+    rng = np.random.default_rng(7)
+    plans, nts, coords, epss, pts, grids = [], [], [], [], [], []
+    for _ in range(64):
+        side = int(round(np.exp(rng.uniform(np.log(64), np.log(1024))) / 2)) * 2
+        M = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        nt = int(rng.choice([1, 4]))
+        eps = float(rng.choice([1e-4, 1e-6]))
+        coord = rng.uniform(-np.pi, np.pi, (M, 2)).astype(np.float32)
+        dc = to_dev(coord)
+        choice = autotune.tune(dc, (side, side), eps, ntrans=nt, reps=1)
+        plans.append(nufft.plan(nu2u=True, coord=dc, grid_shape=(side, side), epsilon=eps,
+                                **autotune.plan_kwargs(choice)))
+        nts.append(nt)
+        coords.append(coord)
+        epss.append(eps)
+        pts.append(torch.randn((nt, M), dtype=torch.complex64, device="cuda"))
+        grids.append(torch.randn((nt, side, side), dtype=torch.complex64, device="cuda"))
+    b = batch.Batch(plans, ntrans=nts)
+    outs = [torch.empty(g.shape, dtype=torch.complex64, device="cuda") for g in grids]
+    pouts = [torch.empty(v.shape, dtype=torch.complex64, device="cuda") for v in pts]
+    b.nu2u(points=pts, out=outs, forward=True)
+    b.u2nu(grids=grids, out=pouts, forward=False)
+    torch.cuda.synchronize()
+    worst = 0.0
+    for i in range(64):
+        c64 = coords[i].astype(np.float64)
+        side = grids[i].shape[-1]
+        for t in range(nts[i]):
+            r1 = np.empty((side, side), np.complex128)
+            R.nufft.nu2u(points=pts[i][t].cpu().numpy().astype(np.complex128), coord=c64,
+                         forward=True, epsilon=1e-12, nthreads=NTHR, out=r1)
+            e1 = O.l2error(outs[i][t].cpu().numpy(), r1)
+            r2 = R.nufft.u2nu(grid=grids[i][t].cpu().numpy().astype(np.complex128), coord=c64,
+                              forward=False, epsilon=1e-12, nthreads=NTHR)
+            e2 = O.l2error(pouts[i][t].cpu().numpy(), r2)
+            assert e1 < 2 * epss[i] and e2 < 2 * epss[i], (i, t, epss[i], e1, e2)
+            worst = max(worst, e1 / epss[i], e2 / epss[i])
+    assert worst > 0
+
+
+def test_tc_values_over_eight_decades():
+    """Magnitudes log-uniform in [1e-4, 1e4] with random phases: the tensor-core
+    spreader's single power-of-two operand scale must not cost accuracy
+    against the plain FP32 spreader (both against DUCC FP64)."""
+    R = ducc()
+    rng = np.random.default_rng(21)
+    M, n = 400_000, 512
+    coord = bench.clustered_coords(rng, M)
+    mag = np.exp(rng.uniform(np.log(1e-4), np.log(1e4), M))
+    vals = (mag * np.exp(2j * np.pi * rng.random(M))).astype(np.complex64)
+    r1 = np.empty((n, n), np.complex128)
+    R.nufft.nu2u(points=vals.astype(np.complex128), coord=coord.astype(np.float64),
+                 forward=True, epsilon=1e-13, nthreads=NTHR, out=r1)
+    errs = {}
+    for sp in ("plain", "tc"):
+        out = np.empty((n, n), np.complex64)
+        nufft.nu2u(points=vals, coord=coord, forward=True, epsilon=1e-6, out=out, spreader=sp)
+        errs[sp] = O.l2error(out, r1)
+    assert errs["tc"] < 1e-6, errs
+    assert errs["tc"] <= 1.1 * errs["plain"], errs
+    # the small values on their own: spread only the points below 1e-2
+    small = mag < 1e-2
+    r1s = np.empty((n, n), np.complex128)
+    R.nufft.nu2u(points=vals[small].astype(np.complex128),
+                 coord=coord[small].astype(np.float64), forward=True, epsilon=1e-13,
+                 nthreads=NTHR, out=r1s)
+    outs = np.empty((n, n), np.complex64)
+    nufft.nu2u(points=vals[small], coord=coord[small], forward=True, epsilon=1e-6, out=outs,
+               spreader="tc")
+    assert O.l2error(outs, r1s) < 1e-6
