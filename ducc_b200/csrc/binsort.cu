@@ -41,8 +41,16 @@ __global__ void k_fold_keys(const Tc *__restrict__ coord, int64_t cs0, int64_t c
   } else if constexpr (NDIM == 2) {
     key = uint32_t(t[0] >> g.log2tile) * uint32_t(g.ntiles[1]) + uint32_t(t[1] >> g.log2tile);
     if (qbits) {
-      const int half = 1 << (g.log2tile - 1), m = (1 << g.log2tile) - 1;
+      // quadrant, then the cell inside it in Morton order: consecutive points
+      // (one K-block of the tensor-core spreader) lie close together, so each
+      // accumulator cell receives contributions from fewer K-blocks
+      const int lh = g.log2tile - 1, half = 1 << lh, m = (1 << g.log2tile) - 1;
+      const uint32_t du = uint32_t(t[0] & (half - 1)), dv = uint32_t(t[1] & (half - 1));
+      uint32_t mort = 0;
+      for (int b = 0; b < lh; ++b)
+        mort |= (((du >> b) & 1u) << (2 * b + 1)) | (((dv >> b) & 1u) << (2 * b));
       key = (key << 2) | (((t[0] & m) >= half) ? 2u : 0u) | (((t[1] & m) >= half) ? 1u : 0u);
+      key = (key << (2 * lh)) | mort;
     }
   } else {
     uint32_t ss = uint32_t(g.ssmall), ms = (1u << ss) - 1u;

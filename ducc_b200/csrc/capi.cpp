@@ -339,7 +339,7 @@ struct Setup {
   std::vector<double> corfac[3];
   std::vector<int> factors[3];
   int spreader = DNUFFT_SPREAD_AUTO;
-  bool qbits = false;   // sort key carries the 2D tile quadrant (tensor-core order)
+  bool qbits = false;   // sort key carries the 2D tile quadrant and cell (tensor-core order)
   int keybits = 1;
   int tile_shift = 0;
   uint64_t max_tiles = 0;
@@ -468,8 +468,8 @@ static Setup make_setup(int ndim, const int64_t *nuni, uint64_t npoints, double 
     s.spreader = DNUFFT_SPREAD_TC;
   if (s.spreader == DNUFFT_SPREAD_TC && spread_tc_supported(g, calc_f64)) {
     s.qbits = true;
-    maxkey <<= 2;
-    s.tile_shift = 2;
+    maxkey <<= 2 + tc_cell_bits(g);
+    s.tile_shift = 2 + tc_cell_bits(g);
     // per-chunk set-up and flush of the tensor-core spreader cost more than
     // the plain one's: amortise them over longer chunks
     s.chunk = CHUNK_TC;
@@ -571,7 +571,8 @@ static void build_index(const Setup &s, const View &coord, Index &ix, cudaStream
     DevBuf kws(tc_kblock_workspace_bytes(ix.nchunks), st);
     ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
     ix.nkblk = build_tc_kblocks(ix.keys.as<uint32_t>(), cl, ix.groups, kws.p, ix.kblk.as<uint2>(),
-                                ix.kbrange.as<uint32_t>(), ix.count.as<uint32_t>(), st);
+                                ix.kbrange.as<uint32_t>(), ix.count.as<uint32_t>(),
+                                tc_cell_bits(s.g), st);
   }
 }
 
@@ -1722,11 +1723,12 @@ int dnufft_plan_get_permutation(const dnufft_plan *p, uint32_t *out, void *strea
     if (!p->s.qbits) {
       DN_CUDA(cudaMemcpyAsync(out, p->ix.perm.p, size_t(p->s.npoints) * 4, cudaMemcpyDefault, st));
     } else {
-      // the plan processes points in (tile, quadrant) order; DUCC's permutation
-      // is the stable order by tile alone: re-sort the original coordinates
+      // the plan processes points in (tile, quadrant, cell) order; DUCC's
+      // permutation is the stable order by tile alone: re-sort the original
+      // coordinates
       dnufft::Setup s2 = p->s;
       s2.qbits = false;
-      s2.keybits -= 2;
+      s2.keybits -= 2 + dnufft::tc_cell_bits(s2.g);
       s2.tile_shift = 0;
       s2.chunk = dnufft::CHUNK;
       const uint32_t M = s2.npoints;

@@ -6,11 +6,14 @@
 namespace dnufft {
 
 // ---- binning / sorting (binsort.cu)
-// quadrant_bits: append the point's 16x16 quadrant within its 2D tile as two
-// extra low key bits (the tensor-core spreader's processing order)
+// quadrant_bits: append the point's quadrant within its 2D tile as two extra
+// key bits and, below them, the Morton code of its cell within the quadrant
+// (2 * (log2tile - 1) bits): the tensor-core spreader's processing order
 void launch_fold_keys(bool coord_f64, const void *coord, int64_t cs0, int64_t cs1,
                       uint32_t npts, const Geometry &g, uint32_t *keys, uint32_t *idx,
                       cudaStream_t st, bool quadrant_bits = false);
+// bits of the within-quadrant cell order in a tensor-core sort key
+inline int tc_cell_bits(const Geometry &g) { return 2 * (g.log2tile - 1); }
 size_t scan_workspace_bytes(uint64_t n);
 void exclusive_scan(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *ws,
                     cudaStream_t st);
@@ -82,8 +85,10 @@ struct TcBlocks {
 size_t tc_kblock_workspace_bytes(uint32_t nchunks);
 uint32_t tc_kblock_upper_bound(uint32_t npts, uint32_t nchunks);
 // returns the number of K-blocks (reads it back: synchronises the stream)
+// (cell_bits: the key bits below the quadrant bits, tc_cell_bits)
 uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t groups, void *ws,
-                          uint2 *kblk, uint32_t *range, uint32_t *d_total, cudaStream_t st);
+                          uint2 *kblk, uint32_t *range, uint32_t *d_total, int cell_bits,
+                          cudaStream_t st);
 void launch_spread_tc(const PointsDesc &pts, const TcBlocks &tb, const Geometry &g,
                       const KernelPoly<float> &kp, const void *values, int64_t vs, void *grid,
                       unsigned *absmax, int *err, cudaStream_t st);

@@ -6,15 +6,15 @@
 // over the points p of the tile.  It runs on the 5th-generation tensor cores
 // (tcgen05.mma, kind::f16, FP32 accumulation in tensor memory) with every
 // operand split into FP16 hi + lo parts, x = hi + lo, so that
-//     A.B ~= Ahi.Bhi + Ahi.Blo + Alo.Bhi
-// keeps ~22 significant bits.  One MMA does all three products and both
+//     A.B = Ahi.Bhi + Ahi.Blo + Alo.Bhi + Alo.Blo
+// keeps ~22 significant bits of each operand.  One MMA does all four products and both
 // complex parts at once:
 //     A (M=128 x K=16 points) rows = [Re(c)ku hi | Im(c)ku hi | Re(c)ku lo | Im(c)ku lo]
 //                                    24 rows each (rows 96..127 stay zero)
 //     B (K=16 x N=48)         cols = [kv hi | kv lo], 24 columns each
 //     D (128 x 48, FP32, TMEM):  Re = D[0:24, 0:24] + D[0:24, 24:48] + D[48:72, 0:24]
-//                                Im = D[24:48, 0:24] + D[24:48, 24:48] + D[72:96, 0:24]
-// (the Alo.Blo block is computed and ignored).  A 32x32 tile (DUCC's 2D
+//                                     + D[48:72, 24:48]  (and Im from rows 24:48, 72:96)
+// (the Alo.Blo block costs nothing extra: the MMA computes it anyway).  A 32x32 tile (DUCC's 2D
 // single-precision tile) is split into four 16x16 quadrants with their own
 // accumulators, so a point's <= 8 taps always fit the 24 rows/columns of its
 // quadrant window.  Points arrive sorted by (tile, quadrant); the plan cuts
@@ -74,7 +74,10 @@ constexpr int STAGE_BYTES = ROUND * (A_BYTES + B_BYTES);   // 45056
 constexpr int TMEM_COLS = 512;     // quadrant q, buffer b at column 128*q + 64*b
 constexpr int PL = 40, PP = 41;    // FP32 plane rows, odd pitch
 constexpr int PLANE_FLOATS = PL * PP;
-constexpr int DRAIN_AT = 24;       // K-blocks per quadrant per sub-chunk (chain bound)
+#ifndef DNUFFT_TC_DRAIN_AT
+#define DNUFFT_TC_DRAIN_AT 24
+#endif
+constexpr int DRAIN_AT = DNUFFT_TC_DRAIN_AT;   // K-blocks per quadrant per sub-chunk (chain bound)
 constexpr uint32_t FLUSH_COST = 16;  // CTA balancing: one sub-chunk flush ~ this many records
 
 // warp roles
@@ -700,8 +703,10 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
             float *dst = plane + (u + ((q & 2) ? 16 : 0)) * PP + ((q & 1) ? 16 : 0);
 #pragma unroll
             for (int v = 0; v < 24; ++v) {
-              float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]);
-              if (p < 2) val += __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
+              // columns v (kv hi) and 24 + v (kv lo): hi.hi + hi.lo in the hi
+              // rows, lo.hi + lo.lo in the lo rows
+              const float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]) +
+                                __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
               dst[v] += val;
             }
           }
@@ -785,20 +790,21 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
 }
 
 // ---------------------------------------------------------------- K-block lists
-// A chunk (consecutive sorted points of one tile, ordered by quadrant) is cut
+// A chunk (consecutive sorted points of one tile, ordered by quadrant and, in
+// each quadrant, by cell in Morton order) is cut
 // into sub-chunks with at most DRAIN_AT K-blocks per quadrant, which bounds
 // every tensor-core accumulation chain; a sub-chunk is one accumulator event
 // per quadrant and one flush of the tile planes.  Inside a sub-chunk the
 // records take the quadrants in turn, so the four MMA issuers share each round.
 __device__ __forceinline__ void tc_chunk_bounds(const uint32_t *__restrict__ skeys, const Chunk &ch,
-                                                uint32_t (&b)[5]) {
+                                                int cell_bits, uint32_t (&b)[5]) {
   b[0] = ch.start;
   b[4] = ch.start + ch.count;
   for (uint32_t q = 1; q < 4; ++q) {
     uint32_t lo = b[q - 1], hi = b[4];
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
-      if ((skeys[mid] & 3u) < q) lo = mid + 1;
+      if (((skeys[mid] >> cell_bits) & 3u) < q) lo = mid + 1;
       else hi = mid;
     }
     b[q] = lo;
@@ -814,13 +820,13 @@ __device__ __forceinline__ uint32_t tc_subchunks(const uint32_t (&kq)[4]) {
 // Per chunk: the first sorted index of quadrants 1..3 (binary search on the
 // quadrant bits of the sorted keys) and the number of records.
 __global__ void k_tc_count(const uint32_t *__restrict__ skeys, const Chunk *__restrict__ chunks,
-                           uint32_t nch, uint4 *__restrict__ qb, uint32_t *__restrict__ nrec,
-                           uint32_t *__restrict__ cost) {
+                           uint32_t nch, int cell_bits, uint4 *__restrict__ qb,
+                           uint32_t *__restrict__ nrec, uint32_t *__restrict__ cost) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nch) return;
   const Chunk ch = chunks[c];
   uint32_t b[5];
-  tc_chunk_bounds(skeys, ch, b);
+  tc_chunk_bounds(skeys, ch, cell_bits, b);
   uint32_t kq[4];
   for (int q = 0; q < 4; ++q) kq[q] = (b[q + 1] - b[q] + tc::KB - 1) / tc::KB;
   const uint32_t S = tc_subchunks(kq);
@@ -904,7 +910,8 @@ uint32_t tc_kblock_upper_bound(uint32_t npts, uint32_t nch) {
 }
 
 uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t groups, void *ws,
-                          uint2 *kblk, uint32_t *range, uint32_t *d_total, cudaStream_t st) {
+                          uint2 *kblk, uint32_t *range, uint32_t *d_total, int cell_bits,
+                          cudaStream_t st) {
   const uint32_t nch = cl.nchunks;
   DN_REQUIRE(nch > 0, ST_INTERNAL, "no chunks");
   uint4 *qb = static_cast<uint4 *>(ws);
@@ -915,7 +922,7 @@ uint32_t build_tc_kblocks(const uint32_t *skeys, const ChunkList &cl, uint32_t g
   uint32_t *sws = reinterpret_cast<uint32_t *>(
       (reinterpret_cast<uintptr_t>(cpos + nch) + 255) & ~uintptr_t(255));
   const unsigned gb = (nch + 255) / 256;
-  k_tc_count<<<gb, 256, 0, st>>>(skeys, cl.chunks, nch, qb, nrec, cost);
+  k_tc_count<<<gb, 256, 0, st>>>(skeys, cl.chunks, nch, cell_bits, qb, nrec, cost);
   DN_LAUNCHED();
   exclusive_scan(nrec, pos, nch, sws, st);
   exclusive_scan(cost, cpos, nch, sws, st);
