@@ -1080,6 +1080,19 @@ static void u2nu_dcoord_impl(const dnufft_array *grid_, const dnufft_array *coor
 }  // namespace dnufft
 
 // ---------------------------------------------------------------- plans
+namespace dnufft {
+// One group of a plan's points, split by input order: points [a, b) with
+// their own index and sorted coordinates.  A plan made from host coordinates
+// with many points keeps these beside its whole-plan index, so that calls on
+// host arrays copy one group's values in (type 1) or its results out (type 2)
+// while other groups are spread or interpolated.
+struct PlanGroup {
+  uint64_t a = 0, b = 0;
+  Index ix;
+  DevBuf sorted_coord;
+};
+}  // namespace dnufft
+
 struct dnufft_plan {
   dnufft::Setup s;
   dnufft::DevConst dc;
@@ -1087,6 +1100,7 @@ struct dnufft_plan {
   dnufft::DevBuf sorted_coord;
   dnufft::DevBuf grid;   // oversampled grid, allocated on first execution
   dnufft::DevBuf work;   // FFT column-pass scratch (2D), allocated on first execution
+  std::vector<dnufft::PlanGroup> groups;   // host-coordinate plans with many points
   dnufft_opts o;
   int device = 0;
 };
@@ -1117,9 +1131,126 @@ static void plan_create_impl(int nu2u, const dnufft_array *coord_, const int64_t
     // the plan keeps the sorted coordinates (and, for the tensor-core
     // spreader, the K-block list); the sorted keys are no longer needed
     p->ix.keys.release();
+    // coordinates from the host: the caller will likely pass host arrays,
+    // whose copies the per-group index lets overlap with the work
+    const int G = pipe_groups(p->s.npoints);
+    if (coord.host && G > 1) {
+      const size_t cb = f64 ? 8 : 4;
+      p->groups.resize(size_t(G));
+      for (int gi = 0; gi < G; ++gi) {
+        PlanGroup &pg = p->groups[size_t(gi)];
+        pg.a = group_start(p->s.npoints, G, gi);
+        pg.b = group_start(p->s.npoints, G, gi + 1);
+        Setup sg = p->s;
+        sg.npoints = uint32_t(pg.b - pg.a);
+        const View cv = coord_range(coord, sc.dev.data, pg.a, pg.b, cb);
+        build_index(sg, cv, pg.ix, st);
+        pg.sorted_coord = DevBuf(size_t(sg.npoints) * ndim * cb, st);
+        launch_gather_coords(f64, cv.data, cv.stride[0], cv.stride[1], ndim,
+                             pg.ix.perm.as<uint32_t>(), sg.npoints, pg.sorted_coord.p, st);
+        pg.ix.keys.release();
+      }
+    }
   }
   DN_CUDA(cudaStreamSynchronize(st));
   *out = p.release();
+}
+
+static void plan_buffers(dnufft_plan *p, cudaStream_t st) {
+  if (p->grid.p) return;
+  // allocated once, on first use, and made visible to every stream
+  const size_t vb = p->s.calc_f64 ? 16 : 8;
+  p->grid = DevBuf(grid_cells(p->s.g) * vb, st);
+  const size_t wb = fft_work_bytes(p->s.g, vb);
+  if (wb) p->work = DevBuf(wb, st);
+  DN_CUDA(cudaStreamSynchronize(st));
+}
+
+static PointsDesc group_points(const dnufft_plan *p, const PlanGroup &pg) {
+  return PointsDesc{pg.sorted_coord.p, int64_t(p->s.g.ndim), 1, true, p->s.coord_f64,
+                    pg.ix.perm.as<uint32_t>(), uint32_t(pg.b - pg.a)};
+}
+
+// Planned type 1 on host values, group by group: the values of later groups
+// are copied in (side stream) while earlier groups are spread.
+template <typename T>
+static void plan_nu2u_groups(dnufft_plan *p, const View &points, const View &out, bool forward,
+                             StageTimer &tm, cudaStream_t st) {
+  const Setup &s = p->s;
+  const size_t vb = sizeof(T) * 2;
+  const int G = int(p->groups.size());
+  Staged so(out, false, true, st);
+  DevBuf dvals(size_t(s.npoints) * vb, st);
+  EventSet copied(G);
+  // declared after the buffers: destroyed (after synchronising) before them
+  SideStream up(st, true);
+  up.start();
+  for (int gi = 0; gi < G; ++gi) {
+    const PlanGroup &pg = p->groups[size_t(gi)];
+    DN_CUDA(cudaMemcpyAsync(static_cast<char *>(dvals.p) + pg.a * vb,
+                            static_cast<const char *>(points.data) + pg.a * vb,
+                            (pg.b - pg.a) * vb, cudaMemcpyHostToDevice, up.s));
+    DN_CUDA(cudaEventRecord(copied.ev[size_t(gi)], up.s));
+  }
+  tm.mark("zeroing grid");
+  DN_CUDA(cudaMemsetAsync(p->grid.p, 0, grid_cells(s.g) * vb, st));
+  tm.mark("groups: spreading");
+  int *err = device_error_word();
+  for (int gi = 0; gi < G; ++gi) {
+    const PlanGroup &pg = p->groups[size_t(gi)];
+    DN_CUDA(cudaStreamWaitEvent(st, copied.ev[size_t(gi)], 0));
+    Setup sg = s;
+    sg.npoints = uint32_t(pg.b - pg.a);
+    const ChunkList cl{pg.ix.chunks.as<Chunk>(), pg.ix.nchunks};
+    const TcBlocks tb = pg.ix.tc();
+    spread_points<T>(sg, group_points(p, pg), cl, s.qbits ? &tb : nullptr,
+                     static_cast<char *>(dvals.p) + pg.a * vb, 1, p->grid.p, err, st);
+  }
+  tm.mark("FFT + correction");
+  fft_nu2u_tail<T>(p->grid.p, s.g, p->dc.ax, forward, p->dc.cf, p->o.fft_order != 0,
+                   so.dev.data, so.dev.stride, st, p->work.p, err);
+  tm.mark("output copy");
+  check_device_error(err, st);
+  up.merge();
+  so.finish();
+}
+
+// Planned type 2 into a host array, group by group: each group's results go
+// back (side stream) while the next groups are interpolated.
+template <typename T>
+static void plan_u2nu_groups(dnufft_plan *p, const View &uni, const View &out, bool forward,
+                             StageTimer &tm, cudaStream_t st) {
+  const Setup &s = p->s;
+  const size_t vb = sizeof(T) * 2;
+  const int G = int(p->groups.size());
+  Staged su(uni, true, false, st);
+  DevBuf dout(size_t(s.npoints) * vb, st);
+  EventSet done(G);
+  // declared after the buffers: destroyed (after synchronising) before them
+  SideStream down(st, true);
+  down.start();
+  int *err = device_error_word();
+  tm.mark("correction + FFT");
+  fft_u2nu_head<T>(su.dev.data, su.dev.stride, s.g, p->dc.ax, forward, p->dc.cf,
+                   p->o.fft_order != 0, p->grid.p, st, p->work.p, err);
+  tm.mark("groups: interpolation");
+  const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
+      sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
+  for (int gi = 0; gi < G; ++gi) {
+    const PlanGroup &pg = p->groups[size_t(gi)];
+    const ChunkList cl{pg.ix.chunks.as<Chunk>(), pg.ix.nchunks};
+    launch_interp<T>(group_points(p, pg), cl, s.g, kp, p->grid.p, 0,
+                     static_cast<char *>(dout.p) + pg.a * vb, 1, 0, 1, st);
+    DN_CUDA(cudaEventRecord(done.ev[size_t(gi)], st));
+    DN_CUDA(cudaStreamWaitEvent(down.s, done.ev[size_t(gi)], 0));
+    DN_CUDA(cudaMemcpyAsync(static_cast<char *>(out.data) + pg.a * vb,
+                            static_cast<const char *>(dout.p) + pg.a * vb, (pg.b - pg.a) * vb,
+                            cudaMemcpyDeviceToHost, down.s));
+  }
+  tm.mark("output copy");
+  down.merge();
+  check_device_error(err, st);
+  DN_CUDA(cudaStreamSynchronize(st));
 }
 
 static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosity,
@@ -1142,19 +1273,26 @@ static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosit
     DN_REQUIRE(uv.shape[d] == s.g.nuni[d], ST_BADARG, "uniform grid dimensions mismatch");
   StageTimer tm(verbosity > 0, st);
   if (verbosity > 0) report_sizes(s, type1);
+  if (!p->groups.empty() && (type1 ? in.host : out.host)) {
+    plan_buffers(p, st);
+    if (type1) {
+      if (f64) plan_nu2u_groups<double>(p, in, out, forward != 0, tm, st);
+      else plan_nu2u_groups<float>(p, in, out, forward != 0, tm, st);
+      tm.report("nu2u (planned, host values)");
+    } else {
+      if (f64) plan_u2nu_groups<double>(p, in, out, forward != 0, tm, st);
+      else plan_u2nu_groups<float>(p, in, out, forward != 0, tm, st);
+      tm.report("u2nu (planned, host output)");
+    }
+    return;
+  }
   Staged si(in, true, false, st), so(out, false, true, st);
   if (s.npoints == 0) {
     if (type1) zero_view(so.dev, st);
     so.finish();
     return;
   }
-  if (!p->grid.p) {
-    // allocated once, on first use, and made visible to every stream
-    p->grid = DevBuf(grid_cells(s.g) * (f64 ? 16 : 8), st);
-    const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
-    if (wb) p->work = DevBuf(wb, st);
-    DN_CUDA(cudaStreamSynchronize(st));
-  }
+  plan_buffers(p, st);
   PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
                  p->ix.perm.as<uint32_t>(), s.npoints};
   ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
@@ -1686,6 +1824,11 @@ int dnufft_plan_destroy(dnufft_plan *plan) {
       plan->grid.st = st;
       plan->work.st = st;
       for (int d = 0; d < 3; ++d) plan->dc.corfac[d].st = plan->dc.tw[d].st = st;
+      for (auto &pg : plan->groups) {
+        pg.ix.perm.st = pg.ix.chunks.st = pg.ix.count.st = pg.ix.keys.st = st;
+        pg.ix.kblk.st = pg.ix.kbrange.st = st;
+        pg.sorted_coord.st = st;
+      }
       delete plan;
       DN_CUDA(cudaDeviceSynchronize());
     }

@@ -110,3 +110,37 @@ def test_pipelined_1d_3d(shape, single):
     idx = rng.choice(M, 300, replace=False)
     ref = O.direct_u2nu(grid, coord[idx], False)
     assert O.l2error(h_pts[idx], ref) < 2 * eps
+
+
+@pytest.mark.parametrize("single,spreader", [(True, "tc"), (True, "plain"), (False, "auto")])
+def test_planned_host_groups_match_device_calls(single, spreader):
+    """A plan made from host coordinates with many points keeps a per-group
+    index: its calls on host arrays copy groups in / results out while other
+    groups are spread / interpolated.  Same plan, same results as its calls on
+    device arrays (one index over all points), repeated calls included."""
+    import torch
+    rng = np.random.default_rng(12)
+    cdt, vdt = (np.float32, np.complex64) if single else (np.float64, np.complex128)
+    eps = 1e-6 if single else 1e-10
+    coord = rng.uniform(-np.pi, np.pi, (M, 2)).astype(cdt)
+    vals = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(vdt)
+    grid = (rng.standard_normal(SHAPE) + 1j * rng.standard_normal(SHAPE)).astype(vdt)
+    dv, dg = (torch.from_numpy(x).cuda() for x in (vals, grid))
+    tol = 2e-6 if single else 1e-12
+    p = nufft.plan(nu2u=True, coord=coord, grid_shape=SHAPE, epsilon=eps, spreader=spreader)
+    for forward in (True, False):
+        for _ in range(2):
+            h_out = np.zeros(SHAPE, vdt)
+            p.nu2u(points=vals, forward=forward, out=h_out)
+            d_out = p.nu2u(points=dv, forward=forward)
+            assert O.l2error(h_out, d_out.cpu().numpy()) < tol
+            h_pts = np.empty(M, vdt)
+            p.u2nu(grid=grid, forward=forward, out=h_pts)
+            d_pts = p.u2nu(grid=dg, forward=forward)
+            assert O.l2error(h_pts, d_pts.cpu().numpy()) < tol
+        idx = rng.choice(M, 300, replace=False)
+        assert O.l2error(h_pts[idx], O.direct_u2nu(grid, coord[idx], forward)) < 2 * eps
+    # device uniform grid, host output: the grouped path reads the device array
+    h_pts2 = np.empty(M, vdt)
+    p.u2nu(grid=dg, forward=True, out=h_pts2)
+    assert O.l2error(h_pts2, p.u2nu(grid=dg, forward=True).cpu().numpy()) < tol
