@@ -1253,14 +1253,46 @@ static void plan_u2nu_groups(dnufft_plan *p, const View &uni, const View &out, b
   DN_CUDA(cudaStreamSynchronize(st));
 }
 
+static void plan_exec_one(dnufft_plan *p, bool type1, int forward, int verbosity, const View &in,
+                          const View &out, cudaStream_t st);
+
+// The array without its leading (transform) axis, at transform t.
+static View slice0(const View &v, int64_t t) {
+  View r = v;
+  r.data = static_cast<char *>(v.data) + t * v.stride[0] * int64_t(dtype_size(v.dtype));
+  r.ndim = v.ndim - 1;
+  for (int d = 0; d < r.ndim; ++d) {
+    r.shape[d] = v.shape[d + 1];
+    r.stride[d] = v.stride[d + 1];
+  }
+  return r;
+}
+
 static void plan_exec_impl(dnufft_plan *p, bool type1, int forward, int verbosity,
                            const dnufft_array *in_, dnufft_array *out_, cudaStream_t st) {
   DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  View in = view_of(in_, type1 ? "points" : "grid");
+  View out = view_of(out_, "out");
+  // several transforms over the plan's points: a leading axis of ntrans on
+  // both the point array (ntrans, M) and the uniform array (ntrans, N...)
+  const View &pv = type1 ? in : out;
+  if (pv.ndim == 2) {
+    const View &uv = type1 ? out : in;
+    DN_REQUIRE(uv.ndim == p->s.g.ndim + 1 && uv.shape[0] == pv.shape[0], ST_BADARG,
+               "several transforms: the point array (ntrans, M) and the uniform array "
+               "(ntrans, N...) must have the same leading extent");
+    for (int64_t t = 0; t < pv.shape[0]; ++t)
+      plan_exec_one(p, type1, forward, verbosity, slice0(in, t), slice0(out, t), st);
+    return;
+  }
+  plan_exec_one(p, type1, forward, verbosity, in, out, st);
+}
+
+static void plan_exec_one(dnufft_plan *p, bool type1, int forward, int verbosity, const View &in,
+                          const View &out, cudaStream_t st) {
   const Setup &s = p->s;
   bool f64 = s.calc_f64;
   int cdt = f64 ? DNUFFT_C128 : DNUFFT_C64;
-  View in = view_of(in_, type1 ? "points" : "grid");
-  View out = view_of(out_, "out");
   DN_REQUIRE(in.dtype == cdt && out.dtype == cdt, ST_BADARG,
              f64 ? "a float64-coordinate plan needs complex128 data"
                  : "a float32-coordinate plan needs complex64 data");

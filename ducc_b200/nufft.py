@@ -223,9 +223,13 @@ class plan:
         return np.empty(shape, dtype=dt)
 
     def nu2u(self, *, forward, verbosity=0, points, out=None, stream=None):
+        """Type 1 over the plan's points.  ``points`` of shape ``(M,)``, or
+        ``(ntrans, M)`` for ntrans transforms at once (then ``out`` is
+        ``(ntrans,) + grid_shape``; an extension of DUCC's plan)."""
         points = _prepare_in(points)
         if out is None:
-            out = self._alloc(points, self.grid_shape)
+            lead = tuple(points.shape[:-1]) if len(points.shape) == 2 else ()
+            out = self._alloc(points, lead + self.grid_shape)
         op = _OutProxy(out)
         a_p, a_o = C.describe(points), C.describe(op.buf)
         C.check(C.lib().dnufft_plan_nu2u(self._ptr, 1 if forward else 0, int(verbosity),
@@ -234,9 +238,13 @@ class plan:
         return op.finish()
 
     def u2nu(self, *, forward, verbosity=0, grid, out=None, stream=None):
+        """Type 2 at the plan's points.  ``grid`` of shape ``grid_shape``, or
+        ``(ntrans,) + grid_shape`` for ntrans transforms at once (then ``out``
+        is ``(ntrans, M)``; an extension of DUCC's plan)."""
         grid = _prepare_in(grid)
         if out is None:
-            out = self._alloc(grid, (self.npoints,))
+            lead = tuple(grid.shape[:1]) if len(grid.shape) == len(self.grid_shape) + 1 else ()
+            out = self._alloc(grid, lead + (self.npoints,))
         op = _OutProxy(out)
         a_g, a_o = C.describe(grid), C.describe(op.buf)
         C.check(C.lib().dnufft_plan_u2nu(self._ptr, 1 if forward else 0, int(verbosity),

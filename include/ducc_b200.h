@@ -126,7 +126,10 @@ int dnufft_plan_create(int nu2u, const dnufft_array *coord, const int64_t *grid_
                        dnufft_plan **plan);
 
 /* Replaces plan.nu2u (python/nufft_pymod.cc:240-249, :170-183;
- * Julia nufft_nu2u_planned, julia/ducc_julia.cc:394-457). */
+ * Julia nufft_nu2u_planned, julia/ducc_julia.cc:394-457).  Extension: with a
+ * leading axis of ntrans on both arrays, points (ntrans, M) and out
+ * (ntrans, N...), the call runs ntrans transforms over the plan's points
+ * (the same for dnufft_plan_u2nu, grid (ntrans, N...) and out (ntrans, M)). */
 int dnufft_plan_nu2u(dnufft_plan *plan, int forward, int verbosity,
                      const dnufft_array *points, dnufft_array *out, void *stream);
 

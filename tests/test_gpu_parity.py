@@ -170,3 +170,31 @@ def test_cfg1_full_size_vs_oracle():
     ev = np.exp(-1j * np.outer(coord[:, 1], kv))
     exact = np.einsum("m,mi,mj->ij", vals, eu, ev, optimize=True)
     assert O.l2error(out[100:104], exact) < 1e-6
+
+
+@pytest.mark.parametrize("shape,single", [((37,), False), ((40, 33), True), ((40, 33), False),
+                                          ((12, 10, 14), True)])
+@pytest.mark.parametrize("device", [False, True])
+def test_plan_ntrans(shape, single, device):
+    """Several transforms over one plan's points in one call (a leading ntrans
+    axis): each equals the single-transform call."""
+    rng = np.random.default_rng(31)
+    M, nt = 3000, 3
+    cdt, vdt = (np.float32, np.complex64) if single else (np.float64, np.complex128)
+    eps = 1e-5 if single else 1e-10
+    coord = rng.uniform(-np.pi, np.pi, (M, len(shape))).astype(cdt)
+    vals = (rng.standard_normal((nt, M)) + 1j * rng.standard_normal((nt, M))).astype(vdt)
+    grid = (rng.standard_normal((nt,) + shape) + 1j * rng.standard_normal((nt,) + shape)).astype(vdt)
+    conv = torch_dev if device else (lambda x: x)
+    back = (lambda x: x.cpu().numpy()) if device else (lambda x: x)
+    p1 = nufft.plan(nu2u=True, coord=conv(coord), grid_shape=shape, epsilon=eps)
+    r1 = back(p1.nu2u(points=conv(vals), forward=True))
+    r2 = back(p1.u2nu(grid=conv(grid), forward=False))
+    assert r1.shape == (nt,) + shape and r2.shape == (nt, M)
+    for t in range(nt):
+        assert O.l2error(r1[t], back(p1.nu2u(points=conv(vals[t]), forward=True))) < 1e-12
+        assert O.l2error(r2[t], back(p1.u2nu(grid=conv(grid[t]), forward=False))) < 1e-12
+        ref = O.direct_nu2u(coord.astype(np.float64), vals[t], shape, True)
+        assert O.l2error(r1[t], ref) < 4 * eps
+    with pytest.raises(RuntimeError, match="leading extent"):
+        p1.nu2u(points=conv(vals), forward=True, out=conv(np.empty((nt + 1,) + shape, vdt)))
