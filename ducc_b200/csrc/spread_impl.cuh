@@ -150,7 +150,9 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
     if (i < end) {
       Tc x[NDIM];
       uint32_t j = load_point<Tc, NDIM>(pts, i, x);
-      cplx<T> v = values[int64_t(j) * vs];
+      // a gather through the permutation: cached in L2 only, so a miss
+      // brings one 32-byte sector instead of a whole L1 line
+      cplx<T> v = __ldcg(values + int64_t(j) * vs);
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) {
         int i0;

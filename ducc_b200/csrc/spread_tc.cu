@@ -23,9 +23,9 @@
 // The kernel is persistent (one CTA per SM, a contiguous range of K-blocks
 // per CTA, balanced at chunk boundaries) and warp-specialised, every hand-off
 // an mbarrier:
-//   loader warps (4)   : K-block records, permutation, then cp.async of the
-//                        coordinates and values of one round (8 K-blocks) into
-//                        a 16-slot ring;
+//   loader warps (4)   : K-block records, permutation, value gathers (L2-only
+//                        loads) and cp.async of the coordinates of one round
+//                        (8 K-blocks) into a 16-slot ring;
 //   builder warps (8)  : 2 threads per point (A column: Re(c)ku and Im(c)ku, B
 //                        row: kv): fold, Horner weights, FP16 hi/lo split,
 //                        placement; MN-major operand tiles in 3 stages;
@@ -429,6 +429,13 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         idx[j] = st + uint32_t(e);
         pj[j] = ok[j] ? pts.perm[idx[j]] : 0u;
       }
+      // values: gathered through the permutation with loads cached in L2
+      // only (a miss brings one 32-byte sector, not a whole L1 line), in
+      // flight while the loader waits for its ring slot
+      float2 vv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        vv[j] = ok[j] ? __ldcg(values + int64_t(pj[j]) * vs) : make_float2(0.f, 0.f);
       const int slot = r % NPRE;
       if (r >= NPRE && !mbar_wait(&pre_empty[slot], uint32_t((r / NPRE - 1) & 1), abortp, err))
         break;
@@ -469,8 +476,10 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
           cp_async(cdst, crd + int64_t(pj[j]) * pts.cs0, int(sizeof(Tc)));
           cp_async(cdst + 1, crd + int64_t(pj[j]) * pts.cs0 + pts.cs1, int(sizeof(Tc)));
         }
-        cp_async(sl + PL_::VAL + 8 * p, values + int64_t(pj[j]) * vs, 8);
+        reinterpret_cast<float2 *>(sl + PL_::VAL)[p] = vv[j];
       }
+      // the value stores are ordered before lane 0's arrival (release) by
+      // this warp barrier
       __syncwarp();
       if (lane == 0) mbar_arrive(&pre_full[slot]);
       cp_async_arrive(&pre_full[slot]);

@@ -191,9 +191,12 @@ def test_plan_ntrans(shape, single, device):
     r1 = back(p1.nu2u(points=conv(vals), forward=True))
     r2 = back(p1.u2nu(grid=conv(grid), forward=False))
     assert r1.shape == (nt,) + shape and r2.shape == (nt, M)
+    # the spreaders add with atomics, whose order varies from call to call:
+    # repeated single precision transforms agree to rounding, not bit for bit
+    same = 1e-6 if single else 1e-12
     for t in range(nt):
-        assert O.l2error(r1[t], back(p1.nu2u(points=conv(vals[t]), forward=True))) < 1e-12
-        assert O.l2error(r2[t], back(p1.u2nu(grid=conv(grid[t]), forward=False))) < 1e-12
+        assert O.l2error(r1[t], back(p1.nu2u(points=conv(vals[t]), forward=True))) < same
+        assert O.l2error(r2[t], back(p1.u2nu(grid=conv(grid[t]), forward=False))) < same
         ref = O.direct_nu2u(coord.astype(np.float64), vals[t], shape, True)
         assert O.l2error(r1[t], ref) < 4 * eps
     with pytest.raises(RuntimeError, match="leading extent"):
