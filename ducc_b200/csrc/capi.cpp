@@ -771,8 +771,18 @@ struct EventSet {
   }
 };
 
-// first point of group gi of G over M points
-static uint64_t group_start(uint32_t M, int G, int gi) { return uint64_t(M) * uint64_t(gi) / uint64_t(G); }
+// First point of group gi of G over M points.  With three or more groups the
+// first and the last get a quarter of the share of the others: type 1 ends
+// with the last group's spreading after its copy, type 2 starts with the first
+// group's interpolation before any result can go back, so small end groups
+// shorten the part of the call that no copy overlaps.
+static uint64_t group_start(uint32_t M, int G, int gi) {
+  if (G < 3) return uint64_t(M) * uint64_t(gi) / uint64_t(G);
+  // group weights 1, 4, 4, ..., 4, 1 (in quarters)
+  const uint64_t total = 4 * uint64_t(G - 2) + 2;
+  const uint64_t before = gi == 0 ? 0 : (gi >= G ? total : 1 + 4 * uint64_t(gi - 1));
+  return uint64_t(M) * before / total;
+}
 
 // coordinates (C-contiguous (M, d) device copy) of points [a, b)
 static View coord_range(const View &coord, void *dev, uint64_t a, uint64_t b, size_t cb) {
