@@ -52,7 +52,7 @@ EXPORTS = [
     "dnufft_plan_u2nu_dcoord", "dnufft_batch_create", "dnufft_batch_nu2u", "dnufft_batch_u2nu",
     "dnufft_batch_destroy", "dnufft_kernel_candidates", "dnufft_selftest_wait_timeout",
     "dnufft_plan_spread", "dnufft_plan_grid_to_uniform", "dnufft_find_parameters",
-    "dnufft_plan_rows_fft", "dnufft_plan_cols_to_uniform",
+    "dnufft_plan_rows_fft", "dnufft_plan_cols_to_uniform", "dnufft_plan_cols_to_uniform_range",
 ]
 
 
@@ -86,6 +86,8 @@ def lib():
     L.dnufft_plan_grid_to_uniform.argtypes = [vp, ctypes.c_int, P(Array), P(Array), vp]
     L.dnufft_plan_rows_fft.argtypes = [vp, ctypes.c_int, P(Array), vp]
     L.dnufft_plan_cols_to_uniform.argtypes = [vp, ctypes.c_int, P(Array), P(Array), vp]
+    L.dnufft_plan_cols_to_uniform_range.argtypes = [vp, ctypes.c_int, P(Array), ctypes.c_int64,
+                                                     P(Array), vp]
     L.dnufft_find_parameters.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int64),
                                          ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, P(Opts), P(ctypes.c_int32),

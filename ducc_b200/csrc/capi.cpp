@@ -771,18 +771,8 @@ struct EventSet {
   }
 };
 
-// First point of group gi of G over M points.  With three or more groups the
-// first and the last get a quarter of the share of the others: type 1 ends
-// with the last group's spreading after its copy, type 2 starts with the first
-// group's interpolation before any result can go back, so small end groups
-// shorten the part of the call that no copy overlaps.
-static uint64_t group_start(uint32_t M, int G, int gi) {
-  if (G < 3) return uint64_t(M) * uint64_t(gi) / uint64_t(G);
-  // group weights 1, 4, 4, ..., 4, 1 (in quarters)
-  const uint64_t total = 4 * uint64_t(G - 2) + 2;
-  const uint64_t before = gi == 0 ? 0 : (gi >= G ? total : 1 + 4 * uint64_t(gi - 1));
-  return uint64_t(M) * before / total;
-}
+// first point of group gi of G over M points
+static uint64_t group_start(uint32_t M, int G, int gi) { return uint64_t(M) * uint64_t(gi) / uint64_t(G); }
 
 // coordinates (C-contiguous (M, d) device copy) of points [a, b)
 static View coord_range(const View &coord, void *dev, uint64_t a, uint64_t b, size_t cb) {
@@ -1540,6 +1530,43 @@ static void plan_cols_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array 
   so.finish();
 }
 
+static void plan_cols_range_impl(dnufft_plan *p, int forward, dnufft_array *cols_, int64_t col0,
+                                 dnufft_array *out_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  DN_REQUIRE(s.g.ndim == 2, ST_UNSUPPORTED, "row and column halves: 2D plans only");
+  const bool f64 = s.calc_f64;
+  const int dt = f64 ? DNUFFT_C128 : DNUFFT_C64;
+  View cols = view_of(cols_, "cols"), out = view_of(out_, "out");
+  DN_REQUIRE(!cols.host && !out.host, ST_BADARG, "column blocks: device arrays only");
+  DN_REQUIRE(cols.dtype == dt && out.dtype == dt, ST_BADARG,
+             "column blocks must have the plan's data type");
+  DN_REQUIRE(cols.ndim == 2 && cols.shape[0] == s.g.nover[0], ST_BADARG,
+             "cols must be (nover[0], ncols)");
+  const int64_t nc = cols.shape[1];
+  DN_REQUIRE(nc >= 1 && col0 >= 0 && col0 + nc <= s.g.nuni[1], ST_BADARG,
+             "column block outside the kept columns");
+  DN_REQUIRE(cols.stride[1] == 1 && cols.stride[0] == nc, ST_BADARG,
+             "cols must be C-contiguous");
+  DN_REQUIRE(out.ndim == 2 && out.shape[0] == s.g.nuni[0] && out.shape[1] == nc, ST_BADARG,
+             "out must be (nuni[0], ncols)");
+  const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
+  if (wb && !p->work.p) {
+    p->work = DevBuf(wb, st);
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
+  const bool fo = p->o.fft_order != 0;
+  const bool ok =
+      f64 ? fft_nu2u_cols_range<double>(cols.data, int(nc), int(col0), s.g, p->dc.ax,
+                                        forward != 0, p->dc.cf, fo, out.data, out.stride, st,
+                                        p->work.p)
+          : fft_nu2u_cols_range<float>(cols.data, int(nc), int(col0), s.g, p->dc.ax,
+                                       forward != 0, p->dc.cf, fo, out.data, out.stride, st,
+                                       p->work.p);
+  DN_REQUIRE(ok, ST_UNSUPPORTED,
+             "column blocks need the four-step column passes (oversampled rows >= 1024)");
+}
+
 static void find_parameters_impl(int nu2u, int ndim, const int64_t *shape, uint64_t npoints,
                                  double eps, int calc_f64, int coord_f64, const dnufft_opts *opts_,
                                  int32_t *kidx, int64_t *nover) {
@@ -1847,6 +1874,12 @@ int dnufft_plan_cols_to_uniform(dnufft_plan *plan, int forward, dnufft_array *gr
                                 dnufft_array *out, void *stream) {
   DN_GUARD(dnufft::plan_cols_to_uniform_impl(plan, forward, grid, out,
                                              static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_cols_to_uniform_range(dnufft_plan *plan, int forward, dnufft_array *cols,
+                                      int64_t col0, dnufft_array *out, void *stream) {
+  DN_GUARD(dnufft::plan_cols_range_impl(plan, forward, cols, col0, out,
+                                        static_cast<cudaStream_t>(stream)))
 }
 
 int dnufft_find_parameters(int nu2u, int ndim, const int64_t *grid_shape, uint64_t npoints,

@@ -896,6 +896,11 @@ struct ColSpec {
   int lc;       // log2 columns per CTA
   int in_mode;  // pass A: 0 grid, 1 uniform array (type 2); pass B: work
   int out_mode; // pass A: work; pass B: 0 grid (natural order), 1 uniform array (type 1)
+  // column x of this pass is column x0 + x of a transform with N1t kept of
+  // n1t grid columns (uniform index and correction factor); with packed_out
+  // the uniform result of column x goes to column x of out (x0 = 0, N1t = N1,
+  // n1t = n1 and packed_out = 0 for a whole transform)
+  int x0, N1t, n1t, packed_out;
 };
 
 template <typename T, int PASS, bool FWD>
@@ -932,8 +937,9 @@ __global__ void __launch_bounds__(256, cols_min_ctas<T>())
   int iu1 = 0, icf1 = 0;
   double cf1 = 0.0;
   if (colok && ((PASS == 0 && cs.in_mode != 0) || (PASS == 1 && cs.out_mode != 0))) {
-    grid_to_uni(gx, cs.N1, cs.n1, u.fft_order, iu1, icf1);
+    grid_to_uni(cs.x0 + gx, cs.N1t, cs.n1t, u.fft_order, iu1, icf1);
     cf1 = u.corfac[1][icf1];
+    if (cs.packed_out) iu1 = x;
   }
   auto load_m = [&](int m) -> cplx<T> {
     cplx<T> v = mkc<T>(T(0), T(0));
@@ -1117,7 +1123,8 @@ static bool run_rows_v3(cplx<T> *grid, int n, int nlines, int64_t rs, int Nk, bo
 template <typename T>
 static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
                         const FFTAxisPlan &p, const UniSpec &u, bool type1, bool fwd,
-                        cudaStream_t st) {
+                        cudaStream_t st, int x0 = 0, int N1t = -1, int n1t = -1,
+                        bool packed_out = false) {
   if (work == nullptr || n0 < 1024) return false;
   int P, Q;
   if (!split_pq(n0, P, Q)) return false;
@@ -1133,6 +1140,10 @@ static bool run_cols_v3(cplx<T> *grid, cplx<T> *work, int n0, int n1, int N1,
   cs.N1 = N1;
   cs.n1 = n1;
   cs.lc = lc;
+  cs.x0 = x0;
+  cs.N1t = N1t < 0 ? N1 : N1t;
+  cs.n1t = n1t < 0 ? n1 : n1t;
+  cs.packed_out = packed_out ? 1 : 0;
   const cplx<T> *tw = static_cast<const cplx<T> *>(p.tw);
   const int nblk = (N1 + C - 1) / C;
   for (int pass = 0; pass < 2; ++pass) {
@@ -1261,6 +1272,25 @@ void fft_nu2u_cols(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool f
   if (!run_cols_v3<T>(grid, work, n0, n1, N1, ax[0], u, true, fwd, st))
     run_lines<T>(grid, mk_spec(n0, 0, n1, 1, N1, 0, 1, -1, 1, 0, 1, IO_FULL, IO_UNI), ax[0], u,
                  fwd, st);
+}
+
+// 2D type 1, second half for a block of kept columns: cols is (n0, ncols),
+// the kept columns col0 .. col0 + ncols - 1 (of N1) packed, already
+// transformed along axis 1; column FFTs, correction and crop into out, an
+// (N0, ncols) array whose column x is the uniform column of kept column
+// col0 + x.  Four-step column passes only (n0 >= 1024): false otherwise.
+template <typename T>
+bool fft_nu2u_cols_range(void *colsv, int ncols, int col0, const Geometry &g,
+                         const FFTAxisPlan *ax, bool fwd, const double *const corfac[3],
+                         bool fft_order, void *out, const int64_t *ostride, cudaStream_t st,
+                         void *workv) {
+  cplx<T> *cols = static_cast<cplx<T> *>(colsv);
+  cplx<T> *work = static_cast<cplx<T> *>(workv);
+  const UniSpec u = mk_uni(out, ostride, g, corfac, fft_order);
+  const int n0 = int(g.nover[0]);
+  const int N1 = int(g.nuni[1]);
+  return run_cols_v3<T>(cols, work, n0, ncols, ncols, ax[0], u, true, fwd, st, col0, N1, N1,
+                        true);
 }
 
 template <typename T>
@@ -1555,6 +1585,12 @@ template void fft_nu2u_rows<float>(void *, int, const Geometry &, const FFTAxisP
                                    cudaStream_t, int *);
 template void fft_nu2u_rows<double>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
                                     cudaStream_t, int *);
+template bool fft_nu2u_cols_range<float>(void *, int, int, const Geometry &, const FFTAxisPlan *,
+                                         bool, const double *const[3], bool, void *,
+                                         const int64_t *, cudaStream_t, void *);
+template bool fft_nu2u_cols_range<double>(void *, int, int, const Geometry &,
+                                          const FFTAxisPlan *, bool, const double *const[3],
+                                          bool, void *, const int64_t *, cudaStream_t, void *);
 template void fft_nu2u_cols<float>(void *, const Geometry &, const FFTAxisPlan *, bool,
                                    const double *const[3], bool, void *, const int64_t *,
                                    cudaStream_t, void *);

@@ -123,6 +123,14 @@ template <typename T>
 void fft_nu2u_cols(void *grid, const Geometry &g, const FFTAxisPlan *ax, bool forward,
                    const double *const corfac[3], bool fft_order, void *out,
                    const int64_t *ostride, cudaStream_t st, void *work);
+// The same for kept columns col0 .. col0 + ncols - 1 only, packed in (n0, ncols)
+// cols, into an (N0, ncols) out (column x: kept column col0 + x); false when the
+// four-step column passes do not apply (n0 < 1024 or no pencil plan)
+template <typename T>
+bool fft_nu2u_cols_range(void *cols, int ncols, int col0, const Geometry &g,
+                         const FFTAxisPlan *ax, bool forward, const double *const corfac[3],
+                         bool fft_order, void *out, const int64_t *ostride, cudaStream_t st,
+                         void *work);
 
 // Type 2 head: deconvolution + zero-pad of the caller's uniform array into the
 // oversampled grid, then FFTs with input pruning.

@@ -333,6 +333,22 @@ class plan:
                                                     C.stream_of(grid, op.buf, stream=stream)))
         return op.finish()
 
+    def cols_to_uniform_range(self, *, forward, cols, col0, out=None, stream=None):
+        """Column pass, correction and crop of one block of kept columns:
+        ``cols`` (nover[0], ncols), the kept columns col0 .. col0 + ncols - 1
+        packed (transformed along axis 1; overwritten).  Returns ``out``
+        (nuni[0], ncols): column x holds uniform column (col0 + x + s) mod N1,
+        s = N1 // 2 (centred mode order) or 0 (fft_order)."""
+        import torch
+        if out is None:
+            out = torch.empty((self.grid_shape[0], cols.shape[1]), dtype=cols.dtype,
+                              device=cols.device)
+        a_c, a_o = C.describe(cols), C.describe(out)
+        C.check(C.lib().dnufft_plan_cols_to_uniform_range(
+            self._ptr, 1 if forward else 0, ctypes.byref(a_c), int(col0), ctypes.byref(a_o),
+            C.stream_of(cols, out, stream=stream)))
+        return out
+
     def info(self):
         """Kernel support, oversampled sizes etc. of this plan."""
         inf = C.PlanInfo()

@@ -188,6 +188,19 @@ int dnufft_plan_rows_fft(dnufft_plan *plan, int forward, dnufft_array *rows, voi
 int dnufft_plan_cols_to_uniform(dnufft_plan *plan, int forward, dnufft_array *grid,
                                 dnufft_array *out, void *stream);
 
+/* The column half for one block of the kept columns, so that the column pass
+ * is split over the processes too: cols is a C-contiguous device array of
+ * (nover[0], ncols) cells, the kept columns col0 .. col0 + ncols - 1 (kept
+ * column x is grid column x for x < (nuni[1]+1)/2, else nover[1] - nuni[1] +
+ * x) of every row, already transformed along axis 1 (dnufft_plan_rows_fft);
+ * it is overwritten.  out: an (nuni[0], ncols) device array that receives the
+ * corrected uniform column of each: column x of out is uniform column
+ * (col0 + x + s) mod nuni[1], with s = nuni[1]/2 in DUCC's default mode order
+ * and s = 0 with fft_order.  Needs nover[0] >= 1024 (DNUFFT_ERR_UNSUPPORTED
+ * otherwise).  src/ducc0/nufft/nufft.h:1291-1312 over a range of columns. */
+int dnufft_plan_cols_to_uniform_range(dnufft_plan *plan, int forward, dnufft_array *cols,
+                                      int64_t col0, dnufft_array *out, void *stream);
+
 /* Kernel-table row and oversampled sizes (nover[0..2], 1 beyond ndim) that
  * DUCC's parameter choice gives for a transform of npoints points; its cost
  * model depends on npoints and opts->nthreads, so processes sharing one

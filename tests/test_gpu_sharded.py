@@ -232,3 +232,33 @@ def test_rows_cols_argument_errors():
     with pytest.raises(RuntimeError, match="oversampled sizes"):
         p.cols_to_uniform(forward=True, grid=torch.zeros((n[0] - 1, n[1]), dtype=torch.complex64,
                                                          device="cuda"))
+
+
+@pytest.mark.parametrize("single,fft_order,shape", [(True, False, (600, 300)),
+                                                    (False, True, (800, 300))])
+def test_column_blocks_equal_one_piece(single, fft_order, shape):
+    """The column pass split into blocks of kept columns (the sharded column
+    pass), each block's uniform columns packed, reassembled by the documented
+    column rule, equals the one-piece column pass."""
+    import torch
+    coord, vals = _problem(2, 100_000, single, 12)
+    dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+    p = nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=1e-6 if single else 1e-11,
+                   fft_order=fft_order)
+    assert p.info()["nover"][0] >= 1024   # the four-step column passes
+    N0, N1 = shape
+    lo, hi = (N1 + 1) // 2, N1 // 2
+    for forward in (True, False):
+        g = p.spread(points=dv)
+        p.rows_fft(forward=forward, rows=g)
+        packed = torch.cat([g[:, :lo], g[:, g.shape[1] - hi:]], dim=1).contiguous()
+        ref = p.cols_to_uniform(forward=forward, grid=packed.clone()).cpu().numpy()
+        got = np.zeros(shape, ref.dtype)
+        s = 0 if fft_order else N1 // 2
+        for c0, c1 in ((0, 37), (37, 150), (150, 151), (151, N1)):
+            blk = packed[:, c0:c1].contiguous()
+            o = p.cols_to_uniform_range(forward=forward, cols=blk, col0=c0).cpu().numpy()
+            got[:, (np.arange(c0, c1) + s) % N1] = o
+        assert O.l2error(got, ref) < (1e-7 if single else 1e-15)
+    with pytest.raises(RuntimeError, match="outside the kept columns"):
+        p.cols_to_uniform_range(forward=True, cols=packed[:, :10].contiguous(), col0=N1 - 5)
