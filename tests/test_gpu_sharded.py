@@ -262,3 +262,43 @@ def test_column_blocks_equal_one_piece(single, fft_order, shape):
         assert O.l2error(got, ref) < (1e-7 if single else 1e-15)
     with pytest.raises(RuntimeError, match="outside the kept columns"):
         p.cols_to_uniform_range(forward=True, cols=packed[:, :10].contiguous(), col0=N1 - 5)
+
+
+def test_sharded_plan_row_partition_one_rank():
+    """The row-slab partition on a one-rank NCCL group: points routed to their
+    owner (itself), spread, row FFTs of the slab, the kept columns as one
+    column block through the block column pass, the block gathered; type 2
+    results routed back.  Equal to the plain plan's transforms."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    td.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                          world_size=1, timeout=datetime.timedelta(seconds=60),
+                          device_id=torch.device("cuda", torch.cuda.current_device()))
+    try:
+        shape = (600, 400)
+        coord, vals = _problem(2, 150_000, True, 13)
+        dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
+        for fo in (False, True):
+            sp = D.ShardedPlan(nu2u=True, coord=dc, grid_shape=shape, epsilon=1e-6,
+                               partition="rows", fft_order=fo)
+            assert sp.partition == "rows" and sp.nover[0] >= 1024
+            ref_p = nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=1e-6,
+                               fft_order=fo)
+            for forward in (True, False):
+                a = sp.nu2u(forward=forward, points=dv).cpu().numpy()
+                b = ref_p.nu2u(points=dv, forward=forward).cpu().numpy()
+                assert O.l2error(a, b) < 1e-6
+                g = torch.randn(shape, dtype=torch.complex64, device="cuda")
+                r2 = sp.u2nu(forward=forward, grid=g).cpu().numpy()
+                assert O.l2error(r2, ref_p.u2nu(grid=g, forward=forward).cpu().numpy()) < 1e-6
+        td.barrier()
+    finally:
+        td.destroy_process_group()

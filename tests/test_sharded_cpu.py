@@ -229,3 +229,99 @@ def test_exchange_helpers_one_rank():
         assert torch.equal(D.sum_grids(s), torch.ones(4, 3, dtype=torch.complex64))
     finally:
         td.destroy_process_group()
+
+
+def _rows_worker(rank, world, port, outdir):
+    """Row-slab partition on `gloo` ranks: points routed to their slab owners,
+    spread there (the oracle's FP64 spreading), halo rows exchanged, row FFTs
+    per slab, kept columns transposed into column blocks, each block's column
+    pass (numpy FFT + the oracle's correction factors) and the all-gather of
+    the blocks; then type-2 results routed back to the points' own ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    td.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                          world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(33)
+        M = 2600
+        coord = rng.uniform(-np.pi, np.pi, (M, 2))
+        coord[:40, 0] = np.pi * (1 - 1e-9)   # footprints across the periodic edge
+        vals = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+        cuts = np.linspace(0, M, world + 1).astype(int)
+        mine = slice(cuts[rank], cuts[rank + 1])
+        kidx, nover, total = D.global_parameters(nu2u=True, grid_shape=SHAPE,
+                                                 npoints_local=cuts[rank + 1] - cuts[rank],
+                                                 epsilon=EPS, singleprec=False, nthreads=4)
+        p = O.Params(SHAPE, EPS, False, total, True, force=(kidx, nover))
+        slabs = D.RowSlabs(nover[0], SHAPE[1], world)
+        c_mine = torch.from_numpy(coord[mine])
+        owner = slabs.owner(D.row_estimate(c_mine[:, 0], nover[0], 2 * np.pi))
+        order, send, recv, owned = D.route_points(owner, c_mine, world)
+        ovals = D.route_values(torch.from_numpy(vals[mine]), order, send, recv)
+        # every owned point's footprint stays within its owner's slab and halos
+        s0, s1 = slabs.slab(rank)
+        fold, _ = O.getpix(p, owned.numpy())
+        W = p.W
+        for i0 in fold[:, 0]:
+            rows = np.arange(i0, i0 + W) % nover[0]
+            rel = (rows - (s0 - slabs.HALO)) % nover[0]
+            assert np.all(rel < (s1 - s0) + 2 * slabs.HALO)
+        maps = O._index_maps(p, False)
+        icf0, iu0, ig0 = maps[0]
+        icf1, iu1, ig1 = maps[1]
+        N0, N1 = SHAPE
+        lo = (N1 + 1) // 2
+        rows_done = []
+
+        def spread_into(buf):
+            buf.copy_(torch.from_numpy(O.spread(p, owned.numpy(), ovals.numpy())))
+
+        def rows_fft(rows):
+            rows_done.append(rows.shape[0])
+            rows.copy_(torch.from_numpy(np.fft.fft(rows.numpy(), axis=1)))
+
+        def cols_block(cols, c0):
+            full = np.fft.fft(cols.numpy(), axis=0)
+            w = cols.shape[1]
+            out = np.zeros((N0, w), np.complex128)
+            for x in range(w):
+                xg = c0 + x
+                gx = xg if xg < lo else nover[1] - N1 + xg
+                j = int(np.nonzero(ig1 == gx)[0][0])
+                out[iu0, x] = full[ig0, x] * p.corfac[0][icf0] * p.corfac[1][icf1[j]]
+            return torch.from_numpy(out)
+
+        got = D.type1_by_row_slabs(spread_into=spread_into, rows_fft=rows_fft,
+                                   cols_block=cols_block, slabs=slabs, nover=nover,
+                                   nuni0=N0, shift=N1 // 2, dtype=torch.complex128,
+                                   device=torch.device("cpu"))
+        err = O.l2error(got.numpy(), O.nu2u(p, coord, vals, True))
+        # type 2: the owners evaluate their points, the results go back
+        grid = rng.standard_normal(SHAPE) + 1j * rng.standard_normal(SHAPE)
+        p2 = O.Params(SHAPE, EPS, False, total, False, force=(kidx, nover))
+        back = D.route_back(torch.from_numpy(O.u2nu(p2, grid, owned.numpy(), False)), order,
+                            send, recv)
+        err2 = O.l2error(back.numpy(), O.u2nu(p2, grid, coord[mine], False))
+        td.barrier()
+    finally:
+        td.destroy_process_group()
+    with open(os.path.join(outdir, "rank%d.json" % rank), "w") as f:
+        json.dump({"err": err, "err2": err2, "rows": rows_done, "nover": nover,
+                   "owned": int(owned.shape[0])}, f)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_type1_row_slab_partition(tmp_path, world):
+    import torch.multiprocessing as mp
+    mp.spawn(_rows_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    res = [json.load(open(tmp_path / ("rank%d.json" % r))) for r in range(world)]
+    n0 = res[0]["nover"][0]
+    assert sum(sum(x["rows"]) for x in res) == n0       # every row transformed once
+    assert sum(x["owned"] for x in res) == 2600          # every point owned once
+    for x in res:
+        assert x["err"] < 1e-13
+        assert x["err2"] < 1e-13
