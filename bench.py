@@ -691,6 +691,67 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line))
 
 
+def run_sharded(args, rank, world, local_rank):
+    """One transform split over the ranks (strong scaling): every rank holds
+    1/world of the bench workload's points, ShardedPlan with the row-slab
+    partition (2D) does the type 1 and type 2 of all of them."""
+    import torch
+    import torch.distributed as td
+    from ducc_b200 import distributed as D
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    m, n = args.m, args.n
+    coord, vals, grid = make_inputs(1234, m, n)
+    a, b = m * rank // world, m * (rank + 1) // world
+    d_coord = torch.from_numpy(coord[a:b]).to(dev)
+    d_vals = torch.from_numpy(vals[a:b]).to(dev)
+    d_grid = torch.from_numpy(grid).to(dev)
+    del coord, vals, grid
+    t0 = time.perf_counter()
+    sp = D.ShardedPlan(nu2u=True, coord=d_coord, grid_shape=(n, n), epsilon=EPS,
+                       nthreads=args.param_threads, spreader=args.spreaders[0],
+                       partition="rows")
+    torch.cuda.synchronize(dev)
+    plan_s = time.perf_counter() - t0
+    out = torch.empty((n, n), dtype=torch.complex64, device=dev)
+
+    def step():
+        sp.nu2u(forward=True, points=d_vals, out=out)
+        sp.u2nu(forward=False, grid=d_grid)
+
+    for _ in range(args.warmup):
+        step()
+    td.barrier()
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    td.barrier()
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    td.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dev, True)
+    if rank != 0:
+        return
+    cfg = bench_config(args)
+    cfg["parallelism"] = "one transform over %d GPUs: row-slab partition" % world
+    print(json.dumps({
+        "metric": METRIC, "value": 2 * m / (ms * 1e-3) / 1e6, "unit": "Mpts/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "c64 (f32 arithmetic)", "data": "synthetic", "config": cfg,
+        "partition": sp.partition, "plan_create_s": plan_s, "clocks": clocks,
+        "step": "ShardedPlan.nu2u (all points, result on every rank) + ShardedPlan.u2nu"}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -709,6 +770,9 @@ def main():
                     help="skip the FP64 error report (DUCC on the host)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched / autograd / 3D workloads")
+    ap.add_argument("--sharded", action="store_true",
+                    help="one transform split over the ranks (strong scaling) instead of one "
+                         "independent transform per rank")
     args = ap.parse_args()
     args.spreaders = args.spreaders.split(",")
     rank = int(os.environ.get("RANK", 0))
@@ -717,16 +781,25 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
-    if world > 1:
+    if world > 1 or args.sharded:
         import datetime
         import torch
         import torch.distributed as td
         torch.cuda.set_device(local_rank)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if world == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29531")
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                              device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.sharded:
+            run_sharded(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
-        if world > 1:
+        if world > 1 or args.sharded:
             import torch.distributed as td
             td.destroy_process_group()
 
