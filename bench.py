@@ -489,15 +489,16 @@ def kernel_rooflines(stages, spreader, info, m, n, recs, hbm, bf16, sm_mhz, peak
     ip = stages.get("u2nu (planned)/interpolation")
     if ip:
         h = pts_bytes + cells * 8
-        e = hbm_entry("u2nu (planned)/interpolation", h)
-        e["bound"] = "smem"
+        e = {"bound": "smem", "avg_launch_ms": ip,
+             "hbm_view": {"algorithmic_bytes": h, "achieved_gbs": h / (ip * 1e-3) / 1e9,
+                          "frac": h / (ip * 1e-3) / 1e9 / hbm}}
         if (n, m) == PROFILED["workload"] and sm_mhz:
             wf = PROFILED["smem_wavefronts"]["interp"]
-            e["smem_view"] = {"wavefronts_per_launch": wf,
-                              "achieved": wf / (ip * 1e-3), "peak": 148 * sm_mhz * 1e6,
-                              "unit": "wavefronts/s",
-                              "frac": wf / (ip * 1e-3) / (148 * sm_mhz * 1e6),
-                              "note": "shared-memory load wavefronts (ncu count, profiles/)"}
+            pk = 148 * sm_mhz * 1e6
+            e.update({"achieved": wf / (ip * 1e-3), "peak": pk, "unit": "wavefronts/s",
+                      "frac": wf / (ip * 1e-3) / pk, "wavefronts_per_launch": wf,
+                      "note": "shared-memory load wavefronts (ncu count, profiles/); peak "
+                              "one wavefront per SM per clock at the sampled clock"})
         out["k_interp"] = e
     return out
 
