@@ -410,6 +410,8 @@ def error_report(args, coord, vals, grid, err_idx, ours, ducc_f32):
         rep["type2"]["ducc_f32"] = l2error(ducc_f32[1][err_idx], ref2)
     if "tc" in ours and "plain" in ours:
         rep["type1_tc_over_plain"] = rep["type1"]["tc"] / rep["type1"]["plain"]
+    if "tc" in ours and "plain_matched" in ours:
+        rep["type1_tc_over_plain_matched"] = rep["type1"]["tc"] / rep["type1"]["plain_matched"]
     rep["seconds"] = time.perf_counter() - t0
     return rep
 
@@ -530,10 +532,16 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
 
     results, kept = {}, {}
-    for spreader in args.spreaders:
+    # the arms: each spreader at the requested epsilon, and the plain spreader
+    # at a looser epsilon whose error is not below the tensor-core spreader's
+    # at the requested one (the comparison at equal or lower error)
+    arms = [(sp, sp, EPS) for sp in args.spreaders]
+    if args.matched_eps > 0 and "tc" in args.spreaders:
+        arms.append(("plain_matched", "plain", args.matched_eps))
+    for spreader, kind, eps in arms:
         t0 = time.perf_counter()
-        plan = nufft.plan(nu2u=True, coord=d_coord, grid_shape=(n, n), epsilon=EPS,
-                          nthreads=args.param_threads, spreader=spreader)
+        plan = nufft.plan(nu2u=True, coord=d_coord, grid_shape=(n, n), epsilon=eps,
+                          nthreads=args.param_threads, spreader=kind)
         torch.cuda.synchronize(dev)
         plan_s = time.perf_counter() - t0
 
@@ -684,11 +692,15 @@ def run_ours(args, rank, world, local_rank):
         "errors": errors,
         "workloads": workloads,
     }
-    for other in args.spreaders[1:]:
+    for other in [k for k in results if k != head]:
         o = results[other]
         line["alt_" + other] = {"value": world * 2 * m / (o["ms"] * 1e-3) / 1e6,
                                 "ms_per_step": o["ms"], "stages_ms": _stage_ms(o["prof"]),
                                 "clocks": o["clocks"]}
+        if other == "plain_matched":
+            line["alt_" + other]["eps"] = args.matched_eps
+            line["alt_" + other]["kernel_support"] = o["info"]["supp"]
+            line["alt_" + other]["oversampled"] = o["info"]["nover"]
     print(json.dumps(line))
 
 
@@ -769,6 +781,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-errors", action="store_true",
                     help="skip the FP64 error report (DUCC on the host)")
+    ap.add_argument("--matched-eps", type=float, default=3e-6,
+                    help="also time the plain spreader at this epsilon (its error at the bench "
+                         "workload is not below the tensor-core spreader's at 1e-6); 0: skip")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched / autograd / 3D workloads")
     ap.add_argument("--sharded", action="store_true",
