@@ -53,6 +53,7 @@ EXPORTS = [
     "dnufft_batch_destroy", "dnufft_kernel_candidates", "dnufft_selftest_wait_timeout",
     "dnufft_plan_spread", "dnufft_plan_grid_to_uniform", "dnufft_find_parameters",
     "dnufft_plan_rows_fft", "dnufft_plan_cols_to_uniform", "dnufft_plan_cols_to_uniform_range",
+    "dnufft_plan_uniform_to_cols_range", "dnufft_plan_rows_fft_kept_in", "dnufft_plan_interp",
 ]
 
 
@@ -88,6 +89,10 @@ def lib():
     L.dnufft_plan_cols_to_uniform.argtypes = [vp, ctypes.c_int, P(Array), P(Array), vp]
     L.dnufft_plan_cols_to_uniform_range.argtypes = [vp, ctypes.c_int, P(Array), ctypes.c_int64,
                                                      P(Array), vp]
+    L.dnufft_plan_uniform_to_cols_range.argtypes = [vp, ctypes.c_int, P(Array), ctypes.c_int64,
+                                                     P(Array), vp]
+    L.dnufft_plan_rows_fft_kept_in.argtypes = [vp, ctypes.c_int, P(Array), vp]
+    L.dnufft_plan_interp.argtypes = [vp, P(Array), P(Array), vp]
     L.dnufft_find_parameters.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int64),
                                          ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, P(Opts), P(ctypes.c_int32),

@@ -1488,6 +1488,76 @@ static void plan_rows_fft_impl(dnufft_plan *p, int forward, dnufft_array *rows_,
   check_device_error(err, st);
 }
 
+static void plan_rows_fft_kept_in_impl(dnufft_plan *p, int forward, dnufft_array *rows_,
+                                       cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const View r = rows_view(p, rows_);
+  if (r.shape[0] == 0) return;
+  int *err = device_error_word();
+  if (p->s.calc_f64)
+    fft_u2nu_rows<double>(r.data, int(r.shape[0]), p->s.g, p->dc.ax, forward != 0, st, err);
+  else
+    fft_u2nu_rows<float>(r.data, int(r.shape[0]), p->s.g, p->dc.ax, forward != 0, st, err);
+  check_device_error(err, st);
+}
+
+static void plan_uniform_to_cols_impl(dnufft_plan *p, int forward, const dnufft_array *uni_,
+                                      int64_t col0, dnufft_array *cols_, cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  DN_REQUIRE(s.g.ndim == 2, ST_UNSUPPORTED, "row and column halves: 2D plans only");
+  const bool f64 = s.calc_f64;
+  const int dt = f64 ? DNUFFT_C128 : DNUFFT_C64;
+  View uni = view_of(uni_, "grid"), cols = view_of(cols_, "cols");
+  DN_REQUIRE(!uni.host && !cols.host, ST_BADARG, "column blocks: device arrays only");
+  DN_REQUIRE(uni.dtype == dt && cols.dtype == dt, ST_BADARG,
+             "column blocks must have the plan's data type");
+  DN_REQUIRE(uni.ndim == 2 && uni.shape[0] == s.g.nuni[0] && uni.shape[1] == s.g.nuni[1],
+             ST_BADARG, "uniform grid dimensions mismatch");
+  DN_REQUIRE(cols.ndim == 2 && cols.shape[0] == s.g.nover[0], ST_BADARG,
+             "cols must be (nover[0], ncols)");
+  const int64_t nc = cols.shape[1];
+  DN_REQUIRE(nc >= 1 && col0 >= 0 && col0 + nc <= s.g.nuni[1], ST_BADARG,
+             "column block outside the kept columns");
+  DN_REQUIRE(cols.stride[1] == 1 && cols.stride[0] == nc, ST_BADARG,
+             "cols must be C-contiguous");
+  const size_t wb = fft_work_bytes(s.g, f64 ? 16 : 8);
+  if (wb && !p->work.p) {
+    p->work = DevBuf(wb, st);
+    DN_CUDA(cudaStreamSynchronize(st));
+  }
+  const bool fo = p->o.fft_order != 0;
+  const bool ok =
+      f64 ? fft_u2nu_cols_range<double>(uni.data, uni.stride, s.g, p->dc.ax, forward != 0,
+                                        p->dc.cf, fo, cols.data, int(nc), int(col0), st,
+                                        p->work.p)
+          : fft_u2nu_cols_range<float>(uni.data, uni.stride, s.g, p->dc.ax, forward != 0,
+                                       p->dc.cf, fo, cols.data, int(nc), int(col0), st,
+                                       p->work.p);
+  DN_REQUIRE(ok, ST_UNSUPPORTED,
+             "column blocks need the four-step column passes (oversampled rows >= 1024)");
+}
+
+static void plan_interp_impl(dnufft_plan *p, const dnufft_array *grid_, dnufft_array *out_,
+                             cudaStream_t st) {
+  DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
+  const Setup &s = p->s;
+  View grid = over_grid_view(p, grid_);
+  View out = view_of(out_, "out");
+  DN_REQUIRE(!out.host, ST_BADARG, "out must be a device array");
+  DN_REQUIRE(out.dtype == grid.dtype, ST_BADARG, "out must have the plan's data type");
+  DN_REQUIRE(out.ndim == 1 && uint64_t(out.shape[0]) == s.npoints, ST_BADARG,
+             "number of points mismatch");
+  if (s.npoints == 0) return;
+  PointsDesc pts{p->sorted_coord.p, int64_t(s.g.ndim), 1, true, s.coord_f64,
+                 p->ix.perm.as<uint32_t>(), s.npoints};
+  ChunkList cl{p->ix.chunks.as<Chunk>(), p->ix.nchunks};
+  if (s.calc_f64)
+    launch_interp<double>(pts, cl, s.g, s.kpd, grid.data, 0, out.data, out.stride[0], 0, 1, st);
+  else
+    launch_interp<float>(pts, cl, s.g, s.kpf, grid.data, 0, out.data, out.stride[0], 0, 1, st);
+}
+
 static void plan_cols_to_uniform_impl(dnufft_plan *p, int forward, dnufft_array *grid_,
                                       dnufft_array *out_, cudaStream_t st) {
   DN_REQUIRE(p != nullptr, ST_BADARG, "null plan");
@@ -1880,6 +1950,23 @@ int dnufft_plan_cols_to_uniform_range(dnufft_plan *plan, int forward, dnufft_arr
                                       int64_t col0, dnufft_array *out, void *stream) {
   DN_GUARD(dnufft::plan_cols_range_impl(plan, forward, cols, col0, out,
                                         static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_uniform_to_cols_range(dnufft_plan *plan, int forward, const dnufft_array *grid,
+                                      int64_t col0, dnufft_array *cols, void *stream) {
+  DN_GUARD(dnufft::plan_uniform_to_cols_impl(plan, forward, grid, col0, cols,
+                                             static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_rows_fft_kept_in(dnufft_plan *plan, int forward, dnufft_array *rows,
+                                 void *stream) {
+  DN_GUARD(dnufft::plan_rows_fft_kept_in_impl(plan, forward, rows,
+                                              static_cast<cudaStream_t>(stream)))
+}
+
+int dnufft_plan_interp(dnufft_plan *plan, const dnufft_array *grid, dnufft_array *out,
+                       void *stream) {
+  DN_GUARD(dnufft::plan_interp_impl(plan, grid, out, static_cast<cudaStream_t>(stream)))
 }
 
 int dnufft_find_parameters(int nu2u, int ndim, const int64_t *grid_shape, uint64_t npoints,

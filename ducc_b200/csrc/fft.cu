@@ -1293,6 +1293,43 @@ bool fft_nu2u_cols_range(void *colsv, int ncols, int col0, const Geometry &g,
                         true);
 }
 
+// 2D type 2, first half for a block of kept columns: the uniform columns of
+// kept columns col0 .. col0 + ncols - 1 (with the correction factors and the
+// zero padding) are transformed along axis 0 into cols, an (n0, ncols) array
+// (column x: kept column col0 + x).  Four-step column passes only.
+template <typename T>
+bool fft_u2nu_cols_range(const void *uni, const int64_t *istride, const Geometry &g,
+                         const FFTAxisPlan *ax, bool fwd, const double *const corfac[3],
+                         bool fft_order, void *colsv, int ncols, int col0, cudaStream_t st,
+                         void *workv) {
+  cplx<T> *cols = static_cast<cplx<T> *>(colsv);
+  cplx<T> *work = static_cast<cplx<T> *>(workv);
+  const UniSpec u = mk_uni(const_cast<void *>(uni), istride, g, corfac, fft_order);
+  const int n0 = int(g.nover[0]);
+  const int N1 = int(g.nuni[1]);
+  return run_cols_v3<T>(cols, work, n0, ncols, ncols, ax[0], u, false, fwd, st, col0, N1, N1,
+                        false);
+}
+
+// 2D type 2, rows of a slab: nrows rows of n1 cells with only the kept
+// columns set on input (the middle is not read), transformed along axis 1
+// into whole rows, in place.
+template <typename T>
+void fft_u2nu_rows(void *rowsv, int nrows, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
+                   cudaStream_t st, int *err) {
+  cplx<T> *rows = static_cast<cplx<T> *>(rowsv);
+  const int n1 = int(g.nover[1]);
+  const int N1 = int(g.nuni[1]);
+  if (nrows <= 0) return;
+  if (!run_rows_v3<T>(rows, n1, nrows, n1, N1, true, false, ax[1], fwd, err, st)) {
+    static const int64_t zs[3] = {0, 0, 0};
+    const double *const nocf[3] = {nullptr, nullptr, nullptr};
+    const UniSpec u = mk_uni(nullptr, zs, g, nocf, false);
+    run_lines<T>(rows, mk_spec(n1, 1, 1, nrows, 1, n1, 0, -1, -1, 0, 0, IO_KEPT, IO_FULL), ax[1],
+                 u, fwd, st);
+  }
+}
+
 template <typename T>
 void fft_nu2u_tail(void *gridv, const Geometry &g, const FFTAxisPlan *ax, bool fwd,
                    const double *const corfac[3], bool fft_order, void *out,
@@ -1584,6 +1621,16 @@ template void fft_nu2u_tail<double>(void *, const Geometry &, const FFTAxisPlan 
 template void fft_nu2u_rows<float>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
                                    cudaStream_t, int *);
 template void fft_nu2u_rows<double>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
+                                    cudaStream_t, int *);
+template bool fft_u2nu_cols_range<float>(const void *, const int64_t *, const Geometry &,
+                                         const FFTAxisPlan *, bool, const double *const[3], bool,
+                                         void *, int, int, cudaStream_t, void *);
+template bool fft_u2nu_cols_range<double>(const void *, const int64_t *, const Geometry &,
+                                          const FFTAxisPlan *, bool, const double *const[3], bool,
+                                          void *, int, int, cudaStream_t, void *);
+template void fft_u2nu_rows<float>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
+                                   cudaStream_t, int *);
+template void fft_u2nu_rows<double>(void *, int, const Geometry &, const FFTAxisPlan *, bool,
                                     cudaStream_t, int *);
 template bool fft_nu2u_cols_range<float>(void *, int, int, const Geometry &, const FFTAxisPlan *,
                                          bool, const double *const[3], bool, void *,

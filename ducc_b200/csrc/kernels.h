@@ -132,6 +132,19 @@ bool fft_nu2u_cols_range(void *cols, int ncols, int col0, const Geometry &g,
                          bool fft_order, void *out, const int64_t *ostride, cudaStream_t st,
                          void *work);
 
+// Type 2 halves for a split transform (2D): the column pass of a block of kept
+// columns from the uniform array into an (n0, ncols) array (false when the
+// four-step column passes do not apply), and the row FFTs of a slab of rows
+// whose kept columns are set (whole rows out, in place)
+template <typename T>
+bool fft_u2nu_cols_range(const void *uni, const int64_t *istride, const Geometry &g,
+                         const FFTAxisPlan *ax, bool forward, const double *const corfac[3],
+                         bool fft_order, void *cols, int ncols, int col0, cudaStream_t st,
+                         void *work);
+template <typename T>
+void fft_u2nu_rows(void *rows, int nrows, const Geometry &g, const FFTAxisPlan *ax, bool forward,
+                   cudaStream_t st, int *err);
+
 // Type 2 head: deconvolution + zero-pad of the caller's uniform array into the
 // oversampled grid, then FFTs with input pruning.
 template <typename T>

@@ -25,8 +25,13 @@ and the ranks gather the kept columns of all rows for a column pass that every
 rank runs (``type1_by_slabs``), in 1D / 3D whole grids are summed
 (``sum_grids``).
 
-Type 2 (``ShardedPlan.u2nu``): every rank has the whole uniform grid and
-interpolates its own points; nothing crosses between ranks.
+Type 2 (``ShardedPlan.u2nu``), every rank given the whole uniform grid: with
+the row-slab partition the mirror of type 1 (the column pass of each rank's
+block of kept columns, one all-to-all into row slabs, the slab's row FFTs,
+halo rows copied from the neighbours, interpolation of the owned points, the
+results routed back); with the point partition every rank runs the whole
+transform head and interpolates its own points, nothing crossing between
+ranks.
 
 Both use the kernel and oversampled sizes that DUCC's parameter choice
 (src/ducc0/nufft/nufft.h:155-216) gives for the total number of points,
@@ -44,7 +49,8 @@ from . import nufft
 __all__ = ["global_parameters", "sum_grids", "reduce_scatter_rows", "gather_kept_columns",
            "type1_by_slabs", "RowSlabs", "row_estimate", "route_points", "route_values",
            "exchange_halos", "transpose_kept_columns", "gather_column_blocks",
-           "route_back", "type1_by_row_slabs", "ShardedPlan"]
+           "route_back", "type1_by_row_slabs", "columns_to_row_slabs", "fill_halos",
+           "type2_by_row_slabs", "ShardedPlan"]
 
 
 def _count_device(group):
@@ -343,6 +349,89 @@ def type1_by_row_slabs(*, spread_into, rows_fft, cols_block, slabs, nover, nuni0
     return gather_column_blocks(ob, slabs, shift, group)
 
 
+def columns_to_row_slabs(block, slabs, group=None):
+    """Column blocks -> rows (collective), the inverse of
+    ``transpose_kept_columns``: ``block`` is this rank's (n0, width) block of
+    kept columns; returns (slab rows, N1): this rank's rows, kept columns
+    packed."""
+    import torch
+    import torch.distributed as dist
+    world, rank = slabs.world, dist.get_rank(group)
+    c0, c1 = slabs.col_block(rank)
+    w = c1 - c0
+    src = torch.cat([torch.view_as_real(block[a:b]).reshape(-1)
+                     for a, b in (slabs.slab(k) for k in range(world))])
+    send = [(b - a) * w * 2 for a, b in (slabs.slab(k) for k in range(world))]
+    s0, s1 = slabs.slab(rank)
+    nr = s1 - s0
+    recv = [nr * (b - a) * 2 for a, b in (slabs.col_block(j) for j in range(world))]
+    dst = src.new_empty(sum(recv))
+    dist.all_to_all_single(dst, src, recv, send, group=group)
+    parts, off = [], 0
+    for j in range(world):
+        a, b = slabs.col_block(j)
+        n = nr * (b - a) * 2
+        parts.append(dst[off:off + n].reshape(nr, b - a, 2))
+        off += n
+    return torch.view_as_complex(torch.cat(parts, dim=1).contiguous())
+
+
+def fill_halos(grid, slabs, group=None):
+    """Copy the HALO rows on either side of this rank's slab from the ranks
+    that own them (collective; nothing to do on one rank): the interpolation
+    of the owned points reads them."""
+    import torch
+    import torch.distributed as dist
+    world, rank = slabs.world, dist.get_rank(group)
+    if world == 1:
+        return grid
+    H, n0 = slabs.HALO, slabs.n0
+    s0, s1 = slabs.slab(rank)
+    nxt, prv = (rank + 1) % world, (rank - 1) % world
+    if group is not None:
+        nxt, prv = dist.get_global_rank(group, nxt), dist.get_global_rank(group, prv)
+    first = torch.view_as_real(grid[s0:s0 + H]).contiguous()   # rank k - 1's rows below it
+    last = torch.view_as_real(grid[s1 - H:s1]).contiguous()    # rank k + 1's rows above it
+    from_prev = torch.empty_like(last)
+    from_next = torch.empty_like(first)
+    ops = [dist.P2POp(dist.isend, first, prv, group),
+           dist.P2POp(dist.isend, last, nxt, group),
+           dist.P2POp(dist.irecv, from_next, nxt, group),
+           dist.P2POp(dist.irecv, from_prev, prv, group)]
+    for r in dist.batch_isend_irecv(ops):
+        r.wait()
+    grid.index_copy_(0, _rows_mod(s0 - H, s0, n0, grid.device), torch.view_as_complex(from_prev))
+    grid.index_copy_(0, _rows_mod(s1, s1 + H, n0, grid.device), torch.view_as_complex(from_next))
+    return grid
+
+
+def type2_by_row_slabs(*, uniform_to_cols, rows_fft_kept_in, interp, slabs, nover, dtype,
+                       device, group=None):
+    """The row-slab type 2 with the local steps passed in: ``uniform_to_cols(
+    col0, ncols)`` returns the column pass of a block of kept columns ((n0,
+    ncols)), ``rows_fft_kept_in(rows)`` transforms rows whose kept columns
+    are set into whole rows in place, ``interp(grid)`` interpolates this
+    rank's owned points from a (n0, n1) grid whose slab and halo rows are set.
+    Collective; returns the owned points' results."""
+    import torch
+    import torch.distributed as dist
+    rank = dist.get_rank(group)
+    n0, n1 = int(nover[0]), int(nover[1])
+    c0, c1 = slabs.col_block(rank)
+    block = (uniform_to_cols(c0, c1 - c0) if c1 > c0
+             else torch.empty((n0, 0), dtype=dtype, device=device))
+    packed = columns_to_row_slabs(block, slabs, group)
+    s0, s1 = slabs.slab(rank)
+    lo, hi = (slabs.nkept + 1) // 2, slabs.nkept // 2
+    grid = torch.zeros((n0, n1), dtype=dtype, device=device)
+    grid[s0:s1, :lo] = packed[:, :lo]
+    grid[s0:s1, n1 - hi:] = packed[:, lo:]
+    if s1 > s0:
+        rows_fft_kept_in(grid[s0:s1])
+    fill_halos(grid, slabs, group)
+    return interp(grid)
+
+
 class ShardedPlan:
     """Plan of this rank's points of one transform split over the ranks of a
     process group.  Arguments as ``ducc_b200.nufft.plan``; ``coord`` holds only
@@ -444,14 +533,26 @@ class ShardedPlan:
 
     def u2nu(self, *, forward, grid, out=None):
         """Type 2 at this rank's points from the whole uniform grid.  With the
-        point partition nothing crosses between ranks; with the row partition
-        the owners interpolate and the results go back to the ranks the points
-        came from (collective)."""
+        point partition nothing crosses between ranks.  With the row partition
+        (collective) each rank runs the column pass of its block of kept
+        columns, the blocks become row slabs (one all-to-all), each rank
+        transforms its slab's rows, copies the halo rows from its neighbours,
+        interpolates its owned points, and the results go back to the ranks
+        the points came from."""
         if self.partition != "rows":
             return self.plan.u2nu(forward=forward, grid=grid, out=out)
+        import torch
         order, send, recv, _ = self.route
-        res = route_back(self.plan.u2nu(forward=forward, grid=grid), order, send, recv,
-                         self.group)
+        dtype = torch.complex128 if self.plan._f64 else torch.complex64
+        owned = type2_by_row_slabs(
+            uniform_to_cols=lambda c0, nc: self.plan.uniform_to_cols_range(
+                forward=forward, grid=grid, col0=c0, ncols=nc),
+            rows_fft_kept_in=lambda rows: self.plan.rows_fft_kept_in(forward=forward,
+                                                                     rows=rows),
+            interp=lambda g: self.plan.interp(grid=g),
+            slabs=self.slabs, nover=self.nover, dtype=dtype, device=self.device,
+            group=self.group)
+        res = route_back(owned, order, send, recv, self.group)
         if out is None:
             return res
         out.copy_(res)

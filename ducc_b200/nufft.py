@@ -349,6 +349,39 @@ class plan:
             C.stream_of(cols, out, stream=stream)))
         return out
 
+    def uniform_to_cols_range(self, *, forward, grid, col0, ncols, out=None, stream=None):
+        """Type 2 first half for one block of kept columns: correction, zero
+        padding and column FFTs of uniform columns of kept columns col0 ..
+        col0 + ncols - 1 into ``out`` (nover[0], ncols)."""
+        import torch
+        if out is None:
+            out = torch.empty((self.info()["nover"][0], int(ncols)), dtype=grid.dtype,
+                              device=grid.device)
+        a_g, a_o = C.describe(grid), C.describe(out)
+        C.check(C.lib().dnufft_plan_uniform_to_cols_range(
+            self._ptr, 1 if forward else 0, ctypes.byref(a_g), int(col0), ctypes.byref(a_o),
+            C.stream_of(grid, out, stream=stream)))
+        return out
+
+    def rows_fft_kept_in(self, *, forward, rows, stream=None):
+        """Type 2 row FFTs of a slab of rows whose kept columns are set; whole
+        rows out, in place."""
+        a_r = C.describe(rows)
+        C.check(C.lib().dnufft_plan_rows_fft_kept_in(self._ptr, 1 if forward else 0,
+                                                     ctypes.byref(a_r),
+                                                     C.stream_of(rows, stream=stream)))
+        return rows
+
+    def interp(self, *, grid, out=None, stream=None):
+        """Interpolation of the plan's points from an oversampled grid (type 2
+        second half)."""
+        if out is None:
+            out = self._alloc(grid, (self.npoints,))
+        a_g, a_o = C.describe(grid), C.describe(out)
+        C.check(C.lib().dnufft_plan_interp(self._ptr, ctypes.byref(a_g), ctypes.byref(a_o),
+                                           C.stream_of(grid, out, stream=stream)))
+        return out
+
     def info(self):
         """Kernel support, oversampled sizes etc. of this plan."""
         inf = C.PlanInfo()

@@ -201,6 +201,25 @@ int dnufft_plan_cols_to_uniform(dnufft_plan *plan, int forward, dnufft_array *gr
 int dnufft_plan_cols_to_uniform_range(dnufft_plan *plan, int forward, dnufft_array *cols,
                                       int64_t col0, dnufft_array *out, void *stream);
 
+/* The type-2 counterparts, for a type 2 split over processes by row slabs
+ * (2D): dnufft_plan_uniform_to_cols_range runs the correction, zero padding
+ * and column FFTs of one block of kept columns of the uniform array grid
+ * (device, (nuni[0], nuni[1])) into cols, an (nover[0], ncols) C-contiguous
+ * device array (column x: kept column col0 + x; needs nover[0] >= 1024);
+ * dnufft_plan_rows_fft_kept_in transforms rows (C-contiguous device (r,
+ * nover[1])) along axis 1 in place, reading only their kept columns (the
+ * first (nuni[1]+1)/2 and the last nuni[1]/2) and writing whole rows;
+ * dnufft_plan_interp interpolates the plan's points from a C-contiguous
+ * device oversampled grid (the rows their footprints reach must be set) into
+ * out (device, (M,)).  src/ducc0/nufft/nufft.h:1317-1362 (uni2nonuni) in its
+ * three stages. */
+int dnufft_plan_uniform_to_cols_range(dnufft_plan *plan, int forward, const dnufft_array *grid,
+                                      int64_t col0, dnufft_array *cols, void *stream);
+int dnufft_plan_rows_fft_kept_in(dnufft_plan *plan, int forward, dnufft_array *rows,
+                                 void *stream);
+int dnufft_plan_interp(dnufft_plan *plan, const dnufft_array *grid, dnufft_array *out,
+                       void *stream);
+
 /* Kernel-table row and oversampled sizes (nover[0..2], 1 beyond ndim) that
  * DUCC's parameter choice gives for a transform of npoints points; its cost
  * model depends on npoints and opts->nthreads, so processes sharing one

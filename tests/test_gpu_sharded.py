@@ -302,3 +302,35 @@ def test_sharded_plan_row_partition_one_rank():
         td.barrier()
     finally:
         td.destroy_process_group()
+
+
+@pytest.mark.parametrize("single,fft_order,shape", [(True, True, (600, 300)),
+                                                    (False, False, (800, 300))])
+def test_type2_halves_equal_one_piece(single, fft_order, shape):
+    """Type 2 in its three stages — column pass of blocks of kept columns from
+    the uniform array, row FFTs of slabs with only the kept columns set,
+    interpolation from the assembled grid — equals the plan's one-piece u2nu."""
+    import torch
+    coord, _ = _problem(2, 100_000, single, 14)
+    dc = torch.from_numpy(coord).cuda()
+    p = nufft.plan(nu2u=False, coord=dc, grid_shape=shape, epsilon=1e-6 if single else 1e-11,
+                   fft_order=fft_order)
+    n0, n1 = p.info()["nover"]
+    assert n0 >= 1024
+    N1 = shape[1]
+    lo, hi = (N1 + 1) // 2, N1 // 2
+    ct = torch.complex64 if single else torch.complex128
+    for forward in (True, False):
+        g = torch.randn(shape, dtype=ct, device="cuda")
+        ref = p.u2nu(grid=g, forward=forward).cpu().numpy()
+        blocks = [p.uniform_to_cols_range(forward=forward, grid=g, col0=a, ncols=b - a)
+                  for a, b in ((0, 41), (41, 150), (150, N1))]
+        packed = torch.cat(blocks, dim=1)
+        grid = torch.zeros((n0, n1), dtype=ct, device="cuda")
+        grid[:, :lo] = packed[:, :lo]
+        grid[:, n1 - hi:] = packed[:, lo:]
+        cut = n0 // 3
+        p.rows_fft_kept_in(forward=forward, rows=grid[:cut])
+        p.rows_fft_kept_in(forward=forward, rows=grid[cut:])
+        got = p.interp(grid=grid).cpu().numpy()
+        assert O.l2error(got, ref) < (1e-7 if single else 1e-14)

@@ -325,3 +325,76 @@ def test_gloo_ranks_type1_row_slab_partition(tmp_path, world):
     for x in res:
         assert x["err"] < 1e-13
         assert x["err2"] < 1e-13
+
+
+def _rows2_worker(rank, world, port, outdir):
+    """Row-slab type 2 on `gloo` ranks: column blocks of the uniform grid
+    (numpy FFT with the oracle's correction and padding), blocks to row slabs,
+    row FFTs of the slab, halo rows from the neighbours, the oracle's FP64
+    interpolation of the owned points, results routed back."""
+    import datetime
+
+    import torch
+    import torch.distributed as td
+
+    from ducc_b200 import distributed as D
+    td.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                          world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(34)
+        M = 2400
+        coord = rng.uniform(-np.pi, np.pi, (M, 2))
+        coord[:30, 0] = -np.pi * (1 - 1e-9)
+        cuts = np.linspace(0, M, world + 1).astype(int)
+        mine = slice(cuts[rank], cuts[rank + 1])
+        kidx, nover, total = D.global_parameters(nu2u=False, grid_shape=SHAPE,
+                                                 npoints_local=cuts[rank + 1] - cuts[rank],
+                                                 epsilon=EPS, singleprec=False, nthreads=4)
+        p = O.Params(SHAPE, EPS, False, total, False, force=(kidx, nover))
+        slabs = D.RowSlabs(nover[0], SHAPE[1], world)
+        c_mine = torch.from_numpy(coord[mine])
+        owner = slabs.owner(D.row_estimate(c_mine[:, 0], nover[0], 2 * np.pi))
+        order, send, recv, owned = D.route_points(owner, c_mine, world)
+        grid_u = rng.standard_normal(SHAPE) + 1j * rng.standard_normal(SHAPE)
+        # the padded, corrected oversampled grid of the uniform array (the
+        # oracle's type-2 first step) and its column FFT
+        maps = O._index_maps(p, False)
+        icf0, iu0, ig0 = maps[0]
+        icf1, iu1, ig1 = maps[1]
+        full = np.zeros(tuple(nover), np.complex128)
+        full[np.ix_(ig0, ig1)] = grid_u[np.ix_(iu0, iu1)] * np.outer(p.corfac[0][icf0],
+                                                                     p.corfac[1][icf1])
+        colfft = np.fft.fft(full, axis=0)
+        N1 = SHAPE[1]
+        lo = (N1 + 1) // 2
+
+        def uniform_to_cols(c0, nc):
+            xs = np.arange(c0, c0 + nc)
+            gx = np.where(xs < lo, xs, nover[1] - N1 + xs)
+            return torch.from_numpy(np.ascontiguousarray(colfft[:, gx]))
+
+        def rows_fft_kept_in(rows):
+            rows.copy_(torch.from_numpy(np.fft.fft(rows.numpy(), axis=1)))
+
+        def interp(g):
+            return torch.from_numpy(O.interpolate(p, g.numpy(), owned.numpy()))
+
+        res = D.type2_by_row_slabs(uniform_to_cols=uniform_to_cols,
+                                   rows_fft_kept_in=rows_fft_kept_in, interp=interp,
+                                   slabs=slabs, nover=nover, dtype=torch.complex128,
+                                   device=torch.device("cpu"))
+        back = D.route_back(res, order, send, recv)
+        err = O.l2error(back.numpy(), O.u2nu(p, grid_u, coord[mine], True))
+        td.barrier()
+    finally:
+        td.destroy_process_group()
+    with open(os.path.join(outdir, "rank%d.json" % rank), "w") as f:
+        json.dump({"err": err}, f)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_type2_row_slab_partition(tmp_path, world):
+    import torch.multiprocessing as mp
+    mp.spawn(_rows2_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    for r in range(world):
+        assert json.load(open(tmp_path / ("rank%d.json" % r)))["err"] < 1e-13
