@@ -14,6 +14,9 @@ parameter cost model).  Each case checks, as the reference does:
   vdot(nu2u, grid) within 3e-5 (single) / 2e-13 (double) of the largest norm;
 * in double precision, the same through plans.
 
+The 2D single-precision cases run once more with the split-precision
+tensor-core spreader forced (unplanned and planned), against the same bound.
+
 The reference imports ``ducc0``; here ``ducc0.nufft`` is this library's drop-in
 module and ``ducc0.misc`` the oracle's long-double vdot / l2error.  The
 reference's optional comparison against finufft is left out (finufft is not
@@ -134,3 +137,34 @@ def test_nufft_3d(nx, ny, nz, npoints, epsilon, forward, singleprec, periodicity
                   nthreads):
     run_case((nx, ny, nz), npoints, epsilon, forward, singleprec, periodicity, fft_order,
              nthreads, 1)
+
+
+@pmp("nx", [1, 20, 21, 250, 257])
+@pmp("ny", [1, 21, 32, 257])
+@pmp("npoints", (1, 37, 10))
+@pmp("epsilon", (1e-1, 3e-5))
+@pmp("forward", (True, False))
+@pmp("periodicity", ((1., 1.), 2 * np.pi))
+@pmp("fft_order", (False, True))
+def test_nufft_2d_tensor_core_spreader(nx, ny, npoints, epsilon, forward, periodicity,
+                                       fft_order):
+    """The single-precision 2D cases of the sweep with the tensor-core
+    spreader forced (the automatic choice takes it only from 0.5 points per
+    mode): the same criterion against the direct sum, unplanned and planned."""
+    shape = (nx, ny)
+    uvw, ms, dirty = case_data(shape, npoints, periodicity, True)
+    # float64 coordinates with complex64 values, as the reference's single
+    # precision cases
+    ref = direct(uvw, ms, shape, forward, periodicity, fft_order)
+    d2 = np.empty(shape, np.complex64)
+    d2 = _nufft.nu2u(points=ms, coord=uvw, forward=forward, epsilon=epsilon, out=d2,
+                     periodicity=periodicity, fft_order=fft_order,
+                     spreader="tc").astype(np.complex128)
+    assert ducc0.misc.l2error(d2, ref) <= 2 * epsilon
+    # a single-precision plan takes float32 coordinates
+    u32 = uvw.astype(np.float32)
+    ref32 = direct(u32.astype(np.float64), ms, shape, forward, periodicity, fft_order)
+    p = _nufft.plan(nu2u=True, coord=u32, grid_shape=shape, epsilon=epsilon,
+                    periodicity=periodicity, fft_order=fft_order, spreader="tc")
+    d3 = p.nu2u(points=ms, forward=forward).astype(np.complex128)
+    assert ducc0.misc.l2error(d3, ref32) <= 2 * epsilon
