@@ -801,6 +801,9 @@ def main():
         import datetime
         import torch
         import torch.distributed as td
+        # NCCL's own messages (its version line included) go to stderr, so
+        # that stdout carries the one JSON line only
+        os.environ.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
         torch.cuda.set_device(local_rank)
         if world == 1:
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
