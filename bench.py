@@ -801,17 +801,25 @@ def main():
         import datetime
         import torch
         import torch.distributed as td
-        # NCCL's own messages (its version line included) go to stderr, so
-        # that stdout carries the one JSON line only
-        os.environ.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
         torch.cuda.set_device(local_rank)
         if world == 1:
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
             os.environ.setdefault("MASTER_PORT", "29531")
             os.environ.setdefault("RANK", "0")
             os.environ.setdefault("WORLD_SIZE", "1")
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                              device_id=torch.device("cuda", local_rank))
+        # what the communicator set-up prints (NCCL's version line) goes to
+        # stderr, so that stdout carries the one JSON line only
+        sys.stdout.flush()
+        saved = os.dup(1)
+        os.dup2(2, 1)
+        try:
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                  device_id=torch.device("cuda", local_rank))
+            td.barrier()
+        finally:
+            sys.stdout.flush()
+            os.dup2(saved, 1)
+            os.close(saved)
     try:
         if args.sharded:
             run_sharded(args, rank, world, local_rank)
