@@ -144,3 +144,27 @@ def test_planned_host_groups_match_device_calls(single, spreader):
     h_pts2 = np.empty(M, vdt)
     p.u2nu(grid=dg, forward=True, out=h_pts2)
     assert O.l2error(h_pts2, p.u2nu(grid=dg, forward=True).cpu().numpy()) < tol
+
+
+def test_planned_host_groups_3d_and_ntrans():
+    """The per-group path of a host-coordinate plan in 3D, and with several
+    transforms per call (each transform through the groups), against the same
+    plan on device arrays."""
+    import torch
+    rng = np.random.default_rng(13)
+    M3, shape = 4_300_000, (40, 36, 44)
+    coord = rng.uniform(-np.pi, np.pi, (M3, 3)).astype(np.float32)
+    vals = (rng.standard_normal((2, M3)) + 1j * rng.standard_normal((2, M3))).astype(np.complex64)
+    grid = (rng.standard_normal((2,) + shape) + 1j * rng.standard_normal((2,) + shape)).astype(
+        np.complex64)
+    p = nufft.plan(nu2u=True, coord=coord, grid_shape=shape, epsilon=1e-5, periodicity=[2 * np.pi, 3.0, 5.0])
+    h = p.nu2u(points=vals, forward=True)
+    d = p.nu2u(points=torch.from_numpy(vals).cuda(), forward=True).cpu().numpy()
+    assert h.shape == (2,) + shape
+    for t in range(2):
+        assert O.l2error(h[t], d[t]) < 2e-6
+    h2 = np.empty((2, M3), np.complex64)
+    p.u2nu(grid=grid, forward=False, out=h2)
+    d2 = p.u2nu(grid=torch.from_numpy(grid).cuda(), forward=False).cpu().numpy()
+    for t in range(2):
+        assert O.l2error(h2[t], d2[t]) < 2e-6

@@ -286,12 +286,12 @@ def test_sharded_plan_row_partition_one_rank():
         shape = (600, 400)
         coord, vals = _problem(2, 150_000, True, 13)
         dc, dv = torch.from_numpy(coord).cuda(), torch.from_numpy(vals).cuda()
-        for fo in (False, True):
+        for fo, per in ((False, 2 * np.pi), (True, [3.0, 2 * np.pi])):
             sp = D.ShardedPlan(nu2u=True, coord=dc, grid_shape=shape, epsilon=1e-6,
-                               partition="rows", fft_order=fo)
+                               partition="rows", fft_order=fo, periodicity=per)
             assert sp.partition == "rows" and sp.nover[0] >= 1024
             ref_p = nufft.plan(nu2u=True, coord=dc, grid_shape=shape, epsilon=1e-6,
-                               fft_order=fo)
+                               fft_order=fo, periodicity=per)
             for forward in (True, False):
                 a = sp.nu2u(forward=forward, points=dv).cpu().numpy()
                 b = ref_p.nu2u(points=dv, forward=forward).cpu().numpy()
