@@ -679,7 +679,7 @@ static void do_fft_interp(const Setup &s, const DevConst &dc, const PointsDesc &
   tm.mark("interpolation");
   const KernelPoly<T> &kp = *reinterpret_cast<const KernelPoly<T> *>(
       sizeof(T) == 4 ? static_cast<const void *>(&s.kpf) : static_cast<const void *>(&s.kpd));
-  launch_interp<T>(pts, cl, s.g, kp, grid.p, 0, out.data, out.stride[0], 0, 1, st);
+  launch_interp<T>(pts, cl, s.g, kp, grid.p, 0, out.data, out.stride[0], 0, 1, st, err);
   tm.mark("output copy");
   check_device_error(err, st);
 }
@@ -901,7 +901,7 @@ static void u2nu_pipelined(const Setup &s, const View &uni, const View &coord, c
     ChunkList cl{ix.chunks.as<Chunk>(), ix.nchunks};
     launch_interp<T>(pts, cl, s.g, kp, grid.p, 0,
                      static_cast<char *>(ov.data) + a * size_t(ov.stride[0]) * vb, ov.stride[0], 0,
-                     1, st);
+                     1, st, err);
     if (out.host) {
       // the finished range goes back while the next groups are interpolated
       DN_CUDA(cudaEventRecord(done.ev[gi], st));
@@ -1240,7 +1240,7 @@ static void plan_u2nu_groups(dnufft_plan *p, const View &uni, const View &out, b
     const PlanGroup &pg = p->groups[size_t(gi)];
     const ChunkList cl{pg.ix.chunks.as<Chunk>(), pg.ix.nchunks};
     launch_interp<T>(group_points(p, pg), cl, s.g, kp, p->grid.p, 0,
-                     static_cast<char *>(dout.p) + pg.a * vb, 1, 0, 1, st);
+                     static_cast<char *>(dout.p) + pg.a * vb, 1, 0, 1, st, err);
     DN_CUDA(cudaEventRecord(done.ev[size_t(gi)], st));
     DN_CUDA(cudaStreamWaitEvent(down.s, done.ev[size_t(gi)], 0));
     DN_CUDA(cudaMemcpyAsync(static_cast<char *>(out.data) + pg.a * vb,

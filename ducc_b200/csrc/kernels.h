@@ -57,10 +57,13 @@ void launch_spread(const PointsDesc &pts, const ChunkList &cl, const Geometry &g
                    int64_t vtrans, void *grid, int64_t gtrans, int ntrans,
                    cudaStream_t st);
 
+// err: device error word; with it, 2D single-transform tiles inside the grid
+// are staged by TMA (a copy that never completes sets the word)
 template <typename T>
 void launch_interp(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
                    const KernelPoly<T> &kp, const void *grid, int64_t gtrans,
-                   void *out, int64_t os, int64_t otrans, int ntrans, cudaStream_t st);
+                   void *out, int64_t os, int64_t otrans, int ntrans, cudaStream_t st,
+                   int *err = nullptr);
 
 // grad[j*gs0 + d*gs1] = Re(conj(wts[j*ws]) * d/dx_{j,d} interp(grid)(x_j)), in
 // the coordinates' dtype (interp_grad.cu)

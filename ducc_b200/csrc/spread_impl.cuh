@@ -10,11 +10,17 @@
 // flushed once with vectorised global atomics at wrapped grid positions.
 // Interpolation: the tile plus halo is staged in shared memory and every thread
 // evaluates one point (weights in registers, W^d multiply-adds), writing the
-// result through the tile permutation.
+// result through the tile permutation.  In 2D a tile that lies inside the grid
+// (no periodic wrap) arrives by one TMA tensor copy (cp.async.bulk.tensor.2d,
+// issued by one thread, completion on an mbarrier) while the CTA folds and
+// orders its first batch of points; tiles at the grid edges are loaded by all
+// threads with the wrap.
 //
 // Mirrors HelperNu2u / spreading_helper and HelperU2nu / interpolation_helper
 // (src/ducc0/nufft/nufft.h:917-1272 for 2D, :1391-1729 for 3D, :526-834 for 1D).
 #pragma once
+
+#include <cuda.h>   // CUtensorMap (the map is encoded through the runtime's driver entry point)
 
 #include "common.cuh"
 #include "kernels.h"
@@ -237,12 +243,45 @@ template <typename T> struct InterpOrder {
   static constexpr size_t bytes(int ndim) { return NSLOT * 4 + IB * (8 + ndim * sizeof(T)); }
 };
 
+// Row pitch (cells) of a 2D tile staged by a TMA copy: the copy starts at an
+// even grid column (16-byte aligned for complex64), one column before the tile
+// when the halo width nsafe is odd, and spans an even number of columns.
+__host__ __device__ constexpr int tma_tile_pitch(int S, int nsafe) {
+  return (S + (nsafe & 1) + 1) & ~1;
+}
+
+__device__ __forceinline__ bool tile_bar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t addr = static_cast<uint32_t>(__cvta_generic_to_shared(bar));
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity), "r"(1000u)
+        : "memory");
+    if (ok) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (it == 0) t0 = t;
+    else if (t - t0 > 1000000000ull) return false;   // one second
+  }
+}
+
+// One chunk of one transform (the body of k_interp; also used by the
+// multi-instance kernel of batched transforms, which passes no tensor map).
+// tmap: 2D tensor map of the grid (rows x 2*columns scalars) with box
+// (2*tpitch, S); tbar: an mbarrier in shared memory; err: device error word.
 template <typename T, typename Tc, int NDIM, int W>
 __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk ch, const Geometry &g,
                                              const KernelPoly<T> &kp,
                                              const cplx<T> *__restrict__ grid,
                                              cplx<T> *__restrict__ out, int64_t os,
-                                             unsigned char *smraw) {
+                                             unsigned char *smraw,
+                                             const CUtensorMap *tmap = nullptr, int tpitch = 0,
+                                             uint64_t *tbar = nullptr, int *err = nullptr) {
   constexpr bool SMEM = BufferLayout<T>::smem(NDIM);
   const int S = (1 << g.log2tile) + W;
   int ncell = S;
@@ -251,7 +290,41 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
   int b0[NDIM];
   tile_origin<NDIM>(ch.tile, g, b0);
   cplx<T> *buf = reinterpret_cast<cplx<T> *>(smraw);
-  if constexpr (SMEM) {
+  // staged tile: row pitch (cells) and column of the tile's first cell
+  int pitch = S, sh = 0;
+  bool tma = false;
+  size_t tile_bytes = size_t(ncell) * sizeof(cplx<T>);
+  if constexpr (NDIM == 2 && SMEM) {
+    if (tmap) {
+      tile_bytes = size_t(tpitch) * size_t(S) * sizeof(cplx<T>);
+      const int v0 = b0[1] & ~1;   // even start column (also for negative origins)
+      tma = b0[0] >= 0 && b0[0] + S <= int(g.nover[0]) && v0 >= 0 &&
+            v0 + tpitch <= int(g.nover[1]);
+      if (tma) {
+        pitch = tpitch;
+        sh = b0[1] - v0;
+        if (threadIdx.x == 0) {
+          const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(tbar));
+          asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+          asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(tbar));
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                       "r"(uint32_t(tile_bytes))
+                       : "memory");
+          asm volatile(
+              "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+              " [%0], [%1, {%2, %3}], [%4];"
+              ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(buf))),
+                "l"(reinterpret_cast<uint64_t>(tmap)), "r"(2 * v0), "r"(b0[0]), "r"(bar)
+              : "memory");
+        }
+      }
+    }
+  }
+  if (SMEM && !tma) {
     // tile + halo, LB loads in flight per thread before their stores
     // cell -> grid index by multiply-high division and division-free wrap
     constexpr int LB = 8;
@@ -382,7 +455,7 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
     // in a fixed order, so results do not depend on the assignment.
     using IO = InterpOrder<T>;
     constexpr int NSLOT = IO::NSLOT, IB = IO::IB, PER = IB / SP_THREADS;
-    int *s_cnt = reinterpret_cast<int *>(smraw + size_t(ncell) * sizeof(cplx<T>));
+    int *s_cnt = reinterpret_cast<int *>(smraw + tile_bytes);
     uint32_t *r_j = reinterpret_cast<uint32_t *>(s_cnt + NSLOT);
     int *r_base = reinterpret_cast<int *>(r_j + IB);
     T *r_t = reinterpret_cast<T *>(r_base + IB);   // [NDIM][IB]
@@ -410,7 +483,7 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
             double frac;
             fold<Tc>(x[d], g.coordfct[d], int(g.nover[d]), g.shift[d], g.maxi0[d], i0, frac);
             pt[k][d] = T(double(W - 1) - 2.0 * frac);
-            base = base * S + (i0 - b0[d]);
+            base = (d == NDIM - 1) ? base * pitch + (i0 - b0[d] + sh) : base * S + (i0 - b0[d]);
           }
           pb[k] = base;
           atomicAdd(&s_cnt[base & (NSLOT - 1)], 1);
@@ -442,6 +515,14 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
         }
       }
       __syncthreads();
+      if (tma && s0 == ch.start) {
+        // the tile copy has been in flight while the first batch was ordered
+        const bool ok = tile_bar_wait(tbar, 0u);
+        if (__syncthreads_or(ok ? 0 : 1)) {
+          if (threadIdx.x == 0 && err) atomicExch(err, 1);
+          return;
+        }
+      }
       const int pl = (lane % NSLOT) * (32 / NSLOT) + lane / NSLOT;
       for (int r = warp; r < q; r += SP_WARPS) {
         if (pl * q + r >= nb) continue;
@@ -462,7 +543,7 @@ __device__ __forceinline__ void interp_chunk(const PointsDesc &pts, const Chunk 
         } else if constexpr (NDIM == 2) {
 #pragma unroll
           for (int a = 0; a < W; ++a) {
-            const cplx<T> *row = p0 + a * S;
+            const cplx<T> *row = p0 + a * pitch;
             T rr = 0, ri = 0;
 #pragma unroll
             for (int b = 0; b < W; ++b) {
@@ -506,14 +587,19 @@ template <typename T, int NDIM> constexpr int interp_min_ctas() {
   return (sizeof(T) == 4 && NDIM < 3) ? 6 : 1;
 }
 
+// tpitch > 0: 2D tiles inside the grid are staged by TMA through tmap (one
+// transform); err: device error word for a tile copy that never completes
 template <typename T, typename Tc, int NDIM, int W>
 __global__ void __launch_bounds__(SP_THREADS, interp_min_ctas<T, NDIM>())
     k_interp(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
              const cplx<T> *__restrict__ grid, int64_t gtrans, cplx<T> *__restrict__ out,
-             int64_t os, int64_t otrans) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+             int64_t os, int64_t otrans, const __grid_constant__ CUtensorMap tmap, int tpitch,
+             int *err) {
+  extern __shared__ __align__(128) unsigned char smraw_tile[];
+  __shared__ uint64_t tbar;
   interp_chunk<T, Tc, NDIM, W>(pts, chunks[blockIdx.x], g, kp, grid + int64_t(blockIdx.y) * gtrans,
-                               out + int64_t(blockIdx.y) * otrans, os, smraw);
+                               out + int64_t(blockIdx.y) * otrans, os, smraw_tile,
+                               tpitch > 0 ? &tmap : nullptr, tpitch, &tbar, err);
 }
 
 template <typename T, int NDIM, int W>
@@ -528,13 +614,22 @@ size_t spread_smem_bytes(const Geometry &g) {
   return buf + stage;
 }
 
+// tpitch > 0: the staged 2D tile has that row pitch (TMA staging)
 template <typename T, int NDIM, int W>
-size_t interp_smem_bytes(const Geometry &g) {
+size_t interp_smem_bytes(const Geometry &g, int tpitch = 0) {
   int S = (1 << g.log2tile) + W;
   size_t ncell = size_t(S);
   for (int d = 1; d < NDIM; ++d) ncell *= size_t(S);
+  if (NDIM == 2 && tpitch > 0) ncell = size_t(tpitch) * size_t(S);
   return BufferLayout<T>::smem(NDIM) ? ncell * sizeof(cplx<T>) + InterpOrder<T>::bytes(NDIM) : 0;
 }
+
+// 2D tensor map of a contiguous complex grid (nover[0] rows of nover[1]
+// cells) as rows of 2*nover[1] scalars, box (2*tpitch, S); false where the
+// encoder is unavailable or the grid does not meet the copy's alignment rules
+// (16-byte base address and row pitch)
+bool encode_tile_map(CUtensorMap *map, const void *grid, bool f64, int64_t n0, int64_t n1,
+                     int tpitch, int S);
 
 template <typename T, typename Tc, int NDIM, int W>
 void spread_w(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
@@ -552,13 +647,24 @@ void spread_w(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
 template <typename T, typename Tc, int NDIM, int W>
 void interp_w(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
               const KernelPoly<T> &kp, const void *grid, int64_t gtrans, void *out, int64_t os,
-              int64_t otrans, int ntrans, cudaStream_t st) {
-  size_t sm = interp_smem_bytes<T, NDIM, W>(g);
+              int64_t otrans, int ntrans, cudaStream_t st, int *err) {
+  CUtensorMap map;
+  memset(&map, 0, sizeof(map));
+  int tpitch = 0;
+  if constexpr (NDIM == 2 && BufferLayout<T>::smem(NDIM)) {
+    const int S = (1 << g.log2tile) + W;
+    const int tp = tma_tile_pitch(S, g.nsafe);
+    if (err && ntrans == 1 &&
+        encode_tile_map(&map, grid, sizeof(T) == 8, g.nover[0], g.nover[1], tp, S))
+      tpitch = tp;
+  }
+  size_t sm = interp_smem_bytes<T, NDIM, W>(g, tpitch);
   auto kern = k_interp<T, Tc, NDIM, W>;
   DN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   dim3 grd(cl.nchunks, ntrans);
   kern<<<grd, SP_THREADS, sm, st>>>(pts, cl.chunks, g, kp, static_cast<const cplx<T> *>(grid),
-                                    gtrans, static_cast<cplx<T> *>(out), os, otrans);
+                                    gtrans, static_cast<cplx<T> *>(out), os, otrans, map, tpitch,
+                                    err);
   DN_LAUNCHED();
 }
 
@@ -585,9 +691,9 @@ void spread_dispatch(const PointsDesc &pts, const ChunkList &cl, const Geometry 
 template <typename T, typename Tc, int NDIM>
 void interp_dispatch(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
                      const KernelPoly<T> &kp, const void *grid, int64_t gtrans, void *out,
-                     int64_t os, int64_t otrans, int ntrans, cudaStream_t st) {
+                     int64_t os, int64_t otrans, int ntrans, cudaStream_t st, int *err) {
 #define DN_CASE(WW) \
-  case WW: interp_w<T, Tc, NDIM, WW>(pts, cl, g, kp, grid, gtrans, out, os, otrans, ntrans, st); return;
+  case WW: interp_w<T, Tc, NDIM, WW>(pts, cl, g, kp, grid, gtrans, out, os, otrans, ntrans, st, err); return;
   if constexpr (sizeof(T) == 4) {
     switch (g.W) { DN_FOR_W_FLOAT(DN_CASE) }
   } else {
@@ -615,9 +721,9 @@ void launch_spread_impl(const PointsDesc &pts, const ChunkList &cl, const Geomet
 template <typename T>
 void launch_interp_impl(const PointsDesc &pts, const ChunkList &cl, const Geometry &g,
                         const KernelPoly<T> &kp, const void *grid, int64_t gtrans, void *out,
-                        int64_t os, int64_t otrans, int ntrans, cudaStream_t st) {
+                        int64_t os, int64_t otrans, int ntrans, cudaStream_t st, int *err) {
   if (cl.nchunks == 0 || ntrans == 0) return;
-#define DN_ID(TC, ND) interp_dispatch<T, TC, ND>(pts, cl, g, kp, grid, gtrans, out, os, otrans, ntrans, st)
+#define DN_ID(TC, ND) interp_dispatch<T, TC, ND>(pts, cl, g, kp, grid, gtrans, out, os, otrans, ntrans, st, err)
   if (pts.coord_f64) {
     if (g.ndim == 1) DN_ID(double, 1); else if (g.ndim == 2) DN_ID(double, 2); else DN_ID(double, 3);
   } else {
