@@ -13,7 +13,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libducc_b200.so")
 
-F32, F64, C64, C128 = 1, 2, 3, 4
+F32, F64, C64, C128, U8 = 1, 2, 3, 4, 5
 SPREAD = {"auto": 0, "plain": 1, "tc": 2}
 
 
@@ -41,6 +41,24 @@ class PlanInfo(ctypes.Structure):
                 ("tc_records", ctypes.c_int64)]
 
 
+class WgridOpts(ctypes.Structure):
+    _fields_ = [("nthreads", ctypes.c_size_t), ("sigma_min", ctypes.c_double),
+                ("sigma_max", ctypes.c_double), ("center_x", ctypes.c_double),
+                ("center_y", ctypes.c_double), ("do_wgridding", ctypes.c_int32),
+                ("flip_u", ctypes.c_int32), ("flip_v", ctypes.c_int32),
+                ("flip_w", ctypes.c_int32), ("divide_by_n", ctypes.c_int32),
+                ("allow_nshift", ctypes.c_int32),
+                ("double_precision_accumulation", ctypes.c_int32),
+                ("verbosity", ctypes.c_int32)]
+
+
+class WgridInfo(ctypes.Structure):
+    _fields_ = [("kernel_index", ctypes.c_int32), ("supp", ctypes.c_int32),
+                ("nu", ctypes.c_int64), ("nv", ctypes.c_int64), ("nplanes", ctypes.c_int64),
+                ("dw", ctypes.c_double), ("wmin", ctypes.c_double), ("nshift", ctypes.c_double),
+                ("nvis", ctypes.c_int64)]
+
+
 _lib = None
 
 EXPORTS = [
@@ -54,6 +72,7 @@ EXPORTS = [
     "dnufft_plan_spread", "dnufft_plan_grid_to_uniform", "dnufft_find_parameters",
     "dnufft_plan_rows_fft", "dnufft_plan_cols_to_uniform", "dnufft_plan_cols_to_uniform_range",
     "dnufft_plan_uniform_to_cols_range", "dnufft_plan_rows_fft_kept_in", "dnufft_plan_interp",
+    "dnufft_wgrid_default_opts", "dnufft_vis2dirty", "dnufft_dirty2vis", "dnufft_wgrid_params",
 ]
 
 
@@ -114,6 +133,15 @@ def lib():
     L.dnufft_profile_enable.restype = None
     L.dnufft_profile_json.restype = ctypes.c_char_p
     L.dnufft_selftest_wait_timeout.argtypes = [ctypes.c_int64, vp]
+    L.dnufft_wgrid_default_opts.argtypes = [P(WgridOpts)]
+    L.dnufft_wgrid_default_opts.restype = None
+    for f in (L.dnufft_vis2dirty, L.dnufft_dirty2vis):
+        f.argtypes = [P(Array), P(Array), P(Array), P(Array), P(Array), ctypes.c_double,
+                      ctypes.c_double, ctypes.c_double, P(WgridOpts), P(Array), vp]
+    L.dnufft_wgrid_params.argtypes = [P(Array), P(Array), P(Array), P(Array), P(Array),
+                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                      P(WgridOpts), P(WgridInfo), vp]
     _lib = L
     return L
 
@@ -137,7 +165,7 @@ def is_torch(x):
 def torch_code(t):
     import torch
     return {torch.float32: F32, torch.float64: F64, torch.complex64: C64,
-            torch.complex128: C128}.get(t.dtype)
+            torch.complex128: C128, torch.uint8: U8}.get(t.dtype)
 
 
 def dtype_code(x):

@@ -34,6 +34,8 @@ struct Error : public std::runtime_error {
   do { if (!(cond)) throw ::dnufft::Error((code), (msg)); } while (0)
 
 void cuda_check(cudaError_t e, const char *what);
+// the message dnufft_last_error() returns on this host thread
+void set_last_error(const char *msg);
 #define DN_CUDA(call) ::dnufft::cuda_check((call), #call)
 
 // number of kernels this library launched (diagnostics)
@@ -70,6 +72,10 @@ size_t effective_threads(size_t nthreads);
 std::vector<double> kernel_coeffs(int W, double beta_scaled, double e0);
 std::vector<double> correction_factors(size_t n, double dx, int W, double beta_scaled,
                                        double e0);
+// the quadrature of the correction function 1 / sum_k wpsi[k] cos(pi W x[k] v)
+// (positive Gauss-Legendre nodes x, weights times the kernel, doubled)
+void correction_nodes(int W, double beta_scaled, double e0, std::vector<double> &x,
+                      std::vector<double> &wpsi);
 std::vector<int> fft_factors(int n);
 
 // ---------------------------------------------------------------- device params

@@ -222,12 +222,18 @@ static void gauss_legendre_half(int m, std::vector<double> &x, std::vector<doubl
   }
 }
 
-std::vector<double> correction_factors(size_t n, double dx, int W, double beta, double e0) {
+void correction_nodes(int W, double beta, double e0, std::vector<double> &x,
+                      std::vector<double> &wpsi) {
   int p = int(1.5 * W) + 2;
-  std::vector<double> x, w;
+  std::vector<double> w;
   gauss_legendre_half(2 * p, x, w);   // 2p nodes: p positive ones
-  std::vector<double> wpsi(x.size());
+  wpsi.resize(x.size());
   for (size_t i = 0; i < x.size(); ++i) wpsi[i] = 2 * w[i] * es_kernel(x[i], beta, e0) * W * 0.5;
+}
+
+std::vector<double> correction_factors(size_t n, double dx, int W, double beta, double e0) {
+  std::vector<double> x, wpsi;
+  correction_nodes(W, beta, e0, x, wpsi);
   std::vector<double> res(n);
   for (size_t i = 0; i < n; ++i) {
     double v = double(i) * dx, s = 0;

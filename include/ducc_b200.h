@@ -40,6 +40,7 @@ extern "C" {
 #define DNUFFT_F64 2
 #define DNUFFT_C64 3
 #define DNUFFT_C128 4
+#define DNUFFT_U8 5    /* masks of the w-gridder                                 */
 
 /* spreader selection (type 1) */
 /* AUTO: the tensor-core form for 2D complex64 type 1 with at least 0.5 points
@@ -292,6 +293,68 @@ int dnufft_batch_destroy(dnufft_batch *batch);
 int dnufft_kernel_candidates(int ndim, const int64_t *shape, int singleprec, double epsilon,
                              double sigma_min, double sigma_max, int max, int32_t *kernel_index,
                              int32_t *supp, double *ofactor, int64_t *nover, int *count);
+
+/* ------------------------------------------------------------ w-gridder
+ * Radio-interferometric gridding with w-stacking on top of the 2D transforms,
+ * the counterpart of ducc0.wgridder (python/wgridder_pymod.cc:612-656:
+ * vis2dirty / dirty2vis, and ms2dirty / dirty2ms, which are these with the
+ * default options).  Definitions (src/ducc0/wgridder/wgridder.h): for pixel
+ * (i, j), x = center_x + (i - nx/2) pixsize_x, y = center_y + (j - ny/2)
+ * pixsize_y, n = sqrt(1 - x^2 - y^2), and visibility k at (u, v, w) = uvw *
+ * freq / c (flipped per axis on request):
+ *   vis2dirty: dirty(i,j) = sum_k Re(vis_k wgt_k e^{2 pi i (x u + y v - w (n-1))}) / n
+ *   dirty2vis: vis_k = wgt_k sum_ij dirty(i,j) / n e^{-2 pi i (x u + y v - w (n-1))}
+ * (the w term and the division by n with do_wgridding only; division by n on
+ * request), to the requested epsilon.  A visibility takes part where
+ * |vis|^2 * wgt * mask != 0 (vis2dirty) or wgt * mask != 0 (dirty2vis; the
+ * others are set to zero).  Every array is a device array: uvw (nrows, 3) f64,
+ * freq (nchan) f64, vis (nrows, nchan) c64/c128, wgt (nrows, nchan) real of
+ * the same precision or NULL, mask (nrows, nchan) DNUFFT_U8 or NULL, dirty
+ * (nx, ny) real (nx, ny even).  Error behaviour as in the rest of this header
+ * (DUCC raises the same conditions as exceptions). */
+typedef struct dnufft_wgrid_opts {
+  size_t nthreads;        /* as in DUCC; only feeds its parameter cost model      */
+  double sigma_min;       /* oversampling factor range (DUCC: 1.1 .. 2.6)        */
+  double sigma_max;
+  double center_x;        /* image centre relative to the phase centre           */
+  double center_y;
+  int32_t do_wgridding;   /* 1: w-stacking with the w term; 0: w taken as zero   */
+  int32_t flip_u, flip_v, flip_w;
+  int32_t divide_by_n;    /* DUCC's default 1                                    */
+  int32_t allow_nshift;   /* DUCC's default 1: centre the w-screen phases        */
+  int32_t double_precision_accumulation;   /* single-precision data, double grids */
+  int32_t verbosity;      /* 1: print the chosen parameters                      */
+} dnufft_wgrid_opts;
+
+/* DUCC's keyword defaults of vis2dirty / dirty2vis. */
+void dnufft_wgrid_default_opts(dnufft_wgrid_opts *opts);
+
+int dnufft_vis2dirty(const dnufft_array *uvw, const dnufft_array *freq, const dnufft_array *vis,
+                     const dnufft_array *wgt, const dnufft_array *mask, double pixsize_x,
+                     double pixsize_y, double epsilon, const dnufft_wgrid_opts *opts,
+                     dnufft_array *dirty, void *stream);
+int dnufft_dirty2vis(const dnufft_array *uvw, const dnufft_array *freq, const dnufft_array *dirty,
+                     const dnufft_array *wgt, const dnufft_array *mask, double pixsize_x,
+                     double pixsize_y, double epsilon, const dnufft_wgrid_opts *opts,
+                     dnufft_array *vis, void *stream);
+
+/* The parameters the two calls above choose for these inputs (DUCC's
+ * getNuNv / countRanges, wgridder.h:1499-1579, :675-692): kernel table row,
+ * support, oversampled grid, w planes (count, spacing, first plane's w), the
+ * w-screen shift and the number of visibilities taking part.  gridding: 1 for
+ * vis2dirty (vis is read), 0 for dirty2vis (vis may be NULL). */
+typedef struct dnufft_wgrid_info {
+  int32_t kernel_index;
+  int32_t supp;
+  int64_t nu, nv;
+  int64_t nplanes;
+  double dw, wmin, nshift;
+  int64_t nvis;
+} dnufft_wgrid_info;
+int dnufft_wgrid_params(const dnufft_array *uvw, const dnufft_array *freq, const dnufft_array *vis,
+                        const dnufft_array *wgt, const dnufft_array *mask, int64_t nx, int64_t ny,
+                        double pixsize_x, double pixsize_y, double epsilon, int gridding,
+                        const dnufft_wgrid_opts *opts, dnufft_wgrid_info *info, void *stream);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *dnufft_last_error(void);

@@ -1,5 +1,6 @@
-// Test-infrastructure only: a Python module that compiles DUCC's own NUFFT
-// binding (python/nufft_pymod.cc) from the reference sources where they lie,
+// Test-infrastructure only: a Python module that compiles DUCC's own NUFFT and
+// w-gridder bindings (python/nufft_pymod.cc, python/wgridder_pymod.cc) from the
+// reference sources where they lie,
 // plus a few read-only probes that expose DUCC's internal index computation
 // (getpix, tile keys, the stable bucket-sort permutation), its kernel choice,
 // its piecewise-polynomial kernel coefficients and its correction factors.
@@ -27,6 +28,7 @@
 #include "ducc0/infra/mav.cc"
 #include "ducc0/math/gl_integrator.cc"
 #include "ducc0/math/gridding_kernel.cc"
+#include "ducc0/wgridder/wgridder.cc"
 
 #include <pybind11/pybind11.h>
 #include <pybind11/numpy.h>
@@ -34,6 +36,7 @@
 #include "ducc0/fft/fft1d_impl.h"
 #include "ducc0/fft/fftnd_impl.h"
 #include "python/nufft_pymod.cc"
+#include "python/wgridder_pymod.cc"
 
 namespace py = pybind11;
 using namespace ducc0;
@@ -206,6 +209,7 @@ PYBIND11_MODULE(MODNAME, m)
   {
   using namespace pybind11::literals;
   add_nufft(m);
+  add_wgridder(m);
   m.def("index_probe", &probe::index_probe, py::kw_only(), "coord"_a,
         "shape"_a, "epsilon"_a, "singleprec"_a, "gridding"_a, "nthreads"_a=1,
         "sigma_min"_a=1.2, "sigma_max"_a=2.51, "periodicity"_a,
