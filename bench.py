@@ -352,6 +352,90 @@ def workload_3d(dev, steps=3, warmup=1, seed=9):
     return out
 
 
+WG_NPIX, WG_NROW, WG_NCHAN, WG_EPS = 4096, 500_000, 16, 1e-5
+
+
+def wgridder_inputs(seed=11):
+    """Synthetic measurement set for the w-gridder workload: 500k rows x 16
+    channels (8e6 visibilities, 1.0-1.45 GHz), baselines filling the uv plane of
+    a 4096^2 image at 2 degrees field of view (|u|, |v| up to ~0.45 / pixel size
+    at the top channel), w up to a third of that; complex64 visibilities,
+    float32 weights, a 4096^2 float32 image for the degridding direction."""
+    rng = np.random.default_rng(seed)
+    ps = 2.0 * np.pi / 180 / WG_NPIX
+    freq = 1.0e9 + np.arange(WG_NCHAN) * (0.45e9 / WG_NCHAN)
+    umax = 0.45 / ps * 299792458. / freq[-1]
+    r = umax * np.sqrt(rng.random(WG_NROW))
+    phi = rng.uniform(0, 2 * np.pi, WG_NROW)
+    uvw = np.stack([r * np.cos(phi), r * np.sin(phi),
+                    rng.uniform(-umax / 3, umax / 3, WG_NROW)], 1)
+    vis = (rng.standard_normal((WG_NROW, WG_NCHAN))
+           + 1j * rng.standard_normal((WG_NROW, WG_NCHAN))).astype(np.complex64)
+    wgt = rng.uniform(0.5, 1.5, (WG_NROW, WG_NCHAN)).astype(np.float32)
+    dirty = rng.standard_normal((WG_NPIX, WG_NPIX)).astype(np.float32)
+    return ps, freq, uvw, vis, wgt, dirty
+
+
+def workload_wgridder(dev, steps=3, warmup=1):
+    """w-gridder (ducc0.wgridder counterpart): vis2dirty and dirty2vis with
+    w-stacking at eps 1e-5 on the synthetic set above, device-resident."""
+    import torch
+    from ducc_b200 import wgridder as WG
+    ps, freq, uvw, vis, wgt, dirty = wgridder_inputs()
+    d_uvw = torch.from_numpy(uvw).to(dev)
+    d_freq = torch.from_numpy(freq).to(dev)
+    d_vis = torch.from_numpy(vis).to(dev)
+    d_wgt = torch.from_numpy(wgt).to(dev)
+    d_dirty = torch.from_numpy(dirty).to(dev)
+    out_dirty = torch.empty((WG_NPIX, WG_NPIX), dtype=torch.float32, device=dev)
+    out_vis = torch.empty((WG_NROW, WG_NCHAN), dtype=torch.complex64, device=dev)
+    kw = dict(uvw=d_uvw, freq=d_freq, wgt=d_wgt, pixsize_x=ps, pixsize_y=ps, epsilon=WG_EPS,
+              do_wgridding=True, nthreads=16)
+    out = {}
+    for name, call in (
+            ("vis2dirty", lambda: WG.vis2dirty(vis=d_vis, dirty=out_dirty, **kw)),
+            ("dirty2vis", lambda: WG.dirty2vis(dirty=d_dirty, vis=out_vis, **kw))):
+        for _ in range(warmup):
+            call()
+        torch.cuda.synchronize(dev)
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            call()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms": ms, "mvis_per_s": WG_NROW * WG_NCHAN / (ms * 1e-3) / 1e6}
+    prm = WG.wgrid_params(uvw=d_uvw, freq=d_freq, vis=d_vis, wgt=d_wgt, npix_x=WG_NPIX,
+                          npix_y=WG_NPIX, pixsize_x=ps, pixsize_y=ps, epsilon=WG_EPS,
+                          do_wgridding=True, nthreads=16)
+    out["parameters"] = {k: prm[k] for k in ("supp", "nu", "nv", "nplanes")}
+    out["config"] = ("w-gridder, %d rows x %d channels (complex64), %d^2 image at 2 deg, "
+                     "w-stacking, eps %g; device-resident vis2dirty / dirty2vis"
+                     % (WG_NROW, WG_NCHAN, WG_NPIX, WG_EPS))
+    return out
+
+
+def cpu_baseline_wgridder(nthreads):
+    """DUCC's own w-gridder on the host cores, one call of each direction on the
+    w-gridder workload's inputs."""
+    from oracle import ref
+    R = ref.load()
+    if R is None or not hasattr(R, "wgridder"):
+        return None
+    ps, freq, uvw, vis, wgt, dirty = wgridder_inputs()
+    kw = dict(uvw=uvw, freq=freq, wgt=wgt, pixsize_x=ps, pixsize_y=ps, epsilon=WG_EPS,
+              do_wgridding=True, nthreads=nthreads)
+    res = {"cores": nthreads, "kind": "reference", "sample": "one call of each direction"}
+    t0 = time.perf_counter()
+    R.wgridder.vis2dirty(vis=vis, npix_x=WG_NPIX, npix_y=WG_NPIX, **kw)
+    res["vis2dirty_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    R.wgridder.dirty2vis(dirty=dirty, **kw)
+    res["dirty2vis_ms"] = (time.perf_counter() - t0) * 1e3
+    return res
+
+
 # ---------------------------------------------------------------- our arm
 def cpu_baseline_leg(args, coord, vals, grid, budget_s=20.0):
     """DUCC's CPU NUFFT on the host cores (same planned step, same inputs),
@@ -665,11 +749,17 @@ def run_ours(args, rank, world, local_rank):
         workloads = {}
         for name, fn in (("batched_uneven_2d", workload_batched),
                          ("radial_autograd_2d", workload_autograd),
-                         ("type2_3d_256", workload_3d)):
+                         ("type2_3d_256", workload_3d),
+                         ("wgridder", workload_wgridder)):
             try:
                 workloads[name] = fn(dev)
             except Exception as e:   # reported, never fatal for the headline line
                 workloads[name] = {"error": str(e)[:200]}
+        if not args.no_cpu and "error" not in workloads["wgridder"]:
+            try:
+                workloads["wgridder"]["cpu_baseline"] = cpu_baseline_wgridder(args.param_threads)
+            except Exception as e:
+                workloads["wgridder"]["cpu_baseline"] = {"error": str(e)[:200]}
     line = {
         "metric": METRIC,
         "value": world * 2 * m / (ms * 1e-3) / 1e6,
