@@ -36,7 +36,10 @@ def _dev(x, dtype=None):
     a = np.asarray(x)
     if dtype is not None:
         a = a.astype(dtype, copy=False)
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda(), True
+    a = np.ascontiguousarray(a)
+    if not a.flags.writeable:   # (torch wraps only writable arrays)
+        a = a.copy()
+    return torch.from_numpy(a).cuda(), True
 
 
 def _opts(nthreads, verbosity, sigma_min, sigma_max, center_x, center_y, do_wgridding, flip_u,
