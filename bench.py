@@ -355,40 +355,39 @@ def workload_3d(dev, steps=3, warmup=1, seed=9):
 WG_NPIX, WG_NROW, WG_NCHAN, WG_EPS = 4096, 500_000, 16, 1e-5
 
 
-def wgridder_inputs(seed=11):
+def wgridder_inputs(seed=11, nrow=WG_NROW, npix=WG_NPIX):
     """Synthetic measurement set for the w-gridder workload: 500k rows x 16
     channels (8e6 visibilities, 1.0-1.45 GHz), baselines filling the uv plane of
     a 4096^2 image at 2 degrees field of view (|u|, |v| up to ~0.45 / pixel size
     at the top channel), w up to a third of that; complex64 visibilities,
     float32 weights, a 4096^2 float32 image for the degridding direction."""
     rng = np.random.default_rng(seed)
-    ps = 2.0 * np.pi / 180 / WG_NPIX
+    ps = 2.0 * np.pi / 180 / npix
     freq = 1.0e9 + np.arange(WG_NCHAN) * (0.45e9 / WG_NCHAN)
     umax = 0.45 / ps * 299792458. / freq[-1]
-    r = umax * np.sqrt(rng.random(WG_NROW))
-    phi = rng.uniform(0, 2 * np.pi, WG_NROW)
-    uvw = np.stack([r * np.cos(phi), r * np.sin(phi),
-                    rng.uniform(-umax / 3, umax / 3, WG_NROW)], 1)
-    vis = (rng.standard_normal((WG_NROW, WG_NCHAN))
-           + 1j * rng.standard_normal((WG_NROW, WG_NCHAN))).astype(np.complex64)
-    wgt = rng.uniform(0.5, 1.5, (WG_NROW, WG_NCHAN)).astype(np.float32)
-    dirty = rng.standard_normal((WG_NPIX, WG_NPIX)).astype(np.float32)
+    r = umax * np.sqrt(rng.random(nrow))
+    phi = rng.uniform(0, 2 * np.pi, nrow)
+    uvw = np.stack([r * np.cos(phi), r * np.sin(phi), rng.uniform(-umax / 3, umax / 3, nrow)], 1)
+    vis = (rng.standard_normal((nrow, WG_NCHAN))
+           + 1j * rng.standard_normal((nrow, WG_NCHAN))).astype(np.complex64)
+    wgt = rng.uniform(0.5, 1.5, (nrow, WG_NCHAN)).astype(np.float32)
+    dirty = rng.standard_normal((npix, npix)).astype(np.float32)
     return ps, freq, uvw, vis, wgt, dirty
 
 
-def workload_wgridder(dev, steps=3, warmup=1):
+def workload_wgridder(dev, steps=3, warmup=1, nrow=WG_NROW, npix=WG_NPIX):
     """w-gridder (ducc0.wgridder counterpart): vis2dirty and dirty2vis with
     w-stacking at eps 1e-5 on the synthetic set above, device-resident."""
     import torch
     from ducc_b200 import wgridder as WG
-    ps, freq, uvw, vis, wgt, dirty = wgridder_inputs()
+    ps, freq, uvw, vis, wgt, dirty = wgridder_inputs(nrow=nrow, npix=npix)
     d_uvw = torch.from_numpy(uvw).to(dev)
     d_freq = torch.from_numpy(freq).to(dev)
     d_vis = torch.from_numpy(vis).to(dev)
     d_wgt = torch.from_numpy(wgt).to(dev)
     d_dirty = torch.from_numpy(dirty).to(dev)
-    out_dirty = torch.empty((WG_NPIX, WG_NPIX), dtype=torch.float32, device=dev)
-    out_vis = torch.empty((WG_NROW, WG_NCHAN), dtype=torch.complex64, device=dev)
+    out_dirty = torch.empty((npix, npix), dtype=torch.float32, device=dev)
+    out_vis = torch.empty((nrow, WG_NCHAN), dtype=torch.complex64, device=dev)
     kw = dict(uvw=d_uvw, freq=d_freq, wgt=d_wgt, pixsize_x=ps, pixsize_y=ps, epsilon=WG_EPS,
               do_wgridding=True, nthreads=16)
     out = {}
@@ -405,14 +404,14 @@ def workload_wgridder(dev, steps=3, warmup=1):
         e1.record()
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1) / steps
-        out[name] = {"ms": ms, "mvis_per_s": WG_NROW * WG_NCHAN / (ms * 1e-3) / 1e6}
-    prm = WG.wgrid_params(uvw=d_uvw, freq=d_freq, vis=d_vis, wgt=d_wgt, npix_x=WG_NPIX,
-                          npix_y=WG_NPIX, pixsize_x=ps, pixsize_y=ps, epsilon=WG_EPS,
+        out[name] = {"ms": ms, "mvis_per_s": nrow * WG_NCHAN / (ms * 1e-3) / 1e6}
+    prm = WG.wgrid_params(uvw=d_uvw, freq=d_freq, vis=d_vis, wgt=d_wgt, npix_x=npix,
+                          npix_y=npix, pixsize_x=ps, pixsize_y=ps, epsilon=WG_EPS,
                           do_wgridding=True, nthreads=16)
     out["parameters"] = {k: prm[k] for k in ("supp", "nu", "nv", "nplanes")}
     out["config"] = ("w-gridder, %d rows x %d channels (complex64), %d^2 image at 2 deg, "
                      "w-stacking, eps %g; device-resident vis2dirty / dirty2vis"
-                     % (WG_NROW, WG_NCHAN, WG_NPIX, WG_EPS))
+                     % (nrow, WG_NCHAN, npix, WG_EPS))
     return out
 
 
@@ -879,8 +878,24 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="one transform split over the ranks (strong scaling) instead of one "
                          "independent transform per rank")
+    ap.add_argument("--workload", default=None,
+                    choices=["batched_uneven_2d", "radial_autograd_2d", "type2_3d_256",
+                             "wgridder"],
+                    help="run one of the extra workloads alone and print its result (for "
+                         "profiling); the w-gridder one takes --wg-rows / --wg-npix")
+    ap.add_argument("--wg-rows", type=int, default=WG_NROW)
+    ap.add_argument("--wg-npix", type=int, default=WG_NPIX)
     args = ap.parse_args()
     args.spreaders = args.spreaders.split(",")
+    if args.workload:
+        import torch
+        dev = torch.device("cuda", 0)
+        fn = {"batched_uneven_2d": workload_batched, "radial_autograd_2d": workload_autograd,
+              "type2_3d_256": workload_3d}.get(args.workload)
+        res = (fn(dev) if fn else
+               workload_wgridder(dev, nrow=args.wg_rows, npix=args.wg_npix))
+        print(json.dumps({"workload": args.workload, **res}))
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
