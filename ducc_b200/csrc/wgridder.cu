@@ -287,17 +287,27 @@ __global__ void k_wg_count(const uint32_t *__restrict__ flag, const uint32_t *__
   if (threadIdx.x == 0 && blockIdx.x == 0) out[0] = n > 0 ? scan[n - 1] + flag[n - 1] : 0u;
 }
 
-// first plane of every compacted visibility (the sort key) and its histogram
+// first plane of every compacted visibility (the sort key)
 __global__ void k_wg_minplane(const double *__restrict__ wv, uint32_t nvis, double wmin,
                               double xdw, int W, uint32_t *__restrict__ key,
-                              uint32_t *__restrict__ ord, uint32_t *__restrict__ hist) {
+                              uint32_t *__restrict__ ord) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nvis; i += gridDim.x * blockDim.x) {
     // DUCC: max(0, int((w + wshift) * xdw)), wshift = dw - W dw / 2 - wmin
     const double t = (wv[i] - wmin) * xdw + 1. - 0.5 * W;
     const uint32_t p = t > 0 ? uint32_t(t) : 0u;
     key[i] = p;
     ord[i] = i;
-    atomicAdd(&hist[p], 1u);
+  }
+}
+
+// start[p] = first sorted visibility whose first plane is >= p (p = 0..np),
+// from the sorted keys: position i writes the planes in (key[i-1], key[i]]
+__global__ void k_wg_plane_starts(const uint32_t *__restrict__ key, uint32_t n, uint32_t np,
+                                  uint32_t *__restrict__ start) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+    const int64_t lo = i > 0 ? int64_t(key[i - 1]) : -1;
+    const int64_t hi = i < n ? int64_t(min(key[i], np)) : int64_t(np);
+    for (int64_t p = lo + 1; p <= hi; ++p) start[p] = i;
   }
 }
 
@@ -349,20 +359,42 @@ struct ImgGeom {
   double nshift;
 };
 
-// dirty(i, j) += Re(img(i, j) e^{-2 pi i w_p (n - 1 + nshift)})
-template <typename C, typename T>
-__global__ void k_wg_screen_add(const cplx<C> *__restrict__ img, ImgGeom g, double wp,
-                                T *__restrict__ dirty, int64_t ds0, int64_t ds1) {
+// pm(i, j) = n - 1 + nshift of every pixel, once per call for the w screens
+__global__ void k_wg_pixel_nm1(ImgGeom g, double *__restrict__ pm) {
   const int64_t n = g.nx * g.ny;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n;
        e += int64_t(gridDim.x) * blockDim.x) {
     const int64_t i = e / g.ny, j = e - i * g.ny;
-    const double nm1 = nm1_of(g.x0 + i * g.psx, g.y0 + j * g.psy);
-    double cs, sn;
-    cis2pi(-wp * (nm1 + g.nshift), cs, sn);
+    pm[e] = nm1_of(g.x0 + i * g.psx, g.y0 + j * g.psy) + g.nshift;
+  }
+}
+
+// e^{2 pi i t}: the product is formed and reduced to [0, 1) in double, the
+// sine and cosine taken in the compute precision C (as DUCC does for single
+// precision, wgridder.h:392-394)
+template <typename C> __device__ inline void cis2pi_c(double t, C &c, C &s) {
+  t -= floor(t);
+  if constexpr (sizeof(C) == 4) {
+    sincospif(float(2. * t), &s, &c);
+  } else {
+    sincospi(2. * t, &s, &c);
+  }
+}
+
+// dirty(i, j) += Re(img(i, j) e^{-2 pi i w_p (n - 1 + nshift)})
+template <typename C, typename T>
+__global__ void k_wg_screen_add(const cplx<C> *__restrict__ img, const double *__restrict__ pm,
+                                ImgGeom g, double wp, T *__restrict__ dirty, int64_t ds0,
+                                int64_t ds1) {
+  const int64_t n = g.nx * g.ny;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e / g.ny, j = e - i * g.ny;
+    C cs, sn;
+    cis2pi_c<C>(-wp * pm[e], cs, sn);
     const cplx<C> a = img[e];
     T &d = dirty[i * ds0 + j * ds1];
-    d += T(double(a.x) * cs - double(a.y) * sn);
+    d += T(a.x * cs - a.y * sn);
   }
 }
 
@@ -439,17 +471,14 @@ __global__ void k_wg_dirty_in(const T *__restrict__ dirty, int64_t ds0, int64_t 
 
 // plane image for degridding: img0 e^{+2 pi i w_p (n - 1 + nshift)}
 template <typename C>
-__global__ void k_wg_screen_apply(const C *__restrict__ img0, ImgGeom g, double wp,
-                                  cplx<C> *__restrict__ img) {
-  const int64_t n = g.nx * g.ny;
+__global__ void k_wg_screen_apply(const C *__restrict__ img0, const double *__restrict__ pm,
+                                  int64_t n, double wp, cplx<C> *__restrict__ img) {
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n;
        e += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t i = e / g.ny, j = e - i * g.ny;
-    const double nm1 = nm1_of(g.x0 + i * g.psx, g.y0 + j * g.psy);
-    double cs, sn;
-    cis2pi(wp * (nm1 + g.nshift), cs, sn);
-    const double a = double(img0[e]);
-    img[e] = mkc<C>(C(a * cs), C(a * sn));
+    C cs, sn;
+    cis2pi_c<C>(wp * pm[e], cs, sn);
+    const C a = img0[e];
+    img[e] = mkc<C>(a * cs, a * sn);
   }
 }
 
@@ -788,20 +817,17 @@ static void plane_order(Compacted<T, C> &cv, const Params &P, bool gridding,
                         PlaneOrder<C> &po, cudaStream_t st) {
   const uint32_t n = cv.nvis;
   const int64_t np = P.nplanes;
-  Buf key(size_t(n) * 4, st), ord(size_t(n) * 4, st), hist(size_t(np + 1) * 4, st),
-      hscan(size_t(np + 1) * 4, st);
-  DN_CUDA(cudaMemsetAsync(hist.p, 0, size_t(np + 1) * 4, st));
+  Buf key(size_t(n) * 4, st), ord(size_t(n) * 4, st), starts(size_t(np + 1) * 4, st);
   k_wg_minplane<<<grid_for(n), 256, 0, st>>>(ptr<double>(cv.wv), n, P.wmin, P.xdw, P.W,
-                                             ptr<uint32_t>(key), ptr<uint32_t>(ord),
-                                             ptr<uint32_t>(hist));
+                                             ptr<uint32_t>(key), ptr<uint32_t>(ord));
   DN_LAUNCHED();
   int keybits = 1;
   while ((int64_t(1) << keybits) <= np) ++keybits;
   Buf rws(radix_workspace_bytes(n, keybits), st);
   radix_sort_pairs(ptr<uint32_t>(key), ptr<uint32_t>(ord), n, keybits, rws.p, st);
-  Buf sws(scan_workspace_bytes(uint64_t(np + 1)), st);
-  exclusive_scan(ptr<uint32_t>(hist), ptr<uint32_t>(hscan), uint64_t(np + 1), ptr<uint32_t>(sws),
-                 st);
+  k_wg_plane_starts<<<grid_for(int64_t(n) + 1), 256, 0, st>>>(ptr<uint32_t>(key), n,
+                                                               uint32_t(np), ptr<uint32_t>(starts));
+  DN_LAUNCHED();
   po.coord = Buf(size_t(n) * 16, st);
   po.wv = Buf(size_t(n) * 8, st);
   po.idx = Buf(size_t(n) * 4, st);
@@ -813,10 +839,9 @@ static void plane_order(Compacted<T, C> &cv, const Params &P, bool gridding,
   DN_LAUNCHED();
   po.key = std::move(key);
   po.start.assign(size_t(np + 1), 0u);
-  DN_CUDA(cudaMemcpyAsync(po.start.data(), hscan.p, size_t(np + 1) * 4, cudaMemcpyDeviceToHost,
-                          st));
+  DN_CUDA(cudaMemcpyAsync(po.start.data(), starts.p, size_t(np + 1) * 4,
+                          cudaMemcpyDeviceToHost, st));
   DN_CUDA(cudaStreamSynchronize(st));
-  po.start[size_t(np)] = n;   // (the scan's last entry is the count before the last bin)
 }
 
 static dnufft_opts nufft_opts(const Params &P, double psx, double psy, const dnufft_wgrid_opts &o) {
@@ -888,6 +913,10 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
   }
   PlaneOrder<C> po;
   plane_order<T, C>(cv, P, true, po, st);
+  Buf pm(size_t(nx * ny) * 8, st);
+  k_wg_pixel_nm1<<<grid_for(nx * ny), 256, 0, st>>>(img_geom(P, nx, ny, psx, psy),
+                                                    ptr<double>(pm));
+  DN_LAUNCHED();
   const KernelPoly<C> kp = make_poly<C>(P.W, P.beta, P.e0);
   const ImgGeom g = img_geom(P, nx, ny, psx, psy);
   Buf pv(size_t(cv.nvis) * sizeof(cplx<C>), st);
@@ -904,7 +933,8 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
     dnufft_array a_c = dev_array(ptr<double>(po.coord) + 2 * size_t(lo), DNUFFT_F64, 2, cnt, 2);
     check_nufft(dnufft_nu2u(&a_v, &a_c, 0, eps, &a_img, &no, st));
     k_wg_screen_add<C, T><<<grid_for(nx * ny), 256, 0, st>>>(
-        ptr<cplx<C>>(img), g, P.wmin + double(p) * P.dw, dp, dirty.stride[0], dirty.stride[1]);
+        ptr<cplx<C>>(img), ptr<double>(pm), g, P.wmin + double(p) * P.dw, dp, dirty.stride[0],
+        dirty.stride[1]);
     DN_LAUNCHED();
   }
   const CorrNodes cn = make_nodes(P.W, P.beta, P.e0);
@@ -960,6 +990,9 @@ static void dirty2vis_t(const Inputs &in, const Arr &dirty, double psx, double p
   }
   PlaneOrder<C> po;
   plane_order<T, C>(cv, P, false, po, st);
+  Buf pm(size_t(nx * ny) * 8, st);
+  k_wg_pixel_nm1<<<grid_for(nx * ny), 256, 0, st>>>(g, ptr<double>(pm));
+  DN_LAUNCHED();
   const KernelPoly<C> kp = make_poly<C>(P.W, P.beta, P.e0);
   DN_CUDA(cudaMemsetAsync(acc.p, 0, size_t(cv.nvis) * sizeof(cplx<C>), st));
   Buf res(size_t(cv.nvis) * sizeof(cplx<C>), st);
@@ -968,9 +1001,8 @@ static void dirty2vis_t(const Inputs &in, const Arr &dirty, double psx, double p
     const uint32_t hi = po.start[size_t(p + 1)];
     if (hi <= lo) continue;
     const uint32_t cnt = hi - lo;
-    k_wg_screen_apply<C><<<grid_for(nx * ny), 256, 0, st>>>(ptr<C>(img0), g,
-                                                            P.wmin + double(p) * P.dw,
-                                                            ptr<cplx<C>>(img));
+    k_wg_screen_apply<C><<<grid_for(nx * ny), 256, 0, st>>>(
+        ptr<C>(img0), ptr<double>(pm), nx * ny, P.wmin + double(p) * P.dw, ptr<cplx<C>>(img));
     DN_LAUNCHED();
     dnufft_array a_c = dev_array(ptr<double>(po.coord) + 2 * size_t(lo), DNUFFT_F64, 2, cnt, 2);
     dnufft_array a_o = dev_array(res.p, cdt, 1, cnt);
