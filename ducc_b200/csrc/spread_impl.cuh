@@ -151,9 +151,13 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
     __syncthreads();
   }
   const uint32_t end = ch.start + ch.count;
-  for (uint32_t base = ch.start + uint32_t(warp) * 32; base < end; base += SP_WARPS * 32) {
+  // points per warp and round: 32, or fewer for a chunk of fewer than
+  // 32 * SP_WARPS points, so that every warp takes a share of a small chunk
+  // (each warp walks its points one by one)
+  const int pw = min(32, max(1, int((ch.count + SP_WARPS - 1) / SP_WARPS)));
+  for (uint32_t base = ch.start + uint32_t(warp * pw); base < end; base += SP_WARPS * pw) {
     uint32_t i = base + lane;
-    if (i < end) {
+    if (lane < pw && i < end) {
       Tc x[NDIM];
       uint32_t j = load_point<Tc, NDIM>(pts, i, x);
       // a gather through the permutation: cached in L2 only, so a miss
@@ -173,7 +177,7 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
       stv[lane] = v;
     }
     __syncwarp();
-    int np = min(32, int(end - base));
+    int np = min(pw, int(end - base));
     for (int p = 0; p < np; ++p) {
       const cplx<T> v = stv[p];
       const T *wp = stw + p * WS;
