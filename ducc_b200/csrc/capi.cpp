@@ -531,6 +531,50 @@ static void upload_consts(const Setup &s, DevConst &dc, cudaStream_t st) {
   DN_CUDA(cudaStreamSynchronize(st));
 }
 
+// Constants of an unplanned call, shared by later unplanned calls with the same
+// geometry on the same device: the upload (host twiddles, pageable copies and
+// a stream synchronisation) then happens once instead of on every call.  Up to
+// MAX_SHARED geometries per process are kept (about the size of their
+// twiddle tables each) for the life of the process; beyond that a call uploads
+// into the caller's `local` as before.  An entry is complete (its stream was
+// synchronised) before it is published, so any stream may read it.
+static const DevConst &consts_for(const Setup &s, DevConst &local, cudaStream_t st) {
+  constexpr size_t MAX_SHARED = 32;
+  struct Key {
+    int dev, ndim, f64, W;
+    double beta, e0;
+    int64_t nover[3], nuni[3];
+    bool operator<(const Key &o) const {
+      return std::memcmp(this, &o, sizeof(Key)) < 0;
+    }
+  };
+  Key k;
+  std::memset(&k, 0, sizeof(k));   // padding bytes take part in the comparison
+  DN_CUDA(cudaGetDevice(&k.dev));
+  k.ndim = s.g.ndim;
+  k.f64 = s.calc_f64 ? 1 : 0;
+  k.W = s.g.W;
+  k.beta = s.beta;
+  k.e0 = s.e0;
+  for (int d = 0; d < s.g.ndim; ++d) {
+    k.nover[d] = s.g.nover[d];
+    k.nuni[d] = s.g.nuni[d];
+  }
+  static std::mutex mu;
+  static std::map<Key, DevConst *> *cache = new std::map<Key, DevConst *>();   // never freed
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache->find(k);
+  if (it != cache->end()) return *it->second;
+  if (cache->size() >= MAX_SHARED) {
+    upload_consts(s, local, st);
+    return local;
+  }
+  DevConst *dc = new DevConst();   // kept until exit (not destroyed: no frees at teardown)
+  upload_consts(s, *dc, st);
+  (*cache)[k] = dc;
+  return *dc;
+}
+
 // index: tile permutation, sorted keys and chunk list
 struct Index {
   DevBuf perm, keys, chunks, count;
@@ -791,8 +835,8 @@ static void nu2u_pipelined(const Setup &s, const View &points, const View &coord
   const size_t cb = s.coord_f64 ? 8 : 4, vb = sizeof(T) * 2;
   const int G = pipe_groups(M);
   tm.mark("upload constants");
-  DevConst dc;
-  upload_consts(s, dc, st);
+  DevConst dcl;
+  const DevConst &dc = consts_for(s, dcl, st);
   DevBuf dcoord(size_t(M) * nd * cb, st), dvals(size_t(M) * vb, st);
   const size_t cells = grid_cells(s.g);
   DevBuf grid(cells * vb, st), work;
@@ -847,8 +891,8 @@ static void u2nu_pipelined(const Setup &s, const View &uni, const View &coord, c
   const size_t cb = s.coord_f64 ? 8 : 4, vb = sizeof(T) * 2;
   const int G = pipe_groups(M);
   tm.mark("upload constants");
-  DevConst dc;
-  upload_consts(s, dc, st);
+  DevConst dcl;
+  const DevConst &dc = consts_for(s, dcl, st);
   DevBuf dcoord(size_t(M) * nd * cb, st), duni, dout;
   const size_t ubytes = size_t(nelem(uni)) * vb;
   if (uni.host) duni = DevBuf(ubytes, st);
@@ -947,8 +991,8 @@ static void nu2u_impl(const dnufft_array *points_, const dnufft_array *coord_, i
   // constants first (small pageable copies, which would otherwise queue behind
   // the large transfers on the copy engine)
   tm.mark("upload constants");
-  DevConst dc;
-  if (s.npoints) upload_consts(s, dc, st);
+  DevConst dcl;
+  const DevConst &dc = s.npoints ? consts_for(s, dcl, st) : dcl;
   tm.mark("coordinates host->device");
   // host arrays: the coordinates next; the point values follow on a side
   // stream while this stream builds the index
@@ -1009,8 +1053,8 @@ static void u2nu_impl(const dnufft_array *grid_, const dnufft_array *coord_, int
     return;
   }
   tm.mark("upload constants");
-  DevConst dc;
-  upload_consts(s, dc, st);
+  DevConst dcl;
+  const DevConst &dc = consts_for(s, dcl, st);
   tm.mark("coordinates host->device");
   // host arrays: the coordinates first; the uniform grid follows on a side
   // stream, which also runs the FFT pass, while this stream builds the index
@@ -1059,8 +1103,8 @@ static void u2nu_dcoord_impl(const dnufft_array *grid_, const dnufft_array *coor
   Staged su(uni, true, false, st), sc(coord, true, false, st), sw(wts, true, false, st),
       sg(grad, false, true, st);
   tm.mark("upload constants");
-  DevConst dc;
-  upload_consts(s, dc, st);
+  DevConst dcl;
+  const DevConst &dc = consts_for(s, dcl, st);
   tm.mark("building index");
   Index ix;
   build_index(s, sc.dev, ix, st);
