@@ -366,3 +366,25 @@ def test_bad_arguments(ng):
     with pytest.raises(TypeError):
         ng.vis2dirty(uvw=uvw, freq=freq, vis=vis, wgt=wgt.astype("f4"), npix_x=64, npix_y=64,
                      pixsize_x=ps, pixsize_y=ps, epsilon=1e-6)
+
+
+def test_torch_tensors_in_place(ng):
+    """Device tensors in, results written into the given device tensors, the
+    same numbers as the numpy path."""
+    import torch
+    ps, freq, uvw, vis, wgt, mask, dirty = _ms_problem(21, 3000, 4, 128, 10., True, True)
+    args = dict(pixsize_x=ps, pixsize_y=ps, epsilon=1e-5, do_wgridding=True)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    out = torch.zeros((128, 128), dtype=torch.float32, device="cuda")
+    r = ng.vis2dirty(uvw=t(uvw), freq=t(freq), vis=t(vis), wgt=t(wgt), mask=t(mask), dirty=out,
+                     **args)
+    assert r is out
+    ref = ng.vis2dirty(uvw=uvw, freq=freq, vis=vis, wgt=wgt, mask=mask, npix_x=128, npix_y=128,
+                       **args)
+    assert O.l2error(out.cpu().numpy(), ref) < 1e-6
+    vout = torch.empty(vis.shape, dtype=torch.complex64, device="cuda")
+    r = ng.dirty2vis(uvw=t(uvw), freq=t(freq), dirty=t(dirty), wgt=t(wgt), mask=t(mask),
+                     vis=vout, **args)
+    assert r is vout
+    vref = ng.dirty2vis(uvw=uvw, freq=freq, dirty=dirty, wgt=wgt, mask=mask, **args)
+    assert O.l2error(vout.cpu().numpy(), vref) < 1e-6
