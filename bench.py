@@ -375,7 +375,7 @@ def wgridder_inputs(seed=11, nrow=WG_NROW, npix=WG_NPIX):
     return ps, freq, uvw, vis, wgt, dirty
 
 
-def workload_wgridder(dev, steps=3, warmup=1, nrow=WG_NROW, npix=WG_NPIX):
+def workload_wgridder(dev, steps=5, warmup=2, nrow=WG_NROW, npix=WG_NPIX):
     """w-gridder (ducc0.wgridder counterpart): vis2dirty and dirty2vis with
     w-stacking at eps 1e-5 on the synthetic set above, device-resident."""
     import torch

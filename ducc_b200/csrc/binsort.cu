@@ -483,3 +483,106 @@ void launch_scatter_coords(bool coord_f64, const void *sorted, int ndim, const u
 }
 
 }  // namespace dnufft
+
+namespace dnufft {
+
+// ---------------------------------------------------------------- grouped index
+// keys[i] = (keys[i] << gbits) | group[i]: points sorted by (tile, group)
+__global__ void k_group_keys(uint32_t *__restrict__ keys, const uint32_t *__restrict__ group,
+                             uint32_t n, int gbits) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    keys[i] = (keys[i] << gbits) | group[i];
+}
+
+// start[k] = first i with v[i] >= k, k = 0..nk, for ascending v: a binary
+// search per k (the key space may hold long gaps, e.g. past the last tile)
+__global__ void k_key_starts(const uint32_t *__restrict__ v, uint32_t n, uint32_t nk,
+                             uint32_t *__restrict__ start) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= nk; k += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      if (v[mid] < k) lo = mid + 1;
+      else hi = mid;
+    }
+    start[k] = lo;
+  }
+}
+
+// chunks of the points of groups [g0, g1) of every tile (at most `chunk`
+// points each): counts, then (after a scan into pos) the records
+__global__ void k_gchunk_count(const uint32_t *__restrict__ start, uint32_t ntiles, int gbits,
+                               uint32_t g0, uint32_t g1, uint32_t chunk,
+                               uint32_t *__restrict__ cnt) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles;
+       t += gridDim.x * blockDim.x) {
+    if (t == ntiles) {
+      cnt[t] = 0;
+      continue;
+    }
+    const uint32_t s = start[(uint64_t(t) << gbits) + g0], e = start[(uint64_t(t) << gbits) + g1];
+    cnt[t] = (e - s + chunk - 1) / chunk;
+  }
+}
+
+__global__ void k_gchunk_fill(const uint32_t *__restrict__ start,
+                              const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ pos,
+                              uint32_t ntiles, int gbits, uint32_t g0, uint32_t g1,
+                              uint32_t chunk, Chunk *__restrict__ chunks) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles;
+       t += gridDim.x * blockDim.x) {
+    const uint32_t s = start[(uint64_t(t) << gbits) + g0], e = start[(uint64_t(t) << gbits) + g1];
+    for (uint32_t k = 0; k < cnt[t]; ++k) {
+      Chunk c;
+      c.start = s + k * chunk;
+      c.count = min(chunk, e - c.start);
+      c.tile = t;
+      c.pad = 0;
+      chunks[pos[t] + k] = c;
+    }
+  }
+}
+
+static unsigned grid_of(uint64_t n) {
+  uint64_t b = (n + 255) / 256;
+  return unsigned(b < 1 ? 1 : (b > 4096 ? 4096 : b));
+}
+
+void launch_group_keys(uint32_t *keys, const uint32_t *group, uint32_t n, int gbits,
+                       cudaStream_t st) {
+  if (n == 0) return;
+  k_group_keys<<<grid_of(n), 256, 0, st>>>(keys, group, n, gbits);
+  DN_LAUNCHED();
+}
+
+void launch_key_starts(const uint32_t *skeys, uint32_t n, uint32_t nkeys, uint32_t *start,
+                       cudaStream_t st) {
+  k_key_starts<<<grid_of(uint64_t(nkeys) + 1), 256, 0, st>>>(skeys, n, nkeys, start);
+  DN_LAUNCHED();
+}
+
+size_t group_chunk_workspace_bytes(uint32_t ntiles) {
+  return size_t(2) * (ntiles + 1) * 4 + 256 + scan_workspace_bytes(uint64_t(ntiles) + 1);
+}
+
+uint32_t build_group_chunks(const uint32_t *start, uint32_t ntiles, int gbits, uint32_t g0,
+                            uint32_t g1, uint32_t chunk, Chunk *chunks, void *ws,
+                            cudaStream_t st) {
+  uint32_t *cnt = static_cast<uint32_t *>(ws);
+  uint32_t *pos = cnt + (ntiles + 1);
+  uint32_t *sws = reinterpret_cast<uint32_t *>(
+      (reinterpret_cast<uintptr_t>(pos + ntiles + 1) + 255) & ~uintptr_t(255));
+  k_gchunk_count<<<grid_of(uint64_t(ntiles) + 1), 256, 0, st>>>(start, ntiles, gbits, g0, g1,
+                                                                chunk, cnt);
+  DN_LAUNCHED();
+  exclusive_scan(cnt, pos, uint64_t(ntiles) + 1, sws, st);
+  k_gchunk_fill<<<grid_of(ntiles), 256, 0, st>>>(start, cnt, pos, ntiles, gbits, g0, g1, chunk,
+                                                 chunks);
+  DN_LAUNCHED();
+  const uint32_t *src[1] = {pos + ntiles};
+  uint32_t h = 0;
+  read_words(src, 1, &h, st);
+  return h;
+}
+
+}  // namespace dnufft

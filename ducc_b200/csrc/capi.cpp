@@ -1853,6 +1853,154 @@ int nu2u_in_scratch(const dnufft_array *points, const dnufft_array *coord, int f
   }
 }
 
+// ---------------------------------------------------------------- grouped index
+// A 2D index over points that belong to groups (the w-gridder's first w
+// plane): sorted once by (tile, group), so that within every tile the points
+// of any run of groups are one contiguous range, and a type 1 or type 2
+// transform over such a run needs only a chunk list (one chunk per tile and
+// at most CHUNK points, so a tile is still flushed once), not a sort of its
+// own.  Plain spreader; kernel and grid as forced in the options.
+struct GroupedPlan {
+  Setup s;
+  DevConst dcl;
+  const DevConst *dc = nullptr;
+  DevBuf sorted_coord, perm, start, chunks, cws, grid, work;
+  uint32_t ntiles = 0, ngroups = 0, nchunks = 0, g0 = 0, g1 = 0;
+  int gbits = 0;
+};
+
+static int bits_for(uint64_t v) {   // bits to hold 0..v
+  int b = 0;
+  while (b < 64 && (uint64_t(1) << b) <= v) ++b;
+  return b;
+}
+
+GroupedPlan *grouped_plan_create(const double *coord, uint32_t M, const uint32_t *group,
+                                 uint32_t ngroups, const int64_t *shape, double eps,
+                                 bool calc_f64, const dnufft_opts &opts, cudaStream_t st,
+                                 uint32_t *perm_out) {
+  dnufft_opts o = opts;
+  o.spreader = DNUFFT_SPREAD_PLAIN;
+  auto gp = std::make_unique<GroupedPlan>();
+  gp->s = make_setup(2, shape, M, eps, true, calc_f64, true, o);
+  Setup &s = gp->s;
+  DN_REQUIRE(!s.qbits, ST_INTERNAL, "grouped index with a tensor-core key");
+  const int tilebits = s.keybits;
+  gp->gbits = bits_for(ngroups);
+  // the (tile, group) start table has 2^(tilebits + gbits) + 1 entries
+  if (tilebits + gp->gbits > 24 || M == 0 || ngroups == 0) return nullptr;
+  gp->ngroups = ngroups;
+  gp->ntiles = uint32_t(1) << tilebits;
+  gp->dc = &consts_for(s, gp->dcl, st);
+  DevBuf keys(size_t(M) * 4, st);
+  gp->perm = DevBuf(size_t(M) * 4, st);
+  launch_fold_keys(true, coord, 2, 1, M, s.g, keys.as<uint32_t>(), gp->perm.as<uint32_t>(), st,
+                   false);
+  launch_group_keys(keys.as<uint32_t>(), group, M, gp->gbits, st);
+  const int total = tilebits + gp->gbits;
+  {
+    DevBuf ws(radix_workspace_bytes(M, total), st);
+    radix_sort_pairs(keys.as<uint32_t>(), gp->perm.as<uint32_t>(), M, total, ws.p, st);
+  }
+  const uint32_t nkeys = uint32_t(1) << total;
+  gp->start = DevBuf(size_t(nkeys + 1) * 4, st);
+  launch_key_starts(keys.as<uint32_t>(), M, nkeys, gp->start.as<uint32_t>(), st);
+  gp->sorted_coord = DevBuf(size_t(M) * 16, st);
+  launch_gather_coords(true, coord, 2, 1, 2, gp->perm.as<uint32_t>(), M, gp->sorted_coord.p, st);
+  gp->chunks = DevBuf((size_t(gp->ntiles) + M / s.chunk + 2) * sizeof(Chunk), st);
+  gp->cws = DevBuf(group_chunk_workspace_bytes(gp->ntiles), st);
+  if (perm_out)
+    DN_CUDA(cudaMemcpyAsync(perm_out, gp->perm.p, size_t(M) * 4, cudaMemcpyDeviceToDevice, st));
+  const size_t vb = calc_f64 ? 16 : 8;
+  gp->grid = DevBuf(grid_cells(s.g) * vb, st);
+  const size_t wb = fft_work_bytes(s.g, vb);
+  if (wb) gp->work = DevBuf(wb, st);
+  DN_CUDA(cudaStreamSynchronize(st));
+  return gp.release();
+}
+
+void grouped_plan_destroy(GroupedPlan *gp, cudaStream_t st) {
+  if (!gp) return;
+  // buffers go back to the pool in the order of the stream that last used them
+  for (DevBuf *b : {&gp->sorted_coord, &gp->perm, &gp->start, &gp->chunks, &gp->cws, &gp->grid,
+                    &gp->work})
+    b->st = st;
+  delete gp;
+}
+
+const uint32_t *grouped_plan_perm(const GroupedPlan *gp) { return gp->perm.as<uint32_t>(); }
+
+// chunk list of groups [g0, g1), kept for the next call with the same run;
+// false: no point in the run
+static bool grouped_chunks(GroupedPlan *gp, uint32_t g0, uint32_t g1, cudaStream_t st) {
+  if (gp->g1 == 0 || gp->g0 != g0 || gp->g1 != g1) {
+    gp->nchunks = build_group_chunks(gp->start.as<uint32_t>(), gp->ntiles, gp->gbits, g0, g1,
+                                     gp->s.chunk, gp->chunks.as<Chunk>(), gp->cws.p, st);
+    gp->g0 = g0;
+    gp->g1 = g1;
+  }
+  return gp->nchunks > 0;
+}
+
+static View plain_view(void *data, int dtype, int ndim, int64_t s0, int64_t s1 = 0) {
+  View v;
+  std::memset(&v, 0, sizeof(v));
+  v.data = data;
+  v.dtype = dtype;
+  v.ndim = ndim;
+  v.shape[0] = s0;
+  v.shape[1] = s1;
+  v.stride[0] = ndim == 1 ? 1 : s1;
+  v.stride[1] = 1;
+  v.host = false;
+  return v;
+}
+
+// type 1 over the points of groups [g0, g1): values in the caller's order
+// (index = position before sorting), result into out (N0 x N1, contiguous);
+// false (nothing written) where the run has no point
+bool grouped_nu2u(GroupedPlan *gp, uint32_t g0, uint32_t g1, const void *values, void *out,
+                  bool forward, cudaStream_t st) {
+  const Setup &s = gp->s;
+  if (!grouped_chunks(gp, g0, g1, st)) return false;
+  const ChunkList cl{gp->chunks.as<Chunk>(), gp->nchunks};
+  const PointsDesc pts{gp->sorted_coord.p, 2, 1, true, true, gp->perm.as<uint32_t>(),
+                       s.npoints};
+  const int dt = s.calc_f64 ? DNUFFT_C128 : DNUFFT_C64;
+  const View vv = plain_view(const_cast<void *>(values), dt, 1, s.npoints);
+  const View ov = plain_view(out, dt, 2, s.g.nuni[0], s.g.nuni[1]);
+  StageTimer tm(false, st);
+  if (s.calc_f64)
+    do_spread_fft<double>(s, *gp->dc, pts, cl, nullptr, vv, ov, forward, false, tm, st,
+                          &gp->grid, &gp->work);
+  else
+    do_spread_fft<float>(s, *gp->dc, pts, cl, nullptr, vv, ov, forward, false, tm, st,
+                         &gp->grid, &gp->work);
+  return true;
+}
+
+// type 2 at the points of groups [g0, g1): results into out at the caller's
+// positions (other entries untouched); false where the run has no point
+bool grouped_u2nu(GroupedPlan *gp, uint32_t g0, uint32_t g1, const void *uni, void *out,
+                  bool forward, cudaStream_t st) {
+  const Setup &s = gp->s;
+  if (!grouped_chunks(gp, g0, g1, st)) return false;
+  const ChunkList cl{gp->chunks.as<Chunk>(), gp->nchunks};
+  const PointsDesc pts{gp->sorted_coord.p, 2, 1, true, true, gp->perm.as<uint32_t>(),
+                       s.npoints};
+  const int dt = s.calc_f64 ? DNUFFT_C128 : DNUFFT_C64;
+  const View uv = plain_view(const_cast<void *>(uni), dt, 2, s.g.nuni[0], s.g.nuni[1]);
+  const View ov = plain_view(out, dt, 1, s.npoints);
+  StageTimer tm(false, st);
+  if (s.calc_f64)
+    do_fft_interp<double>(s, *gp->dc, pts, cl, uv, ov, forward, false, tm, st, &gp->grid,
+                          &gp->work);
+  else
+    do_fft_interp<float>(s, *gp->dc, pts, cl, uv, ov, forward, false, tm, st, &gp->grid,
+                         &gp->work);
+  return true;
+}
+
 void set_last_error(const char *msg) { g_last_error = msg; }
 
 }  // namespace dnufft

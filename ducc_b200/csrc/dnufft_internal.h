@@ -11,6 +11,8 @@
 
 #include <cuda_runtime.h>
 
+struct dnufft_opts;   // include/ducc_b200.h
+
 namespace dnufft {
 
 // ---------------------------------------------------------------- errors
@@ -109,5 +111,24 @@ struct Chunk {
   uint32_t tile;   // tile id (2D: tu*ntv+tv; 3D: hikey; 1D: tu)
   uint32_t pad;
 };
+
+// A 2D index over points in groups, sorted once by (tile, group) (capi.cpp);
+// the w-gridder's w planes are runs of groups [g0, g1), each transformed
+// without a sort.  create returns null where the (tile, group) table would be
+// too large.  perm_out (device, M words): sorted position -> the caller's
+// point index.  Values and results are in the caller's order; the uniform
+// arrays are contiguous (nuni[0], nuni[1]); the transforms return false
+// (writing nothing) for a run without points.
+struct GroupedPlan;
+GroupedPlan *grouped_plan_create(const double *coord, uint32_t M, const uint32_t *group,
+                                 uint32_t ngroups, const int64_t *shape, double eps,
+                                 bool calc_f64, const ::dnufft_opts &opts,
+                                 cudaStream_t st, uint32_t *perm_out);
+void grouped_plan_destroy(GroupedPlan *gp, cudaStream_t st);
+const uint32_t *grouped_plan_perm(const GroupedPlan *gp);
+bool grouped_nu2u(GroupedPlan *gp, uint32_t g0, uint32_t g1, const void *values, void *out,
+                  bool forward, cudaStream_t st);
+bool grouped_u2nu(GroupedPlan *gp, uint32_t g0, uint32_t g1, const void *uni, void *out,
+                  bool forward, cudaStream_t st);
 
 }  // namespace dnufft

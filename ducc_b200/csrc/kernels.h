@@ -30,6 +30,19 @@ void launch_gather_coords(bool coord_f64, const void *coord, int64_t cs0, int64_
                           int ndim, const uint32_t *perm, uint32_t n, void *out,
                           cudaStream_t st);
 
+// grouped index (points sorted by (tile, group)): keys = keys << gbits | group;
+// start[k] (k = 0..nkeys) = first sorted point whose key is >= k; the chunks
+// (at most `chunk` points) of groups [g0, g1) of every tile, their number
+// returned (read back: synchronises st)
+void launch_group_keys(uint32_t *keys, const uint32_t *group, uint32_t n, int gbits,
+                       cudaStream_t st);
+void launch_key_starts(const uint32_t *skeys, uint32_t n, uint32_t nkeys, uint32_t *start,
+                       cudaStream_t st);
+size_t group_chunk_workspace_bytes(uint32_t ntiles);
+uint32_t build_group_chunks(const uint32_t *start, uint32_t ntiles, int gbits, uint32_t g0,
+                            uint32_t g1, uint32_t chunk, Chunk *chunks, void *ws,
+                            cudaStream_t st);
+
 void launch_scatter_coords(bool coord_f64, const void *sorted, int ndim, const uint32_t *perm,
                            uint32_t n, void *out, cudaStream_t st);
 

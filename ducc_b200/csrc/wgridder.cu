@@ -507,6 +507,27 @@ __global__ void k_wg_degrid_acc(const cplx<C> *__restrict__ res, const double *_
   }
 }
 
+// the degridding accumulation over all compacted visibilities (a grouped
+// index leaves the results of those outside plane p untouched: they are
+// skipped, not weighted by zero)
+template <typename C>
+__global__ void k_wg_degrid_acc_all(const cplx<C> *__restrict__ res,
+                                    const double *__restrict__ wv,
+                                    const uint32_t *__restrict__ key, uint32_t n,
+                                    KernelPoly<C> kp, int W, int p, double wmin, double xdw,
+                                    cplx<C> *__restrict__ acc) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int nth = p - int(key[j]);
+    if (nth < 0 || nth >= W) continue;
+    const C f = plane_weight<C>(kp, W, wv[j], key[j], p, wmin, xdw);
+    const cplx<C> r = res[j];
+    cplx<C> a = acc[j];
+    a.x += f * r.x;
+    a.y += f * r.y;
+    acc[j] = a;
+  }
+}
+
 // vis(row, chan) = wgt * S (S conjugated for a mirrored visibility), S = the
 // accumulated sum times e^{-2 pi i (u l0 + v m0 + w nshift)} at the (mirrored)
 // coordinates
@@ -880,6 +901,33 @@ static void report(const Params &P, const char *what, int64_t nx, int64_t ny, ui
   std::printf("\n");
 }
 
+// The visibilities indexed once by (first w plane, tile), so that no plane
+// sorts its own (null where the keys do not fit 32 bits: then every plane's
+// transform sorts its range).  key: the first plane of every compacted
+// visibility.
+struct Grouped {
+  GroupedPlan *gp = nullptr;
+  cudaStream_t st = nullptr;
+  Grouped(const double *coord, uint32_t n, const uint32_t *key, const Params &P, int64_t nx,
+          int64_t ny, double eps, bool f64, const dnufft_opts &no, cudaStream_t s)
+      : st(s) {
+    const int64_t shape[2] = {nx, ny};
+    gp = grouped_plan_create(coord, n, key, uint32_t(P.nplanes), shape, eps, f64, no, s,
+                             nullptr);
+  }
+  Grouped(const Grouped &) = delete;
+  Grouped &operator=(const Grouped &) = delete;
+  ~Grouped() { grouped_plan_destroy(gp, st); }
+};
+
+static void plane_keys(const double *wv, uint32_t n, const Params &P, Buf &key, cudaStream_t st) {
+  Buf ord(size_t(n) * 4, st);
+  key = Buf(size_t(n) * 4, st);
+  k_wg_minplane<<<grid_for(n), 256, 0, st>>>(wv, n, P.wmin, P.xdw, P.W, ptr<uint32_t>(key),
+                                             ptr<uint32_t>(ord));
+  DN_LAUNCHED();
+}
+
 // ---- vis2dirty
 template <typename T, typename C>
 static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
@@ -911,8 +959,6 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
     DN_LAUNCHED();
     return;
   }
-  PlaneOrder<C> po;
-  plane_order<T, C>(cv, P, true, po, st);
   Buf pm(size_t(nx * ny) * 8, st);
   k_wg_pixel_nm1<<<grid_for(nx * ny), 256, 0, st>>>(img_geom(P, nx, ny, psx, psy),
                                                     ptr<double>(pm));
@@ -920,6 +966,33 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
   const KernelPoly<C> kp = make_poly<C>(P.W, P.beta, P.e0);
   const ImgGeom g = img_geom(P, nx, ny, psx, psy);
   Buf pv(size_t(cv.nvis) * sizeof(cplx<C>), st);
+  Buf key;
+  plane_keys(ptr<double>(cv.wv), cv.nvis, P, key, st);
+  Grouped gr(ptr<double>(cv.coord), cv.nvis, ptr<uint32_t>(key), P, nx, ny, eps, sizeof(C) == 8,
+             no, st);
+  const CorrNodes cn = make_nodes(P.W, P.beta, P.e0);
+  if (gr.gp) {
+    for (int64_t p = 0; p < P.nplanes; ++p) {
+      const uint32_t g0 = uint32_t(std::max<int64_t>(0, p - P.W + 1)), g1 = uint32_t(p + 1);
+      // values of every visibility for plane p (zero outside its planes; the
+      // chunk list of the run reads only the plane's own)
+      k_wg_plane_vals<C><<<grid_for(cv.nvis), 256, 0, st>>>(
+          ptr<cplx<C>>(cv.val), ptr<double>(cv.wv), ptr<uint32_t>(key), 0, cv.nvis, kp, P.W,
+          int(p), P.wmin, P.xdw, ptr<cplx<C>>(pv));
+      DN_LAUNCHED();
+      if (!grouped_nu2u(gr.gp, g0, g1, pv.p, img.p, false, st)) continue;
+      k_wg_screen_add<C, T><<<grid_for(nx * ny), 256, 0, st>>>(
+          ptr<cplx<C>>(img), ptr<double>(pm), g, P.wmin + double(p) * P.dw, dp, dirty.stride[0],
+          dirty.stride[1]);
+      DN_LAUNCHED();
+    }
+    k_wg_correct<T><<<grid_for(nx * ny), 256, 0, st>>>(dp, dirty.stride[0], dirty.stride[1], g,
+                                                       cn, P.dw, o.divide_by_n);
+    DN_LAUNCHED();
+    return;
+  }
+  PlaneOrder<C> po;
+  plane_order<T, C>(cv, P, true, po, st);
   for (int64_t p = 0; p < P.nplanes; ++p) {
     const uint32_t lo = po.start[size_t(std::max<int64_t>(0, p - P.W + 1))];
     const uint32_t hi = po.start[size_t(p + 1)];
@@ -937,7 +1010,6 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
         dirty.stride[1]);
     DN_LAUNCHED();
   }
-  const CorrNodes cn = make_nodes(P.W, P.beta, P.e0);
   k_wg_correct<T><<<grid_for(nx * ny), 256, 0, st>>>(dp, dirty.stride[0], dirty.stride[1], g, cn,
                                                      P.dw, o.divide_by_n);
   DN_LAUNCHED();
@@ -988,14 +1060,36 @@ static void dirty2vis_t(const Inputs &in, const Arr &dirty, double psx, double p
     DN_LAUNCHED();
     return;
   }
-  PlaneOrder<C> po;
-  plane_order<T, C>(cv, P, false, po, st);
   Buf pm(size_t(nx * ny) * 8, st);
   k_wg_pixel_nm1<<<grid_for(nx * ny), 256, 0, st>>>(g, ptr<double>(pm));
   DN_LAUNCHED();
   const KernelPoly<C> kp = make_poly<C>(P.W, P.beta, P.e0);
   DN_CUDA(cudaMemsetAsync(acc.p, 0, size_t(cv.nvis) * sizeof(cplx<C>), st));
   Buf res(size_t(cv.nvis) * sizeof(cplx<C>), st);
+  Buf key;
+  plane_keys(ptr<double>(cv.wv), cv.nvis, P, key, st);
+  Grouped gr(ptr<double>(cv.coord), cv.nvis, ptr<uint32_t>(key), P, nx, ny, eps, sizeof(C) == 8,
+             no, st);
+  if (gr.gp) {
+    for (int64_t p = 0; p < P.nplanes; ++p) {
+      const uint32_t g0 = uint32_t(std::max<int64_t>(0, p - P.W + 1)), g1 = uint32_t(p + 1);
+      k_wg_screen_apply<C><<<grid_for(nx * ny), 256, 0, st>>>(
+          ptr<C>(img0), ptr<double>(pm), nx * ny, P.wmin + double(p) * P.dw, ptr<cplx<C>>(img));
+      DN_LAUNCHED();
+      if (!grouped_u2nu(gr.gp, g0, g1, img.p, res.p, true, st)) continue;
+      k_wg_degrid_acc_all<C><<<grid_for(cv.nvis), 256, 0, st>>>(
+          ptr<cplx<C>>(res), ptr<double>(cv.wv), ptr<uint32_t>(key), cv.nvis, kp, P.W, int(p),
+          P.wmin, P.xdw, ptr<cplx<C>>(acc));
+      DN_LAUNCHED();
+    }
+    k_wg_scatter<T, C><<<grid_for(cv.nvis), 256, 0, st>>>(
+        ptr<cplx<C>>(acc), ptr<double>(cv.coord), ptr<double>(cv.wv), ptr<uint32_t>(cv.idx),
+        cv.nvis, in.c, P.lshift, P.mshift, P.nshift, vp, vis.stride[0], vis.stride[1]);
+    DN_LAUNCHED();
+    return;
+  }
+  PlaneOrder<C> po;
+  plane_order<T, C>(cv, P, false, po, st);
   for (int64_t p = 0; p < P.nplanes; ++p) {
     const uint32_t lo = po.start[size_t(std::max<int64_t>(0, p - P.W + 1))];
     const uint32_t hi = po.start[size_t(p + 1)];
