@@ -1887,10 +1887,14 @@ GroupedPlan *grouped_plan_create(const double *coord, uint32_t M, const uint32_t
   DN_REQUIRE(!s.qbits, ST_INTERNAL, "grouped index with a tensor-core key");
   const int tilebits = s.keybits;
   gp->gbits = bits_for(ngroups);
-  // the (tile, group) start table has 2^(tilebits + gbits) + 1 entries
-  if (tilebits + gp->gbits > 24 || M == 0 || ngroups == 0) return nullptr;
+  // keys (tile << gbits | group) in 32 bits, and a start table of
+  // ntiles * 2^gbits + 1 entries of at most 512 MB
+  const uint64_t ntiles = uint64_t(s.g.ntiles[0]) * uint64_t(s.g.ntiles[1]);
+  if (tilebits + gp->gbits > 32 || (ntiles << gp->gbits) > (uint64_t(1) << 27) || M == 0 ||
+      ngroups == 0)
+    return nullptr;
   gp->ngroups = ngroups;
-  gp->ntiles = uint32_t(1) << tilebits;
+  gp->ntiles = uint32_t(ntiles);
   gp->dc = &consts_for(s, gp->dcl, st);
   DevBuf keys(size_t(M) * 4, st);
   gp->perm = DevBuf(size_t(M) * 4, st);
@@ -1902,7 +1906,7 @@ GroupedPlan *grouped_plan_create(const double *coord, uint32_t M, const uint32_t
     DevBuf ws(radix_workspace_bytes(M, total), st);
     radix_sort_pairs(keys.as<uint32_t>(), gp->perm.as<uint32_t>(), M, total, ws.p, st);
   }
-  const uint32_t nkeys = uint32_t(1) << total;
+  const uint32_t nkeys = gp->ntiles << gp->gbits;
   gp->start = DevBuf(size_t(nkeys + 1) * 4, st);
   launch_key_starts(keys.as<uint32_t>(), M, nkeys, gp->start.as<uint32_t>(), st);
   gp->sorted_coord = DevBuf(size_t(M) * 16, st);
