@@ -225,8 +225,15 @@ __device__ __forceinline__ void spread_chunk(const PointsDesc &pts, const Chunk 
   }
 }
 
+// four CTAs per SM for single-precision values at float64 coordinates (whose
+// exact fold takes many registers): sparse tiles, where the CTAs are short,
+// need the warps
+template <typename T, typename Tc> constexpr int spread_min_ctas() {
+  return (sizeof(T) == 4 && sizeof(Tc) == 8) ? 4 : 1;
+}
+
 template <typename T, typename Tc, int NDIM, int W>
-__global__ void __launch_bounds__(SP_THREADS)
+__global__ void __launch_bounds__(SP_THREADS, spread_min_ctas<T, Tc>())
     k_spread(PointsDesc pts, const Chunk *__restrict__ chunks, Geometry g, KernelPoly<T> kp,
              const cplx<T> *__restrict__ values, int64_t vs, int64_t vtrans,
              cplx<T> *__restrict__ grid, int64_t gtrans) {
