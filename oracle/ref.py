@@ -1,9 +1,11 @@
-"""Loader for DUCC's own CPU NUFFT, built from the reference sources by
-``oracle/Makefile`` into ``oracle/_ref`` - TEST INFRASTRUCTURE ONLY.
+"""Loader for DUCC's own CPU NUFFT and w-gridder, built from the reference
+sources by ``oracle/Makefile`` into ``oracle/_ref`` - TEST INFRASTRUCTURE ONLY.
 
 ``load()`` returns the compiled module (or None when it was not built).  It
 exposes DUCC's ``nufft`` functions and plan class unchanged (``nu2u``, ``u2nu``,
-``plan``, ``bestEpsilon``) plus the read-only probes of ``ref_glue.cc``.
+``plan``, ``bestEpsilon``), its ``wgridder`` module (``vis2dirty``,
+``dirty2vis``, ``ms2dirty``, ``dirty2ms``) and the read-only probes of
+``ref_glue.cc``.
 The widest ISA variant that the running CPU supports is picked.
 """
 import importlib.util
