@@ -617,7 +617,10 @@ static Params choose(int64_t nx, int64_t ny, double psx, double psy, double epsi
   P.nshift = (!o.allow_nshift || !do_w) ? 0. : -0.5 * (P.nm1max + P.nm1min);
   auto idx = available_kernels(epsilon, do_w ? 3 : 2, singleprec, o.sigma_min, o.sigma_max);
   const double nref_fft = 2048, costref_fft = 0.0693;
-  const size_t vlen = singleprec ? 8 : 4;   // DUCC's SIMD width on an AVX2 build
+  // DUCC's SIMD width in this model is min(8, native lanes): 8 for float, and
+  // 8 for double on an AVX-512 build (4 on AVX2); the NUFFT planner's
+  // default assumes the same build
+  const size_t vlen = 8;
   const double nt = double(effective_threads(o.nthreads));
   double mincost = 1e300;
   for (size_t i : idx) {

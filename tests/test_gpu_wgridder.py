@@ -388,3 +388,28 @@ def test_torch_tensors_in_place(ng):
     assert r is vout
     vref = ng.dirty2vis(uvw=uvw, freq=freq, dirty=dirty, wgt=wgt, mask=mask, **args)
     assert O.l2error(vout.cpu().numpy(), vref) < 1e-6
+
+
+@pmp("singleprec,epsilon", [(True, 1e-4), (True, 1e-5), (False, 1e-7), (False, 1e-11)])
+@pmp("do_w", (True, False))
+@pmp("nthreads", (1, 16))
+def test_parameters_match_ducc(ng, ducc, capfd, singleprec, epsilon, do_w, nthreads):
+    """The kernel support, oversampled grid and number of w planes are DUCC's
+    (its cost model, printed with verbosity=1) for the same call."""
+    import re
+    from oracle import ref
+    if not singleprec and ref.simd_lanes_double() != 8:
+        pytest.skip("the reference build's float64 SIMD width is not the modelled one")
+    ps, freq, uvw, vis, wgt, _, _ = _ms_problem(31, 20000, 8, 512, 8., singleprec, False)
+    args = dict(uvw=uvw, freq=freq, wgt=wgt, npix_x=512, npix_y=384, pixsize_x=ps,
+                pixsize_y=ps, epsilon=epsilon, do_wgridding=do_w, nthreads=nthreads)
+    capfd.readouterr()
+    ducc.vis2dirty(vis=vis, verbosity=1, **args)
+    out = capfd.readouterr().out
+    m = re.search(r"grid=\((\d+)x(\d+)(?:x(\d+))?\), supp=(\d+)", out)
+    assert m, out
+    mine = ng.wgrid_params(vis=vis, **args)
+    assert (mine["nu"], mine["nv"], mine["supp"]) == (int(m.group(1)), int(m.group(2)),
+                                                      int(m.group(4)))
+    if do_w:
+        assert mine["nplanes"] == int(m.group(3))
