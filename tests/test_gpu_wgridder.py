@@ -413,3 +413,21 @@ def test_parameters_match_ducc(ng, ducc, capfd, singleprec, epsilon, do_w, nthre
                                                       int(m.group(4)))
     if do_w:
         assert mine["nplanes"] == int(m.group(3))
+
+
+@pmp("singleprec,epsilon", [(True, 1e-5), (False, 1e-9)])
+def test_against_ducc_large(ng, ducc, singleprec, epsilon):
+    """400k visibilities on a 2048^2 image at a 5 degree field of view (some
+    tens of w planes, about 4e5 tiles of the oversampled grid): both
+    directions against DUCC."""
+    ps, freq, uvw, vis, wgt, mask, dirty = _ms_problem(41, 50000, 8, 2048, 5., singleprec, True)
+    args = dict(uvw=uvw, freq=freq, wgt=wgt, mask=mask, pixsize_x=ps, pixsize_y=ps,
+                epsilon=epsilon, do_wgridding=True, nthreads=16)
+    p = ng.wgrid_params(vis=vis, npix_x=2048, npix_y=2048, **args)
+    assert p["nplanes"] >= 10
+    d_ours = ng.vis2dirty(vis=vis, npix_x=2048, npix_y=2048, **args)
+    d_ref = ducc.vis2dirty(vis=vis, npix_x=2048, npix_y=2048, **args)
+    assert O.l2error(d_ours, d_ref) <= 2 * epsilon
+    v_ours = ng.dirty2vis(dirty=dirty, **args)
+    v_ref = ducc.dirty2vis(dirty=dirty, **args)
+    assert O.l2error(v_ours, v_ref) <= 2 * epsilon
