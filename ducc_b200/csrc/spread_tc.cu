@@ -9,12 +9,17 @@
 //     A.B = Ahi.Bhi + Ahi.Blo + Alo.Bhi + Alo.Blo
 // keeps ~22 significant bits of each operand.  One MMA does all four products and both
 // complex parts at once:
-//     A (M=128 x K=16 points) rows = [Re(c)ku hi | Im(c)ku hi | Re(c)ku lo | Im(c)ku lo]
-//                                    24 rows each (rows 96..127 stay zero)
-//     B (K=16 x N=48)         cols = [kv hi | kv lo], 24 columns each
-//     D (128 x 48, FP32, TMEM):  Re = D[0:24, 0:24] + D[0:24, 24:48] + D[48:72, 0:24]
-//                                     + D[48:72, 24:48]  (and Im from rows 24:48, 72:96)
-// (the Alo.Blo block costs nothing extra: the MMA computes it anyway).  A 32x32 tile (DUCC's 2D
+//     A (M=128 x K=16 points) rows: hi block 0..47, row 2u + c = hi part of
+//                             c-th component (Re, Im) of Re/Im(c) ku[u]; lo
+//                             block 48..95 the same for the lo parts (rows
+//                             96..127 stay zero)
+//     B (K=16 x N=48)         column 2v + h: part h (hi, lo) of kv[v]
+//     D (128 x 48, FP32, TMEM):  Re at window (u, v) = D[2u, 2v] + D[2u, 2v+1]
+//                                 + D[48+2u, 2v] + D[48+2u, 2v+1] (Im: rows 2u+1)
+// (the Alo.Blo block costs nothing extra: the MMA computes it anyway).
+// Interleaving the parts puts each tap of a point in one 32-bit word of its
+// operand column (Re and Im of A, hi and lo of B), so a point's taps land at a
+// whole-word offset and are placed with word selects only.  A 32x32 tile (DUCC's 2D
 // single-precision tile) is split into four 16x16 quadrants with their own
 // accumulators, so a point's <= 8 taps always fit the 24 rows/columns of its
 // quadrant window.  Points arrive sorted by (tile, quadrant); the plan cuts
@@ -262,36 +267,51 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
   lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-// 8 halves (4 words) shifted up by r halves (0..7) across two 8-half chunks:
-// z[0..3] = low chunk, z[4..7] = high chunk
-__device__ __forceinline__ void place8(const uint32_t (&h)[4], int r, uint32_t (&z)[8]) {
-  const uint32_t bs = (r & 1) ? 16u : 0u;
-  uint32_t x[5];
-  x[0] = __funnelshift_l(0u, h[0], bs);
-  x[1] = __funnelshift_l(h[0], h[1], bs);
-  x[2] = __funnelshift_l(h[1], h[2], bs);
-  x[3] = __funnelshift_l(h[2], h[3], bs);
-  x[4] = __funnelshift_l(h[3], 0u, bs);
-  const int ws = r >> 1;
-  uint32_t y[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    uint32_t a = (j < 5) ? x[j] : 0u;
-    uint32_t b = (j >= 2 && j - 2 < 5) ? x[j - 2] : 0u;
-    y[j] = (ws & 2) ? b : a;
-  }
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    uint32_t b = (j >= 1) ? y[j - 1] : 0u;
-    z[j] = (ws & 1) ? b : y[j];
-  }
+// hi = RN_fp16(x) in the low half, lo = RN_fp16(x - hi) in the high half
+__device__ __forceinline__ uint32_t split1(float x) {
+  const __half h = __float2half_rn(x);
+  const __half l = __float2half_rn(x - __half2float(h));
+  return uint32_t(__half_as_ushort(h)) | (uint32_t(__half_as_ushort(l)) << 16);
 }
+
+// Words d[0..7] of a point's operand column at word offset off (0..16) of a
+// 24-word (6-chunk) part: y = the words shifted up by off & 3, written to
+// chunks off/4 .. off/4 + 2, zeros to the other three (chunk indices taken
+// mod 6, so the six stores cover the part once; for off = 16 the third of
+// them is a zero chunk that wraps to chunk 0)
+__device__ __forceinline__ void place24(const uint32_t (&d)[8], int off, uint32_t base);
 
 __device__ __forceinline__ void st_v4(uint32_t saddr, uint32_t a, uint32_t b, uint32_t c,
                                       uint32_t d) {
   asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(saddr), "r"(a), "r"(b), "r"(c),
                "r"(d)
                : "memory");
+}
+
+__device__ __forceinline__ void place24(const uint32_t (&d)[8], int off, uint32_t base) {
+  const int r = off & 3, c0 = off >> 2;
+  uint32_t x[10], y[12];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const uint32_t a = (i < 8) ? d[i] : 0u;
+    const uint32_t b = (i >= 2) ? d[i - 2] : 0u;
+    x[i] = (r & 2) ? b : a;
+  }
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const uint32_t a = (i < 10) ? x[i] : 0u;
+    const uint32_t b = (i >= 1) ? x[i - 1] : 0u;
+    y[i] = (r & 1) ? b : a;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    int c = c0 + k;
+    c = (c >= 6) ? c - 6 : c;
+    if (k < 3)
+      st_v4(base + uint32_t(c) * SBO, y[4 * k], y[4 * k + 1], y[4 * k + 2], y[4 * k + 3]);
+    else
+      st_v4(base + uint32_t(c) * SBO, 0u, 0u, 0u, 0u);
+  }
 }
 
 // per-slot layout of the point-data ring
@@ -513,10 +533,11 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         }
       }
       mbar_arrive(&pre_empty[ps]);
-      // part words: A: 0 Re hi, 1 Im hi, 2 Re lo, 3 Im lo; B: 0 hi, 1 lo
-      uint32_t hw[4][4];
+      // one word per tap: A: (Re, Im) hi in wh, (Re, Im) lo in wl; B: (hi, lo)
+      // in wh
+      uint32_t wh[8], wl[8];
 #pragma unroll
-      for (int w = 0; w < 4; ++w) hw[0][w] = hw[1][w] = hw[2][w] = hw[3][w] = 0u;
+      for (int t = 0; t < 8; ++t) wh[t] = wl[t] = 0u;
       int off = 0;
       if (valid) {
         int i0;
@@ -527,16 +548,10 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         kernel_weights<float, W>(kp, float(double(W - 1) - 2.0 * fr), k);
         if (grp == 0) {
 #pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            const float k0 = (2 * w < W) ? k[2 * w] : 0.f, k1 = (2 * w + 1 < W) ? k[2 * w + 1] : 0.f;
-            split2(k0 * s0, k1 * s0, hw[0][w], hw[2][w]);
-            split2(k0 * s1, k1 * s1, hw[1][w], hw[3][w]);
-          }
+          for (int t = 0; t < W; ++t) split2(k[t] * s0, k[t] * s1, wh[t], wl[t]);
         } else {
 #pragma unroll
-          for (int w = 0; w < 4; ++w)
-            split2((2 * w < W) ? k[2 * w] * s0 : 0.f, (2 * w + 1 < W) ? k[2 * w + 1] * s0 : 0.f,
-                   hw[0][w], hw[1][w]);
+          for (int t = 0; t < W; ++t) wh[t] = split1(k[t] * s0);
         }
       }
       const int s = r % NST;
@@ -545,30 +560,20 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         break;
       if (np > 0) {
         unsigned char *stA = stages + s * STAGE_BYTES;
-        const int c0 = off >> 3;   // 0 or 1: taps in chunks c0, c0+1 of the part
-        const int cz = (c0 == 0) ? 2 : 0;
-        // A column of point e: part p at rows 24p..24p+23; B row of point e:
-        // part h at columns 24h..24h+23
+        // A column of point e: hi block at rows 0..47 (chunks 0..5), lo block at
+        // rows 48..95 (chunks 6..11); B row of point e: columns 0..47
         const uint32_t base =
             grp == 0 ? smem_u32(stA + kbl * A_BYTES) + (e & 7) * 16 + (e >> 3) * A_LBO
                      : smem_u32(stA + ROUND * A_BYTES + kbl * B_BYTES) + (e & 7) * 16 +
                            (e >> 3) * B_LBO;
-        const int nparts = grp == 0 ? 4 : 2;
+        if (valid) {
+          place24(wh, off, base);
+          if (grp == 0) place24(wl, off, base + uint32_t(2 * PART) * SBO);
+        } else {
+          const int nchunk = grp == 0 ? 4 * PART : 2 * PART;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          if (h >= nparts) break;
-          const uint32_t pb = base + uint32_t(h * PART) * SBO;
-          if (valid) {
-            uint32_t z[8];
-            place8(hw[h], off & 7, z);
-            st_v4(pb + uint32_t(c0) * SBO, z[0], z[1], z[2], z[3]);
-            st_v4(pb + uint32_t(c0 + 1) * SBO, z[4], z[5], z[6], z[7]);
-            st_v4(pb + uint32_t(cz) * SBO, 0u, 0u, 0u, 0u);
-          } else {
-            st_v4(pb, 0u, 0u, 0u, 0u);
-            st_v4(pb + SBO, 0u, 0u, 0u, 0u);
-            st_v4(pb + 2 * SBO, 0u, 0u, 0u, 0u);
-          }
+          for (int c = 0; c < 4 * PART; ++c)
+            if (c < nchunk) st_v4(base + uint32_t(c) * SBO, 0u, 0u, 0u, 0u);
         }
       }
       fence_proxy_async();
@@ -654,7 +659,9 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
     // planes); when the tile changes, the set goes to the flusher warps and the
     // epilogue continues in the other one.  Hand-off h uses set h & 1.
     const int L = tid;                   // tensor-memory lane 0..127
-    const int p = L / 24, u = L - 24 * (L / 24);
+    // lane 48 b + 2 u + c: window row u of part p = 2 b + c (0 Re hi, 1 Im hi,
+    // 2 Re lo, 3 Im lo); lanes 96..127 hold nothing
+    const int p = (L < 96) ? 2 * (L / 48) + (L & 1) : 4, u = (L % 48) >> 1;
     uint32_t h = 0;                      // plane sets handed to the flusher so far
     bool have = false;                   // set h & 1 holds data of tile cur_tile
     uint32_t cur_tile = 0, cur_dq = 0;   // cur_dq: dirty quadrants of the set
@@ -712,10 +719,11 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
             float *dst = plane + (u + ((q & 2) ? 16 : 0)) * PP + ((q & 1) ? 16 : 0);
 #pragma unroll
             for (int v = 0; v < 24; ++v) {
-              // columns v (kv hi) and 24 + v (kv lo): hi.hi + hi.lo in the hi
-              // rows, lo.hi + lo.lo in the lo rows
-              const float val = __uint_as_float(v < 16 ? d0[v] : d1[v - 16]) +
-                                __uint_as_float(v + 24 < 32 ? d1[v + 8] : d2[v - 8]);
+              // columns 2v (kv hi) and 2v + 1 (kv lo): hi.hi + hi.lo in the
+              // hi rows, lo.hi + lo.lo in the lo rows
+              const int a = 2 * v, b = 2 * v + 1;
+              const float val = __uint_as_float(a < 16 ? d0[a] : (a < 32 ? d1[a - 16] : d2[a - 32])) +
+                                __uint_as_float(b < 16 ? d0[b] : (b < 32 ? d1[b - 16] : d2[b - 32]));
               dst[v] += val;
             }
           }
