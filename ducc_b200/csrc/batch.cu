@@ -44,8 +44,15 @@ __device__ __forceinline__ void load_instance(const SpreadInst<T> *__restrict__ 
                case 14: X(14) break; case 15: X(15) break; case 16: X(16) break;              \
                default: break; }
 
+// CTAs per SM the register allocation must allow: the kernels hold every
+// support and both coordinate types, and without a bound the largest case sets
+// the register count for all (110 for single precision: two CTAs per SM,
+// too few warps for the short CTAs of small instances)
+template <typename T> constexpr int multi_spread_min_ctas() { return sizeof(T) == 4 ? 4 : 1; }
+template <typename T> constexpr int multi_interp_min_ctas() { return sizeof(T) == 4 ? 6 : 1; }
+
 template <typename T>
-__global__ void __launch_bounds__(SP_THREADS)
+__global__ void __launch_bounds__(SP_THREADS, multi_spread_min_ctas<T>())
     k_spread_multi(const SpreadInst<T> *__restrict__ insts, int ninst,
                    const BatchArray *__restrict__ vals) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -73,7 +80,7 @@ __global__ void __launch_bounds__(SP_THREADS)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(SP_THREADS)
+__global__ void __launch_bounds__(SP_THREADS, multi_interp_min_ctas<T>())
     k_interp_multi(const SpreadInst<T> *__restrict__ insts, int ninst,
                    const BatchArray *__restrict__ outs) {
   extern __shared__ __align__(16) unsigned char smraw[];
