@@ -49,7 +49,8 @@ class WgridOpts(ctypes.Structure):
                 ("flip_w", ctypes.c_int32), ("divide_by_n", ctypes.c_int32),
                 ("allow_nshift", ctypes.c_int32),
                 ("double_precision_accumulation", ctypes.c_int32),
-                ("verbosity", ctypes.c_int32)]
+                ("verbosity", ctypes.c_int32), ("plane_begin", ctypes.c_int32),
+                ("plane_count", ctypes.c_int32)]
 
 
 class WgridInfo(ctypes.Structure):

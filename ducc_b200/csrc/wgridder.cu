@@ -868,6 +868,12 @@ static void plane_order(Compacted<T, C> &cv, const Params &P, bool gridding,
   DN_CUDA(cudaStreamSynchronize(st));
 }
 
+// planes [p0, p1) of this call (the caller's share of a split)
+static void plane_range(const Params &P, const dnufft_wgrid_opts &o, int64_t &p0, int64_t &p1) {
+  p0 = std::max<int64_t>(0, o.plane_begin);
+  p1 = o.plane_count > 0 ? std::min<int64_t>(P.nplanes, p0 + o.plane_count) : P.nplanes;
+}
+
 static dnufft_opts nufft_opts(const Params &P, double psx, double psy, const dnufft_wgrid_opts &o) {
   dnufft_opts no;
   dnufft_default_opts(&no, 0);
@@ -947,6 +953,9 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
   if (nvis == 0) return;
   const Params P = choose(nx, ny, psx, psy, eps, sizeof(T) == 4, o, nvis, wmin_d, wmax_d);
   if (o.verbosity > 0) report(P, "vis2dirty", nx, ny, nvis, do_w);
+  int64_t pl0, pl1;
+  plane_range(P, o, pl0, pl1);
+  if (do_w ? pl1 <= pl0 : pl0 > 0) return;   // no plane of this share
   Compacted<T, C> cv;
   compact<T, C>(in, true, &P, cv, st);
   const dnufft_opts no = nufft_opts(P, psx, psy, o);
@@ -975,7 +984,7 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
              no, st);
   const CorrNodes cn = make_nodes(P.W, P.beta, P.e0);
   if (gr.gp) {
-    for (int64_t p = 0; p < P.nplanes; ++p) {
+    for (int64_t p = pl0; p < pl1; ++p) {
       const uint32_t g0 = uint32_t(std::max<int64_t>(0, p - P.W + 1)), g1 = uint32_t(p + 1);
       // values of every visibility for plane p (zero outside its planes; the
       // chunk list of the run reads only the plane's own)
@@ -996,7 +1005,7 @@ static void vis2dirty_t(const Inputs &in, double psx, double psy, double eps,
   }
   PlaneOrder<C> po;
   plane_order<T, C>(cv, P, true, po, st);
-  for (int64_t p = 0; p < P.nplanes; ++p) {
+  for (int64_t p = pl0; p < pl1; ++p) {
     const uint32_t lo = po.start[size_t(std::max<int64_t>(0, p - P.W + 1))];
     const uint32_t hi = po.start[size_t(p + 1)];
     if (hi <= lo) continue;
@@ -1037,6 +1046,9 @@ static void dirty2vis_t(const Inputs &in, const Arr &dirty, double psx, double p
   if (nvis == 0) return;
   const Params P = choose(nx, ny, psx, psy, eps, sizeof(T) == 4, o, nvis, wmin_d, wmax_d);
   if (o.verbosity > 0) report(P, "dirty2vis", nx, ny, nvis, do_w);
+  int64_t pl0, pl1;
+  plane_range(P, o, pl0, pl1);
+  if (do_w ? pl1 <= pl0 : pl0 > 0) return;   // no plane of this share: zeros
   Compacted<T, C> cv;
   compact<T, C>(in, false, &P, cv, st);
   const dnufft_opts no = nufft_opts(P, psx, psy, o);
@@ -1074,7 +1086,7 @@ static void dirty2vis_t(const Inputs &in, const Arr &dirty, double psx, double p
   Grouped gr(ptr<double>(cv.coord), cv.nvis, ptr<uint32_t>(key), P, nx, ny, eps, sizeof(C) == 8,
              no, st);
   if (gr.gp) {
-    for (int64_t p = 0; p < P.nplanes; ++p) {
+    for (int64_t p = pl0; p < pl1; ++p) {
       const uint32_t g0 = uint32_t(std::max<int64_t>(0, p - P.W + 1)), g1 = uint32_t(p + 1);
       k_wg_screen_apply<C><<<grid_for(nx * ny), 256, 0, st>>>(
           ptr<C>(img0), ptr<double>(pm), nx * ny, P.wmin + double(p) * P.dw, ptr<cplx<C>>(img));
@@ -1093,7 +1105,7 @@ static void dirty2vis_t(const Inputs &in, const Arr &dirty, double psx, double p
   }
   PlaneOrder<C> po;
   plane_order<T, C>(cv, P, false, po, st);
-  for (int64_t p = 0; p < P.nplanes; ++p) {
+  for (int64_t p = pl0; p < pl1; ++p) {
     const uint32_t lo = po.start[size_t(std::max<int64_t>(0, p - P.W + 1))];
     const uint32_t hi = po.start[size_t(p + 1)];
     if (hi <= lo) continue;

@@ -41,6 +41,11 @@ floating-point sums.
 
 Independent transforms (batches, separate problems) need no collective at
 all: ``ducc_b200.shard`` splits them over the ranks by weight.
+
+The w-gridder (``vis2dirty_split`` / ``dirty2vis_split``) splits its w
+planes: each rank runs its consecutive share (spreading or interpolation and
+the 2D FFT of each of its planes) into a partial image or partial
+visibilities, and one all-reduce sums them.
 """
 import math
 
@@ -50,7 +55,8 @@ __all__ = ["global_parameters", "sum_grids", "reduce_scatter_rows", "gather_kept
            "type1_by_slabs", "RowSlabs", "row_estimate", "route_points", "route_values",
            "exchange_halos", "transpose_kept_columns", "gather_column_blocks",
            "route_back", "type1_by_row_slabs", "columns_to_row_slabs", "fill_halos",
-           "type2_by_row_slabs", "ShardedPlan"]
+           "type2_by_row_slabs", "ShardedPlan", "plane_share", "vis2dirty_split",
+           "dirty2vis_split"]
 
 
 def _count_device(group):
@@ -557,3 +563,78 @@ class ShardedPlan:
             return res
         out.copy_(res)
         return out
+
+
+# ---------------------------------------------------------------- w-gridder
+def plane_share(nplanes, world, rank):
+    """(begin, count) of rank's w planes: consecutive, sizes differing by at
+    most one."""
+    base, extra = divmod(int(nplanes), int(world))
+    begin = rank * base + min(rank, extra)
+    return begin, base + (1 if rank < extra else 0)
+
+
+def _split_wgridder(run, nplanes, group):
+    """run((begin, count)) -> this rank's partial result (a torch tensor on the
+    communicator's device, or a numpy array); the partials of all ranks are
+    summed (one all-reduce) and every rank gets the sum, in run's type.  A
+    rank without planes asks for the empty range past the last plane (count
+    0 would mean all planes), which gives zeros."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    begin, count = plane_share(nplanes, world, rank)
+    if count == 0:
+        begin, count = nplanes, 1
+    part = run((begin, count))
+    dev = _count_device(group)
+    t = part if (torch.is_tensor(part) and part.device == dev) else \
+        torch.as_tensor(np.asarray(part) if not torch.is_tensor(part) else part).to(dev)
+    dist.all_reduce(t, group=group)
+    if torch.is_tensor(part):
+        return t if t.device == part.device else t.to(part.device)
+    return t.cpu().numpy()
+
+
+def vis2dirty_split(group=None, _run=None, **kwargs):
+    """``ducc_b200.wgridder.vis2dirty`` with its w planes split over the ranks
+    of ``group`` (every rank passes the same arguments): each rank grids its
+    consecutive share of the planes into a partial image, and one all-reduce
+    sums them, so every rank returns the whole dirty image.  What crosses
+    between GPUs is one image per rank.  Without w-stacking rank 0 does the
+    work.  ``_run`` replaces the rank's computation (``_run(planes=...,
+    **kwargs)``; tests on the CPU)."""
+    from . import wgridder
+    run = _run or wgridder.vis2dirty
+    nplanes = 1
+    if kwargs.get("do_wgridding"):
+        q = {k: kwargs[k] for k in ("uvw", "freq", "vis", "wgt", "mask", "npix_x", "npix_y",
+                                    "pixsize_x", "pixsize_y", "epsilon", "do_wgridding",
+                                    "nthreads", "sigma_min", "sigma_max", "center_x",
+                                    "center_y", "flip_u", "flip_v", "flip_w", "allow_nshift")
+             if k in kwargs}
+        nplanes = int(kwargs.pop("_nplanes", 0)) or wgridder.wgrid_params(**q)["nplanes"]
+    kwargs.pop("_nplanes", None)
+    return _split_wgridder(lambda pl: run(planes=pl, **kwargs), max(nplanes, 1), group)
+
+
+def dirty2vis_split(group=None, _run=None, **kwargs):
+    """``ducc_b200.wgridder.dirty2vis`` with its w planes split over the ranks
+    of ``group`` (every rank passes the same arguments): each rank degrids its
+    share of the planes and one all-reduce sums the visibilities."""
+    from . import wgridder
+    run = _run or wgridder.dirty2vis
+    nplanes = 1
+    if kwargs.get("do_wgridding"):
+        q = {k: kwargs[k] for k in ("uvw", "freq", "wgt", "mask", "pixsize_x", "pixsize_y",
+                                    "epsilon", "do_wgridding", "nthreads", "sigma_min",
+                                    "sigma_max", "center_x", "center_y", "flip_u", "flip_v",
+                                    "flip_w", "allow_nshift")
+             if k in kwargs}
+        d = kwargs["dirty"]
+        nplanes = int(kwargs.pop("_nplanes", 0)) or wgridder.wgrid_params(
+            npix_x=d.shape[0], npix_y=d.shape[1], **q)["nplanes"]
+    kwargs.pop("_nplanes", None)
+    return _split_wgridder(lambda pl: run(planes=pl, **kwargs), max(nplanes, 1), group)

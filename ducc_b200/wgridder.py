@@ -43,7 +43,8 @@ def _dev(x, dtype=None):
 
 
 def _opts(nthreads, verbosity, sigma_min, sigma_max, center_x, center_y, do_wgridding, flip_u,
-          flip_v, flip_w, divide_by_n, allow_nshift, double_precision_accumulation=False):
+          flip_v, flip_w, divide_by_n, allow_nshift, double_precision_accumulation=False,
+          planes=None):
     o = C.WgridOpts()
     C.lib().dnufft_wgrid_default_opts(ctypes.byref(o))
     if int(nthreads) < 0:
@@ -61,6 +62,11 @@ def _opts(nthreads, verbosity, sigma_min, sigma_max, center_x, center_y, do_wgri
     o.divide_by_n = 1 if divide_by_n else 0
     o.allow_nshift = 1 if allow_nshift else 0
     o.double_precision_accumulation = 1 if double_precision_accumulation else 0
+    if planes is not None:
+        b, c = planes
+        if int(b) < 0 or int(c) < 0:
+            raise ValueError("planes must be (begin >= 0, count >= 0)")
+        o.plane_begin, o.plane_count = int(b), int(c)
     return o
 
 
@@ -102,9 +108,12 @@ def vis2dirty(*, uvw, freq, vis, wgt=None, npix_x=0, npix_y=0, pixsize_x, pixsiz
               do_wgridding=False, nthreads=1, verbosity=0, mask=None, flip_u=False, flip_v=False,
               flip_w=False, divide_by_n=True, dirty=None, sigma_min=1.1, sigma_max=2.6,
               center_x=0., center_y=0., allow_nshift=True, gpu=False,
-              double_precision_accumulation=False):
+              double_precision_accumulation=False, planes=None):
     """Visibilities to dirty image (``ducc0.wgridder.vis2dirty``).  ``gpu``
-    (DUCC's SYCL switch) is accepted and has no effect."""
+    (DUCC's SYCL switch) is accepted and has no effect.  Addition:
+    ``planes=(begin, count)`` grids only those w planes (a share of a split
+    over processes: the images of a partition of the planes sum to the whole
+    image; ``ducc_b200.distributed.vis2dirty_split`` does the split)."""
     torch = _torch()
     d_vis, host_vis = _dev(vis)
     if d_vis.dtype not in (torch.complex64, torch.complex128):
@@ -128,7 +137,8 @@ def vis2dirty(*, uvw, freq, vis, wgt=None, npix_x=0, npix_y=0, pixsize_x, pixsiz
             d_dirty = torch.empty(tuple(dirty.shape), dtype=rdt, device=d_vis.device)
             host_out = True
     o = _opts(nthreads, verbosity, sigma_min, sigma_max, center_x, center_y, do_wgridding,
-              flip_u, flip_v, flip_w, divide_by_n, allow_nshift, double_precision_accumulation)
+              flip_u, flip_v, flip_w, divide_by_n, allow_nshift, double_precision_accumulation,
+              planes)
     st = ctypes.c_void_p(torch.cuda.current_stream(d_vis.device).cuda_stream)
     a_dirty = C.describe(d_dirty)
     C.check(C.lib().dnufft_vis2dirty(_desc(d_uvw), _desc(d_freq), _desc(d_vis), _desc(d_wgt),
@@ -143,9 +153,11 @@ def vis2dirty(*, uvw, freq, vis, wgt=None, npix_x=0, npix_y=0, pixsize_x, pixsiz
 def dirty2vis(*, uvw, freq, dirty, wgt=None, pixsize_x, pixsize_y, epsilon, do_wgridding=False,
               nthreads=1, verbosity=0, mask=None, flip_u=False, flip_v=False, flip_w=False,
               divide_by_n=True, vis=None, sigma_min=1.1, sigma_max=2.6, center_x=0.,
-              center_y=0., allow_nshift=True, gpu=False):
+              center_y=0., allow_nshift=True, gpu=False, planes=None):
     """Dirty image to visibilities (``ducc0.wgridder.dirty2vis``).  ``gpu`` is
-    accepted and has no effect."""
+    accepted and has no effect.  Addition: ``planes=(begin, count)`` as in
+    ``vis2dirty`` (the visibilities of a partition of the planes sum to the
+    whole result)."""
     torch = _torch()
     d_dirty, host_dirty = _dev(dirty)
     if d_dirty.dtype not in (torch.float32, torch.float64):
@@ -158,7 +170,7 @@ def dirty2vis(*, uvw, freq, dirty, wgt=None, pixsize_x, pixsize_y, epsilon, do_w
     else:
         d_vis = torch.empty((nrows, nchan), dtype=cdt, device=d_dirty.device)
     o = _opts(nthreads, verbosity, sigma_min, sigma_max, center_x, center_y, do_wgridding,
-              flip_u, flip_v, flip_w, divide_by_n, allow_nshift)
+              flip_u, flip_v, flip_w, divide_by_n, allow_nshift, planes=planes)
     st = ctypes.c_void_p(torch.cuda.current_stream(d_dirty.device).cuda_stream)
     a_vis = C.describe(d_vis)
     C.check(C.lib().dnufft_dirty2vis(_desc(d_uvw), _desc(d_freq), _desc(d_dirty), _desc(d_wgt),

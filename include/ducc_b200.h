@@ -324,6 +324,12 @@ typedef struct dnufft_wgrid_opts {
   int32_t allow_nshift;   /* DUCC's default 1: centre the w-screen phases        */
   int32_t double_precision_accumulation;   /* single-precision data, double grids */
   int32_t verbosity;      /* 1: print the chosen parameters                      */
+  /* Only w planes [plane_begin, plane_begin + plane_count) of the call's
+   * planes (plane_count 0: all), for a split over processes: the results of
+   * calls over a partition of the planes sum to the whole result (without
+   * w-stacking the one plane is plane 0).  No DUCC counterpart. */
+  int32_t plane_begin;
+  int32_t plane_count;
 } dnufft_wgrid_opts;
 
 /* DUCC's keyword defaults of vis2dirty / dirty2vis. */

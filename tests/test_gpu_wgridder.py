@@ -431,3 +431,33 @@ def test_against_ducc_large(ng, ducc, singleprec, epsilon):
     v_ours = ng.dirty2vis(dirty=dirty, **args)
     v_ref = ducc.dirty2vis(dirty=dirty, **args)
     assert O.l2error(v_ours, v_ref) <= 2 * epsilon
+
+
+@pmp("singleprec", (False, True))
+def test_plane_shares_sum_to_whole(ng, singleprec):
+    """The planes=(begin, count) shares of ducc_b200.distributed's split: the
+    results over a partition of the w planes sum to the whole call's, a share
+    past the last plane gives zeros, and without w-stacking the one share is
+    plane 0."""
+    ps, freq, uvw, vis, wgt, mask, dirty = _ms_problem(51, 4000, 4, 200, 10., singleprec, True)
+    args = dict(uvw=uvw, freq=freq, wgt=wgt, mask=mask, pixsize_x=ps, pixsize_y=ps,
+                epsilon=1e-5 if singleprec else 1e-9, do_wgridding=True)
+    nplanes = ng.wgrid_params(vis=vis, npix_x=200, npix_y=200, **args)["nplanes"]
+    assert nplanes >= 4
+    cuts = [0, 1, nplanes // 2, nplanes]
+    shares = [(a, b - a) for a, b in zip(cuts[:-1], cuts[1:])]
+    tol = 1e-5 if singleprec else 1e-12
+    whole = ng.vis2dirty(vis=vis, npix_x=200, npix_y=200, **args)
+    parts = sum(ng.vis2dirty(vis=vis, npix_x=200, npix_y=200, planes=s, **args).astype("f8")
+                for s in shares)
+    assert O.l2error(parts, whole) < tol
+    assert np.all(ng.vis2dirty(vis=vis, npix_x=200, npix_y=200, planes=(nplanes, 1), **args) == 0)
+    vwhole = ng.dirty2vis(dirty=dirty, **args)
+    vparts = sum(ng.dirty2vis(dirty=dirty, planes=s, **args).astype("c16") for s in shares)
+    assert O.l2error(vparts, vwhole) < tol
+    assert np.all(ng.dirty2vis(dirty=dirty, planes=(nplanes, 1), **args) == 0)
+    args["do_wgridding"] = False
+    assert np.all(ng.vis2dirty(vis=vis, npix_x=200, npix_y=200, planes=(1, 1), **args) == 0)
+    # (the spreader's atomic additions come in a different order each call)
+    assert O.l2error(ng.vis2dirty(vis=vis, npix_x=200, npix_y=200, planes=(0, 1), **args),
+                     ng.vis2dirty(vis=vis, npix_x=200, npix_y=200, **args)) < tol
