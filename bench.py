@@ -435,6 +435,94 @@ def cpu_baseline_wgridder(nthreads):
     return res
 
 
+SH_LMAX, SH_NPTS, SH_EPS = 2047, 10_000_000, 1e-5
+
+
+def sphere_inputs(seed=12, lmax=SH_LMAX, npts=SH_NPTS):
+    """Synthetic inputs of the sphere workload: a spin-0 expansion to
+    lmax = mmax = 2047 with coefficients uniform in [-1, 1) (a_l0 real, as
+    DUCC's test_sht.py random_alm), complex64; 1e7 points uniform on the
+    sphere (theta = arccos U[-1, 1], phi = U[0, 2 pi)) in float64; map values
+    uniform in [-0.5, 0.5) as float32 for the adjoint direction."""
+    rng = np.random.default_rng(seed)
+    nalm = ((lmax + 1) * (lmax + 2)) // 2
+    alm = (rng.uniform(-1, 1, nalm) + 1j * rng.uniform(-1, 1, nalm)).astype(np.complex64)
+    alm[:lmax + 1] = alm[:lmax + 1].real
+    loc = np.stack([np.arccos(rng.uniform(-1, 1, npts)), rng.uniform(0, 2 * np.pi, npts)], 1)
+    mp = rng.uniform(-0.5, 0.5, (1, npts)).astype(np.float32)
+    return alm[None, :], loc, mp
+
+
+def workload_sphere(dev, steps=3, warmup=2, lmax=SH_LMAX, npts=SH_NPTS, with_outputs=False):
+    """Spin-0 synthesis at arbitrary points and its adjoint
+    (ducc0.sht.synthesis_general / adjoint_synthesis_general counterparts) at
+    eps 1e-5 in single precision, device-resident, each direction timed with
+    CUDA events over its calls."""
+    import torch
+    from ducc_b200 import _capi as C
+    from ducc_b200 import sht as SH
+    alm, loc, mp = sphere_inputs(lmax=lmax, npts=npts)
+    d_alm = torch.from_numpy(alm).to(dev)
+    d_loc = torch.from_numpy(loc).to(dev)
+    d_mp = torch.from_numpy(mp).to(dev)
+    out_map = torch.empty((1, npts), dtype=torch.float32, device=dev)
+    out_alm = torch.empty_like(d_alm)
+    kw = dict(spin=0, lmax=lmax, mmax=lmax, loc=d_loc, epsilon=SH_EPS, nthreads=16)
+    out = {}
+    for name, call in (
+            ("synthesis_general", lambda: SH.synthesis_general(alm=d_alm, map=out_map, **kw)),
+            ("adjoint_synthesis_general",
+             lambda: SH.adjoint_synthesis_general(map=d_mp, alm=out_alm, **kw))):
+        for _ in range(warmup):
+            call()
+        torch.cuda.synchronize(dev)
+        n0 = C.lib().dnufft_kernel_launches()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            call()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms": ms, "mpts_per_s": npts / (ms * 1e-3) / 1e6,
+                     "gpu_launches_per_call": (C.lib().dnufft_kernel_launches() - n0) / steps}
+    out["config"] = ("spin-0 synthesis_general / adjoint, lmax = mmax = %d (complex64 a_lm), "
+                     "%d points uniform on the sphere (float64 theta, phi), eps %g; "
+                     "device-resident" % (lmax, npts, SH_EPS))
+    if with_outputs:
+        out["_map"] = out_map.cpu().numpy()
+        out["_alm"] = out_alm.cpu().numpy()
+    return out
+
+
+def cpu_baseline_sphere(nthreads, ours_map=None, ours_alm=None):
+    """DUCC's own synthesis_general / adjoint_synthesis_general on the host
+    cores, one call of each direction on the sphere workload's inputs, and the
+    relative L2 error of our outputs against DUCC's at eps 1e-5."""
+    from oracle import ref
+    R = ref.load()
+    if R is None or not hasattr(R, "sht"):
+        return None
+    alm, loc, mp = sphere_inputs()
+    kw = dict(spin=0, lmax=SH_LMAX, mmax=SH_LMAX, loc=loc, epsilon=SH_EPS, nthreads=nthreads)
+    res = {"cores": nthreads, "kind": "reference", "sample": "one call of each direction"}
+    t0 = time.perf_counter()
+    m2 = R.sht.synthesis_general(alm=alm, **kw)
+    res["synthesis_general_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    a2 = R.sht.adjoint_synthesis_general(map=mp, **kw)
+    res["adjoint_synthesis_general_ms"] = (time.perf_counter() - t0) * 1e3
+
+    def l2(a, b):
+        a, b = np.asarray(a, np.complex128).ravel(), np.asarray(b, np.complex128).ravel()
+        return float(np.sqrt(np.sum(np.abs(a - b) ** 2) / np.sum(np.abs(b) ** 2)))
+    if ours_map is not None:
+        res["l2_vs_ducc_synthesis"] = l2(ours_map, m2)
+    if ours_alm is not None:
+        res["l2_vs_ducc_adjoint"] = l2(ours_alm, a2)
+    return res
+
+
 # ---------------------------------------------------------------- our arm
 def cpu_baseline_leg(args, coord, vals, grid, budget_s=20.0):
     """DUCC's CPU NUFFT on the host cores (same planned step, same inputs),
@@ -749,7 +837,8 @@ def run_ours(args, rank, world, local_rank):
         for name, fn in (("batched_uneven_2d", workload_batched),
                          ("radial_autograd_2d", workload_autograd),
                          ("type2_3d_256", workload_3d),
-                         ("wgridder", workload_wgridder)):
+                         ("wgridder", workload_wgridder),
+                         ("sphere_synthesis", lambda d: workload_sphere(d, with_outputs=True))):
             try:
                 workloads[name] = fn(dev)
             except Exception as e:   # reported, never fatal for the headline line
@@ -759,6 +848,13 @@ def run_ours(args, rank, world, local_rank):
                 workloads["wgridder"]["cpu_baseline"] = cpu_baseline_wgridder(args.param_threads)
             except Exception as e:
                 workloads["wgridder"]["cpu_baseline"] = {"error": str(e)[:200]}
+        sph = workloads["sphere_synthesis"]
+        om, oa = sph.pop("_map", None), sph.pop("_alm", None)
+        if not args.no_cpu and "error" not in sph:
+            try:
+                sph["cpu_baseline"] = cpu_baseline_sphere(args.param_threads, om, oa)
+            except Exception as e:
+                sph["cpu_baseline"] = {"error": str(e)[:200]}
     line = {
         "metric": METRIC,
         "value": world * 2 * m / (ms * 1e-3) / 1e6,
@@ -880,11 +976,13 @@ def main():
                          "independent transform per rank")
     ap.add_argument("--workload", default=None,
                     choices=["batched_uneven_2d", "radial_autograd_2d", "type2_3d_256",
-                             "wgridder"],
+                             "wgridder", "sphere_synthesis"],
                     help="run one of the extra workloads alone and print its result (for "
                          "profiling); the w-gridder one takes --wg-rows / --wg-npix")
     ap.add_argument("--wg-rows", type=int, default=WG_NROW)
     ap.add_argument("--wg-npix", type=int, default=WG_NPIX)
+    ap.add_argument("--sh-lmax", type=int, default=SH_LMAX)
+    ap.add_argument("--sh-npts", type=int, default=SH_NPTS)
     args = ap.parse_args()
     args.spreaders = args.spreaders.split(",")
     if args.workload:
@@ -892,8 +990,15 @@ def main():
         dev = torch.device("cuda", 0)
         fn = {"batched_uneven_2d": workload_batched, "radial_autograd_2d": workload_autograd,
               "type2_3d_256": workload_3d}.get(args.workload)
-        res = (fn(dev) if fn else
-               workload_wgridder(dev, nrow=args.wg_rows, npix=args.wg_npix))
+        if args.workload == "sphere_synthesis":
+            res = workload_sphere(dev, lmax=args.sh_lmax, npts=args.sh_npts,
+                                  with_outputs=not args.no_cpu)
+            om, oa = res.pop("_map", None), res.pop("_alm", None)
+            if (not args.no_cpu and args.sh_lmax == SH_LMAX and args.sh_npts == SH_NPTS):
+                res["cpu_baseline"] = cpu_baseline_sphere(args.param_threads, om, oa)
+        else:
+            res = (fn(dev) if fn else
+                   workload_wgridder(dev, nrow=args.wg_rows, npix=args.wg_npix))
         print(json.dumps({"workload": args.workload, **res}))
         return
     rank = int(os.environ.get("RANK", 0))

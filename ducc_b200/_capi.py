@@ -53,6 +53,11 @@ class WgridOpts(ctypes.Structure):
                 ("plane_count", ctypes.c_int32)]
 
 
+class ShtOpts(ctypes.Structure):
+    _fields_ = [("nthreads", ctypes.c_size_t), ("sigma_min", ctypes.c_double),
+                ("sigma_max", ctypes.c_double), ("verbosity", ctypes.c_int32)]
+
+
 class WgridInfo(ctypes.Structure):
     _fields_ = [("kernel_index", ctypes.c_int32), ("supp", ctypes.c_int32),
                 ("nu", ctypes.c_int64), ("nv", ctypes.c_int64), ("nplanes", ctypes.c_int64),
@@ -74,6 +79,7 @@ EXPORTS = [
     "dnufft_plan_rows_fft", "dnufft_plan_cols_to_uniform", "dnufft_plan_cols_to_uniform_range",
     "dnufft_plan_uniform_to_cols_range", "dnufft_plan_rows_fft_kept_in", "dnufft_plan_interp",
     "dnufft_wgrid_default_opts", "dnufft_vis2dirty", "dnufft_dirty2vis", "dnufft_wgrid_params",
+    "dnufft_sht_default_opts", "dnufft_synthesis_general", "dnufft_adjoint_synthesis_general",
 ]
 
 
@@ -143,6 +149,12 @@ def lib():
                                       ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                       P(WgridOpts), P(WgridInfo), vp]
+    L.dnufft_sht_default_opts.argtypes = [P(ShtOpts)]
+    L.dnufft_sht_default_opts.restype = None
+    for f in (L.dnufft_synthesis_general, L.dnufft_adjoint_synthesis_general):
+        f.argtypes = [P(Array), ctypes.c_size_t, ctypes.c_size_t, P(ctypes.c_int64),
+                      ctypes.c_size_t, ctypes.c_int64, P(Array), ctypes.c_double, P(ShtOpts),
+                      P(Array), vp]
     _lib = L
     return L
 

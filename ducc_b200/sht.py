@@ -1,0 +1,173 @@
+"""Spherical-harmonic synthesis at arbitrary points on the sphere and its
+adjoint on the GPU: a drop-in for ``ducc0.sht.synthesis_general`` and
+``ducc0.sht.adjoint_synthesis_general`` (python/sht_pymod.cc:805-885,
+:2299-2300 for the signatures and keyword defaults), spin 0.
+
+The work runs in the CUDA library through the C-ABI
+(``dnufft_synthesis_general`` / ``dnufft_adjoint_synthesis_general`` in
+include/ducc_b200_sht.h): a Legendre recurrence kernel onto equiangular
+rings, one 1D transform per m over the rings and one 2D transform of this
+package at the points.  Arrays may be numpy arrays (copied to the current
+CUDA device, the result copied back) or torch CUDA tensors (used in place;
+the result is a tensor).  As in DUCC, the dtype of ``alm`` (synthesis) or
+``map`` (adjoint) sets the precision and ``loc`` is float64 (theta, phi).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+
+__all__ = ["synthesis_general", "adjoint_synthesis_general"]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dev(x):
+    torch = _torch()
+    if C.is_torch(x):
+        if not x.is_cuda:
+            raise ValueError("torch tensors must live on a CUDA device")
+        return x, False
+    a = np.ascontiguousarray(np.asarray(x))
+    if not a.flags.writeable:
+        a = a.copy()
+    return torch.from_numpy(a).cuda(), True
+
+
+def _mstart(lmax, mmax, mstart):
+    """DUCC's get_mstart (python/sht_pymod.cc:124-140)."""
+    if mstart is None:
+        mmax = lmax if mmax is None else int(mmax)
+        if mmax > lmax:
+            raise RuntimeError("mmax>lmax")
+        ms = np.empty(mmax + 1, dtype=np.int64)
+        idx = 0
+        for m in range(mmax + 1):
+            ms[m] = idx - m
+            idx += lmax + 1 - m
+        return ms
+    ms = np.ascontiguousarray(np.asarray(mstart), dtype=np.int64)
+    if mmax is not None and int(mmax) + 1 != ms.shape[0]:
+        raise RuntimeError("mmax and mstart size mismatch")
+    if ms.shape[0] > lmax + 1:
+        raise RuntimeError("mmax>lmax")
+    return ms
+
+
+def _min_almdim(lmax, ms, lstride):
+    """DUCC's min_almdim (python/sht_pymod.cc:168-182)."""
+    res = 0
+    for m in range(ms.shape[0]):
+        first, last = int(ms[m]) + m * lstride, int(ms[m]) + lmax * lstride
+        if first < 0 or last < 0:
+            raise RuntimeError("impossible a_lm memory layout")
+        res = max(res, first, last)
+    return res + 1
+
+
+def _opts(nthreads, sigma_min, sigma_max, verbose):
+    o = C.ShtOpts()
+    C.lib().dnufft_sht_default_opts(ctypes.byref(o))
+    if int(nthreads) < 0:
+        raise ValueError("nthreads must be >= 0")
+    o.nthreads = int(nthreads)
+    o.sigma_min = float(sigma_min)
+    o.sigma_max = float(sigma_max)
+    o.verbosity = 1 if verbose else 0
+    return o
+
+
+def _check_mode(mode, spin):
+    if mode not in ("STANDARD", "GRAD_ONLY", "DERIV1"):
+        raise RuntimeError("unknown SHT mode")
+    if mode != "STANDARD" and spin == 0:
+        raise RuntimeError("number of components mismatch in alm")
+
+
+def _loc(loc):
+    torch = _torch()
+    d_loc, _ = _dev(loc)
+    if d_loc.dtype != torch.float64:
+        raise TypeError("unsupported combination of data types")
+    if d_loc.dim() != 2 or d_loc.shape[1] != 2:
+        raise RuntimeError("last dimension of loc must have size 2")
+    return d_loc
+
+
+def synthesis_general(*, alm, spin, lmax, loc, epsilon=1e-5, mstart=None, lstride=1, mmax=None,
+                      nthreads=1, map=None, sigma_min=1.1, sigma_max=2.6, mode="STANDARD",
+                      verbose=False):
+    """Evaluate the real map of ``alm`` at the points ``loc`` (theta, phi),
+    returning ``map`` of shape (1, npoints) (``ducc0.sht.synthesis_general``)."""
+    torch = _torch()
+    spin, lmax, lstride = int(spin), int(lmax), int(lstride)
+    _check_mode(mode, spin)
+    d_alm, host = _dev(alm)
+    if d_alm.dtype not in (torch.complex64, torch.complex128):
+        raise TypeError("unsupported combination of data types")
+    if d_alm.dim() != 2:
+        raise RuntimeError("alm must be a 2D array")
+    d_loc = _loc(loc)
+    ms = _mstart(lmax, mmax, mstart)
+    rdt = torch.float64 if d_alm.dtype == torch.complex128 else torch.float32
+    npts = int(d_loc.shape[0])
+    shape = (1 if spin == 0 else 2, npts)
+    if map is not None and C.is_torch(map):
+        d_map = map
+    else:
+        if map is not None and tuple(map.shape) != shape:
+            raise RuntimeError("bad map shape")
+        d_map = torch.empty(shape, dtype=rdt, device=d_alm.device)
+    o = _opts(nthreads, sigma_min, sigma_max, verbose)
+    st = ctypes.c_void_p(torch.cuda.current_stream(d_alm.device).cuda_stream)
+    a_alm, a_loc, a_map = C.describe(d_alm), C.describe(d_loc), C.describe(d_map)
+    C.check(C.lib().dnufft_synthesis_general(
+        ctypes.byref(a_alm), spin, lmax, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        ms.shape[0], lstride, ctypes.byref(a_loc), float(epsilon), ctypes.byref(o),
+        ctypes.byref(a_map), st))
+    if map is not None and not C.is_torch(map):
+        map[...] = d_map.cpu().numpy()
+        return map
+    return d_map.cpu().numpy() if host else d_map
+
+
+def adjoint_synthesis_general(*, map, spin, lmax, loc, epsilon=1e-5, mstart=None, lstride=1,
+                              mmax=None, nthreads=1, alm=None, sigma_min=1.1, sigma_max=2.6,
+                              mode="STANDARD", verbose=False):
+    """a_lm = sum_i map_i conj(Y_lm(loc_i)) for 0 <= m <= mmax, m <= l <= lmax,
+    returning ``alm`` of shape (1, nalm) (``ducc0.sht.adjoint_synthesis_general``)."""
+    torch = _torch()
+    spin, lmax, lstride = int(spin), int(lmax), int(lstride)
+    _check_mode(mode, spin)
+    d_map, host = _dev(map)
+    if d_map.dtype not in (torch.float32, torch.float64):
+        raise TypeError("type matching failed: 'map' has neither type 'f4' nor 'f8'")
+    if d_map.dim() != 2:
+        raise RuntimeError("map must be a 2D array")
+    d_loc = _loc(loc)
+    ms = _mstart(lmax, mmax, mstart)
+    cdt = torch.complex128 if d_map.dtype == torch.float64 else torch.complex64
+    nalm = _min_almdim(lmax, ms, lstride)
+    if alm is not None and C.is_torch(alm):
+        d_alm = alm
+    elif alm is not None:
+        if alm.shape[0] != 1 or alm.shape[1] < nalm:
+            raise RuntimeError("bad alm shape")
+        d_alm = torch.from_numpy(np.ascontiguousarray(alm)).to(d_map.device)
+    else:
+        d_alm = torch.zeros((1 if spin == 0 else 2, nalm), dtype=cdt, device=d_map.device)
+    o = _opts(nthreads, sigma_min, sigma_max, verbose)
+    st = ctypes.c_void_p(torch.cuda.current_stream(d_map.device).cuda_stream)
+    a_map, a_loc, a_alm = C.describe(d_map), C.describe(d_loc), C.describe(d_alm)
+    C.check(C.lib().dnufft_adjoint_synthesis_general(
+        ctypes.byref(a_map), spin, lmax, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        ms.shape[0], lstride, ctypes.byref(a_loc), float(epsilon), ctypes.byref(o),
+        ctypes.byref(a_alm), st))
+    if alm is not None and not C.is_torch(alm):
+        alm[...] = d_alm.cpu().numpy()
+        return alm
+    return d_alm.cpu().numpy() if host else d_alm

@@ -1,6 +1,7 @@
-// Test-infrastructure only: a Python module that compiles DUCC's own NUFFT and
-// w-gridder bindings (python/nufft_pymod.cc, python/wgridder_pymod.cc) from the
-// reference sources where they lie,
+// Test-infrastructure only: a Python module that compiles DUCC's own NUFFT,
+// w-gridder and spherical-harmonic bindings (python/nufft_pymod.cc,
+// python/wgridder_pymod.cc, python/sht_pymod.cc) from the reference sources
+// where they lie,
 // plus a few read-only probes that expose DUCC's internal index computation
 // (getpix, tile keys, the stable bucket-sort permutation), its kernel choice,
 // its piecewise-polynomial kernel coefficients and its correction factors.
@@ -29,6 +30,12 @@
 #include "ducc0/math/gl_integrator.cc"
 #include "ducc0/math/gridding_kernel.cc"
 #include "ducc0/wgridder/wgridder.cc"
+#include "ducc0/sht/sht.cc"
+#include "ducc0/healpix/healpix_tables.cc"
+#include "ducc0/healpix/healpix_base.cc"
+#include "ducc0/math/geom_utils.cc"
+#include "ducc0/math/space_filling.cc"
+#include "ducc0/math/pointing.cc"
 
 #include <pybind11/pybind11.h>
 #include <pybind11/numpy.h>
@@ -37,6 +44,7 @@
 #include "ducc0/fft/fftnd_impl.h"
 #include "python/nufft_pymod.cc"
 #include "python/wgridder_pymod.cc"
+#include "python/sht_pymod.cc"
 
 namespace py = pybind11;
 using namespace ducc0;
@@ -210,6 +218,7 @@ PYBIND11_MODULE(MODNAME, m)
   using namespace pybind11::literals;
   add_nufft(m);
   add_wgridder(m);
+  add_sht(m);
   m.def("index_probe", &probe::index_probe, py::kw_only(), "coord"_a,
         "shape"_a, "epsilon"_a, "singleprec"_a, "gridding"_a, "nthreads"_a=1,
         "sigma_min"_a=1.2, "sigma_max"_a=2.51, "periodicity"_a,
