@@ -233,16 +233,74 @@ __device__ inline void ring_sc(int j, int nring, double &s, double &c) {
   sincospi(2. * double(j) / double(nring), &s, &c);
 }
 
+// Recurrence data of the l values l0 .. l0+n-1 (n <= LCHUNK = 64) of one m,
+// staged in shared memory by the whole block (two __syncthreads inside):
+//   al, be   alpha_l, beta_l of lambda_l = alpha_l (x lambda_{l-1} - beta_l lambda_{l-2})
+//   q        Q_l = prod_{k=l0..l} alpha_k
+//   gm       gamma_l0 = beta_l0, gamma_l = beta_l / alpha_{l-1} (l > l0)
+// With mu_l = lambda_l / Q_l (mu_{l0-1} = lambda_{l0-1}, and lambda_{l0-2} in
+// the place of mu_{l0-2}) the recurrence is mu_l = x mu_{l-1} - gamma_l mu_{l-2}:
+// two FP64 operations per step instead of three, the factors Q_l going into
+// the coefficients (synthesis) or into the per-l sums (adjoint).  Q_l grows
+// by about 2 per l (far more just above l = m), so the chunk length bounds it.
+__device__ inline void stage_rec(int l0, int n, int m, double *s_al, double *s_be, double *s_q,
+                                 double *s_g) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) rec_coeffs(l0 + i, m, s_al[i], s_be[i]);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double p0 = lane < n ? s_al[lane] : 1., p1 = lane + 32 < n ? s_al[lane + 32] : 1.;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double t0 = __shfl_up_sync(0xffffffffu, p0, off);
+      const double t1 = __shfl_up_sync(0xffffffffu, p1, off);
+      if (lane >= off) {
+        p0 *= t0;
+        p1 *= t1;
+      }
+    }
+    p1 *= __shfl_sync(0xffffffffu, p0, 31);
+    if (lane < n) {
+      s_q[lane] = p0;
+      s_g[lane] = lane == 0 ? s_be[0] : s_be[lane] / s_al[lane - 1];
+    }
+    if (lane + 32 < n) {
+      s_q[lane + 32] = p1;
+      s_g[lane + 32] = s_be[lane + 32] / s_al[lane + 31];
+    }
+  }
+  __syncthreads();
+}
+
+// one step of the plain recurrence with the underflow guard
+template <int NP>
+__device__ inline void step_guarded(double al, double be, const double (&x)[NP], double (&l1)[NP],
+                                    double (&l2)[NP], int (&sc)[NP]) {
+#pragma unroll
+  for (int r = 0; r < NP; ++r) {
+    const double ln = al * fma(x[r], l1[r], -be * l2[r]);
+    l2[r] = l1[r];
+    l1[r] = ln;
+    if (sc[r] < 0 && fabs(ln) > RESCALE_ABOVE) {
+      l1[r] *= RESCALE_BY;
+      l2[r] *= RESCALE_BY;
+      ++sc[r];
+    }
+  }
+}
+
 // F_m on every ring: V[m][j] = w_m / nring * sum_l a_lm lambda_lm(theta_j),
 // rings past the south pole by F_m(2 pi - theta) = (-1)^m F_m(theta).
-// grid (mmax + 1, ceil(npairs / (THREADS * PAIRS))), THREADS threads.
+// grid (mmax + 1, ceil(npairs / (THREADS * PAIRS))), THREADS threads.  A warp
+// whose values are all in the double range (scale 0) runs a chunk in the
+// rescaled form without the guard; the others step lambda with it.
 template <typename C>
 __global__ void __launch_bounds__(THREADS) k_alm2leg(
     const C *__restrict__ alm, int64_t astride, const int64_t *__restrict__ mstart,
     int64_t lstride, int lmax, int nring, int npairs, const double *__restrict__ nmant,
     const int *__restrict__ nexp, double2 *__restrict__ V) {
-  __shared__ double2 s_a[LCHUNK];
-  __shared__ double s_al[LCHUNK], s_be[LCHUNK];
+  __shared__ double2 s_a[LCHUNK], s_aq[LCHUNK];
+  __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_q[LCHUNK], s_g[LCHUNK];
   const int m = blockIdx.x;
   const int64_t m0 = mstart[m];
   double x[PAIRS], l1[PAIRS], l2[PAIRS];
@@ -265,38 +323,75 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg(
     E[r] = make_double2(amm.x * v, amm.y * v);
     O[r] = make_double2(0., 0.);
   }
+  // chunks start at l0 = m + 1 + 64 k: l0 - m is odd, so even i add to O
   for (int l0 = m + 1; l0 <= lmax; l0 += LCHUNK) {
     const int n = min(LCHUNK, lmax - l0 + 1);
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += THREADS) {
-      const int l = l0 + i;
-      s_a[i] = load_c(alm + (m0 + int64_t(l) * lstride) * astride);
-      rec_coeffs(l, m, s_al[i], s_be[i]);
-    }
+    for (int i = threadIdx.x; i < n; i += THREADS)
+      s_a[i] = load_c(alm + (m0 + int64_t(l0 + i) * lstride) * astride);
+    stage_rec(l0, n, m, s_al, s_be, s_q, s_g);
+    for (int i = threadIdx.x; i < n; i += THREADS)
+      s_aq[i] = make_double2(s_a[i].x * s_q[i], s_a[i].y * s_q[i]);
     __syncthreads();
-    // (l - m) odd at i = 0 when l0 - m is odd: keep the parity in a flag
-    const bool odd0 = ((l0 - m) & 1) != 0;
-    for (int i = 0; i < n; ++i) {
-      const double al = s_al[i], be = s_be[i];
-      const double2 a = s_a[i];
-      const bool odd = odd0 ^ ((i & 1) != 0);
+    bool inrange = true;
+#pragma unroll
+    for (int r = 0; r < PAIRS; ++r) inrange &= sc[r] == 0;
+    if (__all_sync(0xffffffffu, inrange)) {
+      // mu form: u1 = mu_{l-1}, u2 = mu_{l-2}
+      double u1[PAIRS], u2[PAIRS];
 #pragma unroll
       for (int r = 0; r < PAIRS; ++r) {
-        const double ln = al * fma(x[r], l1[r], -be * l2[r]);
-        l2[r] = l1[r];
-        l1[r] = ln;
-        if (sc[r] < 0 && fabs(ln) > RESCALE_ABOVE) {
-          l1[r] *= RESCALE_BY;
-          l2[r] *= RESCALE_BY;
-          ++sc[r];
+        u1[r] = l1[r];
+        u2[r] = l2[r];
+      }
+      int i = 0;
+      for (; i + 1 < n; i += 2) {
+        const double g0 = s_g[i], g1 = s_g[i + 1];
+        const double2 a0 = s_aq[i], a1 = s_aq[i + 1];
+#pragma unroll
+        for (int r = 0; r < PAIRS; ++r) {
+          const double t0 = fma(x[r], u1[r], -g0 * u2[r]);
+          O[r].x = fma(a0.x, t0, O[r].x);
+          O[r].y = fma(a0.y, t0, O[r].y);
+          const double t1 = fma(x[r], t0, -g1 * u1[r]);
+          E[r].x = fma(a1.x, t1, E[r].x);
+          E[r].y = fma(a1.y, t1, E[r].y);
+          u2[r] = t0;
+          u1[r] = t1;
         }
-        const double v = sc[r] == 0 ? l1[r] : 0.;
-        if (odd) {
-          O[r].x = fma(a.x, v, O[r].x);
-          O[r].y = fma(a.y, v, O[r].y);
-        } else {
-          E[r].x = fma(a.x, v, E[r].x);
-          E[r].y = fma(a.y, v, E[r].y);
+      }
+      if (i < n) {
+        const double g0 = s_g[i];
+        const double2 a0 = s_aq[i];
+#pragma unroll
+        for (int r = 0; r < PAIRS; ++r) {
+          const double t0 = fma(x[r], u1[r], -g0 * u2[r]);
+          O[r].x = fma(a0.x, t0, O[r].x);
+          O[r].y = fma(a0.y, t0, O[r].y);
+          u2[r] = u1[r];
+          u1[r] = t0;
+        }
+      }
+      const double q1 = s_q[n - 1], q2 = n >= 2 ? s_q[n - 2] : 1.;
+#pragma unroll
+      for (int r = 0; r < PAIRS; ++r) {
+        l1[r] = u1[r] * q1;
+        l2[r] = u2[r] * q2;
+      }
+    } else {
+      for (int i = 0; i < n; ++i) {
+        const double2 a = s_a[i];
+        step_guarded(s_al[i], s_be[i], x, l1, l2, sc);
+#pragma unroll
+        for (int r = 0; r < PAIRS; ++r) {
+          const double v = sc[r] == 0 ? l1[r] : 0.;
+          if ((i & 1) == 0) {
+            O[r].x = fma(a.x, v, O[r].x);
+            O[r].y = fma(a.y, v, O[r].y);
+          } else {
+            E[r].x = fma(a.x, v, E[r].x);
+            E[r].y = fma(a.y, v, E[r].y);
+          }
         }
       }
     }
@@ -326,13 +421,15 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg(
 // rings 0 .. nring/2 (g(theta_j) + (-1)^m g(2 pi - theta_j)).  Per thread the
 // contributions of its pairs are summed in registers, per warp through a
 // shared-memory transpose of 8 l values at a time, per block over its warps.
-// grid (mmax + 1, nblk), THREADS threads.
+// grid (mmax + 1, nblk), THREADS threads.  Chunks after the first run in the
+// rescaled form for warps whose values are all in the double range (the
+// warp's per-l sums then take the factor Q_l).
 __global__ void __launch_bounds__(THREADS) k_leg2alm(
     const double2 *__restrict__ g, int lmax, int nring, int npairs,
     const double *__restrict__ nmant, const int *__restrict__ nexp,
     const int64_t *__restrict__ mofs, int64_t nalm_dense, double2 *__restrict__ part) {
   constexpr int NW = THREADS / 32;
-  __shared__ double s_al[LCHUNK], s_be[LCHUNK];
+  __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_q[LCHUNK], s_g[LCHUNK];
   __shared__ double2 s_tr[NW][8][33];
   __shared__ double2 s_blk[LCHUNK][NW];
   const int m = blockIdx.x;
@@ -374,50 +471,59 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
     Q[r] = make_double2(gn.x - gs.x, gn.y - gs.y);
   }
   const int li = lane & 7, part8 = lane >> 3;
+  // chunks start at l0 = m + 64 k: l0 - m is even, so odd i take Q
   for (int l0 = m; l0 <= lmax; l0 += LCHUNK) {
     const int n = min(LCHUNK, lmax - l0 + 1);
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += THREADS) {
-      const int l = l0 + i;
-      if (l > m) {
-        rec_coeffs(l, m, s_al[i], s_be[i]);
-      } else {
-        s_al[i] = 0.;
-        s_be[i] = 0.;
-      }
-    }
-    __syncthreads();
-    for (int i8 = 0; i8 < n; i8 += 8) {
+    stage_rec(l0, n, m, s_al, s_be, s_q, s_g);
+    bool inrange = true;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int i = i8 + k;
-        const int l = l0 + i;
-        double2 c = make_double2(0., 0.);
-        if (i < n) {
-          if (l > m) {
-            const double al = s_al[i], be = s_be[i];
+    for (int r = 0; r < PAIRS; ++r) inrange &= sc[r] == 0;
+    const bool fast = l0 > m && __all_sync(0xffffffffu, inrange);
+    double u1[PAIRS], u2[PAIRS];
+#pragma unroll
+    for (int r = 0; r < PAIRS; ++r) {
+      u1[r] = l1[r];
+      u2[r] = l2[r];
+    }
+    for (int i8 = 0; i8 < n; i8 += 8) {
+      if (fast) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int i = i8 + k;
+          double2 c = make_double2(0., 0.);
+          if (i < n) {
+            const double gi = s_g[i];
 #pragma unroll
             for (int r = 0; r < PAIRS; ++r) {
-              const double ln = al * fma(x[r], l1[r], -be * l2[r]);
-              l2[r] = l1[r];
-              l1[r] = ln;
-              if (sc[r] < 0 && fabs(ln) > RESCALE_ABOVE) {
-                l1[r] *= RESCALE_BY;
-                l2[r] *= RESCALE_BY;
-                ++sc[r];
-              }
+              const double t = fma(x[r], u1[r], -gi * u2[r]);
+              u2[r] = u1[r];
+              u1[r] = t;
+              const double2 f = (k & 1) ? Q[r] : P[r];
+              c.x = fma(t, f.x, c.x);
+              c.y = fma(t, f.y, c.y);
             }
           }
-          const bool odd = ((l - m) & 1) != 0;
-#pragma unroll
-          for (int r = 0; r < PAIRS; ++r) {
-            const double v = sc[r] == 0 ? l1[r] : 0.;
-            const double2 f = odd ? Q[r] : P[r];
-            c.x = fma(v, f.x, c.x);
-            c.y = fma(v, f.y, c.y);
-          }
+          s_tr[warp][k][lane] = c;
         }
-        s_tr[warp][k][lane] = c;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int i = i8 + k;
+          const int l = l0 + i;
+          double2 c = make_double2(0., 0.);
+          if (i < n) {
+            if (l > m) step_guarded(s_al[i], s_be[i], x, l1, l2, sc);
+#pragma unroll
+            for (int r = 0; r < PAIRS; ++r) {
+              const double v = sc[r] == 0 ? l1[r] : 0.;
+              const double2 f = (k & 1) ? Q[r] : P[r];
+              c.x = fma(v, f.x, c.x);
+              c.y = fma(v, f.y, c.y);
+            }
+          }
+          s_tr[warp][k][lane] = c;
+        }
       }
       __syncwarp();
       double2 t = make_double2(0., 0.);
@@ -431,8 +537,23 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
       t.y += __shfl_xor_sync(0xffffffffu, t.y, 8);
       t.x += __shfl_xor_sync(0xffffffffu, t.x, 16);
       t.y += __shfl_xor_sync(0xffffffffu, t.y, 16);
-      if (part8 == 0 && i8 + li < LCHUNK) s_blk[i8 + li][warp] = t;
+      if (part8 == 0) {
+        if (fast && i8 + li < n) {
+          const double q = s_q[i8 + li];
+          t.x *= q;
+          t.y *= q;
+        }
+        s_blk[i8 + li][warp] = t;
+      }
       __syncwarp();
+    }
+    if (fast) {
+      const double q1 = s_q[n - 1], q2 = n >= 2 ? s_q[n - 2] : 1.;
+#pragma unroll
+      for (int r = 0; r < PAIRS; ++r) {
+        l1[r] = u1[r] * q1;
+        l2[r] = u2[r] * q2;
+      }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += THREADS) {
