@@ -468,11 +468,24 @@ def workload_sphere(dev, steps=3, warmup=2, lmax=SH_LMAX, npts=SH_NPTS, with_out
     out_map = torch.empty((1, npts), dtype=torch.float32, device=dev)
     out_alm = torch.empty_like(d_alm)
     kw = dict(spin=0, lmax=lmax, mmax=lmax, loc=d_loc, epsilon=SH_EPS, nthreads=16)
+    # spin 2 (E and B rows -> Q and U) on the same points
+    d_alm2 = torch.cat([d_alm, d_alm.flip(1)]).contiguous()
+    d_alm2[:, :lmax + 1] = d_alm2[:, :lmax + 1].real.to(d_alm2.dtype)
+    d_alm2[:, 0:2] = 0
+    d_alm2[:, lmax + 1] = 0
+    d_mp2 = torch.cat([d_mp, d_mp.flip(1)]).contiguous()
+    out_map2 = torch.empty((2, npts), dtype=torch.float32, device=dev)
+    out_alm2 = torch.empty_like(d_alm2)
+    kw2 = dict(kw, spin=2)
     out = {}
     for name, call in (
             ("synthesis_general", lambda: SH.synthesis_general(alm=d_alm, map=out_map, **kw)),
             ("adjoint_synthesis_general",
-             lambda: SH.adjoint_synthesis_general(map=d_mp, alm=out_alm, **kw))):
+             lambda: SH.adjoint_synthesis_general(map=d_mp, alm=out_alm, **kw)),
+            ("synthesis_general_spin2",
+             lambda: SH.synthesis_general(alm=d_alm2, map=out_map2, **kw2)),
+            ("adjoint_synthesis_general_spin2",
+             lambda: SH.adjoint_synthesis_general(map=d_mp2, alm=out_alm2, **kw2))):
         for _ in range(warmup):
             call()
         torch.cuda.synchronize(dev)
@@ -486,16 +499,18 @@ def workload_sphere(dev, steps=3, warmup=2, lmax=SH_LMAX, npts=SH_NPTS, with_out
         ms = e0.elapsed_time(e1) / steps
         out[name] = {"ms": ms, "mpts_per_s": npts / (ms * 1e-3) / 1e6,
                      "gpu_launches_per_call": (C.lib().dnufft_kernel_launches() - n0) / steps}
-    out["config"] = ("spin-0 synthesis_general / adjoint, lmax = mmax = %d (complex64 a_lm), "
-                     "%d points uniform on the sphere (float64 theta, phi), eps %g; "
-                     "device-resident" % (lmax, npts, SH_EPS))
+    out["config"] = ("synthesis_general / adjoint, spin 0 and spin 2, lmax = mmax = %d "
+                     "(complex64 a_lm), %d points uniform on the sphere (float64 theta, phi), "
+                     "eps %g; device-resident" % (lmax, npts, SH_EPS))
     if with_outputs:
         out["_map"] = out_map.cpu().numpy()
         out["_alm"] = out_alm.cpu().numpy()
+        out["_spin2"] = (d_alm2.cpu().numpy(), d_mp2.cpu().numpy(), out_map2.cpu().numpy(),
+                         out_alm2.cpu().numpy())
     return out
 
 
-def cpu_baseline_sphere(nthreads, ours_map=None, ours_alm=None):
+def cpu_baseline_sphere(nthreads, ours_map=None, ours_alm=None, spin2=None):
     """DUCC's own synthesis_general / adjoint_synthesis_general on the host
     cores, one call of each direction on the sphere workload's inputs, and the
     relative L2 error of our outputs against DUCC's at eps 1e-5."""
@@ -520,6 +535,17 @@ def cpu_baseline_sphere(nthreads, ours_map=None, ours_alm=None):
         res["l2_vs_ducc_synthesis"] = l2(ours_map, m2)
     if ours_alm is not None:
         res["l2_vs_ducc_adjoint"] = l2(ours_alm, a2)
+    if spin2 is not None:
+        alm2, mp2, om2, oa2 = spin2
+        kw2 = dict(kw, spin=2)
+        t0 = time.perf_counter()
+        m2 = R.sht.synthesis_general(alm=alm2, **kw2)
+        res["synthesis_general_spin2_ms"] = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        a2 = R.sht.adjoint_synthesis_general(map=mp2, **kw2)
+        res["adjoint_synthesis_general_spin2_ms"] = (time.perf_counter() - t0) * 1e3
+        res["l2_vs_ducc_synthesis_spin2"] = l2(om2, m2)
+        res["l2_vs_ducc_adjoint_spin2"] = l2(oa2, a2)
     return res
 
 
@@ -849,10 +875,10 @@ def run_ours(args, rank, world, local_rank):
             except Exception as e:
                 workloads["wgridder"]["cpu_baseline"] = {"error": str(e)[:200]}
         sph = workloads["sphere_synthesis"]
-        om, oa = sph.pop("_map", None), sph.pop("_alm", None)
+        om, oa, s2 = sph.pop("_map", None), sph.pop("_alm", None), sph.pop("_spin2", None)
         if not args.no_cpu and "error" not in sph:
             try:
-                sph["cpu_baseline"] = cpu_baseline_sphere(args.param_threads, om, oa)
+                sph["cpu_baseline"] = cpu_baseline_sphere(args.param_threads, om, oa, s2)
             except Exception as e:
                 sph["cpu_baseline"] = {"error": str(e)[:200]}
     line = {
@@ -993,9 +1019,9 @@ def main():
         if args.workload == "sphere_synthesis":
             res = workload_sphere(dev, lmax=args.sh_lmax, npts=args.sh_npts,
                                   with_outputs=not args.no_cpu)
-            om, oa = res.pop("_map", None), res.pop("_alm", None)
+            om, oa, s2 = res.pop("_map", None), res.pop("_alm", None), res.pop("_spin2", None)
             if (not args.no_cpu and args.sh_lmax == SH_LMAX and args.sh_npts == SH_NPTS):
-                res["cpu_baseline"] = cpu_baseline_sphere(args.param_threads, om, oa)
+                res["cpu_baseline"] = cpu_baseline_sphere(args.param_threads, om, oa, s2)
         else:
             res = (fn(dev) if fn else
                    workload_wgridder(dev, nrow=args.wg_rows, npix=args.wg_npix))

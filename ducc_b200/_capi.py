@@ -152,9 +152,9 @@ def lib():
     L.dnufft_sht_default_opts.argtypes = [P(ShtOpts)]
     L.dnufft_sht_default_opts.restype = None
     for f in (L.dnufft_synthesis_general, L.dnufft_adjoint_synthesis_general):
-        f.argtypes = [P(Array), ctypes.c_size_t, ctypes.c_size_t, P(ctypes.c_int64),
-                      ctypes.c_size_t, ctypes.c_int64, P(Array), ctypes.c_double, P(ShtOpts),
-                      P(Array), vp]
+        f.argtypes = [P(Array), ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t,
+                      P(ctypes.c_int64), ctypes.c_size_t, ctypes.c_int64, P(Array),
+                      ctypes.c_double, P(ShtOpts), P(Array), vp]
     _lib = L
     return L
 

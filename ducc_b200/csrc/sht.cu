@@ -1,6 +1,7 @@
-// Spherical-harmonic synthesis at arbitrary points and its adjoint, spin 0:
-// the counterparts of ducc0.sht.synthesis_general / adjoint_synthesis_general
-// (src/ducc0/sht/sht.cc:2926-2994, python/sht_pymod.cc:805-885).
+// Spherical-harmonic synthesis at arbitrary points and its adjoint: the
+// counterparts of ducc0.sht.synthesis_general / adjoint_synthesis_general
+// (src/ducc0/sht/sht.cc:2926-2994, python/sht_pymod.cc:805-885), spin 0 and
+// spin > 0 (modes STANDARD, GRAD_ONLY, DERIV1).
 //
 // DUCC evaluates the expansion on an equiangular grid (alm2leg), resamples
 // the rings in theta, transforms them in phi and interpolates the resulting
@@ -29,6 +30,12 @@
 //   3. the map: a 2D type-2 transform of this library at (theta_i, phi_i)
 //      over the modes (k, m - s), s = (mmax + 1) / 2, in the data precision,
 //      and Re(z_i e^{i s phi_i}) (k_points_out).
+//
+// Spin s > 0 (the spin section below): Q + iU is one complex field,
+// sum over -mmax <= m <= mmax of F_m(theta) e^{i m phi} with F_m from the
+// Wigner-d recurrence (k_alm2leg_spin, one ring per thread), continued by
+// F_m(2 pi - theta) = (-1)^(m+s) F_m(theta); the 2D transform runs over
+// (2 lmax + 1) x (2 mmax + 1) modes and its complex result is (Q, U).
 //
 // The adjoint runs the transposed steps: values map_i e^{-i s phi_i}
 // (k_points_in) -> 2D type 1 -> inverse DFT back to the rings -> the rings
@@ -650,6 +657,404 @@ __global__ void k_ring_theta(double *__restrict__ th, int nring) {
   if (j < nring) th[j] = 2. * 3.14159265358979323846 * (double(j) / double(nring));
 }
 
+// ---------------------------------------------------------------- spin > 0
+template <typename B> __device__ inline B from_d2b(const double2 &v) {
+  B o;
+  o.x = decltype(o.x)(v.x);
+  o.y = decltype(o.y)(v.y);
+  return o;
+}
+
+// D_lm(theta) = sqrt((2l+1)/(4 pi)) d^l_{m,-s}(theta) for l >= l0 = max(|m|, s):
+// the three-term recurrence of the Wigner d functions in l,
+//   D_l = alpha_l (x - beta_l) D_{l-1} - gamma_l D_{l-2},
+//   alpha_l = l sqrt((2l+1)(2l-1)) / sqrt((l^2-m^2)(l^2-s^2)),
+//   beta_l  = -m s / (l (l-1)),
+//   gamma_l = l/(l-1) sqrt((2l+1)/(2l-3)) sqrt(((l-1)^2-m^2)((l-1)^2-s^2)/((l^2-m^2)(l^2-s^2))),
+// started from D_l0 = N_m cos(theta/2)^pc sin(theta/2)^ps (the single term
+// of Wigner's sum at l = l0; N_m with its sign from the host table).
+struct SpinStart {
+  int l0, pc, ps;
+  double mant;   // N_m = mant * 2^ex
+  int ex;
+};
+
+__device__ inline void spin_coeffs(int l, int m, int sp, double &al, double &be, double &ga) {
+  const double dl = l, dm = m, ds = sp;
+  const double den = sqrt((dl * dl - dm * dm) * (dl * dl - ds * ds));
+  al = dl * sqrt((2. * dl + 1.) * (2. * dl - 1.)) / den;
+  be = -dm * ds / (dl * (dl - 1.));
+  const double l1 = dl - 1.;
+  ga = dl / l1 * sqrt((2. * dl + 1.) / (2. * dl - 3.)) *
+       sqrt(fmax((l1 * l1 - dm * dm) * (l1 * l1 - ds * ds), 0.)) / den;
+}
+
+// c^pc sn^ps * mant * 2^ex as value * 2^(SCALE_EXP * scale)
+__device__ inline void spin_start(double c, double sn, const SpinStart &S, double &v, int &scale) {
+  scale = 0;
+  if ((c <= 0. && S.pc > 0) || (sn <= 0. && S.ps > 0)) {
+    v = 0.;
+    return;
+  }
+  double rm = S.mant;
+  long long re = S.ex;
+  const double bases[2] = {c, sn};
+  const int pw[2] = {S.pc, S.ps};
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    int k = pw[b];
+    if (k == 0) continue;
+    int be;
+    double bm = frexp(bases[b], &be);
+    while (true) {
+      int t;
+      if (k & 1) {
+        rm = frexp(rm * bm, &t);
+        re += be + t;
+      }
+      k >>= 1;
+      if (!k) break;
+      bm = frexp(bm * bm, &t);
+      be = 2 * be + t;
+    }
+  }
+  int t;
+  rm = frexp(rm, &t);
+  re += t;
+  long long q = re + SCALE_EXP / 2;
+  long long sc = q >= 0 ? q / SCALE_EXP : -((-q + SCALE_EXP - 1) / SCALE_EXP);
+  v = ldexp(rm, int(re - SCALE_EXP * sc));
+  scale = int(sc);
+}
+
+// the coefficient of D_lm in Q + iU: sigma (E + iB) for m >= 0,
+// sigma (-1)^m (conj E + i conj B) for m < 0 (E_{l,-m} = (-1)^m conj E_lm);
+// sigma = (-1)^(s+1); DERIV1: E sqrt(l (l+1)), no B
+template <typename C>
+__device__ inline double2 spin_coef(const C *alm, int64_t cstride, int64_t astride, int64_t idx,
+                                    int m, int l, int mode, double sigma) {
+  double2 e = load_c(alm + idx * astride);
+  double2 b = make_double2(0., 0.);
+  if (mode == DNUFFT_SHT_STANDARD) b = load_c(alm + cstride + idx * astride);
+  if (mode == DNUFFT_SHT_DERIV1) {
+    const double f = sqrt(double(l) * double(l + 1));
+    e.x *= f;
+    e.y *= f;
+  }
+  if (m >= 0) return make_double2(sigma * (e.x - b.y), sigma * (e.y + b.x));
+  const double sg = (m & 1) ? -sigma : sigma;
+  return make_double2(sg * (e.x + b.y), sg * (b.x - e.y));
+}
+
+// F_m on the rings for m = row - mmax: V[row][j] = sum_l A_lm D_lm(theta_j) / nring,
+// V[row][nring - j] = (-1)^(m+s) V[row][j].  RINGS rings per thread; grid
+// (2 mmax + 1, blocks over rings 0 .. nring/2).  Chunks of warps whose values
+// are all in the double range run without the underflow guard.
+constexpr int RINGS = 4;
+template <typename C>
+__global__ void __launch_bounds__(THREADS) k_alm2leg_spin(
+    const C *__restrict__ alm, int64_t cstride, int64_t astride,
+    const int64_t *__restrict__ mstart, int64_t lstride, int lmax, int mmax, int sp, int mode,
+    int nring, const SpinStart *__restrict__ starts, double2 *__restrict__ V) {
+  __shared__ double2 s_a[LCHUNK];
+  __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_ga[LCHUNK];
+  const int row = blockIdx.x, m = row - mmax, mu = m < 0 ? -m : m;
+  const SpinStart S = starts[row];
+  const int half = nring / 2;
+  const double sigma = (sp & 1) ? 1. : -1.;
+  const int64_t m0 = mstart[mu];
+  double x[RINGS], d1[RINGS], d2[RINGS];
+  int sc[RINGS], jr[RINGS];
+  double2 F[RINGS];
+  const double2 a0 =
+      spin_coef(alm, cstride, astride, m0 + int64_t(S.l0) * lstride, m, S.l0, mode, sigma);
+#pragma unroll
+  for (int r = 0; r < RINGS; ++r) {
+    jr[r] = (blockIdx.y * RINGS + r) * THREADS + threadIdx.x;
+    double c = 1., sn = 0.;
+    x[r] = 1.;
+    if (jr[r] <= half) {
+      sincospi(double(jr[r]) / double(nring), &sn, &c);
+      x[r] = cospi(2. * double(jr[r]) / double(nring));
+    }
+    spin_start(c, sn, S, d1[r], sc[r]);
+    if (jr[r] > half) d1[r] = 0.;
+    d2[r] = 0.;
+    const double v = sc[r] == 0 ? d1[r] : 0.;
+    F[r] = make_double2(a0.x * v, a0.y * v);
+  }
+  for (int l0 = S.l0 + 1; l0 <= lmax; l0 += LCHUNK) {
+    const int n = min(LCHUNK, lmax - l0 + 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += THREADS) {
+      const int l = l0 + i;
+      s_a[i] = spin_coef(alm, cstride, astride, m0 + int64_t(l) * lstride, m, l, mode, sigma);
+      spin_coeffs(l, m, sp, s_al[i], s_be[i], s_ga[i]);
+    }
+    __syncthreads();
+    bool inrange = true;
+#pragma unroll
+    for (int r = 0; r < RINGS; ++r) inrange &= sc[r] == 0;
+    if (__all_sync(0xffffffffu, inrange)) {
+      // every value of the warp in the double range: no guard
+      for (int i = 0; i < n; ++i) {
+        const double al = s_al[i], be = s_be[i], ga = s_ga[i];
+        const double2 a = s_a[i];
+#pragma unroll
+        for (int r = 0; r < RINGS; ++r) {
+          const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
+          d2[r] = d1[r];
+          d1[r] = dn;
+          F[r].x = fma(a.x, dn, F[r].x);
+          F[r].y = fma(a.y, dn, F[r].y);
+        }
+      }
+    } else {
+      for (int i = 0; i < n; ++i) {
+        const double al = s_al[i], be = s_be[i], ga = s_ga[i];
+        const double2 a = s_a[i];
+#pragma unroll
+        for (int r = 0; r < RINGS; ++r) {
+          const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
+          d2[r] = d1[r];
+          d1[r] = dn;
+          if (sc[r] < 0 && fabs(dn) > RESCALE_ABOVE) {
+            d1[r] *= RESCALE_BY;
+            d2[r] *= RESCALE_BY;
+            ++sc[r];
+          }
+          const double v = sc[r] == 0 ? d1[r] : 0.;
+          F[r].x = fma(a.x, v, F[r].x);
+          F[r].y = fma(a.y, v, F[r].y);
+        }
+      }
+    }
+  }
+  const double w = 1. / double(nring);
+  const double sg = ((m + sp) & 1) ? -w : w;
+  double2 *out = V + int64_t(row) * nring;
+#pragma unroll
+  for (int r = 0; r < RINGS; ++r) {
+    const int j = jr[r];
+    if (j > half) continue;
+    out[j] = make_double2(w * F[r].x, w * F[r].y);
+    if (j > 0 && j < half) out[nring - j] = make_double2(sg * F[r].x, sg * F[r].y);
+  }
+}
+
+// Transposed: part[b][row][l] = sum over the rings of block b of
+// D_lm(theta_j) G(theta_j), G = g[row][j] + (-1)^(m+s) g[row][nring - j]
+// (0 < j < nring/2), for l0 <= l <= lmax; sums per warp through the
+// shared-memory transpose of 8 l values, per block over its warps.
+__global__ void __launch_bounds__(THREADS) k_leg2alm_spin(
+    const double2 *__restrict__ g, int lmax, int mmax, int sp, int nring,
+    const SpinStart *__restrict__ starts, double2 *__restrict__ part) {
+  constexpr int NW = THREADS / 32;
+  __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_ga[LCHUNK];
+  __shared__ double2 s_tr[NW][8][33];
+  __shared__ double2 s_blk[LCHUNK][NW];
+  const int row = blockIdx.x, m = row - mmax;
+  const SpinStart S = starts[row];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int half = nring / 2;
+  const double2 *in = g + int64_t(row) * nring;
+  const double sgn = ((m + sp) & 1) ? -1. : 1.;
+  double x[RINGS], d1[RINGS], d2[RINGS];
+  int sc[RINGS];
+  double2 G[RINGS];
+#pragma unroll
+  for (int r = 0; r < RINGS; ++r) {
+    const int j = (blockIdx.y * RINGS + r) * THREADS + threadIdx.x;
+    double c = 1., sn = 0.;
+    x[r] = 1.;
+    G[r] = make_double2(0., 0.);
+    if (j <= half) {
+      sincospi(double(j) / double(nring), &sn, &c);
+      x[r] = cospi(2. * double(j) / double(nring));
+      G[r] = in[j];
+      if (j > 0 && j < half) {
+        const double2 t = in[nring - j];
+        G[r].x += sgn * t.x;
+        G[r].y += sgn * t.y;
+      }
+    }
+    spin_start(c, sn, S, d1[r], sc[r]);
+    if (j > half) d1[r] = 0.;
+    d2[r] = 0.;
+  }
+  const int li = lane & 7, part8 = lane >> 3;
+  const int64_t rowofs = (int64_t(blockIdx.y) * (2 * mmax + 1) + row) * (lmax + 1);
+  for (int l0 = S.l0; l0 <= lmax; l0 += LCHUNK) {
+    const int n = min(LCHUNK, lmax - l0 + 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += THREADS) {
+      const int l = l0 + i;
+      if (l > S.l0) {
+        spin_coeffs(l, m, sp, s_al[i], s_be[i], s_ga[i]);
+      } else {
+        s_al[i] = 0.;
+        s_be[i] = 0.;
+        s_ga[i] = 0.;
+      }
+    }
+    __syncthreads();
+    bool inrange = true;
+#pragma unroll
+    for (int r = 0; r < RINGS; ++r) inrange &= sc[r] == 0;
+    const bool fast = l0 > S.l0 && __all_sync(0xffffffffu, inrange);
+    for (int i8 = 0; i8 < n; i8 += 8) {
+      if (fast) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int i = i8 + k;
+          double2 c = make_double2(0., 0.);
+          if (i < n) {
+            const double al = s_al[i], be = s_be[i], ga = s_ga[i];
+#pragma unroll
+            for (int r = 0; r < RINGS; ++r) {
+              const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
+              d2[r] = d1[r];
+              d1[r] = dn;
+              c.x = fma(dn, G[r].x, c.x);
+              c.y = fma(dn, G[r].y, c.y);
+            }
+          }
+          s_tr[warp][k][lane] = c;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int i = i8 + k;
+          double2 c = make_double2(0., 0.);
+          if (i < n) {
+            if (l0 + i > S.l0) {
+              const double al = s_al[i], be = s_be[i], ga = s_ga[i];
+#pragma unroll
+              for (int r = 0; r < RINGS; ++r) {
+                const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
+                d2[r] = d1[r];
+                d1[r] = dn;
+                if (sc[r] < 0 && fabs(dn) > RESCALE_ABOVE) {
+                  d1[r] *= RESCALE_BY;
+                  d2[r] *= RESCALE_BY;
+                  ++sc[r];
+                }
+              }
+            }
+#pragma unroll
+            for (int r = 0; r < RINGS; ++r) {
+              const double v = sc[r] == 0 ? d1[r] : 0.;
+              c.x = fma(v, G[r].x, c.x);
+              c.y = fma(v, G[r].y, c.y);
+            }
+          }
+          s_tr[warp][k][lane] = c;
+        }
+      }
+      __syncwarp();
+      double2 t = make_double2(0., 0.);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double2 u = s_tr[warp][li][part8 * 8 + k];
+        t.x += u.x;
+        t.y += u.y;
+      }
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, 8);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, 8);
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, 16);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, 16);
+      if (part8 == 0) s_blk[i8 + li][warp] = t;
+      __syncwarp();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += THREADS) {
+      double2 t = s_blk[i][0];
+#pragma unroll
+      for (int w = 1; w < NW; ++w) {
+        t.x += s_blk[i][w].x;
+        t.y += s_blk[i][w].y;
+      }
+      part[rowofs + l0 + i] = t;
+    }
+  }
+}
+
+// E' = sigma (W_m + (-1)^m conj W_-m) / 2, B' = -i sigma (W_m - (-1)^m conj W_-m) / 2
+// with W summed over the blocks in order and divided by nring; DERIV1: E'
+// times sqrt(l (l+1)); zero for l < s.  One thread per (m >= 0, l) of the
+// dense layout.
+template <typename C>
+__global__ void k_alm_out_spin(const double2 *__restrict__ part, int nblk, int64_t nalm_dense,
+                               const int64_t *__restrict__ mofs,
+                               const int64_t *__restrict__ mstart, int64_t lstride,
+                               int64_t cstride, int64_t astride, int lmax, int mmax, int sp,
+                               int mode, double scale, C *__restrict__ alm) {
+  const int nm = mmax + 1;
+  const int64_t rowlen = lmax + 1, blkstride = int64_t(2 * mmax + 1) * rowlen;
+  const double sigma = (sp & 1) ? 1. : -1.;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < nalm_dense;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    int lo = 0, hi = nm - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (mofs[mid] + mid <= e) lo = mid;
+      else hi = mid - 1;
+    }
+    const int m = lo;
+    const int l = int(e - mofs[m]);
+    double2 E = make_double2(0., 0.), B = make_double2(0., 0.);
+    if (l >= sp) {
+      double2 wp = make_double2(0., 0.), wn = make_double2(0., 0.);
+      for (int b = 0; b < nblk; ++b) {
+        const double2 u = part[b * blkstride + (mmax + m) * rowlen + l];
+        const double2 v = part[b * blkstride + (mmax - m) * rowlen + l];
+        wp.x += u.x;
+        wp.y += u.y;
+        wn.x += v.x;
+        wn.y += v.y;
+      }
+      const double f = (m & 1) ? -1. : 1.;
+      const double h = 0.5 * sigma * scale;
+      // conj(wn) = (wn.x, -wn.y)
+      E = make_double2(h * (wp.x + f * wn.x), h * (wp.y - f * wn.y));
+      // -i (a + i b) = b - i a with (a + i b) = wp - f conj(wn)
+      const double ar = wp.x - f * wn.x, ai = wp.y + f * wn.y;
+      B = make_double2(h * ai, -h * ar);
+      if (mode == DNUFFT_SHT_DERIV1) {
+        const double d = sqrt(double(l) * double(l + 1));
+        E.x *= d;
+        E.y *= d;
+      }
+    }
+    const int64_t idx = (mstart[m] + int64_t(l) * lstride) * astride;
+    alm[idx] = from_d2b<C>(E);
+    if (mode == DNUFFT_SHT_STANDARD) alm[cstride + idx] = from_d2b<C>(B);
+  }
+}
+
+// Q_i + i U_i = z_i (synthesis) and z_i = Q_i + i U_i (adjoint)
+template <typename C, typename T>
+__global__ void k_points_out_spin(const C *__restrict__ z, int64_t n, T *__restrict__ map,
+                                  int64_t rs, int64_t ms) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const C v = z[i];
+    map[i * ms] = T(v.x);
+    map[rs + i * ms] = T(v.y);
+  }
+}
+template <typename C, typename T>
+__global__ void k_points_in_spin(const T *__restrict__ map, int64_t rs, int64_t ms, int64_t n,
+                                 C *__restrict__ z) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    C v;
+    v.x = map[i * ms];
+    v.y = map[rs + i * ms];
+    z[i] = v;
+  }
+}
+
 // The DFT along the rings, for ring counts that are powers of two up to
 // FFT_MAX: one CTA per m, an in-place radix-2 transform in shared memory
 // (bit-reversed load, log2 N butterfly stages, twiddles from a table made by
@@ -724,6 +1129,9 @@ __global__ void __launch_bounds__(FFT_THREADS) k_ring_fft(const Cin *__restrict_
 // ---------------------------------------------------------------- host side
 struct Problem {
   int lmax = 0, mmax = 0;
+  int spin = 0, mode = 0;
+  int rows = 0;            // transforms along the rings: mmax + 1 (spin 0), 2 mmax + 1
+  int nblk_spin = 0;       // blocks over the rings 0 .. nring/2 (spin > 0)
   int log2n = 0;           // > 0: ring DFT by k_ring_fft over nring = 2^log2n rings
   int nring = 0, npairs = 0, nk = 0, nblk = 0;
   int64_t npts = 0;
@@ -758,12 +1166,19 @@ static void forced(dnufft_opts &po, int nu2u, int ndim, const int64_t *shape, ui
   for (int d = 0; d < 3; ++d) po.force_nover[d] = nover[d];
 }
 
-static Problem setup(size_t spin, size_t lmax, size_t nm, const int64_t *mstart, int64_t lstride,
-                     const Arr &alm, const Arr &map, const Arr &loc, double epsilon,
-                     const dnufft_sht_opts *o, bool adjoint) {
+static Problem setup(size_t spin, int mode, size_t lmax, size_t nm, const int64_t *mstart,
+                     int64_t lstride, const Arr &alm, const Arr &map, const Arr &loc,
+                     double epsilon, const dnufft_sht_opts *o, bool adjoint) {
   DN_REQUIRE(o != nullptr, ST_BADARG, "null options");
-  DN_REQUIRE(spin == 0, ST_UNSUPPORTED,
-             "synthesis_general: spin > 0 is not supported by this build (spin 0 only)");
+  DN_REQUIRE(mode == DNUFFT_SHT_STANDARD || mode == DNUFFT_SHT_GRAD_ONLY ||
+                 mode == DNUFFT_SHT_DERIV1,
+             ST_BADARG, "unknown SHT mode");
+  DN_REQUIRE(spin > 0 || mode == DNUFFT_SHT_STANDARD, ST_BADARG,
+             "spin must be positive for grad-only SHTs");
+  DN_REQUIRE(mode != DNUFFT_SHT_DERIV1 || spin == 1, ST_BADARG,
+             "DERIV1 needs spin 1");
+  DN_REQUIRE(spin <= lmax, ST_BADARG, "incorrect l_max: must be >= spin");
+  DN_REQUIRE(spin <= 1024, ST_UNSUPPORTED, "spin above 1024");
   DN_REQUIRE(nm >= 1, ST_BADARG, "need at least m=0");
   DN_REQUIRE(nm <= lmax + 1, ST_BADARG, "mmax>lmax");
   DN_REQUIRE(lmax <= 65535, ST_UNSUPPORTED, "lmax above 65535");
@@ -778,8 +1193,10 @@ static Problem setup(size_t spin, size_t lmax, size_t nm, const int64_t *mstart,
              "map must be real with the precision of alm");
   DN_REQUIRE(loc.dtype == DNUFFT_F64, ST_BADARG, "loc must be float64");
   DN_REQUIRE(loc.shape[1] == 2, ST_BADARG, "last dimension of loc must have size 2");
-  DN_REQUIRE(alm.shape[0] == 1, ST_BADARG, "number of components mismatch in alm");
-  DN_REQUIRE(map.shape[0] == 1, ST_BADARG, "number of components mismatch in map");
+  const int64_t nalm_c = (spin == 0 || mode != DNUFFT_SHT_STANDARD) ? 1 : 2;
+  const int64_t nmaps = spin == 0 ? 1 : 2;
+  DN_REQUIRE(alm.shape[0] == nalm_c, ST_BADARG, "number of components mismatch in alm");
+  DN_REQUIRE(map.shape[0] == nmaps, ST_BADARG, "number of components mismatch in map");
   DN_REQUIRE(map.shape[1] == loc.shape[0], ST_BADARG, "map and loc disagree on the points");
   // DUCC's min_almdim (python/sht_pymod.cc:153-176)
   int64_t need = 0;
@@ -793,6 +1210,9 @@ static Problem setup(size_t spin, size_t lmax, size_t nm, const int64_t *mstart,
   Problem P;
   P.lmax = int(lmax);
   P.mmax = int(nm) - 1;
+  P.spin = int(spin);
+  P.mode = mode;
+  P.rows = spin == 0 ? P.mmax + 1 : 2 * P.mmax + 1;
   // rings: a power of two up to FFT_MAX (the DFT along the rings in shared
   // memory), else 2 lmax + 2 with the DFT as 1D transforms of this library
   P.nring = 2 * P.lmax + 2;
@@ -803,8 +1223,9 @@ static Problem setup(size_t spin, size_t lmax, size_t nm, const int64_t *mstart,
   P.npairs = (P.nring / 2) / 2 + 1;
   P.nk = 2 * P.lmax + 1;
   P.nblk = (P.npairs + THREADS * PAIRS - 1) / (THREADS * PAIRS);
+  P.nblk_spin = (P.nring / 2 + 1 + THREADS * RINGS - 1) / (THREADS * RINGS);
   P.npts = loc.shape[0];
-  P.s = double(nm / 2);
+  P.s = spin == 0 ? double(nm / 2) : 0.;
   P.f64 = f64;
   P.eps2 = epsilon;
   // the theta sums in FP64 to a tenth of the request (or the best FP64 1D accuracy)
@@ -826,7 +1247,7 @@ static Problem setup(size_t spin, size_t lmax, size_t nm, const int64_t *mstart,
   P.po2.nthreads = o->nthreads;
   P.po2.sigma_min = o->sigma_min;
   P.po2.sigma_max = o->sigma_max;
-  const int64_t shape2[2] = {P.nk, P.mmax + 1};
+  const int64_t shape2[2] = {P.nk, P.rows};
   forced(P.po2, 1, 2, shape2, uint64_t(P.npts), P.eps2, P.f64);
   return P;
 }
@@ -863,8 +1284,8 @@ static void make_tables(const Problem &P, const int64_t *mstart, cudaStream_t st
   upload(t.mofs, mofs.data(), nm * sizeof(int64_t), st);
   upload(t.nmant, mant.data(), nm * sizeof(double), st);
   upload(t.nexp, ex.data(), nm * sizeof(int), st);
-  // the uploads read pageable host vectors that end with this function
-  DN_CUDA(cudaStreamSynchronize(st));
+  // (copies from pageable host memory are staged before cudaMemcpyAsync
+  // returns, so the vectors may end with this function)
 }
 
 static dnufft_plan *ring_plan(const Problem &P, bool nu2u, const Buf &theta, cudaStream_t st) {
@@ -888,7 +1309,204 @@ static void report(const Problem &P, const char *what) {
                "%s: lmax %d, mmax %d, %lld points; %d rings (1D transforms of %d modes, "
                "epsilon %.3g), 2D modes %d x %d (epsilon %.3g)\n",
                what, P.lmax, P.mmax, (long long)P.npts, P.nring, P.nk, P.eps1, P.nk,
-               P.mmax + 1, P.eps2);
+               P.rows, P.eps2);
+}
+
+
+// the DFT along the rings of `rows` transforms: V (rows, nring) FP64 -> c
+// (nk, rows) in the data precision (forward), or h (nk, rows) in the data
+// precision -> g (rows, nring) FP64 (inverse)
+template <typename C>
+static void rings_forward(const Problem &P, const Buf &V, Buf &cdat, cudaStream_t st) {
+  const int rows = P.rows;
+  if (P.log2n > 0) {
+    const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
+    k_ring_fft<double2, C, false><<<rows, FFT_THREADS, smem, st>>>(
+        ptr<double2>(V), ptr<C>(cdat), P.log2n, P.lmax, rows);
+    DN_LAUNCHED();
+    return;
+  }
+  Buf theta(size_t(P.nring) * sizeof(double), st);
+  k_ring_theta<<<(P.nring + 255) / 256, 256, 0, st>>>(ptr<double>(theta), P.nring);
+  DN_LAUNCHED();
+  Buf c64(size_t(rows) * P.nk * sizeof(double2), st);
+  {
+    PlanGuard pg{ring_plan(P, true, theta, st)};
+    dnufft_array a_v = dev_array(V.p, DNUFFT_C128, rows, P.nring, P.nring, 1);
+    dnufft_array a_c = dev_array(c64.p, DNUFFT_C128, rows, P.nk, 1, rows);
+    check_nufft(dnufft_plan_nu2u(pg.p, 1, 0, &a_v, &a_c, st), "synthesis_general (rings)");
+  }
+  k_convert<double2, C><<<grid_for(int64_t(rows) * P.nk), 256, 0, st>>>(
+      ptr<double2>(c64), int64_t(rows) * P.nk, ptr<C>(cdat));
+  DN_LAUNCHED();
+}
+
+template <typename C>
+static void rings_inverse(const Problem &P, const Buf &hdat, Buf &gr, cudaStream_t st) {
+  const int rows = P.rows;
+  if (P.log2n > 0) {
+    const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
+    k_ring_fft<C, double2, true><<<rows, FFT_THREADS, smem, st>>>(
+        ptr<C>(hdat), ptr<double2>(gr), P.log2n, P.lmax, rows);
+    DN_LAUNCHED();
+    return;
+  }
+  Buf hconv(size_t(rows) * P.nk * sizeof(double2), st);
+  k_convert<C, double2><<<grid_for(int64_t(rows) * P.nk), 256, 0, st>>>(
+      ptr<C>(hdat), int64_t(rows) * P.nk, ptr<double2>(hconv));
+  DN_LAUNCHED();
+  Buf theta(size_t(P.nring) * sizeof(double), st);
+  k_ring_theta<<<(P.nring + 255) / 256, 256, 0, st>>>(ptr<double>(theta), P.nring);
+  DN_LAUNCHED();
+  PlanGuard pg{ring_plan(P, false, theta, st)};
+  dnufft_array a_h = dev_array(hconv.p, DNUFFT_C128, rows, P.nk, 1, rows);
+  dnufft_array a_g = dev_array(gr.p, DNUFFT_C128, rows, P.nring, P.nring, 1);
+  check_nufft(dnufft_plan_u2nu(pg.p, 0, 0, &a_h, &a_g, st), "adjoint_synthesis_general (rings)");
+}
+
+// N_m of D_l0 per row (m = row - mmax), with its sign, and the powers of
+// cos(theta/2), sin(theta/2): the single term of Wigner's sum at l0 =
+// max(|m|, s); the binomial C(2 l0, l0 - s) accumulated over |m| in long
+// double (its ratio between consecutive |m| is a product of four integers).
+static std::vector<SpinStart> spin_starts(int mmax, int sp) {
+  std::vector<SpinStart> res(2 * mmax + 1);
+  const long double inv4pi = 1.0L / (4.0L * 3.141592653589793238462643383279502884L);
+  std::vector<long double> bm(mmax + 1, 0.L);   // C(2 mu, mu - s) as mantissa * 2^be
+  std::vector<long> be(mmax + 1, 0);
+  long double b = 1.L;
+  long e = 0;
+  for (int mu = sp; mu <= mmax; ++mu) {
+    if (mu > sp) {
+      b *= (long double)(2 * mu) * (long double)(2 * mu - 1) /
+           ((long double)(mu - sp) * (long double)(mu + sp));
+      int t;
+      b = frexpl(b, &t);
+      e += t;
+    }
+    bm[mu] = b;
+    be[mu] = e;
+  }
+  for (int row = 0; row <= 2 * mmax; ++row) {
+    const int m = row - mmax, mu = m < 0 ? -m : m;
+    SpinStart S;
+    long double bin;
+    long bexp;
+    int sign = ((m + sp) & 1) ? -1 : 1;
+    if (mu >= sp) {
+      S.l0 = mu;
+      bin = bm[mu];
+      bexp = be[mu];
+      if (m >= 0) {
+        S.pc = mu - sp;
+        S.ps = mu + sp;
+      } else {
+        S.pc = mu + sp;
+        S.ps = mu - sp;
+        if ((mu - sp) & 1) sign = -sign;
+      }
+    } else {
+      S.l0 = sp;
+      const int k = sp - m;   // C(2s, s - m), 1 <= k <= 2s - 1
+      long double bb = 1.L;
+      long ee = 0;
+      for (int i = 1; i <= k; ++i) {
+        bb *= (long double)(2 * sp - k + i) / (long double)i;
+        int t;
+        bb = frexpl(bb, &t);
+        ee += t;
+      }
+      bin = bb;
+      bexp = ee;
+      S.pc = sp - m;
+      S.ps = sp + m;
+    }
+    // N = sign sqrt((2 l0 + 1)/(4 pi) bin 2^bexp)
+    int t;
+    long double v = frexpl((long double)(2 * S.l0 + 1) * inv4pi * bin, &t);
+    long ex = bexp + t;
+    if (ex & 1) {
+      v *= 2.L;
+      ex -= 1;
+    }
+    S.mant = double(sign * sqrtl(v));
+    S.ex = int(ex / 2);
+    res[row] = S;
+  }
+  return res;
+}
+
+template <typename T, typename C>
+static void synthesis_spin_t(const Problem &P, const Arr &alm, const int64_t *mstart,
+                             int64_t lstride, const Arr &loc, const dnufft_sht_opts &o,
+                             const Arr &map, cudaStream_t st) {
+  if (o.verbosity) report(P, "synthesis_general");
+  if (P.npts == 0) return;
+  Tables tb;
+  make_tables(P, mstart, st, tb);
+  const std::vector<SpinStart> ss = spin_starts(P.mmax, P.spin);
+  Buf dstarts(ss.size() * sizeof(SpinStart), st);
+  upload(dstarts, ss.data(), ss.size() * sizeof(SpinStart), st);
+  Buf V(size_t(P.rows) * P.nring * sizeof(double2), st);
+  k_alm2leg_spin<C><<<dim3(P.rows, P.nblk_spin), THREADS, 0, st>>>(
+      static_cast<const C *>(alm.p), alm.stride[0], alm.stride[1], ptr<int64_t>(tb.mstart),
+      lstride, P.lmax, P.mmax, P.spin, P.mode, P.nring, ptr<SpinStart>(dstarts),
+      ptr<double2>(V));
+  DN_LAUNCHED();
+  Buf cdat(size_t(P.rows) * P.nk * sizeof(C), st);
+  rings_forward<C>(P, V, cdat, st);
+  const int cdt = P.f64 ? DNUFFT_C128 : DNUFFT_C64;
+  Buf z(size_t(P.npts) * sizeof(C), st);
+  {
+    dnufft_array a_u = dev_array(cdat.p, cdt, P.nk, P.rows, P.rows, 1);
+    dnufft_array a_l = dev_array(loc.p, DNUFFT_F64, P.npts, 2, loc.stride[0], loc.stride[1]);
+    dnufft_array a_z = dev_array(z.p, cdt, P.npts, 1, 1, 1);
+    a_z.ndim = 1;
+    check_nufft(dnufft_u2nu(&a_u, &a_l, 0, P.eps2, &a_z, &P.po2, st),
+                "synthesis_general (points)");
+  }
+  k_points_out_spin<C, T><<<grid_for(P.npts), 256, 0, st>>>(
+      ptr<C>(z), P.npts, static_cast<T *>(map.p), map.stride[0], map.stride[1]);
+  DN_LAUNCHED();
+}
+
+template <typename T, typename C>
+static void adjoint_spin_t(const Problem &P, const Arr &map, const int64_t *mstart,
+                           int64_t lstride, const Arr &loc, const dnufft_sht_opts &o,
+                           const Arr &alm, cudaStream_t st) {
+  if (o.verbosity) report(P, "adjoint_synthesis_general");
+  Tables tb;
+  make_tables(P, mstart, st, tb);
+  const std::vector<SpinStart> ss = spin_starts(P.mmax, P.spin);
+  Buf dstarts(ss.size() * sizeof(SpinStart), st);
+  upload(dstarts, ss.data(), ss.size() * sizeof(SpinStart), st);
+  const int cdt = P.f64 ? DNUFFT_C128 : DNUFFT_C64;
+  Buf hdat(size_t(P.rows) * P.nk * sizeof(C), st);
+  {
+    Buf z(size_t(std::max<int64_t>(P.npts, 1)) * sizeof(C), st);
+    if (P.npts > 0) {
+      k_points_in_spin<C, T><<<grid_for(P.npts), 256, 0, st>>>(
+          static_cast<const T *>(map.p), map.stride[0], map.stride[1], P.npts, ptr<C>(z));
+      DN_LAUNCHED();
+    }
+    dnufft_array a_z = dev_array(z.p, cdt, P.npts, 1, 1, 1);
+    a_z.ndim = 1;
+    dnufft_array a_l = dev_array(loc.p, DNUFFT_F64, P.npts, 2, loc.stride[0], loc.stride[1]);
+    dnufft_array a_h = dev_array(hdat.p, cdt, P.nk, P.rows, P.rows, 1);
+    check_nufft(dnufft_nu2u(&a_z, &a_l, 1, P.eps2, &a_h, &P.po2, st),
+                "adjoint_synthesis_general (points)");
+  }
+  Buf gr(size_t(P.rows) * P.nring * sizeof(double2), st);
+  rings_inverse<C>(P, hdat, gr, st);
+  Buf part(size_t(P.nblk_spin) * P.rows * (P.lmax + 1) * sizeof(double2), st);
+  k_leg2alm_spin<<<dim3(P.rows, P.nblk_spin), THREADS, 0, st>>>(
+      ptr<double2>(gr), P.lmax, P.mmax, P.spin, P.nring, ptr<SpinStart>(dstarts),
+      ptr<double2>(part));
+  DN_LAUNCHED();
+  k_alm_out_spin<C><<<grid_for(P.nalm_dense), 256, 0, st>>>(
+      ptr<double2>(part), P.nblk_spin, P.nalm_dense, ptr<int64_t>(tb.mofs),
+      ptr<int64_t>(tb.mstart), lstride, alm.stride[0], alm.stride[1], P.lmax, P.mmax, P.spin,
+      P.mode, 1. / double(P.nring), static_cast<C *>(alm.p));
+  DN_LAUNCHED();
 }
 
 template <typename T, typename C>
@@ -908,26 +1526,7 @@ static void synthesis_t(const Problem &P, const Arr &alm, const int64_t *mstart,
   DN_LAUNCHED();
   // 2. c_km, written [k][m] (row-major (nk, nm)) in the data precision
   Buf cdat(size_t(nm) * P.nk * sizeof(C), st);
-  if (P.log2n > 0) {
-    const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
-    k_ring_fft<double2, C, false><<<nm, FFT_THREADS, smem, st>>>(
-        ptr<double2>(V), ptr<C>(cdat), P.log2n, P.lmax, nm);
-    DN_LAUNCHED();
-  } else {
-    Buf theta(size_t(P.nring) * sizeof(double), st);
-    k_ring_theta<<<(P.nring + 255) / 256, 256, 0, st>>>(ptr<double>(theta), P.nring);
-    DN_LAUNCHED();
-    Buf c64(size_t(nm) * P.nk * sizeof(double2), st);
-    {
-      PlanGuard pg{ring_plan(P, true, theta, st)};
-      dnufft_array a_v = dev_array(V.p, DNUFFT_C128, nm, P.nring, P.nring, 1);
-      dnufft_array a_c = dev_array(c64.p, DNUFFT_C128, nm, P.nk, 1, nm);
-      check_nufft(dnufft_plan_nu2u(pg.p, 1, 0, &a_v, &a_c, st), "synthesis_general (rings)");
-    }
-    k_convert<double2, C><<<grid_for(int64_t(nm) * P.nk), 256, 0, st>>>(
-        ptr<double2>(c64), int64_t(nm) * P.nk, ptr<C>(cdat));
-    DN_LAUNCHED();
-  }
+  rings_forward<C>(P, V, cdat, st);
   // 3. the 2D type 2 at the points, in the data precision
   const void *uni = cdat.p;
   const int cdt = P.f64 ? DNUFFT_C128 : DNUFFT_C64;
@@ -973,24 +1572,7 @@ static void adjoint_t(const Problem &P, const Arr &map, const int64_t *mstart, i
   }
   // 2. back to the rings (FP64)
   Buf gr(size_t(nm) * P.nring * sizeof(double2), st);
-  if (P.log2n > 0) {
-    const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
-    k_ring_fft<C, double2, true><<<nm, FFT_THREADS, smem, st>>>(
-        ptr<C>(hdat), ptr<double2>(gr), P.log2n, P.lmax, nm);
-    DN_LAUNCHED();
-  } else {
-    Buf hconv(size_t(nm) * P.nk * sizeof(double2), st);
-    k_convert<C, double2><<<grid_for(int64_t(nm) * P.nk), 256, 0, st>>>(
-        ptr<C>(hdat), int64_t(nm) * P.nk, ptr<double2>(hconv));
-    DN_LAUNCHED();
-    Buf theta(size_t(P.nring) * sizeof(double), st);
-    k_ring_theta<<<(P.nring + 255) / 256, 256, 0, st>>>(ptr<double>(theta), P.nring);
-    DN_LAUNCHED();
-    PlanGuard pg{ring_plan(P, false, theta, st)};
-    dnufft_array a_h = dev_array(hconv.p, DNUFFT_C128, nm, P.nk, 1, nm);
-    dnufft_array a_g = dev_array(gr.p, DNUFFT_C128, nm, P.nring, P.nring, 1);
-    check_nufft(dnufft_plan_u2nu(pg.p, 0, 0, &a_h, &a_g, st), "adjoint_synthesis_general (rings)");
-  }
+  rings_inverse<C>(P, hdat, gr, st);
   // 3. the transposed recurrence, per-block partial sums, summed in block order
   Buf part(size_t(P.nblk) * P.nalm_dense * sizeof(double2), st);
   k_leg2alm<<<dim3(nm, P.nblk), THREADS, 0, st>>>(
@@ -1003,23 +1585,40 @@ static void adjoint_t(const Problem &P, const Arr &map, const int64_t *mstart, i
   DN_LAUNCHED();
 }
 
-static void synthesis_impl(const dnufft_array *alm_, size_t spin, size_t lmax,
+static void synthesis_impl(const dnufft_array *alm_, size_t spin, int mode, size_t lmax,
                            const int64_t *mstart, size_t nm, int64_t lstride,
                            const dnufft_array *loc_, double epsilon, const dnufft_sht_opts *o,
                            dnufft_array *map_, cudaStream_t st) {
   const Arr alm = arr_of(alm_, "alm"), map = arr_of(map_, "map"), loc = arr_of(loc_, "loc");
-  const Problem P = setup(spin, lmax, nm, mstart, lstride, alm, map, loc, epsilon, o, false);
+  const Problem P =
+      setup(spin, mode, lmax, nm, mstart, lstride, alm, map, loc, epsilon, o, false);
+  if (P.spin > 0) {
+    if (P.f64)
+      synthesis_spin_t<double, double2>(P, alm, mstart, lstride, loc, *o, map, st);
+    else
+      synthesis_spin_t<float, float2>(P, alm, mstart, lstride, loc, *o, map, st);
+    return;
+  }
   if (P.f64)
     synthesis_t<double, double2>(P, alm, mstart, lstride, loc, *o, map, st);
   else
     synthesis_t<float, float2>(P, alm, mstart, lstride, loc, *o, map, st);
 }
 
-static void adjoint_impl(const dnufft_array *map_, size_t spin, size_t lmax, const int64_t *mstart,
-                         size_t nm, int64_t lstride, const dnufft_array *loc_, double epsilon,
-                         const dnufft_sht_opts *o, dnufft_array *alm_, cudaStream_t st) {
+static void adjoint_impl(const dnufft_array *map_, size_t spin, int mode, size_t lmax,
+                         const int64_t *mstart, size_t nm, int64_t lstride,
+                         const dnufft_array *loc_, double epsilon, const dnufft_sht_opts *o,
+                         dnufft_array *alm_, cudaStream_t st) {
   const Arr alm = arr_of(alm_, "alm"), map = arr_of(map_, "map"), loc = arr_of(loc_, "loc");
-  const Problem P = setup(spin, lmax, nm, mstart, lstride, alm, map, loc, epsilon, o, true);
+  const Problem P =
+      setup(spin, mode, lmax, nm, mstart, lstride, alm, map, loc, epsilon, o, true);
+  if (P.spin > 0) {
+    if (P.f64)
+      adjoint_spin_t<double, double2>(P, map, mstart, lstride, loc, *o, alm, st);
+    else
+      adjoint_spin_t<float, float2>(P, map, mstart, lstride, loc, *o, alm, st);
+    return;
+  }
   if (P.f64)
     adjoint_t<double, double2>(P, map, mstart, lstride, loc, *o, alm, st);
   else
@@ -1052,21 +1651,22 @@ void dnufft_sht_default_opts(dnufft_sht_opts *o) {
   o->sigma_max = 2.6;
 }
 
-int dnufft_synthesis_general(const dnufft_array *alm, size_t spin, size_t lmax,
+int dnufft_synthesis_general(const dnufft_array *alm, size_t spin, int mode, size_t lmax,
                              const int64_t *mstart, size_t nm, int64_t lstride,
                              const dnufft_array *loc, double epsilon, const dnufft_sht_opts *opts,
                              dnufft_array *map, void *stream) {
-  DN_SHT_GUARD(dnufft::sht::synthesis_impl(alm, spin, lmax, mstart, nm, lstride, loc, epsilon,
-                                           opts, map, static_cast<cudaStream_t>(stream)))
+  DN_SHT_GUARD(dnufft::sht::synthesis_impl(alm, spin, mode, lmax, mstart, nm, lstride, loc,
+                                           epsilon, opts, map,
+                                           static_cast<cudaStream_t>(stream)))
 }
 
-int dnufft_adjoint_synthesis_general(const dnufft_array *map, size_t spin, size_t lmax,
-                                     const int64_t *mstart, size_t nm, int64_t lstride,
-                                     const dnufft_array *loc, double epsilon,
+int dnufft_adjoint_synthesis_general(const dnufft_array *map, size_t spin, int mode,
+                                     size_t lmax, const int64_t *mstart, size_t nm,
+                                     int64_t lstride, const dnufft_array *loc, double epsilon,
                                      const dnufft_sht_opts *opts, dnufft_array *alm,
                                      void *stream) {
-  DN_SHT_GUARD(dnufft::sht::adjoint_impl(map, spin, lmax, mstart, nm, lstride, loc, epsilon, opts,
-                                         alm, static_cast<cudaStream_t>(stream)))
+  DN_SHT_GUARD(dnufft::sht::adjoint_impl(map, spin, mode, lmax, mstart, nm, lstride, loc,
+                                         epsilon, opts, alm, static_cast<cudaStream_t>(stream)))
 }
 
 }  // extern "C"

@@ -1,13 +1,14 @@
 """Spherical-harmonic synthesis at arbitrary points on the sphere and its
 adjoint on the GPU: a drop-in for ``ducc0.sht.synthesis_general`` and
 ``ducc0.sht.adjoint_synthesis_general`` (python/sht_pymod.cc:805-885,
-:2299-2300 for the signatures and keyword defaults), spin 0.
+:2299-2300 for the signatures and keyword defaults), any spin, modes
+STANDARD, GRAD_ONLY and DERIV1.
 
 The work runs in the CUDA library through the C-ABI
 (``dnufft_synthesis_general`` / ``dnufft_adjoint_synthesis_general`` in
-include/ducc_b200_sht.h): a Legendre recurrence kernel onto equiangular
-rings, one 1D transform per m over the rings and one 2D transform of this
-package at the points.  Arrays may be numpy arrays (copied to the current
+include/ducc_b200_sht.h): a Legendre (spin 0) or Wigner-d (spin > 0)
+recurrence kernel onto equiangular rings, the DFT along the rings and one 2D
+transform of this package at the points.  Arrays may be numpy arrays (copied to the current
 CUDA device, the result copied back) or torch CUDA tensors (used in place;
 the result is a tensor).  As in DUCC, the dtype of ``alm`` (synthesis) or
 ``map`` (adjoint) sets the precision and ``loc`` is float64 (theta, phi).
@@ -81,11 +82,16 @@ def _opts(nthreads, sigma_min, sigma_max, verbose):
     return o
 
 
-def _check_mode(mode, spin):
-    if mode not in ("STANDARD", "GRAD_ONLY", "DERIV1"):
+_MODES = {"STANDARD": 0, "GRAD_ONLY": 1, "DERIV1": 2}
+
+
+def _mode(mode, spin):
+    """DUCC's get_mode and component counts (python/sht_pymod.cc get_nalm,
+    get_nmaps): (mode code, a_lm rows, map rows)."""
+    if mode not in _MODES:
         raise RuntimeError("unknown SHT mode")
-    if mode != "STANDARD" and spin == 0:
-        raise RuntimeError("number of components mismatch in alm")
+    nalm = 1 if (spin == 0 or mode != "STANDARD") else 2
+    return _MODES[mode], nalm, (1 if spin == 0 else 2)
 
 
 def _loc(loc):
@@ -98,24 +104,27 @@ def _loc(loc):
     return d_loc
 
 
-def synthesis_general(*, alm, spin, lmax, loc, epsilon=1e-5, mstart=None, lstride=1, mmax=None,
+def synthesis_general(*, alm, spin, lmax, loc, epsilon, mstart=None, lstride=1, mmax=None,
                       nthreads=1, map=None, sigma_min=1.1, sigma_max=2.6, mode="STANDARD",
                       verbose=False):
-    """Evaluate the real map of ``alm`` at the points ``loc`` (theta, phi),
-    returning ``map`` of shape (1, npoints) (``ducc0.sht.synthesis_general``)."""
+    """Evaluate the map(s) of ``alm`` at the points ``loc`` (theta, phi),
+    returning ``map`` of shape (1, npoints) for spin 0, (2, npoints) (Q, U)
+    otherwise (``ducc0.sht.synthesis_general``)."""
     torch = _torch()
     spin, lmax, lstride = int(spin), int(lmax), int(lstride)
-    _check_mode(mode, spin)
+    mcode, nalm_c, nmaps = _mode(mode, spin)
     d_alm, host = _dev(alm)
     if d_alm.dtype not in (torch.complex64, torch.complex128):
         raise TypeError("unsupported combination of data types")
     if d_alm.dim() != 2:
         raise RuntimeError("alm must be a 2D array")
+    if d_alm.shape[0] != nalm_c:
+        raise RuntimeError("number of components mismatch in alm")
     d_loc = _loc(loc)
     ms = _mstart(lmax, mmax, mstart)
     rdt = torch.float64 if d_alm.dtype == torch.complex128 else torch.float32
     npts = int(d_loc.shape[0])
-    shape = (1 if spin == 0 else 2, npts)
+    shape = (nmaps, npts)
     if map is not None and C.is_torch(map):
         d_map = map
     else:
@@ -126,7 +135,8 @@ def synthesis_general(*, alm, spin, lmax, loc, epsilon=1e-5, mstart=None, lstrid
     st = ctypes.c_void_p(torch.cuda.current_stream(d_alm.device).cuda_stream)
     a_alm, a_loc, a_map = C.describe(d_alm), C.describe(d_loc), C.describe(d_map)
     C.check(C.lib().dnufft_synthesis_general(
-        ctypes.byref(a_alm), spin, lmax, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        ctypes.byref(a_alm), spin, mcode, lmax,
+        ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
         ms.shape[0], lstride, ctypes.byref(a_loc), float(epsilon), ctypes.byref(o),
         ctypes.byref(a_map), st))
     if map is not None and not C.is_torch(map):
@@ -135,19 +145,22 @@ def synthesis_general(*, alm, spin, lmax, loc, epsilon=1e-5, mstart=None, lstrid
     return d_map.cpu().numpy() if host else d_map
 
 
-def adjoint_synthesis_general(*, map, spin, lmax, loc, epsilon=1e-5, mstart=None, lstride=1,
+def adjoint_synthesis_general(*, map, spin, lmax, loc, epsilon, mstart=None, lstride=1,
                               mmax=None, nthreads=1, alm=None, sigma_min=1.1, sigma_max=2.6,
                               mode="STANDARD", verbose=False):
-    """a_lm = sum_i map_i conj(Y_lm(loc_i)) for 0 <= m <= mmax, m <= l <= lmax,
-    returning ``alm`` of shape (1, nalm) (``ducc0.sht.adjoint_synthesis_general``)."""
+    """The adjoint of ``synthesis_general`` for DUCC's inner product of a_lm
+    (m > 0 counted twice): spin 0, a_lm = sum_i map_i conj(Y_lm(loc_i)); every
+    a_lm with m <= l <= lmax is written (``ducc0.sht.adjoint_synthesis_general``)."""
     torch = _torch()
     spin, lmax, lstride = int(spin), int(lmax), int(lstride)
-    _check_mode(mode, spin)
+    mcode, nalm_c, nmaps = _mode(mode, spin)
     d_map, host = _dev(map)
     if d_map.dtype not in (torch.float32, torch.float64):
         raise TypeError("type matching failed: 'map' has neither type 'f4' nor 'f8'")
     if d_map.dim() != 2:
         raise RuntimeError("map must be a 2D array")
+    if d_map.shape[0] != nmaps:
+        raise RuntimeError("number of components mismatch in map")
     d_loc = _loc(loc)
     ms = _mstart(lmax, mmax, mstart)
     cdt = torch.complex128 if d_map.dtype == torch.float64 else torch.complex64
@@ -155,16 +168,17 @@ def adjoint_synthesis_general(*, map, spin, lmax, loc, epsilon=1e-5, mstart=None
     if alm is not None and C.is_torch(alm):
         d_alm = alm
     elif alm is not None:
-        if alm.shape[0] != 1 or alm.shape[1] < nalm:
+        if alm.shape[0] != nalm_c or alm.shape[1] < nalm:
             raise RuntimeError("bad alm shape")
         d_alm = torch.from_numpy(np.ascontiguousarray(alm)).to(d_map.device)
     else:
-        d_alm = torch.zeros((1 if spin == 0 else 2, nalm), dtype=cdt, device=d_map.device)
+        d_alm = torch.zeros((nalm_c, nalm), dtype=cdt, device=d_map.device)
     o = _opts(nthreads, sigma_min, sigma_max, verbose)
     st = ctypes.c_void_p(torch.cuda.current_stream(d_map.device).cuda_stream)
     a_map, a_loc, a_alm = C.describe(d_map), C.describe(d_loc), C.describe(d_alm)
     C.check(C.lib().dnufft_adjoint_synthesis_general(
-        ctypes.byref(a_map), spin, lmax, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        ctypes.byref(a_map), spin, mcode, lmax,
+        ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
         ms.shape[0], lstride, ctypes.byref(a_loc), float(epsilon), ctypes.byref(o),
         ctypes.byref(a_alm), st))
     if alm is not None and not C.is_torch(alm):

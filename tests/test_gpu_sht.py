@@ -1,12 +1,16 @@
-"""Spin-0 synthesis at arbitrary points and its adjoint on the GPU
-(ducc_b200.sht) against the direct sums of oracle/sht_oracle.py, against the
-golden fixtures made by DUCC itself, and against DUCC's compiled sht module
-(oracle/_ref, where it was built) at sizes the direct sums cannot reach.
+"""Synthesis at arbitrary points and its adjoint on the GPU (ducc_b200.sht),
+spin 0 and spin > 0, against the direct sums of oracle/sht_oracle.py, against
+the golden fixtures made by DUCC itself, and against DUCC's compiled sht
+module (oracle/_ref, where it was built) at sizes the direct sums cannot reach.
 
-Restated from DUCC's python/test/test_sht.py (spin 0; nthreads only feeds
-the cost model):
-  test_adjointness_general   test_sht.py:234-262 (rtol 1e-9 at epsilon 1e-5)
-  test_synthesis_general     test_sht.py:265-281 (l2 error below epsilon 1e-7)
+Restated from DUCC's python/test/test_sht.py (its parameter grids; nthreads
+only feeds the cost model):
+  test_adjointness_general   test_sht.py:234-262 (rtol 1e-9 at epsilon 1e-5,
+                             spin 0, 1, 2 and GRAD_ONLY for spin > 0)
+  test_synthesis_general     test_sht.py:265-281 (l2 error below epsilon 1e-7
+                             on the HEALPix nside 32 pixel centres, spin 0, 1, 2;
+                             DUCC compares with its ring synthesis, here the
+                             direct sums stand in for it)
 """
 import glob
 import os
@@ -63,74 +67,110 @@ def healpix_ring_centres(nside):
 
 
 # ---------------------------------------------------------------- DUCC's tests
+def direct(alm, spin, lmax, mmax, loc, mode="STANDARD"):
+    if spin == 0:
+        return O.synthesis(alm[0], lmax, mmax, loc)[None]
+    return O.synthesis_spin(alm, spin, lmax, mmax, loc, mode)
+
+
+def direct_adjoint(mp, spin, lmax, mmax, loc, mode="STANDARD"):
+    if spin == 0:
+        return O.adjoint_synthesis(mp[0], lmax, mmax, loc)[None]
+    return O.adjoint_synthesis_spin(mp, spin, lmax, mmax, loc, mode)
+
+
+@pmp("spin", (0, 1, 2))
 @pmp("lmmax", ((10, 8), (100, 100)))
 @pmp("nside", (32,))
 @pmp("nthreads", (1, 4))
-def test_synthesis_general(sht, lmmax, nside, nthreads):
+def test_synthesis_general(sht, lmmax, nside, spin, nthreads):
     rng = np.random.default_rng(48)
     lmax, mmax = lmmax
     epsilon = 1e-7
-    slm = O.random_alm(lmax, mmax, rng)[None, :]
+    ncomp = 1 if spin == 0 else 2
+    slm = O.random_alm_spin(lmax, mmax, spin, ncomp, rng)
     loc = healpix_ring_centres(nside)
     assert loc.shape[0] == 12 * nside * nside
-    v1 = sht.synthesis_general(lmax=lmax, mmax=mmax, alm=slm, loc=loc, spin=0,
+    v1 = sht.synthesis_general(lmax=lmax, mmax=mmax, alm=slm, loc=loc, spin=spin,
                                epsilon=epsilon, nthreads=nthreads)
-    v2 = O.synthesis(slm[0], lmax, mmax, loc)
-    assert l2err(v1[0], v2) < epsilon
+    v2 = direct(slm, spin, lmax, mmax, loc)
+    assert l2err(v1, v2) < epsilon
 
 
+@pmp("spin", (0, 1, 2))
 @pmp("nthreads", (1, 4))
 @pmp("npix", (33, 200))
 @pmp("lmmax", ((10, 8), (100, 100)))
-def test_adjointness_general(sht, lmmax, npix, nthreads):
+def test_adjointness_general(sht, lmmax, npix, spin, nthreads):
     rng = np.random.default_rng(48)
     lmax, mmax = lmmax
     epsilon = 1e-5
-    slm1 = O.random_alm(lmax, mmax, rng)[None, :]
+    ncomp = 1 if spin == 0 else 2
+    slm1 = O.random_alm_spin(lmax, mmax, spin, ncomp, rng)
     loc = rng.uniform(0., 1., (npix, 2))
     loc[:, 0] *= np.pi
     loc[:, 1] *= 2 * np.pi
-    points2 = rng.uniform(-0.5, 0.5, (loc.shape[0], 1)).T
-    points1 = sht.synthesis_general(lmax=lmax, mmax=mmax, alm=slm1, loc=loc, spin=0,
+    points2 = rng.uniform(-0.5, 0.5, (loc.shape[0], ncomp)).T
+    points1 = sht.synthesis_general(lmax=lmax, mmax=mmax, alm=slm1, loc=loc, spin=spin,
                                     epsilon=epsilon, nthreads=nthreads)
-    slm2 = sht.adjoint_synthesis_general(lmax=lmax, mmax=mmax, map=points2, loc=loc, spin=0,
+    slm2 = sht.adjoint_synthesis_general(lmax=lmax, mmax=mmax, map=points2, loc=loc, spin=spin,
                                          epsilon=epsilon, nthreads=nthreads)
-    v1 = O.almdot(slm1[0], slm2[0], lmax)
-    v2 = np.dot(points2[0], points1[0])
+    v1 = np.sum([O.almdot(slm1[c], slm2[c], lmax) for c in range(ncomp)])
+    v2 = np.sum(points2 * points1)
     np.testing.assert_allclose(v1, v2, rtol=1e-9)
+    if spin > 0:
+        points1 = sht.synthesis_general(lmax=lmax, mmax=mmax, alm=slm1[:1], loc=loc, spin=spin,
+                                        epsilon=epsilon, nthreads=nthreads, mode="GRAD_ONLY")
+        slm2 = sht.adjoint_synthesis_general(lmax=lmax, mmax=mmax, map=points2, loc=loc,
+                                             spin=spin, epsilon=epsilon, nthreads=nthreads,
+                                             mode="GRAD_ONLY")
+        v1 = O.almdot(slm1[0], slm2[0], lmax)
+        v2 = np.sum(points2 * points1)
+        np.testing.assert_allclose(v1, v2, rtol=1e-9)
 
 
 # ---------------------------------------------------------------- direct sums
 CASES = [
-    # lmax, mmax, npoints, precision, epsilon
-    (0, 0, 20, np.complex128, 1e-10),
-    (1, 1, 40, np.complex128, 1e-12),
-    (7, 0, 50, np.complex128, 1e-9),
-    (13, 9, 300, np.complex128, 1e-11),
-    (64, 64, 500, np.complex128, 1e-12),
-    (150, 40, 400, np.complex128, 1e-8),
-    (31, 31, 500, np.complex64, 1e-5),
-    (90, 77, 700, np.complex64, 2e-6),
+    # lmax, mmax, npoints, precision, epsilon, spin, mode
+    (0, 0, 20, np.complex128, 1e-10, 0, "STANDARD"),
+    (1, 1, 40, np.complex128, 1e-12, 0, "STANDARD"),
+    (7, 0, 50, np.complex128, 1e-9, 0, "STANDARD"),
+    (13, 9, 300, np.complex128, 1e-11, 0, "STANDARD"),
+    (64, 64, 500, np.complex128, 1e-12, 0, "STANDARD"),
+    (150, 40, 400, np.complex128, 1e-8, 0, "STANDARD"),
+    (31, 31, 500, np.complex64, 1e-5, 0, "STANDARD"),
+    (90, 77, 700, np.complex64, 2e-6, 0, "STANDARD"),
+    (1, 1, 40, np.complex128, 1e-12, 1, "STANDARD"),
+    (2, 0, 40, np.complex128, 1e-12, 2, "STANDARD"),
+    (20, 13, 300, np.complex128, 1e-11, 1, "STANDARD"),
+    (40, 40, 400, np.complex128, 1e-12, 2, "STANDARD"),
+    (33, 20, 300, np.complex128, 1e-10, 3, "GRAD_ONLY"),
+    (25, 25, 300, np.complex128, 1e-11, 1, "DERIV1"),
+    (60, 50, 500, np.complex64, 1e-5, 2, "STANDARD"),
+    (30, 7, 300, np.complex64, 2e-6, 1, "GRAD_ONLY"),
 ]
 
 
 @pmp("case", CASES)
 def test_against_direct_sums(sht, case):
-    lmax, mmax, npts, cdt, eps = case
-    rng = np.random.default_rng(lmax * 1000 + mmax)
-    alm = O.random_alm(lmax, mmax, rng).astype(cdt)[None, :]
+    lmax, mmax, npts, cdt, eps, spin, mode = case
+    rng = np.random.default_rng(lmax * 1000 + mmax + 17 * spin)
+    ncomp = 1 if (spin == 0 or mode != "STANDARD") else 2
+    nmaps = 1 if spin == 0 else 2
+    alm = O.random_alm_spin(lmax, mmax, spin, ncomp, rng).astype(cdt)
     loc = locs(rng, npts)
     rdt = np.float64 if cdt == np.complex128 else np.float32
-    m1 = sht.synthesis_general(alm=alm, spin=0, lmax=lmax, mmax=mmax, loc=loc, epsilon=eps)
-    assert m1.dtype == rdt and m1.shape == (1, npts)
-    assert l2err(m1[0], O.synthesis(alm[0], lmax, mmax, loc)) < eps
-    mp = rng.uniform(-1, 1, (1, npts)).astype(rdt)
-    a1 = sht.adjoint_synthesis_general(map=mp, spin=0, lmax=lmax, mmax=mmax, loc=loc,
-                                       epsilon=eps)
-    assert a1.dtype == cdt and a1.shape == (1, O.nalm(lmax, mmax))
-    ref = O.adjoint_synthesis(mp[0], lmax, mmax, loc)
-    assert l2err(a1[0], ref) < eps
-    assert np.all(a1[0, :lmax + 1].imag == 0)
+    m1 = sht.synthesis_general(alm=alm, spin=spin, lmax=lmax, mmax=mmax, loc=loc, epsilon=eps,
+                               mode=mode)
+    assert m1.dtype == rdt and m1.shape == (nmaps, npts)
+    assert l2err(m1, direct(alm, spin, lmax, mmax, loc, mode)) < eps
+    mp = rng.uniform(-1, 1, (nmaps, npts)).astype(rdt)
+    a1 = sht.adjoint_synthesis_general(map=mp, spin=spin, lmax=lmax, mmax=mmax, loc=loc,
+                                       epsilon=eps, mode=mode)
+    assert a1.dtype == cdt and a1.shape == (ncomp, O.nalm(lmax, mmax))
+    ref = direct_adjoint(mp, spin, lmax, mmax, loc, mode)
+    assert l2err(a1, ref) < eps
+    assert np.all(a1[:, :lmax + 1].imag == 0)
 
 
 def test_custom_layout(sht):
@@ -172,17 +212,17 @@ def test_custom_layout(sht):
 
 def test_golden_fixtures(sht):
     files = sorted(glob.glob(os.path.join(HERE, "golden", "sht_*.npz")))
-    assert files
+    assert len(files) >= 9
     for fn in files:
         g = np.load(fn)
-        lmax, mmax = int(g["lmax"]), int(g["mmax"])
+        lmax, mmax, spin, mode = int(g["lmax"]), int(g["mmax"]), int(g["spin"]), str(g["mode"])
         f64 = g["alm"].dtype == np.complex128
         eps = 1e-11 if f64 else 1e-5
-        m1 = sht.synthesis_general(alm=g["alm"], spin=0, lmax=lmax, mmax=mmax, loc=g["loc"],
-                                   epsilon=eps)
+        m1 = sht.synthesis_general(alm=g["alm"], spin=spin, lmax=lmax, mmax=mmax, loc=g["loc"],
+                                   epsilon=eps, mode=mode)
         assert l2err(m1, g["synthesis"]) < eps, fn
-        a1 = sht.adjoint_synthesis_general(map=g["map_in"], spin=0, lmax=lmax, mmax=mmax,
-                                           loc=g["loc"], epsilon=eps)
+        a1 = sht.adjoint_synthesis_general(map=g["map_in"], spin=spin, lmax=lmax, mmax=mmax,
+                                           loc=g["loc"], epsilon=eps, mode=mode)
         assert l2err(a1, g["adjoint"]) < eps, fn
 
 
@@ -211,23 +251,36 @@ def test_errors(sht):
     rng = np.random.default_rng(1)
     alm = O.random_alm(10, 10, rng)[None, :]
     loc = locs(rng, 10)
-    with pytest.raises(RuntimeError, match="spin"):
-        sht.synthesis_general(alm=np.concatenate([alm, alm]), spin=1, lmax=10, loc=loc)
+    kw = dict(lmax=10, epsilon=1e-6)
+    with pytest.raises(RuntimeError, match="components"):
+        sht.synthesis_general(alm=alm, spin=1, loc=loc, **kw)   # spin 1 needs E and B
+    with pytest.raises(RuntimeError, match="grad-only"):
+        sht.synthesis_general(alm=alm, spin=0, loc=loc, mode="GRAD_ONLY", **kw)
+    with pytest.raises(RuntimeError, match="DERIV1"):
+        sht.synthesis_general(alm=alm, spin=2, loc=loc, mode="DERIV1", **kw)
     with pytest.raises(RuntimeError):
-        sht.synthesis_general(alm=alm[:, :-3], spin=0, lmax=10, loc=loc)
+        sht.synthesis_general(alm=alm, spin=0, loc=loc, mode="CURL", **kw)
     with pytest.raises(RuntimeError):
-        sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=loc, mmax=11)
+        sht.synthesis_general(alm=np.concatenate([alm, alm]), spin=11, loc=loc, **kw)
     with pytest.raises(RuntimeError):
-        sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=loc[:, :1].copy())
+        sht.synthesis_general(alm=alm[:, :-3], spin=0, loc=loc, **kw)
+    with pytest.raises(RuntimeError):
+        sht.synthesis_general(alm=alm, spin=0, loc=loc, mmax=11, **kw)
+    with pytest.raises(RuntimeError):
+        sht.synthesis_general(alm=alm, spin=0, loc=loc[:, :1].copy(), **kw)
     with pytest.raises(RuntimeError):
         sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=loc, epsilon=1e-30)
     with pytest.raises(TypeError):
-        sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=loc.astype(np.float32))
+        sht.synthesis_general(alm=alm, spin=0, loc=loc.astype(np.float32), **kw)
+    with pytest.raises(TypeError):
+        sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=loc)   # epsilon is required
     # no points: an empty map, an all-zero adjoint
-    e = sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=np.zeros((0, 2)))
+    e = sht.synthesis_general(alm=alm, spin=0, loc=np.zeros((0, 2)), **kw)
     assert e.shape == (1, 0)
-    a = sht.adjoint_synthesis_general(map=np.zeros((1, 0)), spin=0, lmax=10, loc=np.zeros((0, 2)))
+    a = sht.adjoint_synthesis_general(map=np.zeros((1, 0)), spin=0, loc=np.zeros((0, 2)), **kw)
     assert a.shape == (1, O.nalm(10, 10)) and not np.any(a)
+    a = sht.adjoint_synthesis_general(map=np.zeros((2, 0)), spin=2, loc=np.zeros((0, 2)), **kw)
+    assert a.shape == (2, O.nalm(10, 10)) and not np.any(a)
 
 
 # ---------------------------------------------------------------- against DUCC, large
@@ -240,27 +293,31 @@ def ducc():
     return m.sht
 
 
-@pmp("lmax,mmax,npts,cdt,eps", [
-    (1023, 1023, 200000, np.complex128, 1e-10),
-    (1023, 700, 200000, np.complex64, 1e-5),
-    (4095, 4095, 50000, np.complex128, 1e-9),
+@pmp("lmax,mmax,npts,cdt,eps,spin", [
+    (1023, 1023, 200000, np.complex128, 1e-10, 0),
+    (1023, 700, 200000, np.complex64, 1e-5, 0),
+    (4095, 4095, 50000, np.complex128, 1e-9, 0),
+    (1023, 1023, 100000, np.complex128, 1e-10, 2),
+    (2047, 1500, 100000, np.complex64, 1e-5, 1),
+    (4095, 1500, 30000, np.complex128, 1e-9, 2),
 ])
-def test_against_ducc_large(sht, ducc, lmax, mmax, npts, cdt, eps):
-    """Sizes where the Legendre recurrence needs its carried exponent
-    (sin^m theta below the double range for m in the thousands)."""
-    rng = np.random.default_rng(lmax + npts)
-    alm = O.random_alm(lmax, mmax, rng).astype(cdt)[None, :]
+def test_against_ducc_large(sht, ducc, lmax, mmax, npts, cdt, eps, spin):
+    """Sizes where the recurrences need their carried exponent (sin^m theta
+    below the double range for m in the thousands)."""
+    rng = np.random.default_rng(lmax + npts + spin)
+    ncomp = 1 if spin == 0 else 2
+    alm = O.random_alm_spin(lmax, mmax, spin, ncomp, rng).astype(cdt)
     loc = locs(rng, npts)
     nthr = os.cpu_count() or 1
-    m1 = sht.synthesis_general(alm=alm, spin=0, lmax=lmax, mmax=mmax, loc=loc, epsilon=eps)
-    m2 = ducc.synthesis_general(alm=alm.astype(np.complex128), spin=0, lmax=lmax, mmax=mmax,
+    m1 = sht.synthesis_general(alm=alm, spin=spin, lmax=lmax, mmax=mmax, loc=loc, epsilon=eps)
+    m2 = ducc.synthesis_general(alm=alm.astype(np.complex128), spin=spin, lmax=lmax, mmax=mmax,
                                 loc=loc, epsilon=min(eps, 1e-12), nthreads=nthr)
     assert l2err(m1, m2) < eps
     rdt = np.float64 if cdt == np.complex128 else np.float32
-    mp = rng.uniform(-1, 1, (1, npts)).astype(rdt)
-    a1 = sht.adjoint_synthesis_general(map=mp, spin=0, lmax=lmax, mmax=mmax, loc=loc,
+    mp = rng.uniform(-1, 1, (ncomp, npts)).astype(rdt)
+    a1 = sht.adjoint_synthesis_general(map=mp, spin=spin, lmax=lmax, mmax=mmax, loc=loc,
                                        epsilon=eps)
-    a2 = ducc.adjoint_synthesis_general(map=mp.astype(np.float64), spin=0, lmax=lmax,
+    a2 = ducc.adjoint_synthesis_general(map=mp.astype(np.float64), spin=spin, lmax=lmax,
                                         mmax=mmax, loc=loc, epsilon=min(eps, 1e-12),
                                         nthreads=nthr)
     assert l2err(a1, a2) < eps
