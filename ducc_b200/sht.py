@@ -19,7 +19,7 @@ import numpy as np
 
 from . import _capi as C
 
-__all__ = ["synthesis_general", "adjoint_synthesis_general"]
+__all__ = ["synthesis_general", "adjoint_synthesis_general", "pseudo_analysis_general", "lsmr"]
 
 
 def _torch():
@@ -185,3 +185,172 @@ def adjoint_synthesis_general(*, map, spin, lmax, loc, epsilon, mstart=None, lst
         alm[...] = d_alm.cpu().numpy()
         return alm
     return d_alm.cpu().numpy() if host else d_alm
+
+
+def lsmr(op, op_adj, xnorm, bnorm, b, x0, damp=0., atol=1e-6, btol=1e-6, conlim=1e8,
+         itnlim=None):
+    """LSMR (Fong & Saunders, SIAM J. Sci. Comput. 33 (2011) 2950-2971), the
+    least-squares solver DUCC's pseudo_analysis_general uses
+    (src/ducc0/math/solvers.h), restated for any vectors with +, - and scalar
+    * (numpy arrays, torch tensors): minimises |b - A x| given A x = op(x) and
+    A^T y = op_adj(y), with the norms xnorm (solution space) and bnorm (data
+    space).  Returns (x, istop, itn, normr, normar, normA, condA, normx, normb)."""
+    x = x0
+    u = b - op(x0)
+    beta = bnorm(u)
+    if beta > 0:
+        u = u * (1. / beta)
+    v = op_adj(u)
+    alpha = xnorm(v)
+    if alpha > 0:
+        v = v * (1. / alpha)
+    itnlim = itnlim if itnlim is not None else 1000000
+    itn, zetabar, alphabar, rho, rhobar, cbar, sbar = 0, alpha * beta, alpha, 1., 1., 1., 0.
+    h, hbar = v, v * 0.
+    betadd, betad, rhodold, tautildeold, thetatilde, zeta, d = beta, 0., 1., 0., 0., 0., 0.
+    normA2 = alpha * alpha
+    maxrbar, minrbar = 0., 1e100
+    normA, condA, normx = alpha, 1., 0.
+    normb, istop = beta, 0
+    ctol = 1. / conlim if conlim > 0 else 0.
+    normr, normar = beta, alpha * beta
+    if normar == 0:
+        return x, istop, itn, normr, normar, normA, condA, normx, normb
+    while itn < itnlim:
+        itn += 1
+        u = op(v) - u * alpha
+        beta = bnorm(u)
+        if beta > 0:
+            u = u * (1. / beta)
+            v = op_adj(u) - v * beta
+            alpha = xnorm(v)
+            if alpha > 0:
+                v = v * (1. / alpha)
+        # rotation that removes the damping term
+        alphahat = np.hypot(alphabar, damp)
+        chat, shat = alphabar / alphahat, damp / alphahat
+        # plane rotation Q_k
+        rhoold = rho
+        rho = np.hypot(alphahat, beta)
+        c, s = alphahat / rho, beta / rho
+        thetanew = s * alpha
+        alphabar = c * alpha
+        # plane rotation Qbar_k
+        rhobarold, zetaold = rhobar, zeta
+        thetabar = sbar * rho
+        rhotemp = cbar * rho
+        rhobar = np.hypot(cbar * rho, thetanew)
+        cbar, sbar = cbar * rho / rhobar, thetanew / rhobar
+        zeta = cbar * zetabar
+        zetabar = -sbar * zetabar
+        # h, hbar, x
+        hbar = h - hbar * (thetabar * rho / (rhoold * rhobarold))
+        x = x + hbar * (zeta / (rho * rhobar))
+        h = v - h * (thetanew / rho)
+        # estimate of |r|
+        betaacute = chat * betadd
+        betacheck = -shat * betadd
+        betahat = c * betaacute
+        betadd = -s * betaacute
+        thetatildeold = thetatilde
+        rhotildeold = np.hypot(rhodold, thetabar)
+        ctildeold, stildeold = rhodold / rhotildeold, thetabar / rhotildeold
+        thetatilde = stildeold * rhobar
+        rhodold = ctildeold * rhobar
+        betad = -stildeold * betad + ctildeold * betahat
+        tautildeold = (zetaold - thetatildeold * tautildeold) / rhotildeold
+        taud = (zeta - thetatilde * tautildeold) / rhodold
+        d += betacheck * betacheck
+        normr = np.sqrt(d + (betad - taud) ** 2 + betadd * betadd)
+        # estimates of |A| and cond(A)
+        normA2 += beta * beta
+        normA = np.sqrt(normA2)
+        normA2 += alpha * alpha
+        maxrbar = max(maxrbar, rhobarold)
+        if itn > 1:
+            minrbar = min(minrbar, rhobarold)
+        condA = max(maxrbar, rhotemp) / min(minrbar, rhotemp)
+        # stopping rules
+        normar = abs(zetabar)
+        normx = xnorm(x)
+        test1 = normr / normb
+        test2 = normar / (normA * normr) if normA * normr != 0 else np.inf
+        test3 = 1. / condA
+        t1 = test1 / (1. + normA * normx / normb)
+        rtol = btol + atol * normA * normx / normb
+        if itn >= itnlim:
+            istop = 7
+        if 1. + test3 <= 1.:
+            istop = 6
+        if 1. + test2 <= 1.:
+            istop = 5
+        if 1. + t1 <= 1.:
+            istop = 4
+        if test3 <= ctol:
+            istop = 3
+        if test2 <= atol:
+            istop = 2
+        if test1 <= rtol:
+            istop = 1
+        if istop > 0:
+            break
+    return x, istop, itn, normr, normar, normA, condA, normx, normb
+
+
+def pseudo_analysis_general(*, lmax, map, loc, spin, nthreads, maxiter, epsilon=1e-5,
+                            sigma_min=1.1, sigma_max=2.6, mstart=None, lstride=1, mmax=None,
+                            alm=None, verbose=False):
+    """a_lm whose synthesis at ``loc`` best fits ``map`` in the least-squares
+    sense, by LSMR over ``synthesis_general`` and its adjoint at a tenth of
+    ``epsilon`` (``ducc0.sht.pseudo_analysis_general``, src/ducc0/sht/sht.cc:3003-3057:
+    atol = 1e-14 sqrt(npoints), btol = epsilon, conlim 1e8, the a_lm norm
+    counting m > 0 twice).  Returns (alm, istop, itn, |r| / |map|,
+    |A^T r| / (|A| |r|))."""
+    torch = _torch()
+    spin, lmax, lstride = int(spin), int(lmax), int(lstride)
+    d_map, host = _dev(map)
+    if d_map.dtype not in (torch.float32, torch.float64):
+        raise TypeError("type matching failed: 'alm' has neither type 'c8' nor 'c16'")
+    ncomp = 1 if spin == 0 else 2
+    if d_map.dim() != 2 or d_map.shape[0] != ncomp:
+        raise RuntimeError("number of components mismatch in map")
+    d_loc = _loc(loc)
+    ms = _mstart(lmax, mmax, mstart)
+    nalm = _min_almdim(lmax, ms, lstride)
+    cdt = torch.complex128 if d_map.dtype == torch.float64 else torch.complex64
+    # weights of the a_lm norm: 1 for m = 0, 2 for m > 0, 0 off the layout
+    w = np.zeros(nalm)
+    for m in range(ms.shape[0]):
+        w[int(ms[m]) + np.arange(m, lmax + 1) * lstride] = 1. if m == 0 else 2.
+    d_w = torch.from_numpy(w).to(d_map.device)
+    kw = dict(spin=spin, lmax=lmax, loc=d_loc, epsilon=0.1 * float(epsilon), mstart=ms,
+              lstride=lstride, nthreads=nthreads, sigma_min=sigma_min, sigma_max=sigma_max,
+              verbose=verbose)
+
+    def op(x):
+        return synthesis_general(alm=x, **kw)
+
+    def op_adj(y):
+        return adjoint_synthesis_general(map=y.contiguous(), **kw)
+
+    def almnorm(x):
+        return float(torch.sqrt(torch.sum(d_w * (x.real.double() ** 2 + x.imag.double() ** 2))))
+
+    def mapnorm(y):
+        return float(torch.sqrt(torch.sum(y.double() ** 2)))
+
+    x0 = torch.zeros((ncomp, nalm), dtype=cdt, device=d_map.device)
+    atol = 1e-14 * np.sqrt(d_map.shape[1])
+    x, istop, itn, normr, normar, normA, condA, normx, normb = lsmr(
+        op, op_adj, almnorm, mapnorm, d_map, x0, 0., atol, float(epsilon), 1e8, int(maxiter))
+    rnorm = normr / normb if normb else 0.
+    sqnorm = normar / (normA * normr) if normA * normr else 0.
+    if alm is not None:
+        if C.is_torch(alm):
+            alm[:, :nalm] = x
+        else:
+            alm[:, :nalm] = x.cpu().numpy()
+        res = alm
+    else:
+        res = x.cpu().numpy() if host else x
+    return res, istop, itn, rnorm, sqnorm

@@ -321,3 +321,30 @@ def test_against_ducc_large(sht, ducc, lmax, mmax, npts, cdt, eps, spin):
                                         mmax=mmax, loc=loc, epsilon=min(eps, 1e-12),
                                         nthreads=nthr)
     assert l2err(a1, a2) < eps
+
+
+@pmp("spin", (0, 2))
+@pmp("f64", (True, False))
+def test_pseudo_analysis_general_against_ducc(sht, ducc, spin, f64):
+    """LSMR over the GPU synthesis and its adjoint recovers the a_lm of a
+    band-limited map on the HEALPix nside 32 pixel centres, as DUCC's own
+    pseudo_analysis_general does, with the same stopping reason."""
+    rng = np.random.default_rng(77 + spin)
+    lmax = 40
+    ncomp = 1 if spin == 0 else 2
+    alm = O.random_alm_spin(lmax, lmax, spin, ncomp, rng)
+    loc = healpix_ring_centres(32)
+    mp = ducc.synthesis_general(alm=alm, spin=spin, lmax=lmax, loc=loc, epsilon=1e-13)
+    eps = 1e-9 if f64 else 1e-5
+    if not f64:
+        mp = mp.astype(np.float32)
+    a1, istop1, itn1, r1, q1 = sht.pseudo_analysis_general(
+        lmax=lmax, map=mp, loc=loc, spin=spin, nthreads=1, maxiter=100, epsilon=eps)
+    a2, istop2, itn2, r2, q2 = ducc.pseudo_analysis_general(
+        lmax=lmax, map=mp, loc=loc, spin=spin, nthreads=4, maxiter=100, epsilon=eps)
+    assert a1.dtype == (np.complex128 if f64 else np.complex64)
+    tol = 1e-7 if f64 else 1e-4
+    assert l2err(a1, alm) < tol
+    assert l2err(a1, a2) < tol
+    assert istop1 == istop2 and abs(itn1 - itn2) <= 2
+    assert r1 < 10 * eps and r2 < 10 * eps
