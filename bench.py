@@ -453,11 +453,11 @@ def sphere_inputs(seed=12, lmax=SH_LMAX, npts=SH_NPTS):
     return alm[None, :], loc, mp
 
 
-def workload_sphere(dev, steps=3, warmup=2, lmax=SH_LMAX, npts=SH_NPTS, with_outputs=False):
+def workload_sphere(dev, steps=5, warmup=2, lmax=SH_LMAX, npts=SH_NPTS, with_outputs=False):
     """Spin-0 synthesis at arbitrary points and its adjoint
     (ducc0.sht.synthesis_general / adjoint_synthesis_general counterparts) at
-    eps 1e-5 in single precision, device-resident, each direction timed with
-    CUDA events over its calls."""
+    eps 1e-5 in single precision, device-resident, each call timed with CUDA
+    events (median, min and max over the calls)."""
     import torch
     from ducc_b200 import _capi as C
     from ducc_b200 import sht as SH
@@ -490,14 +490,17 @@ def workload_sphere(dev, steps=3, warmup=2, lmax=SH_LMAX, npts=SH_NPTS, with_out
             call()
         torch.cuda.synchronize(dev)
         n0 = C.lib().dnufft_kernel_launches()
-        e0, e1 = _events()
-        e0.record()
+        per = []
         for _ in range(steps):
+            e0, e1 = _events()
+            e0.record()
             call()
-        e1.record()
-        torch.cuda.synchronize(dev)
-        ms = e0.elapsed_time(e1) / steps
-        out[name] = {"ms": ms, "mpts_per_s": npts / (ms * 1e-3) / 1e6,
+            e1.record()
+            torch.cuda.synchronize(dev)
+            per.append(e0.elapsed_time(e1))
+        ms = float(np.median(per))
+        out[name] = {"ms": ms, "ms_min": float(min(per)), "ms_max": float(max(per)),
+                     "mpts_per_s": npts / (ms * 1e-3) / 1e6,
                      "gpu_launches_per_call": (C.lib().dnufft_kernel_launches() - n0) / steps}
     out["config"] = ("synthesis_general / adjoint, spin 0 and spin 2, lmax = mmax = %d "
                      "(complex64 a_lm), %d points uniform on the sphere (float64 theta, phi), "

@@ -33,7 +33,7 @@
 //
 // Spin s > 0 (the spin section below): Q + iU is one complex field,
 // sum over -mmax <= m <= mmax of F_m(theta) e^{i m phi} with F_m from the
-// Wigner-d recurrence (k_alm2leg_spin, one ring per thread), continued by
+// Wigner-d recurrence (k_alm2leg_spin, rows m and -m from one recurrence), continued by
 // F_m(2 pi - theta) = (-1)^(m+s) F_m(theta); the 2D transform runs over
 // (2 lmax + 1) x (2 mmax + 1) modes and its complex result is (Q, U).
 //
@@ -746,28 +746,37 @@ __device__ inline double2 spin_coef(const C *alm, int64_t cstride, int64_t astri
   return make_double2(sg * (e.x + b.y), sg * (b.x - e.y));
 }
 
-// F_m on the rings for m = row - mmax: V[row][j] = sum_l A_lm D_lm(theta_j) / nring,
-// V[row][nring - j] = (-1)^(m+s) V[row][j].  RINGS rings per thread; grid
-// (2 mmax + 1, blocks over rings 0 .. nring/2).  Chunks of warps whose values
-// are all in the double range run without the underflow guard.
-constexpr int RINGS = 4;
+// F_m on the rings: V[mmax + m][j] = sum_l A_lm D_lm(theta_j) / nring, continued
+// by V[row][nring - j] = (-1)^(m+s) V[row][j].  One block row per m >= 0: since
+// D_{l,-m}(theta) = (-1)^(l+s) D_lm(pi - theta), the recurrence of D_lm at ring j
+// also gives row -m at ring nring/2 - j (its coefficient staged with the sign).
+// RINGS rings per thread; grid (mmax + 1, blocks over rings 0 .. nring/2).
+// Chunks of warps whose values are all in the double range run without the
+// underflow guard.
+constexpr int RINGS = 2;
 template <typename C>
 __global__ void __launch_bounds__(THREADS) k_alm2leg_spin(
     const C *__restrict__ alm, int64_t cstride, int64_t astride,
     const int64_t *__restrict__ mstart, int64_t lstride, int lmax, int mmax, int sp, int mode,
     int nring, const SpinStart *__restrict__ starts, double2 *__restrict__ V) {
-  __shared__ double2 s_a[LCHUNK];
+  __shared__ double2 s_ap[LCHUNK], s_an[LCHUNK];
   __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_ga[LCHUNK];
-  const int row = blockIdx.x, m = row - mmax, mu = m < 0 ? -m : m;
-  const SpinStart S = starts[row];
+  const int m = blockIdx.x;
+  const bool neg = m > 0;   // row -m handled too
+  const SpinStart S = starts[mmax + m];
   const int half = nring / 2;
   const double sigma = (sp & 1) ? 1. : -1.;
-  const int64_t m0 = mstart[mu];
+  const int64_t m0 = mstart[m];
   double x[RINGS], d1[RINGS], d2[RINGS];
   int sc[RINGS], jr[RINGS];
-  double2 F[RINGS];
-  const double2 a0 =
-      spin_coef(alm, cstride, astride, m0 + int64_t(S.l0) * lstride, m, S.l0, mode, sigma);
+  double2 Fp[RINGS], Fn[RINGS];
+  const int64_t i0 = m0 + int64_t(S.l0) * lstride;
+  const double2 a0 = spin_coef(alm, cstride, astride, i0, m, S.l0, mode, sigma);
+  double2 b0 = make_double2(0., 0.);
+  if (neg) {
+    b0 = spin_coef(alm, cstride, astride, i0, -m, S.l0, mode, sigma);
+    if ((S.l0 + sp) & 1) b0 = make_double2(-b0.x, -b0.y);
+  }
 #pragma unroll
   for (int r = 0; r < RINGS; ++r) {
     jr[r] = (blockIdx.y * RINGS + r) * THREADS + threadIdx.x;
@@ -781,14 +790,22 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg_spin(
     if (jr[r] > half) d1[r] = 0.;
     d2[r] = 0.;
     const double v = sc[r] == 0 ? d1[r] : 0.;
-    F[r] = make_double2(a0.x * v, a0.y * v);
+    Fp[r] = make_double2(a0.x * v, a0.y * v);
+    Fn[r] = make_double2(b0.x * v, b0.y * v);
   }
   for (int l0 = S.l0 + 1; l0 <= lmax; l0 += LCHUNK) {
     const int n = min(LCHUNK, lmax - l0 + 1);
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += THREADS) {
       const int l = l0 + i;
-      s_a[i] = spin_coef(alm, cstride, astride, m0 + int64_t(l) * lstride, m, l, mode, sigma);
+      const int64_t idx = m0 + int64_t(l) * lstride;
+      s_ap[i] = spin_coef(alm, cstride, astride, idx, m, l, mode, sigma);
+      double2 b = make_double2(0., 0.);
+      if (neg) {
+        b = spin_coef(alm, cstride, astride, idx, -m, l, mode, sigma);
+        if ((l + sp) & 1) b = make_double2(-b.x, -b.y);
+      }
+      s_an[i] = b;
       spin_coeffs(l, m, sp, s_al[i], s_be[i], s_ga[i]);
     }
     __syncthreads();
@@ -796,23 +813,24 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg_spin(
 #pragma unroll
     for (int r = 0; r < RINGS; ++r) inrange &= sc[r] == 0;
     if (__all_sync(0xffffffffu, inrange)) {
-      // every value of the warp in the double range: no guard
       for (int i = 0; i < n; ++i) {
         const double al = s_al[i], be = s_be[i], ga = s_ga[i];
-        const double2 a = s_a[i];
+        const double2 a = s_ap[i], b = s_an[i];
 #pragma unroll
         for (int r = 0; r < RINGS; ++r) {
           const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
           d2[r] = d1[r];
           d1[r] = dn;
-          F[r].x = fma(a.x, dn, F[r].x);
-          F[r].y = fma(a.y, dn, F[r].y);
+          Fp[r].x = fma(a.x, dn, Fp[r].x);
+          Fp[r].y = fma(a.y, dn, Fp[r].y);
+          Fn[r].x = fma(b.x, dn, Fn[r].x);
+          Fn[r].y = fma(b.y, dn, Fn[r].y);
         }
       }
     } else {
       for (int i = 0; i < n; ++i) {
         const double al = s_al[i], be = s_be[i], ga = s_ga[i];
-        const double2 a = s_a[i];
+        const double2 a = s_ap[i], b = s_an[i];
 #pragma unroll
         for (int r = 0; r < RINGS; ++r) {
           const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
@@ -824,58 +842,81 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg_spin(
             ++sc[r];
           }
           const double v = sc[r] == 0 ? d1[r] : 0.;
-          F[r].x = fma(a.x, v, F[r].x);
-          F[r].y = fma(a.y, v, F[r].y);
+          Fp[r].x = fma(a.x, v, Fp[r].x);
+          Fp[r].y = fma(a.y, v, Fp[r].y);
+          Fn[r].x = fma(b.x, v, Fn[r].x);
+          Fn[r].y = fma(b.y, v, Fn[r].y);
         }
       }
     }
   }
   const double w = 1. / double(nring);
-  const double sg = ((m + sp) & 1) ? -w : w;
-  double2 *out = V + int64_t(row) * nring;
+  const double sg = ((m + sp) & 1) ? -w : w;   // (-1)^(m+s) = (-1)^(-m+s)
+  double2 *op = V + int64_t(mmax + m) * nring;
+  double2 *on = V + int64_t(mmax - m) * nring;
 #pragma unroll
   for (int r = 0; r < RINGS; ++r) {
     const int j = jr[r];
     if (j > half) continue;
-    out[j] = make_double2(w * F[r].x, w * F[r].y);
-    if (j > 0 && j < half) out[nring - j] = make_double2(sg * F[r].x, sg * F[r].y);
+    op[j] = make_double2(w * Fp[r].x, w * Fp[r].y);
+    if (j > 0 && j < half) op[nring - j] = make_double2(sg * Fp[r].x, sg * Fp[r].y);
+    if (neg) {
+      const int jn = half - j;
+      on[jn] = make_double2(w * Fn[r].x, w * Fn[r].y);
+      if (jn > 0 && jn < half) on[nring - jn] = make_double2(sg * Fn[r].x, sg * Fn[r].y);
+    }
   }
 }
 
-// Transposed: part[b][row][l] = sum over the rings of block b of
-// D_lm(theta_j) G(theta_j), G = g[row][j] + (-1)^(m+s) g[row][nring - j]
-// (0 < j < nring/2), for l0 <= l <= lmax; sums per warp through the
-// shared-memory transpose of 8 l values, per block over its warps.
+// Transposed: part[b][mmax + m][l] = sum over the rings of block b of
+// D_lm(theta_j) G_m(theta_j) and part[b][mmax - m][l] =
+// (-1)^(l+s) sum_j D_lm(theta_j) G_-m(theta_{nring/2 - j}) (the same recurrence,
+// D_{l,-m}(theta) = (-1)^(l+s) D_lm(pi - theta)), G = g[row][j] +
+// (-1)^(m+s) g[row][nring - j] (0 < j < nring/2), for l0 <= l <= lmax; sums per
+// warp through the shared-memory transpose of 8 l values, per block over its
+// warps.
 __global__ void __launch_bounds__(THREADS) k_leg2alm_spin(
     const double2 *__restrict__ g, int lmax, int mmax, int sp, int nring,
     const SpinStart *__restrict__ starts, double2 *__restrict__ part) {
   constexpr int NW = THREADS / 32;
   __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_ga[LCHUNK];
-  __shared__ double2 s_tr[NW][8][33];
-  __shared__ double2 s_blk[LCHUNK][NW];
-  const int row = blockIdx.x, m = row - mmax;
-  const SpinStart S = starts[row];
+  __shared__ double2 s_tr[2][NW][8][33];
+  __shared__ double2 s_blk[2][LCHUNK][NW];
+  const int m = blockIdx.x;
+  const bool neg = m > 0;
+  const SpinStart S = starts[mmax + m];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int half = nring / 2;
-  const double2 *in = g + int64_t(row) * nring;
+  const double2 *inp = g + int64_t(mmax + m) * nring;
+  const double2 *inn = g + int64_t(mmax - m) * nring;
   const double sgn = ((m + sp) & 1) ? -1. : 1.;
   double x[RINGS], d1[RINGS], d2[RINGS];
   int sc[RINGS];
-  double2 G[RINGS];
+  double2 Gp[RINGS], Gn[RINGS];
 #pragma unroll
   for (int r = 0; r < RINGS; ++r) {
     const int j = (blockIdx.y * RINGS + r) * THREADS + threadIdx.x;
     double c = 1., sn = 0.;
     x[r] = 1.;
-    G[r] = make_double2(0., 0.);
+    Gp[r] = make_double2(0., 0.);
+    Gn[r] = make_double2(0., 0.);
     if (j <= half) {
       sincospi(double(j) / double(nring), &sn, &c);
       x[r] = cospi(2. * double(j) / double(nring));
-      G[r] = in[j];
+      Gp[r] = inp[j];
       if (j > 0 && j < half) {
-        const double2 t = in[nring - j];
-        G[r].x += sgn * t.x;
-        G[r].y += sgn * t.y;
+        const double2 t = inp[nring - j];
+        Gp[r].x += sgn * t.x;
+        Gp[r].y += sgn * t.y;
+      }
+      if (neg) {
+        const int jn = half - j;
+        Gn[r] = inn[jn];
+        if (jn > 0 && jn < half) {
+          const double2 t = inn[nring - jn];
+          Gn[r].x += sgn * t.x;
+          Gn[r].y += sgn * t.y;
+        }
       }
     }
     spin_start(c, sn, S, d1[r], sc[r]);
@@ -883,7 +924,8 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm_spin(
     d2[r] = 0.;
   }
   const int li = lane & 7, part8 = lane >> 3;
-  const int64_t rowofs = (int64_t(blockIdx.y) * (2 * mmax + 1) + row) * (lmax + 1);
+  const int64_t rowlen = lmax + 1;
+  const int64_t bofs = int64_t(blockIdx.y) * (2 * mmax + 1) * rowlen;
   for (int l0 = S.l0; l0 <= lmax; l0 += LCHUNK) {
     const int n = min(LCHUNK, lmax - l0 + 1);
     __syncthreads();
@@ -903,78 +945,71 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm_spin(
     for (int r = 0; r < RINGS; ++r) inrange &= sc[r] == 0;
     const bool fast = l0 > S.l0 && __all_sync(0xffffffffu, inrange);
     for (int i8 = 0; i8 < n; i8 += 8) {
-      if (fast) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int i = i8 + k;
-          double2 c = make_double2(0., 0.);
-          if (i < n) {
+      for (int k = 0; k < 8; ++k) {
+        const int i = i8 + k;
+        double2 cp = make_double2(0., 0.), cn = make_double2(0., 0.);
+        if (i < n) {
+          if (l0 + i > S.l0) {
             const double al = s_al[i], be = s_be[i], ga = s_ga[i];
 #pragma unroll
             for (int r = 0; r < RINGS; ++r) {
               const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
               d2[r] = d1[r];
               d1[r] = dn;
-              c.x = fma(dn, G[r].x, c.x);
-              c.y = fma(dn, G[r].y, c.y);
-            }
-          }
-          s_tr[warp][k][lane] = c;
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int i = i8 + k;
-          double2 c = make_double2(0., 0.);
-          if (i < n) {
-            if (l0 + i > S.l0) {
-              const double al = s_al[i], be = s_be[i], ga = s_ga[i];
-#pragma unroll
-              for (int r = 0; r < RINGS; ++r) {
-                const double dn = fma(al * (x[r] - be), d1[r], -ga * d2[r]);
-                d2[r] = d1[r];
-                d1[r] = dn;
-                if (sc[r] < 0 && fabs(dn) > RESCALE_ABOVE) {
-                  d1[r] *= RESCALE_BY;
-                  d2[r] *= RESCALE_BY;
-                  ++sc[r];
-                }
+              if (!fast && sc[r] < 0 && fabs(dn) > RESCALE_ABOVE) {
+                d1[r] *= RESCALE_BY;
+                d2[r] *= RESCALE_BY;
+                ++sc[r];
               }
             }
-#pragma unroll
-            for (int r = 0; r < RINGS; ++r) {
-              const double v = sc[r] == 0 ? d1[r] : 0.;
-              c.x = fma(v, G[r].x, c.x);
-              c.y = fma(v, G[r].y, c.y);
-            }
           }
-          s_tr[warp][k][lane] = c;
+#pragma unroll
+          for (int r = 0; r < RINGS; ++r) {
+            const double v = (fast || sc[r] == 0) ? d1[r] : 0.;
+            cp.x = fma(v, Gp[r].x, cp.x);
+            cp.y = fma(v, Gp[r].y, cp.y);
+            cn.x = fma(v, Gn[r].x, cn.x);
+            cn.y = fma(v, Gn[r].y, cn.y);
+          }
         }
+        s_tr[0][warp][k][lane] = cp;
+        s_tr[1][warp][k][lane] = cn;
       }
       __syncwarp();
-      double2 t = make_double2(0., 0.);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const double2 u = s_tr[warp][li][part8 * 8 + k];
-        t.x += u.x;
-        t.y += u.y;
+      for (int h = 0; h < 2; ++h) {
+        double2 t = make_double2(0., 0.);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const double2 u = s_tr[h][warp][li][part8 * 8 + k];
+          t.x += u.x;
+          t.y += u.y;
+        }
+        t.x += __shfl_xor_sync(0xffffffffu, t.x, 8);
+        t.y += __shfl_xor_sync(0xffffffffu, t.y, 8);
+        t.x += __shfl_xor_sync(0xffffffffu, t.x, 16);
+        t.y += __shfl_xor_sync(0xffffffffu, t.y, 16);
+        if (part8 == 0) s_blk[h][i8 + li][warp] = t;
       }
-      t.x += __shfl_xor_sync(0xffffffffu, t.x, 8);
-      t.y += __shfl_xor_sync(0xffffffffu, t.y, 8);
-      t.x += __shfl_xor_sync(0xffffffffu, t.x, 16);
-      t.y += __shfl_xor_sync(0xffffffffu, t.y, 16);
-      if (part8 == 0) s_blk[i8 + li][warp] = t;
       __syncwarp();
     }
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += THREADS) {
-      double2 t = s_blk[i][0];
+      double2 tp = s_blk[0][i][0], tn = s_blk[1][i][0];
 #pragma unroll
       for (int w = 1; w < NW; ++w) {
-        t.x += s_blk[i][w].x;
-        t.y += s_blk[i][w].y;
+        tp.x += s_blk[0][i][w].x;
+        tp.y += s_blk[0][i][w].y;
+        tn.x += s_blk[1][i][w].x;
+        tn.y += s_blk[1][i][w].y;
       }
-      part[rowofs + l0 + i] = t;
+      const int l = l0 + i;
+      part[bofs + (mmax + m) * rowlen + l] = tp;
+      if (neg) {
+        const double f = ((l + sp) & 1) ? -1. : 1.;
+        part[bofs + (mmax - m) * rowlen + l] = make_double2(f * tn.x, f * tn.y);
+      }
     }
   }
 }
@@ -1447,7 +1482,7 @@ static void synthesis_spin_t(const Problem &P, const Arr &alm, const int64_t *ms
   Buf dstarts(ss.size() * sizeof(SpinStart), st);
   upload(dstarts, ss.data(), ss.size() * sizeof(SpinStart), st);
   Buf V(size_t(P.rows) * P.nring * sizeof(double2), st);
-  k_alm2leg_spin<C><<<dim3(P.rows, P.nblk_spin), THREADS, 0, st>>>(
+  k_alm2leg_spin<C><<<dim3(P.mmax + 1, P.nblk_spin), THREADS, 0, st>>>(
       static_cast<const C *>(alm.p), alm.stride[0], alm.stride[1], ptr<int64_t>(tb.mstart),
       lstride, P.lmax, P.mmax, P.spin, P.mode, P.nring, ptr<SpinStart>(dstarts),
       ptr<double2>(V));
@@ -1498,7 +1533,7 @@ static void adjoint_spin_t(const Problem &P, const Arr &map, const int64_t *msta
   Buf gr(size_t(P.rows) * P.nring * sizeof(double2), st);
   rings_inverse<C>(P, hdat, gr, st);
   Buf part(size_t(P.nblk_spin) * P.rows * (P.lmax + 1) * sizeof(double2), st);
-  k_leg2alm_spin<<<dim3(P.rows, P.nblk_spin), THREADS, 0, st>>>(
+  k_leg2alm_spin<<<dim3(P.mmax + 1, P.nblk_spin), THREADS, 0, st>>>(
       ptr<double2>(gr), P.lmax, P.mmax, P.spin, P.nring, ptr<SpinStart>(dstarts),
       ptr<double2>(part));
   DN_LAUNCHED();
