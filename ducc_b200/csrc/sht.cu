@@ -296,6 +296,14 @@ __device__ inline void step_guarded(double al, double be, const double (&x)[NP],
   }
 }
 
+// For m > 0 the pole pair (ring 0 and ring nring/2) is zero (lambda_lm has a
+// factor sin^m theta): those rows start at pair 1, and their blocks over the
+// pairs number active_blocks(m).
+__host__ __device__ inline int pair_offset(int m) { return m > 0 ? 1 : 0; }
+__host__ __device__ inline int active_blocks(int m, int npairs, int per_block) {
+  return (npairs - pair_offset(m) + per_block - 1) / per_block;
+}
+
 // F_m on every ring: V[m][j] = w_m / nring * sum_l a_lm lambda_lm(theta_j),
 // rings past the south pole by F_m(2 pi - theta) = (-1)^m F_m(theta).
 // grid (mmax + 1, ceil(npairs / (THREADS * PAIRS))), THREADS threads.  A warp
@@ -309,6 +317,12 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg(
   __shared__ double2 s_a[LCHUNK], s_aq[LCHUNK];
   __shared__ double s_al[LCHUNK], s_be[LCHUNK], s_q[LCHUNK], s_g[LCHUNK];
   const int m = blockIdx.x;
+  const int pofs = pair_offset(m);
+  if (m > 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    V[int64_t(m) * nring] = make_double2(0., 0.);
+    V[int64_t(m) * nring + nring / 2] = make_double2(0., 0.);
+  }
+  if (int(blockIdx.y) >= active_blocks(m, npairs, THREADS * PAIRS)) return;
   const int64_t m0 = mstart[m];
   double x[PAIRS], l1[PAIRS], l2[PAIRS];
   int sc[PAIRS];
@@ -319,7 +333,7 @@ __global__ void __launch_bounds__(THREADS) k_alm2leg(
   const double2 amm = load_c(alm + (m0 + int64_t(m) * lstride) * astride);
 #pragma unroll
   for (int r = 0; r < PAIRS; ++r) {
-    jp[r] = (blockIdx.y * PAIRS + r) * THREADS + threadIdx.x;
+    jp[r] = pofs + (blockIdx.y * PAIRS + r) * THREADS + threadIdx.x;
     double s = 0., c = 0.;
     if (jp[r] < npairs) ring_sc(jp[r], nring, s, c);
     x[r] = c;
@@ -440,6 +454,8 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
   __shared__ double2 s_tr[NW][8][33];
   __shared__ double2 s_blk[LCHUNK][NW];
   const int m = blockIdx.x;
+  if (int(blockIdx.y) >= active_blocks(m, npairs, THREADS * PAIRS)) return;
+  const int pofs = pair_offset(m);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int half = nring / 2;
   const double2 *row = g + int64_t(m) * nring;
@@ -449,7 +465,7 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
   double2 P[PAIRS], Q[PAIRS];
 #pragma unroll
   for (int r = 0; r < PAIRS; ++r) {
-    const int j = (blockIdx.y * PAIRS + r) * THREADS + threadIdx.x;
+    const int j = pofs + (blockIdx.y * PAIRS + r) * THREADS + threadIdx.x;
     double s = 0., c = 0.;
     double2 gn = make_double2(0., 0.), gs = make_double2(0., 0.);
     if (j < npairs) {
@@ -576,9 +592,9 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
 }
 
 // alm[(mstart[m] + l lstride) astride] = sum_b part[b][mofs[m] + l] / nring,
-// in the order of b; imaginary part 0 for m = 0 (a_l0 of a real map is real).
+// in the order of b (the active blocks of m); imaginary part 0 for m = 0 (a_l0 of a real map is real).
 template <typename C>
-__global__ void k_alm_out(const double2 *__restrict__ part, int nblk, int64_t nalm_dense,
+__global__ void k_alm_out(const double2 *__restrict__ part, int npairs, int64_t nalm_dense,
                           const int64_t *__restrict__ mofs, const int64_t *__restrict__ mstart,
                           int64_t lstride, int64_t astride, int lmax, int nm, double scale,
                           C *__restrict__ alm) {
@@ -594,6 +610,7 @@ __global__ void k_alm_out(const double2 *__restrict__ part, int nblk, int64_t na
     const int m = lo;
     const int64_t l = e - mofs[m];
     double2 t = make_double2(0., 0.);
+    const int nblk = active_blocks(m, npairs, THREADS * PAIRS);
     for (int b = 0; b < nblk; ++b) {
       const double2 u = part[int64_t(b) * nalm_dense + e];
       t.x += u.x;
@@ -1615,7 +1632,7 @@ static void adjoint_t(const Problem &P, const Arr &map, const int64_t *mstart, i
       ptr<int64_t>(tb.mofs), P.nalm_dense, ptr<double2>(part));
   DN_LAUNCHED();
   k_alm_out<C><<<grid_for(P.nalm_dense), 256, 0, st>>>(
-      ptr<double2>(part), P.nblk, P.nalm_dense, ptr<int64_t>(tb.mofs), ptr<int64_t>(tb.mstart),
+      ptr<double2>(part), P.npairs, P.nalm_dense, ptr<int64_t>(tb.mofs), ptr<int64_t>(tb.mstart),
       lstride, alm.stride[1], P.lmax, nm, 1. / double(P.nring), static_cast<C *>(alm.p));
   DN_LAUNCHED();
 }
