@@ -777,7 +777,7 @@ def run_ours(args, rank, world, local_rank):
         del plan
 
     head = args.spreaders[0]
-    e2e = e2e_unplanned = None
+    e2e = e2e_unplanned = e2e_concurrent = None
     if not args.no_e2e:
         h_coord = torch.from_numpy(coord).pin_memory().numpy()
         h_vals = torch.from_numpy(vals).pin_memory().numpy()
@@ -802,13 +802,50 @@ def run_ours(args, rank, world, local_rank):
             e2e_step()
         barrier()
         et = max_over_ranks((time.perf_counter() - t0) / k, dev, dist)
-        del hplan
         e2e = {"value": world * 2 * m / et / 1e6, "unit": "Mpts/s",
                "h2d_bytes_per_step": int(vals.nbytes + grid.nbytes),
                "d2h_bytes_per_step": int(n * n * 8 + m * 8),
                "call": "ducc_b200.nufft.plan(coord on the host).nu2u + .u2nu on pinned host "
                        "numpy arrays (plan built before the timed region)",
                "ms_per_step": et * 1e3}
+
+        # the step's two transforms are independent (u2nu reads its own grid):
+        # a caller with both can issue them from two host threads on two
+        # streams with a plan each, so that the uploads of one overlap the
+        # downloads of the other (PCIe is full duplex)
+        hplan2 = nufft.plan(nu2u=False, coord=h_coord, grid_shape=(n, n), epsilon=EPS,
+                            nthreads=args.param_threads, spreader=head)
+        s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        errs = []
+
+        def type2_call():
+            try:
+                hplan2.u2nu(grid=h_grid, forward=False, out=h_pts, stream=s2.cuda_stream)
+            except Exception as e:   # re-raised on the main thread
+                errs.append(e)
+
+        def e2e_concurrent_step():
+            th = threading.Thread(target=type2_call)
+            th.start()
+            hplan.nu2u(points=h_vals, forward=True, out=h_out, stream=s1.cuda_stream)
+            th.join()
+            if errs:
+                raise errs[0]
+
+        e2e_concurrent_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            e2e_concurrent_step()
+        barrier()
+        et = max_over_ranks((time.perf_counter() - t0) / k, dev, dist)
+        del hplan, hplan2
+        e2e_concurrent = {"value": world * 2 * m / et / 1e6, "unit": "Mpts/s",
+                          "h2d_bytes_per_step": int(vals.nbytes + grid.nbytes),
+                          "d2h_bytes_per_step": int(n * n * 8 + m * 8),
+                          "call": "the same two planned calls on pinned host numpy arrays, "
+                                  "issued from two host threads on two streams (one plan "
+                                  "each)", "ms_per_step": et * 1e3}
 
         # unplanned functions (each call uploads and sorts the coordinates)
         def e2e_unplanned_step():
@@ -902,6 +939,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(r["launches"]),
         "e2e": e2e,
         "e2e_unplanned": e2e_unplanned,
+        "e2e_concurrent": e2e_concurrent,
         "cpu_baseline": cpu,
         "errors": errors,
         "workloads": workloads,
