@@ -49,6 +49,7 @@ def test_our_arm_line_small():
     for k in ("bound", "achieved", "peak", "unit", "frac"):
         assert k in d["roofline"], k
     assert d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
+    assert d["e2e_concurrent"]["value"] > 0
     if d["errors"] is not None:
         assert d["errors"]["type1"]["tc"] < 1e-6 and d["errors"]["type1"]["plain"] < 1e-6
     assert "alt_plain" in d and "alt_plain_matched" in d
