@@ -59,7 +59,8 @@ namespace sht {
 
 constexpr int LCHUNK = 64;        // l values staged in shared memory per step
 constexpr int THREADS = 128;      // threads of the Legendre kernels
-constexpr int PAIRS = 2;          // ring pairs per thread
+constexpr int PAIRS = 2;          // ring pairs per thread (synthesis)
+constexpr int PAIRS_ADJ = 4;      // ring pairs per thread (adjoint: its per-l sums cost more)
 constexpr int SCALE_EXP = 600;    // a value is v * 2^(SCALE_EXP * scale)
 constexpr double RESCALE_ABOVE = 0x1p300;
 constexpr double RESCALE_BY = 0x1p-600;
@@ -454,18 +455,18 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
   __shared__ double2 s_tr[NW][8][33];
   __shared__ double2 s_blk[LCHUNK][NW];
   const int m = blockIdx.x;
-  if (int(blockIdx.y) >= active_blocks(m, npairs, THREADS * PAIRS)) return;
+  if (int(blockIdx.y) >= active_blocks(m, npairs, THREADS * PAIRS_ADJ)) return;
   const int pofs = pair_offset(m);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int half = nring / 2;
   const double2 *row = g + int64_t(m) * nring;
   const double sgn = (m & 1) ? -1. : 1.;
-  double x[PAIRS], l1[PAIRS], l2[PAIRS];
-  int sc[PAIRS];
-  double2 P[PAIRS], Q[PAIRS];
+  double x[PAIRS_ADJ], l1[PAIRS_ADJ], l2[PAIRS_ADJ];
+  int sc[PAIRS_ADJ];
+  double2 P[PAIRS_ADJ], Q[PAIRS_ADJ];
 #pragma unroll
-  for (int r = 0; r < PAIRS; ++r) {
-    const int j = pofs + (blockIdx.y * PAIRS + r) * THREADS + threadIdx.x;
+  for (int r = 0; r < PAIRS_ADJ; ++r) {
+    const int j = pofs + (blockIdx.y * PAIRS_ADJ + r) * THREADS + threadIdx.x;
     double s = 0., c = 0.;
     double2 gn = make_double2(0., 0.), gs = make_double2(0., 0.);
     if (j < npairs) {
@@ -501,11 +502,11 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
     stage_rec(l0, n, m, s_al, s_be, s_q, s_g);
     bool inrange = true;
 #pragma unroll
-    for (int r = 0; r < PAIRS; ++r) inrange &= sc[r] == 0;
+    for (int r = 0; r < PAIRS_ADJ; ++r) inrange &= sc[r] == 0;
     const bool fast = l0 > m && __all_sync(0xffffffffu, inrange);
-    double u1[PAIRS], u2[PAIRS];
+    double u1[PAIRS_ADJ], u2[PAIRS_ADJ];
 #pragma unroll
-    for (int r = 0; r < PAIRS; ++r) {
+    for (int r = 0; r < PAIRS_ADJ; ++r) {
       u1[r] = l1[r];
       u2[r] = l2[r];
     }
@@ -518,7 +519,7 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
           if (i < n) {
             const double gi = s_g[i];
 #pragma unroll
-            for (int r = 0; r < PAIRS; ++r) {
+            for (int r = 0; r < PAIRS_ADJ; ++r) {
               const double t = fma(x[r], u1[r], -gi * u2[r]);
               u2[r] = u1[r];
               u1[r] = t;
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
           if (i < n) {
             if (l > m) step_guarded(s_al[i], s_be[i], x, l1, l2, sc);
 #pragma unroll
-            for (int r = 0; r < PAIRS; ++r) {
+            for (int r = 0; r < PAIRS_ADJ; ++r) {
               const double v = sc[r] == 0 ? l1[r] : 0.;
               const double2 f = (k & 1) ? Q[r] : P[r];
               c.x = fma(v, f.x, c.x);
@@ -573,7 +574,7 @@ __global__ void __launch_bounds__(THREADS) k_leg2alm(
     if (fast) {
       const double q1 = s_q[n - 1], q2 = n >= 2 ? s_q[n - 2] : 1.;
 #pragma unroll
-      for (int r = 0; r < PAIRS; ++r) {
+      for (int r = 0; r < PAIRS_ADJ; ++r) {
         l1[r] = u1[r] * q1;
         l2[r] = u2[r] * q2;
       }
@@ -610,7 +611,7 @@ __global__ void k_alm_out(const double2 *__restrict__ part, int npairs, int64_t 
     const int m = lo;
     const int64_t l = e - mofs[m];
     double2 t = make_double2(0., 0.);
-    const int nblk = active_blocks(m, npairs, THREADS * PAIRS);
+    const int nblk = active_blocks(m, npairs, THREADS * PAIRS_ADJ);
     for (int b = 0; b < nblk; ++b) {
       const double2 u = part[int64_t(b) * nalm_dense + e];
       t.x += u.x;
@@ -1185,7 +1186,7 @@ struct Problem {
   int rows = 0;            // transforms along the rings: mmax + 1 (spin 0), 2 mmax + 1
   int nblk_spin = 0;       // blocks over the rings 0 .. nring/2 (spin > 0)
   int log2n = 0;           // > 0: ring DFT by k_ring_fft over nring = 2^log2n rings
-  int nring = 0, npairs = 0, nk = 0, nblk = 0;
+  int nring = 0, npairs = 0, nk = 0, nblk = 0, nblk_adj = 0;
   int64_t npts = 0;
   int64_t nalm_dense = 0;
   double s = 0;            // phi mode shift (mmax + 1) / 2
@@ -1275,6 +1276,7 @@ static Problem setup(size_t spin, int mode, size_t lmax, size_t nm, const int64_
   P.npairs = (P.nring / 2) / 2 + 1;
   P.nk = 2 * P.lmax + 1;
   P.nblk = (P.npairs + THREADS * PAIRS - 1) / (THREADS * PAIRS);
+  P.nblk_adj = (P.npairs + THREADS * PAIRS_ADJ - 1) / (THREADS * PAIRS_ADJ);
   P.nblk_spin = (P.nring / 2 + 1 + THREADS * RINGS - 1) / (THREADS * RINGS);
   P.npts = loc.shape[0];
   P.s = spin == 0 ? double(nm / 2) : 0.;
@@ -1626,8 +1628,8 @@ static void adjoint_t(const Problem &P, const Arr &map, const int64_t *mstart, i
   Buf gr(size_t(nm) * P.nring * sizeof(double2), st);
   rings_inverse<C>(P, hdat, gr, st);
   // 3. the transposed recurrence, per-block partial sums, summed in block order
-  Buf part(size_t(P.nblk) * P.nalm_dense * sizeof(double2), st);
-  k_leg2alm<<<dim3(nm, P.nblk), THREADS, 0, st>>>(
+  Buf part(size_t(P.nblk_adj) * P.nalm_dense * sizeof(double2), st);
+  k_leg2alm<<<dim3(nm, P.nblk_adj), THREADS, 0, st>>>(
       ptr<double2>(gr), P.lmax, P.nring, P.npairs, ptr<double>(tb.nmant), ptr<int>(tb.nexp),
       ptr<int64_t>(tb.mofs), P.nalm_dense, ptr<double2>(part));
   DN_LAUNCHED();
