@@ -11,7 +11,7 @@
 //
 //   F_m(theta) = sum_l a_lm lambda_lm(theta), continued past the pole by
 //   F_m(2 pi - theta) = (-1)^m F_m(theta), is a trigonometric polynomial of
-//   degree lmax in theta, so with N = 2 lmax + 2 rings theta_j = 2 pi j / N
+//   degree lmax in theta, so with N >= 2 lmax + 2 rings theta_j = 2 pi j / N
 //     c_km = (w_m / N) sum_j F_m(theta_j) e^{-i k theta_j},  |k| <= lmax
 //   (w_0 = 1, w_m = 2) and the real map is
 //     map(theta, phi) = Re sum_{k, 0 <= m <= mmax} c_km e^{i (k theta + m phi)}.
@@ -31,11 +31,11 @@
 //      over the modes (k, m - s), s = (mmax + 1) / 2, in the data precision,
 //      and Re(z_i e^{i s phi_i}) (k_points_out).
 //
-// Spin s > 0 (the spin section below): Q + iU is one complex field,
-// sum over -mmax <= m <= mmax of F_m(theta) e^{i m phi} with F_m from the
-// Wigner-d recurrence (k_alm2leg_spin, rows m and -m from one recurrence), continued by
-// F_m(2 pi - theta) = (-1)^(m+s) F_m(theta); the 2D transform runs over
-// (2 lmax + 1) x (2 mmax + 1) modes and its complex result is (Q, U).
+// Spin s > 0 (the spin section below): Q + iU is one complex field, the sum
+// over -mmax <= m <= mmax of F_m(theta) e^{i m phi} with F_m from the
+// Wigner-d recurrence (k_alm2leg_spin, rows m and -m from one recurrence),
+// continued by F_m(2 pi - theta) = (-1)^(m+s) F_m(theta); the 2D transform
+// runs over (2 lmax + 1) x (2 mmax + 1) modes and its complex result is (Q, U).
 //
 // The adjoint runs the transposed steps: values map_i e^{-i s phi_i}
 // (k_points_in) -> 2D type 1 -> inverse DFT back to the rings -> the rings
