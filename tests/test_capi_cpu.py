@@ -116,3 +116,32 @@ def test_log2tile_option_checked():
     with pytest.raises(RuntimeError, match="log2tile"):
         nufft.plan(nu2u=True, coord=np.zeros((3, 2), np.float32), grid_shape=(16, 16),
                    epsilon=1e-4, log2tile=7)
+
+
+def test_sht_defaults_and_argument_errors():
+    """The spherical-harmonic entry points: DUCC's keyword defaults, and
+    argument errors (null arrays, host memory, bad options) reported before
+    any kernel launch."""
+    import ctypes
+    L = C.lib()
+    o = C.ShtOpts()
+    L.dnufft_sht_default_opts(ctypes.byref(o))
+    assert o.nthreads == 1 and o.sigma_min == 1.1 and o.sigma_max == 2.6 and o.verbosity == 0
+    ms = np.zeros(3, np.int64)
+    pms = ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    alm = np.zeros((1, 6), np.complex128)
+    loc = np.zeros((4, 2))
+    mp = np.zeros((1, 4))
+    a_alm, a_loc, a_map = C.describe(alm), C.describe(loc), C.describe(mp)
+    n0 = L.dnufft_kernel_launches()
+    # null arrays
+    st = L.dnufft_synthesis_general(None, 0, 0, 2, pms, 3, 1, ctypes.byref(a_loc), 1e-6,
+                                    ctypes.byref(o), ctypes.byref(a_map), None)
+    assert st == 1 and b"null" in L.dnufft_last_error()
+    # host memory is not accepted by these entry points
+    for f, a, b in ((L.dnufft_synthesis_general, a_alm, a_map),
+                    (L.dnufft_adjoint_synthesis_general, a_map, a_alm)):
+        st = f(ctypes.byref(a), 0, 0, 2, pms, 3, 1, ctypes.byref(a_loc), 1e-6,
+               ctypes.byref(o), ctypes.byref(b), None)
+        assert st == 1 and b"device array" in L.dnufft_last_error()
+    assert L.dnufft_kernel_launches() == n0
