@@ -638,3 +638,76 @@ def dirty2vis_split(group=None, _run=None, **kwargs):
             npix_x=d.shape[0], npix_y=d.shape[1], **q)["nplanes"]
     kwargs.pop("_nplanes", None)
     return _split_wgridder(lambda pl: run(planes=pl, **kwargs), max(nplanes, 1), group)
+
+
+def _point_share(npts, group):
+    """This rank's consecutive share [a, b) of npts points."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    b0, c = plane_share(npts, world, rank)
+    return b0, b0 + c, world
+
+
+def _to_comm(x, dev):
+    import numpy as np
+    import torch
+    return x.to(dev) if torch.is_tensor(x) else torch.as_tensor(np.asarray(x)).to(dev)
+
+
+def synthesis_general_split(group=None, _run=None, **kwargs):
+    """``ducc_b200.sht.synthesis_general`` with the points split over the ranks
+    of ``group`` (every rank passes the same arguments): each rank evaluates
+    the expansion at its consecutive share of ``loc`` and one all-gather
+    assembles the map on every rank.  The rings (Legendre part) are computed by
+    every rank; what crosses between GPUs is the map.  ``_run`` replaces the
+    rank's computation (``_run(loc=share, **kwargs)``; tests on the CPU)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from . import sht
+    run = _run or sht.synthesis_general
+    loc = kwargs.pop("loc")
+    npts = int(loc.shape[0])
+    a, b, world = _point_share(npts, group)
+    part = run(loc=loc[a:b], **kwargs)
+    dev = _count_device(group)
+    t = _to_comm(part, dev)
+    # every share padded to the largest one for the all-gather
+    width = (npts + world - 1) // world
+    buf = torch.zeros((t.shape[0], width), dtype=t.dtype, device=dev)
+    buf[:, :t.shape[1]] = t
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    pieces = []
+    for r in range(world):
+        ra, rb = plane_share(npts, world, r)[0], sum(plane_share(npts, world, r))
+        pieces.append(parts[r][:, :rb - ra])
+    full = torch.cat(pieces, dim=1)
+    if torch.is_tensor(part):
+        return full.to(part.device)
+    return full.cpu().numpy()
+
+
+def adjoint_synthesis_general_split(group=None, _run=None, **kwargs):
+    """``ducc_b200.sht.adjoint_synthesis_general`` with the points split over
+    the ranks of ``group`` (every rank passes the same arguments): each rank
+    takes its consecutive share of ``loc`` and of the map's columns, and one
+    all-reduce sums the partial a_lm (the adjoint is a sum over the points).
+    ``_run`` replaces the rank's computation (tests on the CPU)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from . import sht
+    run = _run or sht.adjoint_synthesis_general
+    loc = kwargs.pop("loc")
+    mp = kwargs.pop("map")
+    npts = int(loc.shape[0])
+    a, b, _ = _point_share(npts, group)
+    part = run(loc=loc[a:b], map=mp[:, a:b], **kwargs)
+    dev = _count_device(group)
+    t = _to_comm(part, dev)
+    dist.all_reduce(t, group=group)
+    if torch.is_tensor(part):
+        return t if t.device == part.device else t.to(part.device)
+    return t.cpu().numpy()

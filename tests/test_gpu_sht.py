@@ -348,3 +348,26 @@ def test_pseudo_analysis_general_against_ducc(sht, ducc, spin, f64):
     assert l2err(a1, a2) < tol
     assert istop1 == istop2 and abs(itn1 - itn2) <= 2
     assert r1 < 10 * eps and r2 < 10 * eps
+
+
+@pmp("spin", (0, 2))
+def test_point_shares_add_up(sht, spin):
+    """What ducc_b200.distributed.synthesis_general_split / adjoint_..._split
+    rely on: the maps of consecutive point shares are the columns of the whole
+    map, and the a_lm of the shares sum to the whole adjoint."""
+    rng = np.random.default_rng(31 + spin)
+    lmax, npts, eps = 60, 3000, 1e-11
+    ncomp = 1 if spin == 0 else 2
+    alm = O.random_alm_spin(lmax, lmax, spin, ncomp, rng)
+    loc = locs(rng, npts)
+    mp = rng.uniform(-1, 1, (ncomp, npts))
+    shares = [(0, 1000), (1000, 2200), (2200, 3000)]
+    full = sht.synthesis_general(alm=alm, spin=spin, lmax=lmax, loc=loc, epsilon=eps)
+    parts = np.concatenate([sht.synthesis_general(alm=alm, spin=spin, lmax=lmax, loc=loc[a:b],
+                                                  epsilon=eps) for a, b in shares], axis=1)
+    assert l2err(parts, full) < 2 * eps
+    fa = sht.adjoint_synthesis_general(map=mp, spin=spin, lmax=lmax, loc=loc, epsilon=eps)
+    pa = sum(sht.adjoint_synthesis_general(map=np.ascontiguousarray(mp[:, a:b]), spin=spin,
+                                           lmax=lmax, loc=loc[a:b], epsilon=eps)
+             for a, b in shares)
+    assert l2err(pa, fa) < 2 * eps
