@@ -23,10 +23,8 @@
 //      value so that sin^m theta does not underflow; written for all N rings
 //      with the weights w_m / N;
 //   2. c_km: the DFT along the rings in FP64, by a radix-2 transform in shared
-//      memory per m (k_ring_fft, N the power of two from 2 lmax + 2 up to
-//      8192 rings, lmax <= 4095), or beyond that by a 1D type-1 transform of
-//      this library over the N = 2 lmax + 2 ring positions (a plan with
-//      ntrans = mmax + 1);
+//      memory per m (k_ring_fft, N the power of two from 2 lmax + 2, up to
+//      8192 rings: lmax <= 4095);
 //   3. the map: a 2D type-2 transform of this library at (theta_i, phi_i)
 //      over the modes (k, m - s), s = (mmax + 1) / 2, in the data precision,
 //      and Re(z_i e^{i s phi_i}) (k_points_out).
@@ -670,11 +668,6 @@ __global__ void k_convert(const A *__restrict__ in, int64_t n, B *__restrict__ o
   }
 }
 
-__global__ void k_ring_theta(double *__restrict__ th, int nring) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < nring) th[j] = 2. * 3.14159265358979323846 * (double(j) / double(nring));
-}
-
 // ---------------------------------------------------------------- spin > 0
 template <typename B> __device__ inline B from_d2b(const double2 &v) {
   B o;
@@ -1108,8 +1101,8 @@ __global__ void k_points_in_spin(const T *__restrict__ map, int64_t rs, int64_t 
   }
 }
 
-// The DFT along the rings, for ring counts that are powers of two up to
-// FFT_MAX: one CTA per m, an in-place radix-2 transform in shared memory
+// The DFT along the rings (a power of two of them, up to FFT_MAX): one CTA
+// per m, an in-place radix-2 transform in shared memory
 // (bit-reversed load, log2 N butterfly stages, twiddles from a table made by
 // the CTA).  Forward (synthesis): c[k + lmax][m] = sum_j V[m][j] e^{-2 pi i jk/N}
 // for |k| <= lmax, written in the data precision as the 2D transform's
@@ -1185,14 +1178,14 @@ struct Problem {
   int spin = 0, mode = 0;
   int rows = 0;            // transforms along the rings: mmax + 1 (spin 0), 2 mmax + 1
   int nblk_spin = 0;       // blocks over the rings 0 .. nring/2 (spin > 0)
-  int log2n = 0;           // > 0: ring DFT by k_ring_fft over nring = 2^log2n rings
+  int log2n = 0;           // nring = 2^log2n rings (the ring DFT's length)
   int nring = 0, npairs = 0, nk = 0, nblk = 0, nblk_adj = 0;
   int64_t npts = 0;
   int64_t nalm_dense = 0;
   double s = 0;            // phi mode shift (mmax + 1) / 2
-  double eps2 = 0, eps1 = 0;
+  double eps2 = 0;
   bool f64 = false;
-  dnufft_opts po1, po2;    // ring transforms / point transforms, parameters forced
+  dnufft_opts po2;         // point transforms, parameters forced
 };
 
 struct Tables {
@@ -1266,13 +1259,15 @@ static Problem setup(size_t spin, int mode, size_t lmax, size_t nm, const int64_
   P.spin = int(spin);
   P.mode = mode;
   P.rows = spin == 0 ? P.mmax + 1 : 2 * P.mmax + 1;
-  // rings: a power of two up to FFT_MAX (the DFT along the rings in shared
-  // memory), else 2 lmax + 2 with the DFT as 1D transforms of this library
+  // rings: the power of two from 2 lmax + 2 (the DFT along the rings runs in
+  // shared memory, up to FFT_MAX rings)
   P.nring = 2 * P.lmax + 2;
   P.log2n = 0;
   while ((1 << P.log2n) < P.nring) ++P.log2n;
-  if ((1 << P.log2n) <= FFT_MAX) P.nring = 1 << P.log2n;
-  else P.log2n = 0;
+  P.nring = 1 << P.log2n;
+  DN_REQUIRE(P.nring <= FFT_MAX, ST_UNSUPPORTED,
+             "lmax above 4095 is not supported by this build (the ring DFT runs in shared "
+             "memory, up to 8192 rings)");
   P.npairs = (P.nring / 2) / 2 + 1;
   P.nk = 2 * P.lmax + 1;
   P.nblk = (P.npairs + THREADS * PAIRS - 1) / (THREADS * PAIRS);
@@ -1282,21 +1277,10 @@ static Problem setup(size_t spin, int mode, size_t lmax, size_t nm, const int64_
   P.s = spin == 0 ? double(nm / 2) : 0.;
   P.f64 = f64;
   P.eps2 = epsilon;
-  // the theta sums in FP64 to a tenth of the request (or the best FP64 1D accuracy)
-  double best1 = 0;
-  DN_REQUIRE(dnufft_best_epsilon(1, 0, 1.1, 2.6, &best1) == 0, ST_INTERNAL,
-             "best_epsilon failed");
-  P.eps1 = std::max(0.1 * epsilon, 1.05 * best1);
   P.nalm_dense = 0;
   for (int m = 0; m <= P.mmax; ++m) P.nalm_dense += P.lmax + 1 - m;
   (void)adjoint;
-  // parameters of both transforms, chosen (and checked) before any launch
-  dnufft_default_opts(&P.po1, 1);
-  P.po1.nthreads = o->nthreads;
-  if (P.log2n == 0) {
-    const int64_t shape1[1] = {P.nk};
-    forced(P.po1, 1, 1, shape1, uint64_t(P.nring), P.eps1, true);
-  }
+  // parameters of the point transforms, chosen (and checked) before any launch
   dnufft_default_opts(&P.po2, 0);
   P.po2.nthreads = o->nthreads;
   P.po2.sigma_min = o->sigma_min;
@@ -1329,7 +1313,7 @@ static void make_tables(const Problem &P, const int64_t *mstart, cudaStream_t st
     mofs[m] = idx - m;   // dense index of (l, m) = mofs[m] + l
     idx += P.lmax + 1 - m;
   }
-  if (P.log2n > 0) fft_smem_optin();
+  fft_smem_optin();
   t.mstart = Buf(nm * sizeof(int64_t), st);
   t.mofs = Buf(nm * sizeof(int64_t), st);
   t.nmant = Buf(nm * sizeof(double), st);
@@ -1342,80 +1326,31 @@ static void make_tables(const Problem &P, const int64_t *mstart, cudaStream_t st
   // returns, so the vectors may end with this function)
 }
 
-static dnufft_plan *ring_plan(const Problem &P, bool nu2u, const Buf &theta, cudaStream_t st) {
-  const int64_t shape[1] = {P.nk};
-  const dnufft_array a_th = dev_array(theta.p, DNUFFT_F64, P.nring, 1, 1, 1);
-  dnufft_plan *plan = nullptr;
-  check_nufft(dnufft_plan_create(nu2u ? 1 : 0, &a_th, shape, 1, P.eps1, &P.po1, st, &plan),
-              "synthesis_general (ring transform)");
-  return plan;
-}
-
-struct PlanGuard {
-  dnufft_plan *p;
-  ~PlanGuard() {
-    if (p) dnufft_plan_destroy(p);
-  }
-};
-
 static void report(const Problem &P, const char *what) {
   std::fprintf(stderr,
-               "%s: lmax %d, mmax %d, %lld points; %d rings (1D transforms of %d modes, "
-               "epsilon %.3g), 2D modes %d x %d (epsilon %.3g)\n",
-               what, P.lmax, P.mmax, (long long)P.npts, P.nring, P.nk, P.eps1, P.nk,
-               P.rows, P.eps2);
+               "%s: lmax %d, mmax %d, spin %d, %lld points; %d rings, 2D modes %d x %d "
+               "(epsilon %.3g)\n",
+               what, P.lmax, P.mmax, P.spin, (long long)P.npts, P.nring, P.nk, P.rows, P.eps2);
 }
 
 
 // the DFT along the rings of `rows` transforms: V (rows, nring) FP64 -> c
 // (nk, rows) in the data precision (forward), or h (nk, rows) in the data
-// precision -> g (rows, nring) FP64 (inverse)
+// precision -> g (rows, nring) FP64 (inverse), one CTA per row
 template <typename C>
 static void rings_forward(const Problem &P, const Buf &V, Buf &cdat, cudaStream_t st) {
-  const int rows = P.rows;
-  if (P.log2n > 0) {
-    const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
-    k_ring_fft<double2, C, false><<<rows, FFT_THREADS, smem, st>>>(
-        ptr<double2>(V), ptr<C>(cdat), P.log2n, P.lmax, rows);
-    DN_LAUNCHED();
-    return;
-  }
-  Buf theta(size_t(P.nring) * sizeof(double), st);
-  k_ring_theta<<<(P.nring + 255) / 256, 256, 0, st>>>(ptr<double>(theta), P.nring);
-  DN_LAUNCHED();
-  Buf c64(size_t(rows) * P.nk * sizeof(double2), st);
-  {
-    PlanGuard pg{ring_plan(P, true, theta, st)};
-    dnufft_array a_v = dev_array(V.p, DNUFFT_C128, rows, P.nring, P.nring, 1);
-    dnufft_array a_c = dev_array(c64.p, DNUFFT_C128, rows, P.nk, 1, rows);
-    check_nufft(dnufft_plan_nu2u(pg.p, 1, 0, &a_v, &a_c, st), "synthesis_general (rings)");
-  }
-  k_convert<double2, C><<<grid_for(int64_t(rows) * P.nk), 256, 0, st>>>(
-      ptr<double2>(c64), int64_t(rows) * P.nk, ptr<C>(cdat));
+  const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
+  k_ring_fft<double2, C, false><<<P.rows, FFT_THREADS, smem, st>>>(
+      ptr<double2>(V), ptr<C>(cdat), P.log2n, P.lmax, P.rows);
   DN_LAUNCHED();
 }
 
 template <typename C>
 static void rings_inverse(const Problem &P, const Buf &hdat, Buf &gr, cudaStream_t st) {
-  const int rows = P.rows;
-  if (P.log2n > 0) {
-    const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
-    k_ring_fft<C, double2, true><<<rows, FFT_THREADS, smem, st>>>(
-        ptr<C>(hdat), ptr<double2>(gr), P.log2n, P.lmax, rows);
-    DN_LAUNCHED();
-    return;
-  }
-  Buf hconv(size_t(rows) * P.nk * sizeof(double2), st);
-  k_convert<C, double2><<<grid_for(int64_t(rows) * P.nk), 256, 0, st>>>(
-      ptr<C>(hdat), int64_t(rows) * P.nk, ptr<double2>(hconv));
+  const size_t smem = size_t(P.nring + P.nring / 2) * sizeof(double2);
+  k_ring_fft<C, double2, true><<<P.rows, FFT_THREADS, smem, st>>>(
+      ptr<C>(hdat), ptr<double2>(gr), P.log2n, P.lmax, P.rows);
   DN_LAUNCHED();
-  Buf theta(size_t(P.nring) * sizeof(double), st);
-  k_ring_theta<<<(P.nring + 255) / 256, 256, 0, st>>>(ptr<double>(theta), P.nring);
-  DN_LAUNCHED();
-  PlanGuard pg{ring_plan(P, false, theta, st)};
-  dnufft_array a_h = dev_array(hconv.p, DNUFFT_C128, rows, P.nk, 1, rows);
-  dnufft_array a_g = dev_array(gr.p, DNUFFT_C128, rows, P.nring, P.nring, 1);
-  check_nufft(dnufft_plan_u2nu(pg.p, 0, 0, &a_h, &a_g, st), "adjoint_synthesis_general (rings)");
 }
 
 // N_m of D_l0 per row (m = row - mmax), with its sign, and the powers of

@@ -274,6 +274,10 @@ def test_errors(sht):
         sht.synthesis_general(alm=alm, spin=0, loc=loc.astype(np.float32), **kw)
     with pytest.raises(TypeError):
         sht.synthesis_general(alm=alm, spin=0, lmax=10, loc=loc)   # epsilon is required
+    # beyond 8192 rings (lmax > 4095) this build has no ring DFT
+    big = np.zeros((1, 4201), np.complex64)
+    with pytest.raises(RuntimeError, match="4095"):
+        sht.synthesis_general(alm=big, spin=0, lmax=4200, mmax=0, loc=loc, epsilon=1e-5)
     # no points: an empty map, an all-zero adjoint
     e = sht.synthesis_general(alm=alm, spin=0, loc=np.zeros((0, 2)), **kw)
     assert e.shape == (1, 0)
