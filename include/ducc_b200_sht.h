@@ -2,7 +2,9 @@
  * ducc_b200_sht.h - C-ABI of the spherical-harmonic consumers of the B200
  * NUFFT library: synthesis of a spherical-harmonic expansion at arbitrary
  * points on the sphere and its adjoint, the counterparts of
- * ducc0.sht.synthesis_general / adjoint_synthesis_general.
+ * ducc0.sht.synthesis_general / adjoint_synthesis_general (the third of
+ * DUCC's functions, pseudo_analysis_general, is the least-squares solver
+ * over these two in ducc_b200/sht.py).
  *
  * Conventions (DUCC's, src/ducc0/sht/sht.cc:60-171): a_lm for 0 <= m <= mmax,
  * m <= l <= lmax, at element mstart[m] + l * lstride of each a_lm row (DUCC's
@@ -27,7 +29,11 @@
  * Every function returns 0 on success and a DNUFFT_ERR_* code otherwise
  * (message: dnufft_last_error()); argument errors are detected before any
  * kernel is launched.  DERIV1 needs spin 1 (DUCC accepts other spins there
- * and computes the spin-1 recurrence with that spin's pole parity).
+ * and computes the spin-1 recurrence with that spin's pole parity).  Limits
+ * of this build: lmax <= 4095 (the DFT along the rings runs in shared memory,
+ * up to 8192 rings) and the 2D transform's row limits (in double precision
+ * mmax up to about 4095 for spin 0, 2047 for spin > 0); beyond them
+ * DNUFFT_ERR_UNSUPPORTED.
  */
 #ifndef DUCC_B200_SHT_H
 #define DUCC_B200_SHT_H
